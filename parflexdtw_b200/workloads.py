@@ -1,0 +1,173 @@
+"""Seeded synthetic chroma-like sequence pairs for tests and benchmarks.
+
+The reference's own evaluation data (audio chroma of piano recordings) is not
+available, so every workload here is generated: non-negative 12-d frames drawn
+from a Dirichlet(0.3) distribution (chroma vectors are sparse and
+non-negative), L2-normalised per frame; the second sequence is the first one
+resampled along a random monotone piecewise-linear time warp plus noise, and
+optionally padded with unrelated frames at both ends so that FlexDTW's free
+start / free end matter.
+
+Feature layout follows the reference: ``F`` has shape ``(d, frames)`` and the
+cost matrix is ``C = 1 - L2norm(F1).T @ L2norm(F2)`` with shape ``(N, M)``
+(``FlexDTW.py:213-216``, ``Parflex.py:1470``).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+__all__ = [
+    "l2norm",
+    "cost_matrix_host",
+    "cost_matrix_det",
+    "chroma_sequence",
+    "warped_pair",
+    "PairSpec",
+    "CONFIG0",
+    "CONFIG1",
+    "make_pair",
+]
+
+
+def l2norm(F: np.ndarray) -> np.ndarray:
+    """Column L2 normalisation with the reference's ``+1e-9`` on the norm
+    (``FlexDTW.py:213-216``)."""
+    n = np.sqrt(np.sum(F * F, axis=0)) + 1e-9
+    return F / n.reshape((1, -1))
+
+
+def cost_matrix_host(F1: np.ndarray, F2: np.ndarray) -> np.ndarray:
+    """Host FP64 cosine cost exactly as the reference builds it
+    (``Parflex.py:1470``)."""
+    return 1 - l2norm(F1).T @ l2norm(F2)
+
+
+def cost_matrix_det(F1: np.ndarray, F2: np.ndarray) -> np.ndarray:
+    """FP64 cosine cost with a fixed summation order (k = 0, 1, ..., d-1).
+
+    Each product and each running sum is one IEEE-rounded numpy ufunc, so the
+    result is bit-identical on every machine (a BLAS GEMM's blocking and FMA
+    use are not).  Golden fixtures and parity tests feed this same ``C`` to the
+    reference and to the device path.
+    """
+    A = l2norm(np.asarray(F1, dtype=np.float64))
+    B = l2norm(np.asarray(F2, dtype=np.float64))
+    acc = A[0][:, None] * B[0][None, :]
+    for k in range(1, A.shape[0]):
+        acc = acc + A[k][:, None] * B[k][None, :]
+    return 1.0 - acc
+
+
+def chroma_sequence(rng: np.random.Generator, n: int, d: int = 12,
+                    alpha: float = 0.3) -> np.ndarray:
+    """``n`` Dirichlet(alpha) frames of dimension ``d``, L2-normalised, (d, n)."""
+    F = rng.dirichlet(np.full(d, alpha), size=n).T
+    return l2norm(F)
+
+
+def _warp_positions(rng: np.random.Generator, n_src: int, m_target: int,
+                    seg_lo: int = 40, seg_hi: int = 200,
+                    slope_lo: float = 0.7, slope_hi: float = 1.4) -> np.ndarray:
+    """Monotone piecewise-linear map from ``m_target`` output frames to
+    fractional source positions in ``[0, n_src-1]``.
+
+    Segment lengths (in source frames) are U(seg_lo, seg_hi); each segment's
+    local tempo ratio (output frames per source frame) is U(slope_lo, slope_hi),
+    then all ratios are scaled by one common factor so the total output length
+    is ``m_target``.
+    """
+    lens, slopes = [], []
+    total = 0
+    while total < n_src - 1:
+        L = int(rng.integers(seg_lo, seg_hi + 1))
+        L = min(L, n_src - 1 - total)
+        lens.append(L)
+        slopes.append(rng.uniform(slope_lo, slope_hi))
+        total += L
+    lens = np.asarray(lens, dtype=np.float64)
+    slopes = np.asarray(slopes, dtype=np.float64)
+    out_lens = lens * slopes
+    out_lens *= (m_target - 1) / out_lens.sum()
+    # knots: output position -> source position
+    out_knots = np.concatenate([[0.0], np.cumsum(out_lens)])
+    src_knots = np.concatenate([[0.0], np.cumsum(lens)])
+    m = np.arange(m_target, dtype=np.float64)
+    return np.interp(m, out_knots, src_knots)
+
+
+def warped_pair(rng: np.random.Generator, n: int, m_core: int, d: int = 12,
+                noise: float = 0.05, pad_frac: float = 0.0,
+                latent: str = "dirichlet"):
+    """One (F1, F2) pair.
+
+    ``F1``: ``n`` frames.  ``F2``: ``F1`` resampled (linear interpolation) at
+    the warp positions (``m_core`` frames), plus N(0, noise) noise, clipped at
+    0 for chroma (non-negative) latents, renormalised; then, when
+    ``pad_frac > 0``, U(0, pad_frac) * m_core unrelated frames are prepended
+    and appended.
+    """
+    if latent == "dirichlet":
+        F1 = chroma_sequence(rng, n, d)
+    else:
+        F1 = l2norm(rng.standard_normal((d, n)))
+    pos = _warp_positions(rng, n, m_core)
+    i0 = np.floor(pos).astype(np.int64)
+    i1 = np.minimum(i0 + 1, n - 1)
+    t = (pos - i0)[None, :]
+    F2 = F1[:, i0] * (1.0 - t) + F1[:, i1] * t
+    F2 = F2 + rng.normal(0.0, noise, size=F2.shape)
+    if latent == "dirichlet":
+        F2 = np.clip(F2, 0.0, None)
+    F2 = l2norm(F2)
+    if pad_frac > 0:
+        pre = int(rng.uniform(0, pad_frac) * m_core)
+        post = int(rng.uniform(0, pad_frac) * m_core)
+        parts = []
+        if pre:
+            parts.append(chroma_sequence(rng, pre, d) if latent == "dirichlet"
+                         else l2norm(rng.standard_normal((d, pre))))
+        parts.append(F2)
+        if post:
+            parts.append(chroma_sequence(rng, post, d) if latent == "dirichlet"
+                         else l2norm(rng.standard_normal((d, post))))
+        F2 = np.concatenate(parts, axis=1)
+    return np.ascontiguousarray(F1), np.ascontiguousarray(F2)
+
+
+class PairSpec:
+    """Named workload: sizes, tile length and DP parameters."""
+
+    def __init__(self, name, n, m_core, L, pad_frac=0.0, d=12, noise=0.05,
+                 weights=(2.0, 3.0, 3.0), beta=0.1, seed=0):
+        self.name = name
+        self.n = n
+        self.m_core = m_core
+        self.L = L
+        self.pad_frac = pad_frac
+        self.d = d
+        self.noise = noise
+        self.steps = ((1, 1), (1, 2), (2, 1))
+        self.weights = tuple(float(w) for w in weights)
+        self.beta = beta
+        self.seed = seed
+
+    def describe(self):
+        return {"workload": self.name, "N": self.n, "M_core": self.m_core,
+                "L": self.L, "pad_frac": self.pad_frac, "d": self.d,
+                "weights": list(self.weights), "beta": self.beta,
+                "seed": self.seed}
+
+
+# One pair, 2000 x ~2400 frames, L=500 (runs on CPU in well under a second).
+CONFIG0 = PairSpec("chroma12_pair_2000x2400_L500", 2000, 2400, 500)
+# One long pair, 30000 x ~36000 frames (+0-10 % unrelated padding per end),
+# L=4000, FP64 DP.
+CONFIG1 = PairSpec("chroma12_pair_30000x36000_L4000_fp64", 30000, 36000, 4000,
+                   pad_frac=0.10)
+
+
+def make_pair(spec: PairSpec):
+    """Generate ``(F1, F2)`` for a spec from its seed."""
+    rng = np.random.default_rng(spec.seed)
+    return warped_pair(rng, spec.n, spec.m_core, d=spec.d, noise=spec.noise,
+                       pad_frac=spec.pad_frac)
