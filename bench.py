@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""ParFlex alignment benchmark (one JSON line on rank 0).
+
+Workload (default): one long synthetic chroma pair, 30000 x ~37000 frames
+(12-d Dirichlet frames, random monotone warp, 0-10 % unrelated padding per
+end), L = 4000 tiles, steps {(1,1),(1,2),(2,1)}, weights {2,3,3}, beta 0.1,
+plain FP64 form with a bit-exact path.  One step = one full ParFlex
+alignment of that pair: stage 1 over all 80 tiles, stage-2 propagation,
+overlap sync, edge scan and stitched backtrace.
+
+  value     DP cells/s over the timed steps with C already in HBM
+  e2e       the same metric through the public API from HOST features
+            (tiled_stage1_from_features + run_stage2_from_tiled): feature
+            upload, device cost matrix, both stages, path download
+  roofline  the stage-1 kernel: algorithmic bytes (8 B of C read + 0.25 B of
+            backpointers per cell) / its CUDA-event time vs measured HBM peak
+  cpu_baseline  the C restatement of the reference (oracle/) on the host
+            cores, on the same pair, with all host threads
+
+Multi-GPU (torchrun, one rank per GPU): every rank aligns its own pair
+(independent replicas, weak scaling, no data-path collective); the time is
+the max over ranks.
+
+--impl reference times the reference algorithm's CPU restatement on the
+host cores for the same workload (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from parflexdtw_b200 import workloads as W  # noqa: E402
+
+METRIC = "DP cells/s (ParFlex plain FP64 form, exact-path agreement)"
+UNIT = "cells/s"
+
+
+def tile_cells(N, M, Lb):
+    hop = Lb - 1
+    n1 = -(-(N - 1) // hop)
+    n2 = -(-(M - 1) // hop)
+    rows = [min(Lb, N - i * hop) for i in range(n1)]
+    cols = [min(Lb, M - j * hop) for j in range(n2)]
+    return sum(rows) * sum(cols), n1, n2
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fp:
+            d = json.load(fp)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sms, mx, reasons = [], None, set()
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9 or (self.uuid and self.uuid not in f[0]):
+                continue
+            try:
+                sms.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                                "sw_power_cap"), f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sms:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sms), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sms)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def reference_arm(args, spec):
+    """CPU restatement of the reference on the host cores (rank 0 only)."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import build_oracle, oracle
+    build_oracle.build()
+    threads = os.cpu_count() or 1
+    F1, F2 = W.make_pair(spec)
+    # bounded sample: the first `rows` tile rows of the pair, full width
+    hop = spec.L - 1
+    rows = min(F1.shape[1], args.ref_tile_rows * hop + 1)
+    C = W.cost_matrix_host(F1[:, :rows], F2)
+    cells, n1, n2 = tile_cells(C.shape[0], C.shape[1], spec.L)
+    times = []
+    for s in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        oracle.parflex_full(C, spec.steps, spec.weights, spec.beta, spec.L, threads=threads)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+    tot = sum(times)
+    v = cells * len(times) / tot
+    N, M = F1.shape[1], F2.shape[1]
+    full_cells, _, _ = tile_cells(N, M, spec.L)
+    sample = (f"first {n1} tile rows of the pair ({C.shape[0]} x {C.shape[1]}, {n1 * n2} "
+              f"tiles, {cells} cells) per step, all stages")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config_dict(spec, N, M, full_cells),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(spec, N, M, cells):
+    d = spec.describe()
+    d.update({"N": N, "M": M, "cells_per_step": cells, "pairs_per_step_per_gpu": 1,
+              "l2": "input C larger than L2 (no flush needed)", "parallelism": "replicas"})
+    return d
+
+
+def b200_arm(args, spec):
+    import torch
+    import torch.distributed as dist
+
+    import parflexdtw_b200 as pf
+    from parflexdtw_b200 import _lib
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    # each rank aligns its own pair (seed offset by rank)
+    rs = W.PairSpec(spec.name, spec.n, spec.m_core, spec.L, pad_frac=spec.pad_frac,
+                    weights=spec.weights, beta=spec.beta, seed=spec.seed + rank)
+    F1, F2 = W.make_pair(rs)
+    N, M = F1.shape[1], F2.shape[1]
+    cells, n1, n2 = tile_cells(N, M, spec.L)
+    C_dev = pf.cost_matrix_from_features_gpu(F1, F2)
+    plan = pf.Plan(N, M, spec.L, spec.steps, spec.weights)
+    lib = _lib.load()
+
+    def step():
+        plan.run(C_dev, spec.beta)
+
+    for _ in range(args.warmup):
+        step()
+    best, end, found, n = plan.result()
+    wp = plan.path(n)
+
+    # --- timed region: device-resident input -------------------------------
+    uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = lib.pfx_kernel_launches()
+    with ClockSampler(uuid) as clk:
+        e0.record()
+        for k in range(args.steps):
+            ev[k][0].record()
+            plan.stage1(C_dev)
+            ev[k][1].record()
+            plan.propagate(C_dev)
+            plan.scan(spec.beta)
+            plan.stitch()
+        e1.record()
+        torch.cuda.synchronize()
+    launches = lib.pfx_kernel_launches() - launches0
+    ms_total = e0.elapsed_time(e1)
+    ms_s1 = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    if ws > 1:
+        t = torch.tensor([ms_total], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    value = cells * ws * args.steps / (ms_total / 1e3)
+    best2, end2, _, n2_ = plan.result()
+    assert best2 == best and end2 == end, "non-deterministic result across steps"
+
+    # --- e2e through the public API from pinned host features ---------------
+    f1p = torch.from_numpy(F1).pin_memory()
+    f2p = torch.from_numpy(F2).pin_memory()
+    h2d = f1p.numel() * 8 + f2p.numel() * 8
+
+    def e2e_step():
+        _, tr = pf.tiled_stage1_from_features(f1p, f2p, steps=spec.steps,
+                                              weights=spec.weights, beta=spec.beta, L=spec.L)
+        r = pf.run_stage2_from_tiled(tr, beta=spec.beta)
+        return r["best_cost"], r["stitched_wp"]
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        e2e_step()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e2e_ms = []
+    d2h = 0
+    for _ in range(args.e2e_steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        bc, swp = e2e_step()
+        b.record()
+        torch.cuda.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+        d2h = swp.nbytes + 8 * 9  # path + best cost, best_end[7], length
+        assert bc == best and np.array_equal(swp.T, wp.T), "e2e result differs"
+    e2e_tot = sum(e2e_ms)
+    if ws > 1:
+        t = torch.tensor([e2e_tot], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_tot = float(t.item())
+    e2e_value = cells * ws * len(e2e_ms) / (e2e_tot / 1e3)
+
+    # --- roofline of the stage-1 kernel --------------------------------------
+    peak, peak_kind = load_peaks()
+    alg_bytes = cells * (8 + 0.25)
+    achieved = alg_bytes / (ms_s1 / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "stage1_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as fp:
+            td = json.load(fp)
+        if td.get("workload") == spec.name:
+            traffic = td.get("bytes_per_launch")
+    roofline = {"bound": "hbm", "kernel": "k_stage1_f64", "achieved": achieved,
+                "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                if peak_kind == "measured" else "fallback",
+                "stage1_ms_per_launch": ms_s1,
+                "alg_bytes_per_cell": 8.25,
+                "fp64_dp_cells_per_s": cells / (ms_s1 / 1e3)}
+
+    # --- CPU baseline (rank 0): the oracle on the same pair -----------------
+    cpu = None
+    parity = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import build_oracle, oracle
+        build_oracle.build()
+        C = C_dev.cpu().numpy()
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        ref = oracle.parflex_full(C, spec.steps, spec.weights, spec.beta, spec.L,
+                                  threads=threads)
+        dt = time.perf_counter() - t0
+        cpu = {"value": cells / dt, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"the full pair ({N} x {M}, {n1 * n2} tiles), all stages, once",
+               "seconds": dt}
+        parity = {"best_cost_equal": bool(ref["best_cost"] == best),
+                  "path_equal": bool(np.array_equal(ref["wp"], wp.T)),
+                  "path_len": int(wp.shape[0])}
+        del C
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": config_dict(spec, N, M, cells),
+            "pairs_per_s": ws * args.steps / (ms_total / 1e3),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "steps": len(e2e_ms),
+                    "ms_per_step": e2e_tot / len(e2e_ms),
+                    "api": "tiled_stage1_from_features + run_stage2_from_tiled"},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "parity": parity,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="config1", choices=sorted(W.WORKLOADS))
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--ref-tile-rows", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    spec = W.WORKLOADS[args.workload]
+    if args.impl == "reference":
+        reference_arm(args, spec)
+    else:
+        b200_arm(args, spec)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,173 @@
+/*
+ * parflexdtw_b200.h -- C ABI of the B200-native ParFlex alignment path.
+ *
+ * ParFlex ("sparse parallel FlexDTW") aligns two feature sequences through an
+ * N x M cost matrix C cut into L x L tiles that overlap by one cell.
+ * Stage 1 runs FlexDTW in every tile; stage 2 propagates accumulated cost and
+ * path length across tile edges, scans the global top and right edges for
+ * the best cost-per-length endpoint and stitches the per-tile backtraces into
+ * one warping path.  Everything runs on the GPU; the host sees only the
+ * result (and, on request, stage-2 intermediates).
+ *
+ * Conventions (all follow the reference, ishitajain21/ParFlexDTW):
+ *   - C is row-major FP64, rows = frames of the first sequence, with leading
+ *     dimension ldc >= M (elements).  Device pointers unless stated.
+ *   - steps is n_steps (row, col) pairs, weights n_steps FP64 values.  The
+ *     device kernels accept any ordered subset of {(1,1), (1,2), (2,1)}
+ *     (the reference's default set, in any order); other steps return
+ *     PFX_ERR_STEPS.
+ *   - A warping path is K (row, col) pairs, int64, start first.
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).
+ *   - Every function returns a pfx_status; pfx_last_error() describes the
+ *     last failure of the calling thread.
+ * One plan must not be used by two host threads at the same time.
+ */
+#ifndef PARFLEXDTW_B200_H
+#define PARFLEXDTW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pfx_status {
+    PFX_OK = 0,
+    PFX_ERR_ARG = 1,          /* bad argument (the reference raises ValueError)   */
+    PFX_ERR_STEPS = 2,        /* step set outside {(1,1),(1,2),(2,1)}              */
+    PFX_ERR_CUDA = 3,         /* CUDA runtime error                                */
+    PFX_ERR_NO_ENDPOINT = 4,  /* "Stage 2: No valid endpoint found on global
+                                 top/right edges." (Parflex.py:1285-1286)          */
+    PFX_ERR_TOO_LARGE = 5,    /* tile length beyond the kernel's on-chip limit     */
+    PFX_ERR_NO_DEVICE = 6     /* no CUDA device                                    */
+} pfx_status;
+
+typedef struct pfx_plan pfx_plan;
+
+/* Human-readable status and the calling thread's last error detail. */
+const char *pfx_status_string(int status);
+const char *pfx_last_error(void);
+
+/* Library version as major*10000 + minor*100 + patch. */
+int pfx_version(void);
+
+/* Number of CUDA kernels this library has launched in this process (all
+ * devices, all threads).  No reference counterpart: launch accounting for
+ * benchmarks. */
+int64_t pfx_kernel_launches(void);
+
+/* ---------------------------------------------------------------------------
+ * Plans.  A plan fixes (N, M, L, steps, weights) and owns the device
+ * workspace of one alignment: stage-1 edge tensors and packed backpointers
+ * (0.25 B per cell), the stage-2 slot arrays (n1*n2*2*L each), edge-scan and
+ * stitch buffers.  Created on the current CUDA device.
+ *
+ * Replaces the per-call state of run_flexdtw_on_tiles / propagate_tile_edge_costs
+ * / stage2_scan_and_stitch (Parflex.py:376-469, 862-912, 1229-1356;
+ * Parflex_gpu.py:342-607, 247-339).
+ * ------------------------------------------------------------------------- */
+int pfx_plan_create(int64_t N, int64_t M, int32_t L, const int64_t *steps,
+                    const double *weights, int32_t n_steps, pfx_plan **out);
+void pfx_plan_destroy(pfx_plan *plan);
+
+/* info[0..7] = n1, n2, L, hop, n_steps, b_words_per_tile, device_bytes,
+ * stage-1 warps per CTA. */
+int pfx_plan_info(const pfx_plan *plan, int64_t *info);
+
+/* Device buffers of a plan, for zero-copy views.  which: see pfx_buffer_id. */
+typedef enum pfx_buffer_id {
+    PFX_BUF_EDGE_D = 0,   /* f64 [n1][n2][2][L] stage-1 D on tile edges (+inf past the edge) */
+    PFX_BUF_EDGE_P = 1,   /* i32 [n1][n2][2][L] stage-1 start encoding S on tile edges       */
+    PFX_BUF_BACKPTR = 2,  /* u32 [n1*n2][b_words] packed 2-bit backpointers                   */
+    PFX_BUF_EDGE_CF = 3,  /* f64 [n1][n2][2][L] C at each slot's start cell (edge_Cf_olap)    */
+    PFX_BUF_VALID = 4,    /* u8  [n1][n2][2][L] sparse valid mask                             */
+    PFX_BUF_D_ARR = 5,    /* f64 [n1][n2][2][L] accumulated cost after overlap sync           */
+    PFX_BUF_L_ARR = 6,    /* f64 [n1][n2][2][L] path length after overlap sync                */
+    PFX_BUF_TOP_D = 7,    /* f64 [M] */
+    PFX_BUF_TOP_L = 8,    /* f64 [M] */
+    PFX_BUF_RIGHT_D = 9,  /* f64 [N] */
+    PFX_BUF_RIGHT_L = 10, /* f64 [N] */
+    PFX_BUF_SEG_NORM = 11,/* f64 [2][max_segs] per-segment best cost/length               */
+    PFX_BUF_SEG_META = 12,/* i64 [2][max_segs][6] ci cj edge idx grow gcol (-1 = none)    */
+    PFX_BUF_D_PROP = 13,  /* f64 [n1][n2][2][L] snapshot before overlap sync (pfx_snapshot_prop) */
+    PFX_BUF_L_PROP = 14
+} pfx_buffer_id;
+int pfx_plan_buffer(pfx_plan *plan, int which, void **ptr, int64_t *nbytes);
+
+/* ---------------------------------------------------------------------------
+ * Stages.  All asynchronous on `stream`.
+ * ------------------------------------------------------------------------- */
+
+/* Stage 1: FlexDTW on every tile (run_flexdtw_on_tiles, Parflex.py:376-469;
+ * GPU variant flexdtw_chunk_from_global_C, gpu_flexdtw.py:288-402).  Writes D
+ * and S on tile edges and the packed backpointers. */
+int pfx_stage1(pfx_plan *plan, const double *C, int64_t ldc, void *stream);
+
+/* Stage 2a: edge tensors, valid mask and cross-tile propagation
+ * (propagate_tile_edge_costs, Parflex.py:862-912 / Parflex_gpu.py:247-339). */
+int pfx_stage2_propagate(pfx_plan *plan, const double *C, int64_t ldc, void *stream);
+
+/* Copies D_arr / L_arr into the D_PROP / L_PROP buffers (test hook: the
+ * state between propagation and overlap sync). */
+int pfx_snapshot_prop(pfx_plan *plan, void *stream);
+
+/* Stage 2b: overlap sync and global edge scan (sync_tile_overlap_edges,
+ * Parflex.py:920-969; _nb_scan_edges, Parflex.py:1154-1222) with
+ * buffer_global = min(N,M) * (1 - (1 - beta) * min(N,M) / max(N,M))
+ * (Parflex.py:1520). */
+int pfx_stage2_scan(pfx_plan *plan, double beta, void *stream);
+
+/* Stage 2c: stitched backtrace (backtrace_and_stitch, Parflex.py:1032-1103)
+ * from the scan's best endpoint (from_best = 1) or from tile (i, j), edge,
+ * idx (from_best = 0). */
+int pfx_stage2_stitch(pfx_plan *plan, int from_best, int64_t i, int64_t j,
+                      int64_t edge, int64_t idx, void *stream);
+
+/* Stage 1 + 2a + 2b + 2c in one call on a device-resident C. */
+int pfx_parflex_device(pfx_plan *plan, const double *C, int64_t ldc,
+                       double beta, void *stream);
+
+/* Synchronises `stream` and reads the scan/stitch results: best normalised
+ * cost, best_end[7] = (grow, gcol, ci, cj, edge, idx, found), path length. */
+int pfx_result(pfx_plan *plan, void *stream, double *best_cost,
+               int64_t *best_end7, int64_t *wp_len);
+
+/* Copies the last stitched path (K x 2 int64, start first) into host memory
+ * wp_host of capacity `cap` points (synchronises `stream`). */
+int pfx_copy_path(pfx_plan *plan, void *stream, int64_t *wp_host, int64_t cap);
+
+/* ---------------------------------------------------------------------------
+ * One-call drop-ins.
+ * ------------------------------------------------------------------------- */
+
+/* parflex(C, steps, weights, beta, L) (Parflex.py:1510-1547,
+ * Parflex_gpu.py:656-854) on a HOST cost matrix: copies C to the device,
+ * runs both stages and copies the path back.  wp_out receives K x 2 int64
+ * points (start first) if K <= wp_cap; *wp_len is always set. */
+int pfx_parflex(const double *C_host, int64_t N, int64_t M, int64_t ldc,
+                const int64_t *steps, const double *weights, int32_t n_steps,
+                double beta, int32_t L, double *best_cost, int64_t *wp_out,
+                int64_t wp_cap, int64_t *wp_len);
+
+/* 1 - L2norm(F1)^T L2norm(F2) in FP64 with a fixed summation order
+ * (cost_matrix_from_features_gpu, gpu_flexdtw.py:95-109; Parflex.py:1470).
+ * F1 is d x N and F2 d x M, row-major by feature (the (d, frames) layout).
+ * `norm_scratch` holds d*(N+M) doubles (the normalised features). */
+int pfx_cost_matrix_f64(const double *F1, const double *F2, int32_t d,
+                        int64_t N, int64_t M, double *norm_scratch, double *C,
+                        int64_t ldc, void *stream);
+
+/* FlexDTW.flexdtw's DP on one R x W tile of C with full outputs
+ * (FlexDTW.py:326-370; flexdtw_chunk_from_global_C, gpu_flexdtw.py:288-402):
+ * D (f64), P (int32 start encoding) and B (int8 step index, -1 when no step
+ * won), each R x W row-major on the device. */
+int pfx_flexdtw_tile(const double *C, int64_t ldc, int32_t R, int32_t W,
+                     const int64_t *steps, const double *weights,
+                     int32_t n_steps, double *D, int32_t *P, int8_t *B,
+                     void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PARFLEXDTW_B200_H */

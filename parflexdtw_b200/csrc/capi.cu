@@ -1,0 +1,441 @@
+// extern "C" entry points (declared in include/parflexdtw_b200.h).
+#include <stdarg.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <atomic>
+#include <stdlib.h>
+#include <string.h>
+
+#include <cmath>
+
+#include "common.cuh"
+
+
+
+using namespace pfx;
+
+static thread_local char g_err[512];
+static std::atomic<long long> g_launches{0};
+
+void pfx::count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+extern "C" int64_t pfx_kernel_launches(void) { return (int64_t)g_launches.load(); }
+
+static int fail(int status, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return status;
+}
+
+#define CK(call)                                                                         \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return fail(PFX_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                             \
+    } while (0)
+
+struct pfx_plan {
+    Geo g;
+    int nw;
+    int device;
+    size_t bytes;
+    S1Out s1;
+    S2Buf s2;
+    double* D_prop;
+    double* L_prop;
+    int64_t n4;  // n1*n2*2*L
+    void* blocks[32];
+    int nblocks;
+};
+
+static const char* kStatus[] = {"ok",
+                                "invalid argument",
+                                "unsupported step set",
+                                "CUDA error",
+                                "Stage 2: No valid endpoint found on global top/right edges.",
+                                "tile length too large",
+                                "no CUDA device"};
+
+extern "C" const char* pfx_status_string(int s) {
+    return (s >= 0 && s <= 6) ? kStatus[s] : "unknown status";
+}
+extern "C" const char* pfx_last_error(void) { return g_err; }
+extern "C" int pfx_version(void) { return 100; }
+
+// Steps -> kinds (0 = (1,1), 1 = (1,2), 2 = (2,1)).
+static int parse_steps(const int64_t* steps, const double* weights, int32_t n, Geo* g) {
+    if (n < 1 || n > 3) return fail(PFX_ERR_STEPS, "n_steps=%d; the device DP takes 1..3 steps", n);
+    for (int s = 0; s < n; ++s) {
+        const int64_t a = steps[2 * s], b = steps[2 * s + 1];
+        int kd;
+        if (a == 1 && b == 1) kd = 0;
+        else if (a == 1 && b == 2) kd = 1;
+        else if (a == 2 && b == 1) kd = 2;
+        else
+            return fail(PFX_ERR_STEPS, "step (%lld, %lld) is not one of (1,1), (1,2), (2,1)",
+                        (long long)a, (long long)b);
+        for (int t = 0; t < s; ++t)
+            if (g->kind[t] == kd) return fail(PFX_ERR_STEPS, "step listed twice");
+        g->kind[s] = kd;
+        g->w[s] = weights[s];
+    }
+    for (int s = n; s < 3; ++s) { g->kind[s] = 0; g->w[s] = 0.0; }
+    g->S = n;
+    return PFX_OK;
+}
+
+static int make_geo(int64_t N, int64_t M, int32_t L, const int64_t* steps, const double* weights,
+                    int32_t n_steps, Geo* g) {
+    memset(g, 0, sizeof(*g));
+    if (N < 2 || M < 2) return fail(PFX_ERR_ARG, "cost matrix %lld x %lld: need at least 2 x 2", (long long)N, (long long)M);
+    if (L < 2) return fail(PFX_ERR_ARG, "L=%d: need L >= 2", L);
+    if (N >= (1LL << 31) || M >= (1LL << 31)) return fail(PFX_ERR_ARG, "sequence longer than 2^31");
+    int st = parse_steps(steps, weights, n_steps, g);
+    if (st) return st;
+    g->N = N;
+    g->M = M;
+    g->ldc = M;
+    g->L = L;
+    g->hop = L - 1;
+    g->n1 = (int32_t)ceil_div64(N - 1, g->hop);
+    g->n2 = (int32_t)ceil_div64(M - 1, g->hop);
+    g->b_words = tile_b_words(L);
+    return PFX_OK;
+}
+
+static int num_sms_cur() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+static int check_smem(int32_t L, int nw) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t need = stage1_smem_bytes_host(L, nw);
+    if (need > (size_t)optin)
+        return fail(PFX_ERR_TOO_LARGE, "L=%d needs %zu B of shared memory per tile CTA (limit %d)",
+                    L, need, optin);
+    return PFX_OK;
+}
+
+template <typename T>
+static int plan_alloc(pfx_plan* p, T** ptr, size_t count) {
+    void* q = nullptr;
+    const size_t bytes = count * sizeof(T) > 0 ? count * sizeof(T) : 16;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess)
+        return fail(PFX_ERR_CUDA, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    p->blocks[p->nblocks++] = q;
+    p->bytes += bytes;
+    *ptr = reinterpret_cast<T*>(q);
+    return PFX_OK;
+}
+
+extern "C" void pfx_plan_destroy(pfx_plan* p) {
+    if (!p) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(p->device);
+    for (int i = 0; i < p->nblocks; ++i) cudaFree(p->blocks[i]);
+    cudaSetDevice(cur);
+    free(p);
+}
+
+extern "C" int pfx_plan_create(int64_t N, int64_t M, int32_t L, const int64_t* steps,
+                               const double* weights, int32_t n_steps, pfx_plan** out) {
+    if (!out || !steps || !weights) return fail(PFX_ERR_ARG, "null argument");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(PFX_ERR_NO_DEVICE, "no CUDA device");
+    pfx_plan* p = (pfx_plan*)calloc(1, sizeof(pfx_plan));
+    if (!p) return fail(PFX_ERR_ARG, "out of host memory");
+    int st = make_geo(N, M, L, steps, weights, n_steps, &p->g);
+    if (st) { free(p); return st; }
+    cudaGetDevice(&p->device);
+    p->nw = stage1_pick_warps(p->g, num_sms_cur());
+    if ((st = check_smem(L, p->nw))) { free(p); return st; }
+    const Geo& g = p->g;
+    const int64_t nt = (int64_t)g.n1 * g.n2;
+    p->n4 = nt * 2 * g.L;
+    const int64_t ms = std::max<int64_t>(std::max(ceil_div64(M, L), ceil_div64(N, L)), 1);
+    p->s2.max_segs = (int32_t)ms;
+    p->s2.seg_cap = 2 * (int64_t)L + 8;
+    double* eD;
+    int32_t* eP;
+    uint32_t* Bw;
+#define PA(ptr, n)                                            \
+    do {                                                      \
+        if ((st = plan_alloc(p, ptr, (size_t)(n)))) {         \
+            pfx_plan_destroy(p);                              \
+            return st;                                        \
+        }                                                     \
+    } while (0)
+    PA(&eD, p->n4);
+    PA(&eP, p->n4);
+    PA(&Bw, nt * g.b_words);
+    p->s1.edge_D = eD;
+    p->s1.edge_P = eP;
+    p->s1.Bw = Bw;
+    p->s2.edge_D = eD;
+    p->s2.edge_P = eP;
+    p->s2.Bw = Bw;
+    PA(&p->s2.edge_Cf, p->n4);
+    PA(&p->s2.valid, p->n4);
+    PA(&p->s2.D_arr, p->n4);
+    PA(&p->s2.L_arr, p->n4);
+    PA(&p->D_prop, p->n4);
+    PA(&p->L_prop, p->n4);
+    PA(&p->s2.top_D, M);
+    PA(&p->s2.top_L, M);
+    PA(&p->s2.right_D, N);
+    PA(&p->s2.right_L, N);
+    PA(&p->s2.seg_norm, 2 * ms);
+    PA(&p->s2.seg_meta, 12 * ms);
+    PA(&p->s2.best, 1);
+    PA(&p->s2.best_end, 7);
+    PA(&p->s2.chain, 101 * 12);
+    PA(&p->s2.chain_len, 1);
+    PA(&p->s2.seg_pts, 101 * p->s2.seg_cap * 2);
+    PA(&p->s2.seg_len, 101);
+    PA(&p->s2.wp, 101 * p->s2.seg_cap * 2);
+    PA(&p->s2.wp_len, 1);
+#undef PA
+    CK(cudaMemset(p->s2.best_end, 0, 7 * sizeof(int64_t)));
+    CK(cudaMemset(p->s2.chain_len, 0, sizeof(int32_t)));
+    CK(cudaMemset(p->s2.wp_len, 0, sizeof(int64_t)));
+    *out = p;
+    return PFX_OK;
+}
+
+extern "C" int pfx_plan_info(const pfx_plan* p, int64_t* info) {
+    if (!p || !info) return fail(PFX_ERR_ARG, "null argument");
+    info[0] = p->g.n1;
+    info[1] = p->g.n2;
+    info[2] = p->g.L;
+    info[3] = p->g.hop;
+    info[4] = p->g.S;
+    info[5] = p->g.b_words;
+    info[6] = (int64_t)p->bytes;
+    info[7] = p->nw;
+    return PFX_OK;
+}
+
+extern "C" int pfx_plan_buffer(pfx_plan* p, int which, void** ptr, int64_t* nbytes) {
+    if (!p || !ptr || !nbytes) return fail(PFX_ERR_ARG, "null argument");
+    const int64_t n4 = p->n4, ms = p->s2.max_segs;
+    switch (which) {
+        case PFX_BUF_EDGE_D: *ptr = p->s1.edge_D; *nbytes = n4 * 8; break;
+        case PFX_BUF_EDGE_P: *ptr = p->s1.edge_P; *nbytes = n4 * 4; break;
+        case PFX_BUF_BACKPTR: *ptr = p->s1.Bw; *nbytes = (int64_t)p->g.n1 * p->g.n2 * p->g.b_words * 4; break;
+        case PFX_BUF_EDGE_CF: *ptr = p->s2.edge_Cf; *nbytes = n4 * 8; break;
+        case PFX_BUF_VALID: *ptr = p->s2.valid; *nbytes = n4; break;
+        case PFX_BUF_D_ARR: *ptr = p->s2.D_arr; *nbytes = n4 * 8; break;
+        case PFX_BUF_L_ARR: *ptr = p->s2.L_arr; *nbytes = n4 * 8; break;
+        case PFX_BUF_TOP_D: *ptr = p->s2.top_D; *nbytes = p->g.M * 8; break;
+        case PFX_BUF_TOP_L: *ptr = p->s2.top_L; *nbytes = p->g.M * 8; break;
+        case PFX_BUF_RIGHT_D: *ptr = p->s2.right_D; *nbytes = p->g.N * 8; break;
+        case PFX_BUF_RIGHT_L: *ptr = p->s2.right_L; *nbytes = p->g.N * 8; break;
+        case PFX_BUF_SEG_NORM: *ptr = p->s2.seg_norm; *nbytes = 2 * ms * 8; break;
+        case PFX_BUF_SEG_META: *ptr = p->s2.seg_meta; *nbytes = 12 * ms * 8; break;
+        case PFX_BUF_D_PROP: *ptr = p->D_prop; *nbytes = n4 * 8; break;
+        case PFX_BUF_L_PROP: *ptr = p->L_prop; *nbytes = n4 * 8; break;
+        default: return fail(PFX_ERR_ARG, "unknown buffer id %d", which);
+    }
+    return PFX_OK;
+}
+
+static int check_ldc(const pfx_plan* p, const double* C, int64_t ldc) {
+    if (!C) return fail(PFX_ERR_ARG, "null cost matrix");
+    if (ldc < p->g.M) return fail(PFX_ERR_ARG, "ldc=%lld < M=%lld", (long long)ldc, (long long)p->g.M);
+    return PFX_OK;
+}
+
+extern "C" int pfx_stage1(pfx_plan* p, const double* C, int64_t ldc, void* stream) {
+    if (!p) return fail(PFX_ERR_ARG, "null plan");
+    int st = check_ldc(p, C, ldc);
+    if (st) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    Geo g = p->g;
+    g.ldc = ldc;
+    CK(launch_fill(p->s1.edge_D, p->n4, HUGE_VAL, s));
+    CK(cudaMemsetAsync(p->s1.edge_P, 0, (size_t)p->n4 * 4, s));
+    CK(launch_stage1(C, g, p->s1, 0, g.n1 * g.n2, p->nw, false, s));
+    return PFX_OK;
+}
+
+extern "C" int pfx_stage2_propagate(pfx_plan* p, const double* C, int64_t ldc, void* stream) {
+    if (!p) return fail(PFX_ERR_ARG, "null plan");
+    int st = check_ldc(p, C, ldc);
+    if (st) return st;
+    Geo g = p->g;
+    g.ldc = ldc;
+    CK(launch_stage2(C, g, p->s2, 0, (cudaStream_t)stream));
+    return PFX_OK;
+}
+
+extern "C" int pfx_snapshot_prop(pfx_plan* p, void* stream) {
+    if (!p) return fail(PFX_ERR_ARG, "null plan");
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(cudaMemcpyAsync(p->D_prop, p->s2.D_arr, (size_t)p->n4 * 8, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(p->L_prop, p->s2.L_arr, (size_t)p->n4 * 8, cudaMemcpyDeviceToDevice, s));
+    return PFX_OK;
+}
+
+static int64_t buffer_global(int64_t N, int64_t M, double beta) {
+    // Parflex.py:1520, evaluated in the same order
+    const double mn = (double)(N < M ? N : M), mx = (double)(N < M ? M : N);
+    const double bg = mn * (1 - (1 - beta) * mn / mx);
+    return (int64_t)bg;
+}
+
+extern "C" int pfx_stage2_scan(pfx_plan* p, double beta, void* stream) {
+    if (!p) return fail(PFX_ERR_ARG, "null plan");
+    CK(launch_sync_scan(p->g, p->s2, buffer_global(p->g.N, p->g.M, beta), (cudaStream_t)stream));
+    return PFX_OK;
+}
+
+extern "C" int pfx_stage2_stitch(pfx_plan* p, int from_best, int64_t i, int64_t j, int64_t edge,
+                                 int64_t idx, void* stream) {
+    if (!p) return fail(PFX_ERR_ARG, "null plan");
+    CK(launch_stitch(p->g, p->s2, (cudaStream_t)stream, from_best, i, j, edge, idx));
+    return PFX_OK;
+}
+
+extern "C" int pfx_parflex_device(pfx_plan* p, const double* C, int64_t ldc, double beta,
+                                  void* stream) {
+    int st;
+    if ((st = pfx_stage1(p, C, ldc, stream))) return st;
+    if ((st = pfx_stage2_propagate(p, C, ldc, stream))) return st;
+    if ((st = pfx_stage2_scan(p, beta, stream))) return st;
+    if ((st = pfx_stage2_stitch(p, 1, 0, 0, 0, 0, stream))) return st;
+    return PFX_OK;
+}
+
+extern "C" int pfx_result(pfx_plan* p, void* stream, double* best_cost, int64_t* best_end7,
+                          int64_t* wp_len) {
+    if (!p) return fail(PFX_ERR_ARG, "null plan");
+    cudaStream_t s = (cudaStream_t)stream;
+    double b = 0;
+    int64_t e[7];
+    int64_t n = 0;
+    CK(cudaMemcpyAsync(&b, p->s2.best, 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(e, p->s2.best_end, 56, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&n, p->s2.wp_len, 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (best_cost) *best_cost = b;
+    if (best_end7) memcpy(best_end7, e, sizeof(e));
+    if (wp_len) *wp_len = n;
+    if (!e[6]) return fail(PFX_ERR_NO_ENDPOINT, "%s", kStatus[PFX_ERR_NO_ENDPOINT]);
+    return PFX_OK;
+}
+
+extern "C" int pfx_copy_path(pfx_plan* p, void* stream, int64_t* wp_host, int64_t cap) {
+    if (!p || !wp_host) return fail(PFX_ERR_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    int64_t n = 0;
+    CK(cudaMemcpyAsync(&n, p->s2.wp_len, 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (n > cap) return fail(PFX_ERR_ARG, "path has %lld points, buffer holds %lld", (long long)n, (long long)cap);
+    if (n > 0) CK(cudaMemcpyAsync(wp_host, p->s2.wp, (size_t)n * 16, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return PFX_OK;
+}
+
+extern "C" int pfx_parflex(const double* C_host, int64_t N, int64_t M, int64_t ldc,
+                           const int64_t* steps, const double* weights, int32_t n_steps,
+                           double beta, int32_t L, double* best_cost, int64_t* wp_out,
+                           int64_t wp_cap, int64_t* wp_len) {
+    if (!C_host || ldc < M) return fail(PFX_ERR_ARG, "bad host cost matrix");
+    pfx_plan* p = nullptr;
+    int st = pfx_plan_create(N, M, L, steps, weights, n_steps, &p);
+    if (st) return st;
+    double* Cd = nullptr;
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+        pfx_plan_destroy(p);
+        return fail(PFX_ERR_CUDA, "stream creation failed");
+    }
+    cudaError_t e = cudaMallocAsync((void**)&Cd, (size_t)N * M * 8, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpy2DAsync(Cd, (size_t)M * 8, C_host, (size_t)ldc * 8, (size_t)M * 8, (size_t)N,
+                              cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+        st = fail(PFX_ERR_CUDA, "cost-matrix upload: %s", cudaGetErrorString(e));
+    } else {
+        st = pfx_parflex_device(p, Cd, M, beta, s);
+        int64_t n = 0;
+        if (!st) st = pfx_result(p, s, best_cost, nullptr, &n);
+        if (wp_len) *wp_len = n;
+        if (!st && wp_out && n <= wp_cap) st = pfx_copy_path(p, s, wp_out, wp_cap);
+    }
+    if (Cd) cudaFreeAsync(Cd, s);
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    pfx_plan_destroy(p);
+    return st;
+}
+
+extern "C" int pfx_cost_matrix_f64(const double* F1, const double* F2, int32_t d, int64_t N,
+                                   int64_t M, double* norm_scratch, double* C, int64_t ldc,
+                                   void* stream) {
+    if (!F1 || !F2 || !norm_scratch || !C) return fail(PFX_ERR_ARG, "null argument");
+    if (d < 1 || N < 1 || M < 1 || ldc < M) return fail(PFX_ERR_ARG, "bad shape");
+    CK(launch_cost_f64(F1, F2, d, N, M, norm_scratch, norm_scratch + (int64_t)d * N, C, ldc,
+                       (cudaStream_t)stream));
+    return PFX_OK;
+}
+
+extern "C" int pfx_flexdtw_tile(const double* C, int64_t ldc, int32_t R, int32_t W,
+                                const int64_t* steps, const double* weights, int32_t n_steps,
+                                double* D, int32_t* P, int8_t* B, void* stream) {
+    if (!C || !D || !P || !B || !steps || !weights) return fail(PFX_ERR_ARG, "null argument");
+    if (R < 1 || W < 1) return fail(PFX_ERR_ARG, "Empty chunk: R=%d, C=%d", R, W);
+    if (ldc < W) return fail(PFX_ERR_ARG, "ldc < W");
+    Geo g;
+    memset(&g, 0, sizeof(g));
+    int st = parse_steps(steps, weights, n_steps, &g);
+    if (st) return st;
+    const int32_t L = R > W ? R : W;
+    g.N = R;
+    g.M = W;
+    g.ldc = ldc;
+    g.L = L < 2 ? 2 : L;
+    g.hop = g.L - 1;
+    g.n1 = 1;
+    g.n2 = 1;
+    g.b_words = tile_b_words(g.L);
+    if ((st = check_smem(g.L, 8))) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    S1Out o;
+    memset(&o, 0, sizeof(o));
+    const size_t eb = (size_t)2 * g.L;
+    CK(cudaMallocAsync((void**)&o.edge_D, eb * 8, s));
+    CK(cudaMallocAsync((void**)&o.edge_P, eb * 4, s));
+    CK(cudaMallocAsync((void**)&o.Bw, (size_t)g.b_words * 4, s));
+    o.full_D = D;
+    o.full_P = P;
+    o.full_B = B;
+    cudaError_t e = cudaSuccess;
+    if (R == 1 || W == 1) {
+        // no DP cells: D = C, P = 0, B = 0 (FlexDTW.py:329-334)
+        e = cudaMemcpy2DAsync(D, (size_t)W * 8, C, (size_t)ldc * 8, (size_t)W * 8, (size_t)R,
+                              cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(P, 0, (size_t)R * W * 4, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(B, 0, (size_t)R * W, s);
+    } else {
+        e = launch_stage1(C, g, o, 0, 1, 8, true, s);
+    }
+    cudaFreeAsync(o.edge_D, s);
+    cudaFreeAsync(o.edge_P, s);
+    cudaFreeAsync(o.Bw, s);
+    if (e != cudaSuccess) return fail(PFX_ERR_CUDA, "tile DP: %s", cudaGetErrorString(e));
+    return PFX_OK;
+}

@@ -1,0 +1,123 @@
+// Shared definitions for the ParFlex B200 kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/parflexdtw_b200.h"
+
+namespace pfx {
+
+// Tile-grid geometry and DP parameters, passed by value to every kernel.
+// Matches the reference tiling: hop = L - 1, tile (i, j) covers rows
+// [i*hop, min(i*hop + L, N)) and columns [j*hop, min(j*hop + L, M))
+// (Parflex.py:388-431).
+struct Geo {
+    int64_t N, M;      // cost-matrix rows (F1 frames) and columns (F2 frames)
+    int64_t ldc;       // leading dimension of C (elements)
+    int32_t L, hop;    // tile length and hop
+    int32_t n1, n2;    // tile rows / tile columns
+    int32_t S;         // number of steps (1..3)
+    int32_t kind[3];   // per step: 0 = (1,1), 1 = (1,2), 2 = (2,1)
+    double w[3];       // per step weight
+    int64_t b_words;   // packed-backpointer words reserved per tile
+};
+
+__host__ __device__ inline int64_t ceil_div64(int64_t a, int64_t b) { return (a + b - 1) / b; }
+__host__ __device__ inline int32_t ceil_div32(int32_t a, int32_t b) { return (a + b - 1) / b; }
+
+__host__ __device__ inline void tile_rect(const Geo& g, int ti, int tj, int64_t* r0, int64_t* c0,
+                                          int32_t* R, int32_t* W) {
+    *r0 = (int64_t)ti * g.hop;
+    *c0 = (int64_t)tj * g.hop;
+    int64_t R_ = g.N - *r0, W_ = g.M - *c0;
+    *R = (int32_t)(R_ < g.L ? R_ : g.L);
+    *W = (int32_t)(W_ < g.L ? W_ : g.L);
+}
+
+// Stage-1 wavefront schedule of one tile (see stage1_f64.cu): strips of 32
+// rows, each strip sweeps "local time" tau = c + lane over span steps, strip k
+// starts lag*k steps after the CTA starts.  Backpointers are packed 2 bits per
+// cell into 32-bit words laid out [strip][period][lane], one period = 16
+// consecutive local-time steps of one lane (row).
+constexpr int kBlk = 16;  // steps between CTA barriers == cells per B word
+struct Sched {
+    int32_t nS, span, nP, lag;
+};
+__host__ __device__ inline Sched make_sched(int32_t R, int32_t W, int32_t nwarps) {
+    Sched s;
+    s.nS = ceil_div32(R, 32);
+    s.span = ceil_div32(W + 31, kBlk) * kBlk;
+    s.nP = s.span / kBlk;
+    int32_t lag = ceil_div32(ceil_div32(s.span, nwarps), kBlk) * kBlk;
+    s.lag = lag < 48 ? 48 : lag;
+    return s;
+}
+// Words one tile of at most L x L cells needs.
+__host__ __device__ inline int64_t tile_b_words(int32_t L) {
+    Sched s = make_sched(L, L, 1);
+    return (int64_t)s.nS * s.nP * 32;
+}
+// Backpointer code of cell (r, c) of a tile with W columns, from its word slab.
+__device__ __forceinline__ int bp_code(const uint32_t* __restrict__ slab, int32_t W, int32_t r,
+                                       int32_t c) {
+    const int32_t nP = ceil_div32(W + 31, kBlk);
+    const int32_t k = r >> 5, lane = r & 31, tau = c + lane;
+    const uint32_t word = __ldg(slab + ((int64_t)k * nP + (tau >> 4)) * 32 + lane);
+    return (int)((word >> ((tau & 15) * 2)) & 3u);
+}
+
+// Stage-1 outputs.
+struct S1Out {
+    double* edge_D;   // [tiles][2][L] D on the top / right edge, +inf past the edge
+    int32_t* edge_P;  // [tiles][2][L] start encoding on the edges
+    uint32_t* Bw;     // [tiles][b_words] packed backpointers
+    double* full_D;   // single-tile full outputs (R x W), or null
+    int32_t* full_P;
+    int8_t* full_B;
+};
+
+// Stage-2 device state.  Slot arrays are [n1][n2][2][L].
+struct S2Buf {
+    const double* edge_D;
+    const int32_t* edge_P;
+    const uint32_t* Bw;
+    double* edge_Cf;     // C at each slot's start cell
+    uint8_t* valid;      // sparse compute mask
+    double* D_arr;
+    double* L_arr;
+    double* top_D;       // [M]
+    double* top_L;
+    double* right_D;     // [N]
+    double* right_L;
+    double* seg_norm;    // [2][max_segs]
+    int64_t* seg_meta;   // [2][max_segs][6] ci cj et idx grow gcol
+    int32_t max_segs;
+    double* best;        // [1]
+    int64_t* best_end;   // [7] grow gcol ci cj et idx found
+    int32_t* chain;      // [101][12]
+    int32_t* chain_len;  // [1]
+    int32_t* seg_pts;    // [101][seg_cap][2]
+    int32_t* seg_len;    // [101]
+    int64_t seg_cap;
+    int64_t* wp;         // [K][2] final path, start first
+    int64_t* wp_len;     // [1]
+};
+
+// Count of kernels this library has launched (process-wide).
+void count_launches(int n);
+
+// Launchers (stage1_f64.cu, stage2.cu, cost.cu).
+cudaError_t launch_stage1(const double* C, const Geo& g, const S1Out& o, int tile0, int ntiles,
+                          int nw, bool full, cudaStream_t st);
+size_t stage1_smem_bytes_host(int32_t L, int nw);
+int stage1_pick_warps(const Geo& g, int num_sms);
+cudaError_t launch_fill(double* p, int64_t n, double v, cudaStream_t st);
+cudaError_t launch_stage2(const double* C, const Geo& g, const S2Buf& b, int64_t buf,
+                          cudaStream_t st);
+cudaError_t launch_sync_scan(const Geo& g, const S2Buf& b, int64_t buf, cudaStream_t st);
+cudaError_t launch_stitch(const Geo& g, const S2Buf& b, cudaStream_t st, int from_best,
+                          int64_t si, int64_t sj, int64_t se, int64_t sx);
+cudaError_t launch_cost_f64(const double* F1, const double* F2, int d, int64_t N, int64_t M,
+                            double* An, double* Bn, double* C, int64_t ldc, cudaStream_t st);
+
+}  // namespace pfx

@@ -1,0 +1,158 @@
+"""Device plan: one alignment's geometry and device workspace.
+
+Thin owner of a ``pfx_plan*`` (include/parflexdtw_b200.h).  Device buffers
+are exposed as zero-copy torch views through ``__cuda_array_interface__``.
+torch supplies device memory for inputs and the current CUDA stream.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import weakref
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+_DT = {"f64": ("<f8", torch.float64, 8), "i32": ("<i4", torch.int32, 4),
+       "u32": ("<u4", torch.int32, 4), "u8": ("|u1", torch.uint8, 1),
+       "i64": ("<i8", torch.int64, 8)}
+
+_BUF_DTYPE = {"EDGE_D": "f64", "EDGE_P": "i32", "BACKPTR": "u32", "EDGE_CF": "f64",
+              "VALID": "u8", "D_ARR": "f64", "L_ARR": "f64", "TOP_D": "f64",
+              "TOP_L": "f64", "RIGHT_D": "f64", "RIGHT_L": "f64", "SEG_NORM": "f64",
+              "SEG_META": "i64", "D_PROP": "f64", "L_PROP": "f64"}
+
+
+class _DevView:
+    """Minimal ``__cuda_array_interface__`` exporter for a plan buffer."""
+
+    def __init__(self, ptr, shape, typestr):
+        self.__cuda_array_interface__ = {
+            "shape": tuple(int(s) for s in shape), "typestr": typestr,
+            "data": (int(ptr), False), "version": 2, "strides": None}
+
+
+def current_stream_ptr():
+    return ct.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def normalize_steps(steps, weights):
+    st = np.asarray(steps, dtype=np.int64).reshape(-1, 2)
+    w = np.asarray(weights, dtype=np.float64).reshape(-1)
+    if st.shape[0] != w.shape[0]:
+        raise ValueError("steps and weights must have the same length")
+    return st, w
+
+
+def _free_plan(handle):
+    if handle:
+        L.load().pfx_plan_destroy(handle)
+
+
+class Plan:
+    """Geometry + device workspace for an N x M cost matrix with tile length L."""
+
+    def __init__(self, N, M, Lb, steps, weights):
+        lib = L.load()
+        if not torch.cuda.is_available():
+            raise RuntimeError("parflexdtw_b200 needs a CUDA device")
+        torch.cuda.init()
+        st, w = normalize_steps(steps, weights)
+        self.steps = st
+        self.weights = w
+        self.N, self.M, self.L = int(N), int(M), int(Lb)
+        h = ct.c_void_p()
+        L.check(lib.pfx_plan_create(self.N, self.M, self.L,
+                                    L.i64_array(st.reshape(-1)),
+                                    L.f64_array(w), st.shape[0], ct.byref(h)))
+        self._h = h
+        self._fin = weakref.finalize(self, _free_plan, h)
+        info = (ct.c_int64 * 8)()
+        L.check(lib.pfx_plan_info(h, info))
+        (self.n1, self.n2, _, self.hop, self.S, self.b_words, self.device_bytes,
+         self.warps) = (int(x) for x in info)
+        self.device = torch.cuda.current_device()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        self._fin()
+
+    # -- zero-copy device views ------------------------------------------
+    def view(self, name) -> torch.Tensor:
+        lib = L.load()
+        ptr, nb = ct.c_void_p(), ct.c_int64()
+        L.check(lib.pfx_plan_buffer(self._h, L.BUF[name], ct.byref(ptr), ct.byref(nb)))
+        typestr, tdt, size = _DT[_BUF_DTYPE[name]]
+        n = nb.value // size
+        shape = (n,)
+        s4 = (self.n1, self.n2, 2, self.L)
+        if name in ("EDGE_D", "EDGE_P", "EDGE_CF", "VALID", "D_ARR", "L_ARR", "D_PROP",
+                    "L_PROP"):
+            shape = s4
+        elif name == "SEG_NORM":
+            shape = (2, n // 2)
+        elif name == "SEG_META":
+            shape = (2, n // 12, 6)
+        t = torch.as_tensor(_DevView(ptr.value, shape, typestr),
+                            device=f"cuda:{self.device}")
+        t._pfx_owner = self  # keep the plan alive while the view lives
+        return t
+
+    def host(self, name) -> np.ndarray:
+        return self.view(name).cpu().numpy()
+
+    # -- stages ----------------------------------------------------------
+    def stage1(self, C_dev: torch.Tensor, stream=None):
+        lib = L.load()
+        L.check(lib.pfx_stage1(self._h, ct.c_void_p(C_dev.data_ptr()), C_dev.stride(0),
+                               stream or current_stream_ptr()))
+
+    def propagate(self, C_dev: torch.Tensor, stream=None, snapshot=False):
+        lib = L.load()
+        s = stream or current_stream_ptr()
+        L.check(lib.pfx_stage2_propagate(self._h, ct.c_void_p(C_dev.data_ptr()),
+                                         C_dev.stride(0), s))
+        if snapshot:
+            L.check(lib.pfx_snapshot_prop(self._h, s))
+
+    def scan(self, beta, stream=None):
+        L.check(L.load().pfx_stage2_scan(self._h, float(beta),
+                                         stream or current_stream_ptr()))
+
+    def stitch(self, start=None, stream=None):
+        lib = L.load()
+        s = stream or current_stream_ptr()
+        if start is None:
+            L.check(lib.pfx_stage2_stitch(self._h, 1, 0, 0, 0, 0, s))
+        else:
+            i, j, e, x = (int(v) for v in start)
+            L.check(lib.pfx_stage2_stitch(self._h, 0, i, j, e, x, s))
+
+    def run(self, C_dev: torch.Tensor, beta, stream=None):
+        L.check(L.load().pfx_parflex_device(self._h, ct.c_void_p(C_dev.data_ptr()),
+                                            C_dev.stride(0), float(beta),
+                                            stream or current_stream_ptr()))
+
+    def result(self, stream=None, raise_no_endpoint=True):
+        """(best_cost, best_end[6], found, path_len); synchronises the stream."""
+        lib = L.load()
+        b = ct.c_double()
+        e = (ct.c_int64 * 7)()
+        n = ct.c_int64()
+        st = lib.pfx_result(self._h, stream or current_stream_ptr(), ct.byref(b), e,
+                            ct.byref(n))
+        if st != L.PFX_ERR_NO_ENDPOINT or raise_no_endpoint:
+            L.check(st)
+        return b.value, tuple(int(x) for x in e[:6]), bool(e[6]), n.value
+
+    def path(self, n, stream=None) -> np.ndarray:
+        """The last stitched path as a (K, 2) int64 array, start first."""
+        out = np.empty((max(int(n), 1), 2), dtype=np.int64)
+        L.check(L.load().pfx_copy_path(self._h, stream or current_stream_ptr(),
+                                       out.ctypes.data_as(ct.POINTER(ct.c_int64)),
+                                       out.shape[0]))
+        return out[:n]

@@ -25,6 +25,8 @@ __all__ = [
     "PairSpec",
     "CONFIG0",
     "CONFIG1",
+    "NCU_SMALL",
+    "WORKLOADS",
     "make_pair",
 ]
 
@@ -164,6 +166,12 @@ CONFIG0 = PairSpec("chroma12_pair_2000x2400_L500", 2000, 2400, 500)
 # L=4000, FP64 DP.
 CONFIG1 = PairSpec("chroma12_pair_30000x36000_L4000_fp64", 30000, 36000, 4000,
                    pad_frac=0.10)
+# Profiling case: the 30000 x 36000 workload's tile length and kernel
+# configuration on a 3 x 3 tile grid (C = 0.6 GB, larger than L2).
+NCU_SMALL = PairSpec("chroma12_pair_8000x9600_L4000_fp64", 8000, 9600, 4000,
+                     pad_frac=0.0)
+
+WORKLOADS = {"config0": CONFIG0, "config1": CONFIG1, "ncu_small": NCU_SMALL}
 
 
 def make_pair(spec: PairSpec):
