@@ -56,6 +56,8 @@ SIGNATURES = [
     ("pfx_cost_matrix_f64", ct.c_int, [_vp, _vp, _i32, _i64, _i64, _vp, _vp, _i64, _vp]),
     ("pfx_flexdtw_tile", ct.c_int, [_vp, _i64, _i32, _i32, _i64p, _f64p, _i32, _vp, _vp,
                                     _vp, _vp]),
+    ("pfx_flexdtw_tile_noalloc", ct.c_int, [_vp, _i64, _i32, _i32, _i64p, _f64p, _i32, _vp,
+                                            _vp, _vp, _vp]),
 ]
 
 _lib = None

@@ -88,6 +88,12 @@ static int parse_steps(const int64_t* steps, const double* weights, int32_t n, G
     return PFX_OK;
 }
 
+// Internal helpers shared with other translation units of this library.
+int pfx::report_status(int status, const char* msg) { return fail(status, "%s", msg); }
+int pfx::parse_step_kinds(const int64_t* steps, const double* weights, int32_t n, Geo* g) {
+    return parse_steps(steps, weights, n, g);
+}
+
 static int make_geo(int64_t N, int64_t M, int32_t L, const int64_t* steps, const double* weights,
                     int32_t n_steps, Geo* g) {
     memset(g, 0, sizeof(*g));

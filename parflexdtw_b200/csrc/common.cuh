@@ -103,6 +103,11 @@ struct S2Buf {
     int64_t* wp_len;     // [1]
 };
 
+// Records `msg` as the calling thread's last error and returns `status`.
+int report_status(int status, const char* msg);
+// Parses a step list into Geo::S / kind / w (PFX_OK or PFX_ERR_STEPS).
+int parse_step_kinds(const int64_t* steps, const double* weights, int32_t n, Geo* g);
+
 // Count of kernels this library has launched (process-wide).
 void count_launches(int n);
 
