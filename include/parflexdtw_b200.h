@@ -99,13 +99,27 @@ int pfx_plan_buffer(pfx_plan *plan, int which, void **ptr, int64_t *nbytes);
  * Stages.  All asynchronous on `stream`.
  * ------------------------------------------------------------------------- */
 
+/* Loads the cost matrix into the plan's tile-skewed copy (the layout the
+ * stage-1 kernel reads: per tile, 64-row strips with each row shifted by its
+ * index, so one wavefront step of a warp reads 512 contiguous bytes; about
+ * 1.03x the size of C).  From a row-major C (leading dimension ldc), or
+ * directly from features: F1 d x N and F2 d x M row-major by feature (the
+ * (d, frames) layout), 1 <= d <= 16, giving 1 - L2norm(F1)^T L2norm(F2) with
+ * the same fixed-order FP64 sum as pfx_cost_matrix_f64
+ * (cost_matrix_from_features_gpu, gpu_flexdtw.py:95-109; Parflex.py:1470). */
+int pfx_plan_load_cost(pfx_plan *plan, const double *C, int64_t ldc, void *stream);
+int pfx_plan_load_features(pfx_plan *plan, const double *F1, const double *F2,
+                           int32_t d, void *stream);
+
 /* Stage 1: FlexDTW on every tile (run_flexdtw_on_tiles, Parflex.py:376-469;
  * GPU variant flexdtw_chunk_from_global_C, gpu_flexdtw.py:288-402).  Writes D
- * and S on tile edges and the packed backpointers. */
+ * and S on tile edges and the packed backpointers.  C non-null: loads it
+ * first (pfx_plan_load_cost); C null: uses the loaded cost. */
 int pfx_stage1(pfx_plan *plan, const double *C, int64_t ldc, void *stream);
 
 /* Stage 2a: edge tensors, valid mask and cross-tile propagation
- * (propagate_tile_edge_costs, Parflex.py:862-912 / Parflex_gpu.py:247-339). */
+ * (propagate_tile_edge_costs, Parflex.py:862-912 / Parflex_gpu.py:247-339).
+ * Overlap costs are read from C if non-null, else from the loaded cost. */
 int pfx_stage2_propagate(pfx_plan *plan, const double *C, int64_t ldc, void *stream);
 
 /* Copies D_arr / L_arr into the D_PROP / L_PROP buffers (test hook: the
@@ -124,7 +138,8 @@ int pfx_stage2_scan(pfx_plan *plan, double beta, void *stream);
 int pfx_stage2_stitch(pfx_plan *plan, int from_best, int64_t i, int64_t j,
                       int64_t edge, int64_t idx, void *stream);
 
-/* Stage 1 + 2a + 2b + 2c in one call on a device-resident C. */
+/* Stage 1 + 2a + 2b + 2c in one call on a device-resident C (or, with C
+ * null, on the loaded cost). */
 int pfx_parflex_device(pfx_plan *plan, const double *C, int64_t ldc,
                        double beta, void *stream);
 

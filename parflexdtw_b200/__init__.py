@@ -11,7 +11,9 @@ from .parflex import (  # noqa: F401
     ChunksDict,
     Plan,
     Stage2Result,
+    TiledResult,
     buffer_global,
+    clear_plan_cache,
     cost_matrix_from_features_gpu,
     cost_matrix_to_gpu,
     cost_matrix_to_gpu_f32,

@@ -43,6 +43,8 @@ SIGNATURES = [
     ("pfx_plan_destroy", None, [_vp]),
     ("pfx_plan_info", ct.c_int, [_vp, _i64p]),
     ("pfx_plan_buffer", ct.c_int, [_vp, ct.c_int, ct.POINTER(_vp), _i64p]),
+    ("pfx_plan_load_cost", ct.c_int, [_vp, _vp, _i64, _vp]),
+    ("pfx_plan_load_features", ct.c_int, [_vp, _vp, _vp, _i32, _vp]),
     ("pfx_stage1", ct.c_int, [_vp, _vp, _i64, _vp]),
     ("pfx_stage2_propagate", ct.c_int, [_vp, _vp, _i64, _vp]),
     ("pfx_snapshot_prop", ct.c_int, [_vp, _vp]),

@@ -50,6 +50,12 @@ struct pfx_plan {
     int64_t n4;  // n1*n2*2*L
     void* blocks[32];
     int nblocks;
+    // tile-skewed cost (allocated on first load) and normalised features
+    double* Csk;
+    int64_t skew_stride;  // doubles per tile slab
+    double* feat;         // d*(N+M) doubles
+    int feat_d;
+    int cost_loaded;
 };
 
 static const char* kStatus[] = {"ok",
@@ -109,7 +115,7 @@ static int make_geo(int64_t N, int64_t M, int32_t L, const int64_t* steps, const
     g->hop = L - 1;
     g->n1 = (int32_t)ceil_div64(N - 1, g->hop);
     g->n2 = (int32_t)ceil_div64(M - 1, g->hop);
-    g->b_words = tile_b_words(L);
+    g->b_words = tile_b_words2(L);
     return PFX_OK;
 }
 
@@ -120,11 +126,11 @@ static int num_sms_cur() {
     return sms;
 }
 
-static int check_smem(int32_t L, int nw) {
+static int check_smem(int32_t L, int nw, bool v3 = false) {
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const size_t need = stage1_smem_bytes_host(L, nw);
+    const size_t need = v3 ? stage1_v3_smem_bytes(L, nw, optin) : stage1_smem_bytes_host(L, nw);
     if (need > (size_t)optin)
         return fail(PFX_ERR_TOO_LARGE, "L=%d needs %zu B of shared memory per tile CTA (limit %d)",
                     L, need, optin);
@@ -167,7 +173,8 @@ extern "C" int pfx_plan_create(int64_t N, int64_t M, int32_t L, const int64_t* s
     if (st) { free(p); return st; }
     cudaGetDevice(&p->device);
     p->nw = stage1_pick_warps(p->g, num_sms_cur());
-    if ((st = check_smem(L, p->nw))) { free(p); return st; }
+    if ((st = check_smem(L, p->nw, true))) { free(p); return st; }
+    p->skew_stride = skew_slab_elems(L);
     const Geo& g = p->g;
     const int64_t nt = (int64_t)g.n1 * g.n2;
     p->n4 = nt * 2 * g.L;
@@ -213,10 +220,12 @@ extern "C" int pfx_plan_create(int64_t N, int64_t M, int32_t L, const int64_t* s
     PA(&p->s2.seg_len, 101);
     PA(&p->s2.wp, 101 * p->s2.seg_cap * 2);
     PA(&p->s2.wp_len, 1);
+    PA(&p->s1.status, 1);
 #undef PA
     CK(cudaMemset(p->s2.best_end, 0, 7 * sizeof(int64_t)));
     CK(cudaMemset(p->s2.chain_len, 0, sizeof(int32_t)));
     CK(cudaMemset(p->s2.wp_len, 0, sizeof(int64_t)));
+    CK(cudaMemset(p->s1.status, 0, sizeof(int32_t)));
     *out = p;
     return PFX_OK;
 }
@@ -264,26 +273,66 @@ static int check_ldc(const pfx_plan* p, const double* C, int64_t ldc) {
     return PFX_OK;
 }
 
-extern "C" int pfx_stage1(pfx_plan* p, const double* C, int64_t ldc, void* stream) {
+static int ensure_cost_buffer(pfx_plan* p) {
+    if (p->Csk) return PFX_OK;
+    return plan_alloc(p, &p->Csk, (size_t)p->g.n1 * p->g.n2 * p->skew_stride);
+}
+
+extern "C" int pfx_plan_load_cost(pfx_plan* p, const double* C, int64_t ldc, void* stream) {
     if (!p) return fail(PFX_ERR_ARG, "null plan");
     int st = check_ldc(p, C, ldc);
     if (st) return st;
+    if ((st = ensure_cost_buffer(p))) return st;
+    CK(launch_relayout_skew(C, ldc, p->g, p->Csk, p->skew_stride, (cudaStream_t)stream));
+    p->cost_loaded = 1;
+    return PFX_OK;
+}
+
+extern "C" int pfx_plan_load_features(pfx_plan* p, const double* F1, const double* F2, int32_t d,
+                                      void* stream) {
+    if (!p || !F1 || !F2) return fail(PFX_ERR_ARG, "null argument");
+    if (d < 1 || d > 16)
+        return fail(PFX_ERR_ARG, "feature dimension %d: the fused cost layout takes 1..16", d);
+    int st;
+    if ((st = ensure_cost_buffer(p))) return st;
+    if (p->feat && p->feat_d < d) return fail(PFX_ERR_ARG, "feature dimension grew");
+    if (!p->feat) {
+        if ((st = plan_alloc(p, &p->feat, (size_t)d * (p->g.N + p->g.M)))) return st;
+        p->feat_d = d;
+    }
     cudaStream_t s = (cudaStream_t)stream;
-    Geo g = p->g;
-    g.ldc = ldc;
+    double* An = p->feat;
+    double* Bn = p->feat + (int64_t)d * p->g.N;
+    CK(launch_l2norm(F1, d, p->g.N, An, s));
+    CK(launch_l2norm(F2, d, p->g.M, Bn, s));
+    CK(launch_cost_skew(An, Bn, d, p->g, p->Csk, p->skew_stride, s));
+    p->cost_loaded = 1;
+    return PFX_OK;
+}
+
+extern "C" int pfx_stage1(pfx_plan* p, const double* C, int64_t ldc, void* stream) {
+    if (!p) return fail(PFX_ERR_ARG, "null plan");
+    int st;
+    if (C && (st = pfx_plan_load_cost(p, C, ldc, stream))) return st;
+    if (!p->cost_loaded) return fail(PFX_ERR_ARG, "no cost matrix loaded into the plan");
+    cudaStream_t s = (cudaStream_t)stream;
     CK(launch_fill(p->s1.edge_D, p->n4, HUGE_VAL, s));
     CK(cudaMemsetAsync(p->s1.edge_P, 0, (size_t)p->n4 * 4, s));
-    CK(launch_stage1(C, g, p->s1, 0, g.n1 * g.n2, p->nw, false, s));
+    CK(launch_stage1_v3(p->Csk, p->skew_stride, p->g, p->s1, p->nw, s));
     return PFX_OK;
 }
 
 extern "C" int pfx_stage2_propagate(pfx_plan* p, const double* C, int64_t ldc, void* stream) {
     if (!p) return fail(PFX_ERR_ARG, "null plan");
-    int st = check_ldc(p, C, ldc);
-    if (st) return st;
     Geo g = p->g;
-    g.ldc = ldc;
-    CK(launch_stage2(C, g, p->s2, 0, (cudaStream_t)stream));
+    if (C) {
+        int st = check_ldc(p, C, ldc);
+        if (st) return st;
+        g.ldc = ldc;
+    } else if (!p->cost_loaded) {
+        return fail(PFX_ERR_ARG, "no cost matrix loaded into the plan");
+    }
+    CK(launch_stage2(C, p->Csk, p->skew_stride, g, p->s2, (cudaStream_t)stream));
     return PFX_OK;
 }
 
@@ -332,10 +381,17 @@ extern "C" int pfx_result(pfx_plan* p, void* stream, double* best_cost, int64_t*
     double b = 0;
     int64_t e[7];
     int64_t n = 0;
+    int32_t kst = 0;
+    CK(cudaMemcpyAsync(&kst, p->s1.status, 4, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(&b, p->s2.best, 8, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(e, p->s2.best_end, 56, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(&n, p->s2.wp_len, 8, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    if (kst) {
+        cudaMemsetAsync(p->s1.status, 0, 4, s);
+        return fail(PFX_ERR_CUDA, "stage-1 wavefront wait ran out (status %d); results invalid",
+                    kst);
+    }
     if (best_cost) *best_cost = b;
     if (best_end7) memcpy(best_end7, e, sizeof(e));
     if (wp_len) *wp_len = n;

@@ -66,6 +66,50 @@ __device__ __forceinline__ int bp_code(const uint32_t* __restrict__ slab, int32_
     return (int)((word >> ((tau & 15) * 2)) & 3u);
 }
 
+// ---------------------------------------------------------------------------
+// Stage-1 schedule with two rows per lane (the plan path).  A strip is 64
+// tile rows; lane i of a strip owns rows 64k+2i ("A") and 64k+2i+1 ("B") and
+// at local step tau computes (64k+2i, tau-2i) and (64k+2i+1, tau-2i-1), i.e.
+// row rho = r mod 64 at column tau - rho.  Backpointer words are laid out
+// [strip][period][lane][A|B] (two consecutive words per lane per period).
+constexpr int kStripRows = 64;
+struct Sched2 {
+    int32_t nS, span, nP, lag;
+};
+__host__ __device__ inline Sched2 make_sched2(int32_t R, int32_t W, int32_t nwarps) {
+    Sched2 s;
+    s.nS = ceil_div32(R, kStripRows);
+    s.span = ceil_div32(W + kStripRows - 1, kBlk) * kBlk;
+    s.nP = s.span / kBlk;
+    int32_t lag = ceil_div32(ceil_div32(s.span, nwarps), kBlk) * kBlk;
+    s.lag = lag < 80 ? 80 : lag;
+    return s;
+}
+__host__ __device__ inline int64_t tile_b_words2(int32_t L) {
+    const Sched2 s = make_sched2(L, L, 1);
+    return (int64_t)s.nS * s.nP * 2 * 32;
+}
+// Tile-skewed cost layout: per tile, element (strip k, step tau, lane, half)
+// = C[r0 + 64k + 2*lane + half][c0 + tau - 2*lane - half] (0 outside the
+// tile), stored at ((k*span + tau)*32 + lane)*2 + half, so one warp-step of
+// the stage-1 kernel reads 512 contiguous bytes.  Slab stride per tile is the
+// size of an L x L tile.
+__host__ __device__ inline int64_t skew_slab_elems(int32_t L) {
+    const Sched2 s = make_sched2(L, L, 1);
+    return (int64_t)s.nS * s.span * 2 * 32;
+}
+__host__ __device__ inline int64_t skew_index(int32_t W, int32_t r, int32_t c) {
+    const int32_t span = ceil_div32(W + kStripRows - 1, kBlk) * kBlk;
+    const int32_t k = r >> 6, rho = r & 63, tau = c + rho;
+    return (((int64_t)k * span + tau) * 32 + (rho >> 1)) * 2 + (rho & 1);
+}
+// Backpointer code of cell (r, c) of a tile with W columns (two-row layout).
+__device__ __forceinline__ int64_t bp_word_index2(int32_t W, int32_t r, int32_t tau) {
+    const int32_t nP = ceil_div32(W + kStripRows - 1, kBlk);
+    const int32_t k = r >> 6, rho = r & 63;
+    return (((int64_t)k * nP + (tau >> 4)) * 32 + (rho >> 1)) * 2 + (rho & 1);
+}
+
 // Stage-1 outputs.
 struct S1Out {
     double* edge_D;   // [tiles][2][L] D on the top / right edge, +inf past the edge
@@ -74,7 +118,11 @@ struct S1Out {
     double* full_D;   // single-tile full outputs (R x W), or null
     int32_t* full_P;
     int8_t* full_B;
+    int32_t* status;  // set non-zero by a kernel whose bounded wait ran out, or null
 };
+
+// Status word values written by kernels.
+constexpr int32_t kStatusWaitTimeout = 1;
 
 // Stage-2 device state.  Slot arrays are [n1][n2][2][L].
 struct S2Buf {
@@ -111,14 +159,22 @@ int parse_step_kinds(const int64_t* steps, const double* weights, int32_t n, Geo
 // Count of kernels this library has launched (process-wide).
 void count_launches(int n);
 
-// Launchers (stage1_f64.cu, stage2.cu, cost.cu).
+// Launchers (stage1_f64.cu, stage1_v3.cu, layout.cu, stage2.cu, cost.cu).
+cudaError_t launch_stage1_v3(const double* Csk, int64_t skew_stride, const Geo& g, const S1Out& o,
+                             int nw, cudaStream_t st);
+size_t stage1_v3_smem_bytes(int32_t L, int nw, int smem_limit);
+cudaError_t launch_relayout_skew(const double* C, int64_t ldc, const Geo& g, double* Csk,
+                                 int64_t skew_stride, cudaStream_t st);
+cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Geo& g, double* Csk,
+                             int64_t skew_stride, cudaStream_t st);
+cudaError_t launch_l2norm(const double* F, int d, int64_t n, double* out, cudaStream_t st);
 cudaError_t launch_stage1(const double* C, const Geo& g, const S1Out& o, int tile0, int ntiles,
                           int nw, bool full, cudaStream_t st);
 size_t stage1_smem_bytes_host(int32_t L, int nw);
 int stage1_pick_warps(const Geo& g, int num_sms);
 cudaError_t launch_fill(double* p, int64_t n, double v, cudaStream_t st);
-cudaError_t launch_stage2(const double* C, const Geo& g, const S2Buf& b, int64_t buf,
-                          cudaStream_t st);
+cudaError_t launch_stage2(const double* C, const double* Csk, int64_t skew_stride, const Geo& g,
+                          const S2Buf& b, cudaStream_t st);
 cudaError_t launch_sync_scan(const Geo& g, const S2Buf& b, int64_t buf, cudaStream_t st);
 cudaError_t launch_stitch(const Geo& g, const S2Buf& b, cudaStream_t st, int from_best,
                           int64_t si, int64_t sj, int64_t se, int64_t sx);

@@ -66,6 +66,13 @@ __global__ void __launch_bounds__(256) k_cost_f64(const double* __restrict__ A,
     }
 }
 
+cudaError_t launch_l2norm(const double* F, int d, int64_t n, double* out, cudaStream_t st) {
+    if (d < 1 || n < 1) return cudaErrorInvalidValue;
+    k_l2norm_cols<<<(int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096), 256, 0, st>>>(F, d, n, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 // Normalises F1 and F2 into An (d x N) and Bn (d x M) (caller-provided) and
 // writes C (N x M, leading dimension ldc).
 cudaError_t launch_cost_f64(const double* F1, const double* F2, int d, int64_t N, int64_t M,

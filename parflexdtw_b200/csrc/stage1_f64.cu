@@ -30,12 +30,13 @@
 // column), and 2-bit backpointer codes for every cell (code 3 = "no step
 // won", the reference's B = -1).
 #include "common.cuh"
+#include "select.cuh"
 
 #include <math_constants.h>
 
 namespace pfx {
 
-template <int NW, bool FULL>
+template <int NW, bool FULL, bool STD>
 __global__ void __launch_bounds__(NW * 32, 1)
     k_stage1_f64(const double* __restrict__ C, const Geo g, const S1Out out, const int tile0) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -121,42 +122,8 @@ __global__ void __launch_bounds__(NW * 32, 1)
                     if (r == 0 || c == 0) {
                         oD = cval;
                     } else {
-                        double best = CUDART_INF;
-                        int bs = -1, bk = 0, bPP = 0;
-                        double bD = 0.0;
-#pragma unroll
-                        for (int s = 0; s < 3; ++s) {
-                            if (s < g.S) {
-                                const int kd = g.kind[s];
-                                const bool inb = kd == 0 || (kd == 1 ? c >= 2 : r >= 2);
-                                if (inb) {
-                                    const double pD = kd == 0 ? x1D : (kd == 1 ? x2D : x3D);
-                                    const int pP = kd == 0 ? x1P : (kd == 1 ? x2P : x3P);
-                                    const double pc = __dadd_rn(pD, __dmul_rn(cval, g.w[s]));
-                                    const int md = r + c - abs(pP);
-                                    const double q = __ddiv_rn(pc, (double)md);
-                                    if (q < best) {
-                                        best = q;
-                                        bs = s;
-                                        bk = kd;
-                                        bD = pc;
-                                        bPP = pP;
-                                    }
-                                }
-                            }
-                        }
-                        if (bs < 0) {
-                            // reference: D[-1,-1] (still 0) + C * w[-1], P[-1,-1] (0), B = -1
-                            oD = __dadd_rn(0.0, __dmul_rn(cval, w_last));
-                            oP = 0;
-                            code = 3;
-                        } else {
-                            oD = bD;
-                            code = bs;
-                            const int pr = r - (bk == 2 ? 2 : 1);
-                            const int pcn = c - (bk == 1 ? 2 : 1);
-                            oP = pr == 0 ? pcn : (pcn == 0 ? -pr : bPP);
-                        }
+                        select_step<STD, false>(g, w_last, r, c, cval, x1D, x1P, x2D, x2P, x3D, x3P, oD,
+                                         oP, code);
                     }
                     if (lane >= 30) {
                         const int ws = warp * lag + (Tmod >= lane ? Tmod - lane : Tmod - lane + lag);
@@ -206,14 +173,14 @@ inline size_t stage1_smem_bytes(int32_t L, int nw) {
 
 size_t stage1_smem_bytes_host(int32_t L, int nw) { return stage1_smem_bytes(L, nw); }
 
-template <int NW, bool FULL>
+template <int NW, bool FULL, bool STD>
 static cudaError_t launch_stage1_t(const double* C, const Geo& g, const S1Out& o, int tile0,
                                    int ntiles, cudaStream_t st) {
     const size_t smem = stage1_smem_bytes(g.L, NW);
-    cudaError_t e = cudaFuncSetAttribute(k_stage1_f64<NW, FULL>,
+    cudaError_t e = cudaFuncSetAttribute(k_stage1_f64<NW, FULL, STD>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_stage1_f64<NW, FULL><<<ntiles, NW * 32, smem, st>>>(C, g, o, tile0);
+    k_stage1_f64<NW, FULL, STD><<<ntiles, NW * 32, smem, st>>>(C, g, o, tile0);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -229,12 +196,19 @@ int stage1_pick_warps(const Geo& g, int num_sms) {
 cudaError_t launch_stage1(const double* C, const Geo& g, const S1Out& o, int tile0, int ntiles,
                           int nw, bool full, cudaStream_t st) {
     if (ntiles <= 0) return cudaSuccess;
+    const bool std_steps = g.S == 3 && g.kind[0] == 0 && g.kind[1] == 1 && g.kind[2] == 2;
     if (full) {
-        return nw == 16 ? launch_stage1_t<16, true>(C, g, o, tile0, ntiles, st)
-                        : launch_stage1_t<8, true>(C, g, o, tile0, ntiles, st);
+        if (std_steps)
+            return nw == 16 ? launch_stage1_t<16, true, true>(C, g, o, tile0, ntiles, st)
+                            : launch_stage1_t<8, true, true>(C, g, o, tile0, ntiles, st);
+        return nw == 16 ? launch_stage1_t<16, true, false>(C, g, o, tile0, ntiles, st)
+                        : launch_stage1_t<8, true, false>(C, g, o, tile0, ntiles, st);
     }
-    return nw == 16 ? launch_stage1_t<16, false>(C, g, o, tile0, ntiles, st)
-                    : launch_stage1_t<8, false>(C, g, o, tile0, ntiles, st);
+    if (std_steps)
+        return nw == 16 ? launch_stage1_t<16, false, true>(C, g, o, tile0, ntiles, st)
+                        : launch_stage1_t<8, false, true>(C, g, o, tile0, ntiles, st);
+    return nw == 16 ? launch_stage1_t<16, false, false>(C, g, o, tile0, ntiles, st)
+                    : launch_stage1_t<8, false, false>(C, g, o, tile0, ntiles, st);
 }
 
 }  // namespace pfx

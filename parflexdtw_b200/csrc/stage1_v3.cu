@@ -1,0 +1,405 @@
+// Stage 1 (plan path): FlexDTW on every tile, FP64, two rows per lane, cost
+// read from the tile-skewed layout, warps synchronised pairwise.
+//
+// Recurrence and tie-breaking: FlexDTW.py:326-370 (see stage1_f64.cu).
+//
+// Mapping.  A strip is 64 tile rows; lane i owns rows 64k+2i (A) and
+// 64k+2i+1 (B) and at local step tau computes A = (64k+2i, tau-2i) and
+// B = (64k+2i+1, tau-2i-1): row rho = r mod 64 sits at column tau - rho, and
+// r + c = 64k + tau is the same for every cell of a warp-step.  The
+// predecessors of A are lane i-1's B two steps ago ((1,1)), lane i-1's B
+// three steps ago ((1,2), relayed: what this lane received one step earlier)
+// and lane i-1's A three steps ago ((2,1)); those of B are this lane's own A
+// two and three steps ago and again lane i-1's B three steps ago.  Two
+// shuffles of (D, P) per step feed both cells, which are independent of each
+// other.  mdist = (r + c) - |P| is formed in FP64 (exact: both integers).
+//
+// Lane 0 takes rows 64k-2 and 64k-1 (the previous strip's lane 31) from a
+// per-warp shared-memory ring indexed by (strip start + column) mod RB.
+// Strips start `lag` (>= 80) steps apart.  Warps do not use CTA barriers:
+// each publishes the global step it has completed (release store by lane 31,
+// the ring writer) and, before a block, waits (acquire, bounded) until its
+// producer has written everything the block reads and its consumer has read
+// every slot the block overwrites.  A wait that runs out sets the status word
+// and the warp returns, and so, in turn, do the warps that wait on it.
+//
+// Selection.  Every cell first takes a branch-free, division-free comparison
+// of the three candidates (cross products with a 2^-48 relative margin, see
+// qless_exact); cells too close to call, cells with a predecessor on row 0 /
+// column 0 or outside the tile, and non-finite values go -- one uniform
+// branch per warp-step -- to the exact per-lane routine, which falls back to
+// IEEE division.  Only blocks touching a tile boundary ("edge" blocks) pay
+// for the bounds tests and the edge-row stores.  The cost queue runs two
+// steps ahead.
+#include <cuda/atomic>
+
+#include "common.cuh"
+
+#include <math_constants.h>
+
+namespace pfx {
+
+constexpr int kSpinLimit = 1 << 22;
+
+// Exact RN(b/nd) < RN(a/md) (nd, md positive integers), per lane, no warp
+// collectives.  Division only when the cross products cannot decide.
+__device__ __forceinline__ bool qless_exact(double b, double nd, double a, double md) {
+    const double U = __dmul_rn(b, md);
+    const double V = __dmul_rn(a, nd);
+    const double diff = __dadd_rn(V, -U);
+    const double mag = __dadd_rn(fabs(U), fabs(V));
+    const double tau = __dmul_rn(mag, 0x1p-48);
+    if (mag >= 0x1p-950) {
+        if (diff > tau) return true;
+        if (-diff > tau) return false;
+    }
+    return __ddiv_rn(b, nd) < __ddiv_rn(a, md);
+}
+
+// Exact selection of one cell with r, c >= 1 (generic steps, any position).
+template <bool STD, bool ALLIN>
+__device__ __forceinline__ void select_exact(const Geo& g, double w_last, int r, int c, double rc,
+                                          double cval, double x1D, int x1P, double x2D, int x2P,
+                                          double x3D, int x3P, double& oD, int& oP, int& code) {
+    int bs = -1, bk = 0, bP = 0;
+    double bA = 0.0, bM = 1.0;
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+        if (!STD && s >= g.S) continue;
+        const int kd = STD ? s : g.kind[s];
+        const bool inb = ALLIN || kd == 0 || (kd == 1 ? c >= 2 : r >= 2);
+        if (!inb) continue;
+        const double pD = kd == 0 ? x1D : (kd == 1 ? x2D : x3D);
+        const int pP = kd == 0 ? x1P : (kd == 1 ? x2P : x3P);
+        const double a = __dadd_rn(pD, __dmul_rn(cval, g.w[s]));
+        const double md = __dadd_rn(rc, -fabs((double)pP));
+        const bool take = bs < 0 ? a < CUDART_INF : qless_exact(a, md, bA, bM);
+        if (take) {
+            bs = s;
+            bk = kd;
+            bA = a;
+            bM = md;
+            bP = pP;
+        }
+    }
+    if (bs < 0) {
+        // reference: D[-1,-1] (still 0) + C * w[-1], P[-1,-1] (0), B = -1
+        oD = __dadd_rn(0.0, __dmul_rn(cval, w_last));
+        oP = 0;
+        code = 3;
+    } else {
+        oD = bA;
+        code = bs;
+        const int pr = r - (bk == 2 ? 2 : 1);
+        const int pcn = c - (bk == 1 ? 2 : 1);
+        oP = pr == 0 ? pcn : (pcn == 0 ? -pr : bP);
+    }
+}
+
+// Steps (1,1), (1,2), (2,1): branch-free selection of one cell with r, c >= 1.
+// Returns false when a comparison is too close to call or a value is not
+// finite; the caller then recomputes the cell with select_exact.  EDGE adds
+// the in-bounds tests of (1,2) (c >= 2) and (2,1) (r >= 2) and the start
+// encoding of a predecessor on row 0 / column 0 (FlexDTW.py:365-370).
+template <bool EDGE>
+__device__ __forceinline__ bool select_fast_std(const Geo& g, int r, int c, double rc,
+                                                double cval, double x1D, int x1P, double x2D,
+                                                int x2P, double x3D, int x3P, double& oD,
+                                                int& oP, int& code) {
+    const double a0 = __dadd_rn(x1D, __dmul_rn(cval, g.w[0]));
+    const double a1 = __dadd_rn(x2D, __dmul_rn(cval, g.w[1]));
+    const double a2 = __dadd_rn(x3D, __dmul_rn(cval, g.w[2]));
+    const double m0 = __dadd_rn(rc, -fabs((double)x1P));
+    const double m1 = __dadd_rn(rc, -fabs((double)x2P));
+    const double m2 = __dadd_rn(rc, -fabs((double)x3P));
+    const bool in1 = !EDGE || c >= 2, in2 = !EDGE || r >= 2;
+    const double U1 = __dmul_rn(a1, m0), V1 = __dmul_rn(a0, m1);
+    const double d1 = __dadd_rn(V1, -U1);
+    const double g1 = __dadd_rn(fabs(U1), fabs(V1));
+    const double t1 = __dmul_rn(g1, 0x1p-48);
+    const bool win1 = in1 && d1 > t1;
+    const bool ok1 = !in1 || (g1 >= 0x1p-950 && (d1 > t1 || -d1 > t1));
+    const double bA = win1 ? a1 : a0, bM = win1 ? m1 : m0;
+    const double U2 = __dmul_rn(a2, bM), V2 = __dmul_rn(bA, m2);
+    const double d2 = __dadd_rn(V2, -U2);
+    const double g2 = __dadd_rn(fabs(U2), fabs(V2));
+    const double t2 = __dmul_rn(g2, 0x1p-48);
+    const bool win2 = in2 && d2 > t2;
+    const bool ok2 = !in2 || (g2 >= 0x1p-950 && (d2 > t2 || -d2 > t2));
+    oD = win2 ? a2 : bA;
+    const int inh = win2 ? x3P : (win1 ? x2P : x1P);
+    code = win2 ? 2 : (win1 ? 1 : 0);
+    if (EDGE) {
+        const int pr = r - (win2 ? 2 : 1);
+        const int pcn = c - (win1 && !win2 ? 2 : 1);
+        oP = pr == 0 ? pcn : (pcn == 0 ? -pr : inh);
+    } else {
+        oP = inh;
+    }
+    return a0 < CUDART_INF && ok1 && ok2;
+}
+
+struct Wave {
+    double aD1, aD2, aD3, bD1, bD2, xpD;  // own A outputs 1..3 steps ago, own B 1..2 ago,
+    int aP1, aP2, aP3, bP1, bP2, xpP;     // lane i-1's B received one step ago
+    double2 q[2];                          // cost queue, step tau in slot tau & 1
+};
+
+struct Rings {
+    double* AD;  // [NW][RB] row 64k+62 of each warp's strips
+    double* BD;  // row 64k+63
+    int* AP;
+    int* BP;
+};
+
+template <bool EDGE, bool STD>
+__device__ __forceinline__ void run_block(const Geo& g, Wave& st, const Rings& rg,
+                                          const double2* __restrict__ Cs, int span, int tau0,
+                                          int k, int R, int W, int lane, int prev_base,
+                                          int mine_base, int rmask, int Tb, int lag,
+                                          const S1Out& out, int tile, int nP) {
+    const unsigned F = 0xffffffffu;
+    const double w_last = g.S == 1 ? g.w[0] : (g.S == 2 ? g.w[1] : g.w[2]);
+    const int rA = 64 * k + 2 * lane, rB = rA + 1;
+    uint32_t bitsA = 0, bitsB = 0;
+    const double rc0 = (double)(64 * k + tau0);
+#pragma unroll 1
+    for (int tq = 0; tq < kBlk; tq += 2) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int t = tq + u;
+            const int tau = tau0 + t;
+            const double rc = __dadd_rn(rc0, (double)t);
+            const double2 cc = st.q[u & 1];
+            if (tau + 2 < span) st.q[u & 1] = __ldcs(Cs + (int64_t)(tau + 2) * 32);
+            double x1D = __shfl_up_sync(F, st.bD2, 1);
+            int x1P = __shfl_up_sync(F, st.bP2, 1);
+            double x3D = __shfl_up_sync(F, st.aD3, 1);
+            int x3P = __shfl_up_sync(F, st.aP3, 1);
+            {
+                // every lane reads the same slot (a broadcast); lane 0 keeps it
+                const int rs = prev_base + ((Tb + t - lag - 1) & rmask);
+                const double rBD = rg.BD[rs], rAD = rg.AD[rs];
+                const int rBP = rg.BP[rs], rAP = rg.AP[rs];
+                if (lane == 0) {
+                    x1D = rBD;
+                    x1P = rBP;
+                    x3D = rAD;
+                    x3P = rAP;
+                }
+            }
+            const double x2D = st.xpD;
+            const int x2P = st.xpP;
+            const int cA = tau - 2 * lane, cB = cA - 1;
+            double oAD, oBD;
+            int oAP, oBP, codeA, codeB;
+            bool actA = true, actB = true;
+            bool okA, okB;
+            if (STD) {
+                okA = select_fast_std<EDGE>(g, rA, cA, rc, cc.x, x1D, x1P, x2D, x2P, x3D, x3P, oAD,
+                                            oAP, codeA);
+                okB = select_fast_std<EDGE>(g, rB, cB, rc, cc.y, st.aD2, st.aP2, st.aD3, st.aP3,
+                                            x2D, x2P, oBD, oBP, codeB);
+            } else {
+                okA = okB = false;
+            }
+            if (EDGE) {
+                actA = rA < R && cA >= 0 && cA < W;
+                actB = rB < R && cB >= 0 && cB < W;
+                // boundary cells are set below; absent cells are zeroed
+                okA = !actA || rA == 0 || cA == 0 || okA;
+                okB = !actB || cB == 0 || okB;
+            }
+            if (__any_sync(F, !(okA && okB))) {
+                if (!okA) {
+                    if (rA == 0 || cA == 0) {
+                        oAD = cc.x; oAP = 0; codeA = 0;
+                    } else {
+                        select_exact<STD, !EDGE>(g, w_last, rA, cA, rc, cc.x, x1D, x1P, x2D, x2P,
+                                                 x3D, x3P, oAD, oAP, codeA);
+                    }
+                }
+                if (!okB) {
+                    if (cB == 0) {
+                        oBD = cc.y; oBP = 0; codeB = 0;
+                    } else {
+                        select_exact<STD, !EDGE>(g, w_last, rB, cB, rc, cc.y, st.aD2, st.aP2,
+                                                 st.aD3, st.aP3, x2D, x2P, oBD, oBP, codeB);
+                    }
+                }
+            }
+            if (EDGE) {
+                double* eD = out.edge_D + (int64_t)tile * 2 * g.L;
+                int32_t* eP = out.edge_P + (int64_t)tile * 2 * g.L;
+                if (actA && (rA == 0 || cA == 0)) { oAD = cc.x; oAP = 0; codeA = 0; }
+                if (actB && cB == 0) { oBD = cc.y; oBP = 0; codeB = 0; }
+                if (!actA) { oAD = 0.0; oAP = 0; codeA = 0; }
+                if (!actB) { oBD = 0.0; oBP = 0; codeB = 0; }
+                if (actA && rA == R - 1) { eD[cA] = oAD; eP[cA] = oAP; }
+                if (actB && rB == R - 1) { eD[cB] = oBD; eP[cB] = oBP; }
+                if (actA && cA == W - 1) { eD[g.L + rA] = oAD; eP[g.L + rA] = oAP; }
+                if (actB && cB == W - 1) { eD[g.L + rB] = oBD; eP[g.L + rB] = oBP; }
+            }
+            if (lane == 31) {
+                if (actA) {
+                    const int ws = mine_base + ((Tb + t - 62) & rmask);
+                    rg.AD[ws] = oAD;
+                    rg.AP[ws] = oAP;
+                }
+                if (actB) {
+                    const int ws = mine_base + ((Tb + t - 63) & rmask);
+                    rg.BD[ws] = oBD;
+                    rg.BP[ws] = oBP;
+                }
+            }
+            bitsA |= (uint32_t)codeA << (2 * t);
+            bitsB |= (uint32_t)codeB << (2 * t);
+            st.aD3 = st.aD2; st.aP3 = st.aP2;
+            st.aD2 = st.aD1; st.aP2 = st.aP1;
+            st.aD1 = oAD;    st.aP1 = oAP;
+            st.bD2 = st.bD1; st.bP2 = st.bP1;
+            st.bD1 = oBD;    st.bP1 = oBP;
+            st.xpD = x1D;    st.xpP = x1P;
+        }
+    }
+    if (rA < R) {
+        uint2* Bt = reinterpret_cast<uint2*>(out.Bw + (int64_t)tile * g.b_words);
+        Bt[((int64_t)k * nP + (tau0 >> 4)) * 32 + lane] = make_uint2(bitsA, bitsB);
+    }
+}
+
+__device__ __forceinline__ bool wait_progress(int* p, int target) {
+    cuda::atomic_ref<int, cuda::thread_scope_block> a(*p);
+    for (int it = 0; it < kSpinLimit; ++it) {
+        if (a.load(cuda::memory_order_acquire) >= target) return true;
+        __nanosleep(32);
+    }
+    return false;
+}
+
+// Ring length: the largest power of two whose rings fit the shared-memory
+// limit, capped at the first power of two >= lag + 64 (enough slack that the
+// pairwise waits rarely block); at least lag - 29 (one block of slack).
+__host__ __device__ inline int ring_len(int lag, int nw, int smem_limit) {
+    int cap = 16;
+    while (cap * 2 <= lag + 64) cap *= 2;
+    if (cap < lag + 64) cap *= 2;
+    int fit = 16;
+    const int per = nw * (2 * (int)sizeof(double) + 2 * (int)sizeof(int));
+    while ((fit * 2) * per + nw * (int)sizeof(int) <= smem_limit) fit *= 2;
+    const int rb = cap < fit ? cap : fit;
+    return rb >= lag - 29 ? rb : 0;
+}
+
+template <int NW, bool STD>
+__global__ void __launch_bounds__(NW * 32, 1)
+    k_stage1_v3(const double* __restrict__ Csk, const int64_t skew_stride, const Geo g,
+                const S1Out out, const int RBmax) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tile = (int)blockIdx.x;
+    const int ti = tile / g.n2, tj = tile % g.n2;
+    int64_t r0, c0;
+    int32_t R, W;
+    tile_rect(g, ti, tj, &r0, &c0, &R, &W);
+    const Sched2 sc = make_sched2(R, W, NW);
+    const int lag = sc.lag;
+    const int RB = RBmax;  // >= lag - 29 for every tile (checked on the host for L x L)
+    Rings rg;
+    rg.AD = reinterpret_cast<double*>(smem_raw);
+    rg.BD = rg.AD + NW * RB;
+    rg.AP = reinterpret_cast<int*>(rg.BD + NW * RB);
+    rg.BP = rg.AP + NW * RB;
+    int* prog = rg.BP + NW * RB;
+    if (threadIdx.x < NW) prog[threadIdx.x] = 0;
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int prevw = (warp + NW - 1) % NW, nextw = (warp + 1) % NW;
+    const int Ttot = (sc.nS - 1) * lag + sc.span;
+    const double2* Ct = reinterpret_cast<const double2*>(Csk + (int64_t)tile * skew_stride);
+    cuda::atomic_ref<int, cuda::thread_scope_block> my_prog(prog[warp]);
+
+    Wave st;
+    st.aD1 = st.aD2 = st.aD3 = st.bD1 = st.bD2 = st.xpD = 0.0;
+    st.aP1 = st.aP2 = st.aP3 = st.bP1 = st.bP2 = st.xpP = 0;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) st.q[q] = make_double2(0.0, 0.0);
+
+    for (int Tb = 0; Tb < Ttot; Tb += kBlk) {
+        int k = -1;
+        if (Tb >= warp * lag) {
+            const int j = (Tb - warp * lag) / (NW * lag);
+            const int kk = warp + j * NW;
+            if (kk < sc.nS && Tb < kk * lag + sc.span) k = kk;
+        }
+        if (k >= 0) {
+            int failed = 0;
+            if (lane == 0) {
+                // producer (strip k-1) has written every ring slot this block reads
+                if (k >= 1 && !wait_progress(prog + prevw, Tb - lag + 78)) failed = 1;
+                // consumer (strip k+1) has read every slot this block overwrites
+                if (!failed && k + 1 < sc.nS && !wait_progress(prog + nextw, Tb + lag - RB - 45))
+                    failed = 1;
+                if (failed && out.status) atomicExch(out.status, kStatusWaitTimeout);
+            }
+            if (__shfl_sync(0xffffffffu, failed, 0)) return;
+            const int tau0 = Tb - k * lag;
+            const double2* Cs = Ct + (int64_t)k * sc.span * 32 + lane;
+            if (tau0 == 0) {
+#pragma unroll
+                for (int q = 0; q < 2; ++q) st.q[q] = __ldcs(Cs + q * 32);
+            }
+            const bool interior = k >= 1 && k <= sc.nS - 2 && tau0 >= 80 && tau0 + 17 <= W;
+            if (interior)
+                run_block<false, STD>(g, st, rg, Cs, sc.span, tau0, k, R, W, lane, prevw * RB,
+                                      warp * RB, RB - 1, Tb, lag, out, tile, sc.nP);
+            else
+                run_block<true, STD>(g, st, rg, Cs, sc.span, tau0, k, R, W, lane, prevw * RB,
+                                     warp * RB, RB - 1, Tb, lag, out, tile, sc.nP);
+        }
+        __syncwarp();
+        if (lane == 31) my_prog.store(Tb + kBlk, cuda::memory_order_release);
+    }
+}
+
+static int smem_optin() {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return v;
+}
+
+size_t stage1_v3_smem_bytes(int32_t L, int nw, int smem_limit) {
+    const Sched2 s = make_sched2(L, L, nw);
+    const int rb = ring_len(s.lag, nw, smem_limit);
+    if (rb == 0) return (size_t)1 << 30;  // does not fit
+    return (size_t)nw * rb * (2 * sizeof(double) + 2 * sizeof(int)) + nw * sizeof(int);
+}
+
+template <int NW, bool STD>
+static cudaError_t launch_v3_t(const double* Csk, int64_t stride, const Geo& g, const S1Out& o,
+                               cudaStream_t st) {
+    const int limit = smem_optin();
+    const Sched2 s = make_sched2(g.L, g.L, NW);
+    const int rb = ring_len(s.lag, NW, limit);
+    if (rb == 0) return cudaErrorInvalidValue;
+    const size_t smem = stage1_v3_smem_bytes(g.L, NW, limit);
+    cudaError_t e = cudaFuncSetAttribute(k_stage1_v3<NW, STD>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_stage1_v3<NW, STD><<<g.n1 * g.n2, NW * 32, smem, st>>>(Csk, stride, g, o, rb);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stage1_v3(const double* Csk, int64_t skew_stride, const Geo& g, const S1Out& o,
+                             int nw, cudaStream_t st) {
+    const bool std_steps = g.S == 3 && g.kind[0] == 0 && g.kind[1] == 1 && g.kind[2] == 2;
+    if (std_steps)
+        return nw == 16 ? launch_v3_t<16, true>(Csk, skew_stride, g, o, st)
+                        : launch_v3_t<8, true>(Csk, skew_stride, g, o, st);
+    return nw == 16 ? launch_v3_t<16, false>(Csk, skew_stride, g, o, st)
+                    : launch_v3_t<8, false>(Csk, skew_stride, g, o, st);
+}
+
+}  // namespace pfx

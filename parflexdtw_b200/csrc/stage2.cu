@@ -34,7 +34,10 @@ __global__ void k_fill_f64(double* p, int64_t n, double v) {
 }
 
 // Edge tensors + valid mask (Parflex.py:509-564, 347-373, 582-624) -------
-__global__ void k_edges(const double* __restrict__ C, const Geo g, S2Buf b) {
+// C: row-major cost (leading dimension g.ldc), or null to read the tile-skewed
+// copy Csk (per-tile stride `skew_stride`).
+__global__ void k_edges(const double* __restrict__ C, const double* __restrict__ Csk,
+                        int64_t skew_stride, const Geo g, S2Buf b) {
     const int64_t total = (int64_t)g.n1 * g.n2 * 2 * g.L;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
          q += (int64_t)gridDim.x * blockDim.x) {
@@ -51,7 +54,8 @@ __global__ void k_edges(const double* __restrict__ C, const Geo g, S2Buf b) {
         const int32_t s = b.edge_P[q];
         int32_t sr, sc;
         decode_start(s, &sr, &sc);
-        b.edge_Cf[q] = C[(r0 + sr) * g.ldc + c0 + sc];
+        b.edge_Cf[q] = C ? C[(r0 + sr) * g.ldc + c0 + sc]
+                         : Csk[t * skew_stride + skew_index(W, sr, sc)];
         // mandatory slots: whole top edge of the last tile row, whole right
         // edge of the last tile column, and both ends of every edge
         const bool last = e == 0 ? (i == g.n1 - 1) : (j == g.n2 - 1);
@@ -92,7 +96,7 @@ __device__ __forceinline__ bool prev_slot(const Geo& g, int pi, int pj, int64_t 
 // (i, j-1), so a diagonal's tiles are independent.
 __global__ void k_propagate(const Geo g, S2Buf b, int a) {
     const int ilo = a - (g.n2 - 1) > 0 ? a - (g.n2 - 1) : 0;
-    const int i = ilo + (int)blockIdx.x;
+    const int i = ilo + (int)blockIdx.y;
     const int j = a - i;
     if (i >= g.n1 || j < 0) return;
     int64_t r0, c0;
@@ -101,7 +105,7 @@ __global__ void k_propagate(const Geo g, S2Buf b, int a) {
     double* D = b.D_arr;
     double* Lr = b.L_arr;
     // unconditional inheritance of position 0 on the first tile row / column
-    if (threadIdx.x == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (i == 0 && j >= 1) {
             int64_t pr0, pc0;
             int32_t pR, pW;
@@ -116,7 +120,7 @@ __global__ void k_propagate(const Geo g, S2Buf b, int a) {
             Lr[slot(g, i, 0, 1, 0)] = Lr[slot(g, i - 1, 0, 1, pR - 1)];
         }
     }
-    for (int q = threadIdx.x; q < 2 * g.L; q += blockDim.x) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 2 * g.L; q += gridDim.x * blockDim.x) {
         const int e = q / g.L;
         const int pos = q % g.L;
         const int32_t elen = e == 0 ? W : R;
@@ -367,26 +371,64 @@ __global__ void k_stitch_chain(const Geo g, S2Buf b, int64_t start_i, int64_t st
     *b.chain_len = n;
 }
 
-// One chain entry per thread: walk the packed backpointers from the entry's
+// One chain entry per warp: walk the packed backpointers from the entry's
 // end cell to its start cell (_nb_backtrace_within_chunk,
-// Parflex.py:977-1012), writing global points end-first.
+// Parflex.py:977-1012), writing global points end-first.  The walk only
+// moves up and left, so the warp stages a 64-row x 64-column window of
+// backpointer words in registers (lane l holds rows w0+l and w0+32+l, five
+// 16-cell words each), anchored with the current cell at its bottom-right
+// corner, and reads each step's code with one shuffle; it reloads the window
+// (one coalesced round trip) only when the path leaves it, about every 32-63
+// steps, instead of one dependent global load per step.
+__device__ __forceinline__ uint32_t pick5(const uint32_t (&w)[5], int q) {
+    return q == 0 ? w[0] : q == 1 ? w[1] : q == 2 ? w[2] : q == 3 ? w[3] : w[4];
+}
+
 __global__ void k_stitch_walk(const Geo g, S2Buf b) {
     const int n = *b.chain_len;
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (e >= n) return;
     const int32_t* E = b.chain + e * 12;
     const int32_t ti = E[0], tj = E[1];
     int32_t r = E[4], c = E[5];
     const int32_t sr = E[6], sc = E[7], gro = E[8], gco = E[9], R = E[10], W = E[11];
     const uint32_t* slab = b.Bw + ((int64_t)ti * g.n2 + tj) * g.b_words;
+    const int32_t nP = ceil_div32(W + kStripRows - 1, kBlk);
     int32_t* out = b.seg_pts + (int64_t)e * b.seg_cap * 2;
     int64_t k = 0;
     const int64_t max_iters = (int64_t)R + W;
     bool done = false;
+    int32_t w0r = -1, w0c = 0;  // window origin (row, column); -1 = empty
+    uint32_t wa[5], wb[5];      // words of rows w0r+lane and w0r+32+lane
+    int32_t pa = 0, pbw = 0;    // first period held for each of the two rows
     for (int64_t it = 0; it < max_iters; ++it) {
-        out[2 * k] = r + gro; out[2 * k + 1] = c + gco; ++k;
+        if (lane == 0) { out[2 * k] = r + gro; out[2 * k + 1] = c + gco; }
+        ++k;
         if (r == sr && c == sc) { done = true; break; }
-        const int code = bp_code(slab, W, r, c);
+        if (w0r < 0 || r < w0r || c < w0c) {
+            w0r = r - 63 > 0 ? r - 63 : 0;
+            w0c = c - 63 > 0 ? c - 63 : 0;
+            const int32_t ra = w0r + lane, rb = w0r + 32 + lane;
+            pa = (w0c + (ra & 63)) >> 4;
+            pbw = (w0c + (rb & 63)) >> 4;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                wa[q] = (ra < R && pa + q < nP) ? __ldg(slab + bp_word_index2(W, ra, (pa + q) << 4))
+                                                : 0u;
+                wb[q] = (rb < R && pbw + q < nP) ? __ldg(slab + bp_word_index2(W, rb, (pbw + q) << 4))
+                                                 : 0u;
+            }
+        }
+        // lane holding row r, and the word / bit of column c within that row
+        const int32_t dr = r - w0r;
+        const int src = dr & 31;
+        const bool hi = dr >= 32;
+        const int32_t my_row = w0r + (hi ? 32 : 0) + lane;
+        const int32_t tau = c + (my_row & 63);
+        const uint32_t mine = hi ? pick5(wb, (tau >> 4) - pbw) : pick5(wa, (tau >> 4) - pa);
+        const uint32_t word = __shfl_sync(0xffffffffu, mine, src);
+        const int code = (int)((word >> (((c + (r & 63)) & 15) * 2)) & 3u);
         if (code >= g.S) { done = false; break; }
         const int kd = code == 0 ? g.kind[0] : (code == 1 ? g.kind[1] : g.kind[2]);
         const int32_t pr = r - (kd == 2 ? 2 : 1), pc = c - (kd == 1 ? 2 : 1);
@@ -394,9 +436,10 @@ __global__ void k_stitch_walk(const Geo g, S2Buf b) {
         r = pr; c = pc;
     }
     if (!done && (r != sr || c != sc)) {
-        out[2 * k] = sr + gro; out[2 * k + 1] = sc + gco; ++k;
+        if (lane == 0) { out[2 * k] = sr + gro; out[2 * k + 1] = sc + gco; }
+        ++k;
     }
-    b.seg_len[e] = (int32_t)k;
+    if (lane == 0) b.seg_len[e] = (int32_t)k;
 }
 
 // Concatenate the walks with consecutive-duplicate removal and reverse to
@@ -446,8 +489,8 @@ cudaError_t launch_fill(double* p, int64_t n, double v, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_stage2(const double* C, const Geo& g, const S2Buf& b, int64_t buf,
-                          cudaStream_t st) {
+cudaError_t launch_stage2(const double* C, const double* Csk, int64_t skew_stride, const Geo& g,
+                          const S2Buf& b, cudaStream_t st) {
     const int64_t nslots = (int64_t)g.n1 * g.n2 * 2 * g.L;
     cudaError_t e;
     if ((e = cudaMemsetAsync(b.valid, 0, (size_t)nslots, st)) != cudaSuccess) return e;
@@ -456,14 +499,15 @@ cudaError_t launch_stage2(const double* C, const Geo& g, const S2Buf& b, int64_t
     {
         int64_t blocks = (nslots + 255) / 256;
         if (blocks > 8192) blocks = 8192;
-        k_edges<<<(int)blocks, 256, 0, st>>>(C, g, b);
+        k_edges<<<(int)blocks, 256, 0, st>>>(C, Csk, skew_stride, g, b);
         count_launches(1);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     for (int a = 0; a <= g.n1 + g.n2 - 2; ++a) {
         const int ilo = a - (g.n2 - 1) > 0 ? a - (g.n2 - 1) : 0;
         const int ihi = a < g.n1 - 1 ? a : g.n1 - 1;
-        k_propagate<<<ihi - ilo + 1, 256, 0, st>>>(g, b, a);
+        const dim3 grid((unsigned)ceil_div32(2 * g.L, 256), (unsigned)(ihi - ilo + 1));
+        k_propagate<<<grid, 256, 0, st>>>(g, b, a);
         count_launches(1);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
@@ -499,7 +543,7 @@ cudaError_t launch_stitch(const Geo& g, const S2Buf& b, cudaStream_t st, int fro
     k_stitch_chain<<<1, 32, 0, st>>>(g, b, si, sj, se, sx, from_best);
     count_launches(1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_stitch_walk<<<4, 32, 0, st>>>(g, b);
+    k_stitch_walk<<<26, 128, 0, st>>>(g, b);  // one warp per chain entry (<= 101)
     count_launches(1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     k_stitch_concat<<<1, 1024, 0, st>>>(b);

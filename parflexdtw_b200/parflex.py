@@ -97,6 +97,38 @@ def cost_matrix_from_features_gpu(F1, F2) -> torch.Tensor:
     return C
 
 
+def _features_to_device(F):
+    t = F if isinstance(F, torch.Tensor) else torch.from_numpy(
+        np.ascontiguousarray(F, dtype=np.float64))
+    return t.cuda(non_blocking=True).to(torch.float64).contiguous()
+
+
+class _CostSource:
+    """The row-major FP64 cost matrix on the device: given, or computed from
+    device features on first use (the plan itself holds the tile-skewed copy
+    it works on, so the row-major matrix is only built when a caller asks for
+    ``tiled_result['C_dev']`` or a per-tile ``chunks_dict`` record)."""
+
+    def __init__(self, C_dev=None, F1=None, F2=None):
+        self._C, self._F1, self._F2 = C_dev, F1, F2
+
+    def get(self) -> torch.Tensor:
+        if self._C is None:
+            self._C = cost_matrix_from_features_gpu(self._F1, self._F2)
+        return self._C
+
+
+class TiledResult(dict):
+    """``tiled_result`` dict; ``'C_dev'`` materialises on first access."""
+
+    def __getitem__(self, k):
+        v = dict.__getitem__(self, k)
+        return v.get() if isinstance(v, _CostSource) else v
+
+    def get(self, k, default=None):
+        return self[k] if k in self else default
+
+
 # ---------------------------------------------------------------------------
 # per-tile helpers (FlexDTW.py:104-186 on a materialised tile)
 # ---------------------------------------------------------------------------
@@ -180,7 +212,8 @@ class _Chunk(Mapping):
              "shape", "starts_bot_edge", "starts_left_edge")
 
     def __init__(self, owner, i, j):
-        self._o = owner
+        import weakref
+        self._o = weakref.proxy(owner)  # no reference cycle: the plan lease ends with owner
         self._i, self._j = i, j
         g = owner.plan
         s1, s2 = i * g.hop, j * g.hop
@@ -227,12 +260,16 @@ class _Chunk(Mapping):
 class ChunksDict(Mapping):
     """``chunks_dict`` keyed by ``(i, j)`` over a device stage-1 result."""
 
-    def __init__(self, plan: Plan, C_dev: torch.Tensor):
+    def __init__(self, plan: Plan, cost):
         self.plan = plan
-        self.C_dev = C_dev
+        self._cost = cost if isinstance(cost, _CostSource) else _CostSource(C_dev=cost)
         self._edgeP = None
         self._chunks = {(i, j): _Chunk(self, i, j)
                         for i in range(plan.n1) for j in range(plan.n2)}
+
+    @property
+    def C_dev(self) -> torch.Tensor:
+        return self._cost.get()
 
     def __getitem__(self, k):
         return self._chunks[k]
@@ -321,24 +358,38 @@ class _Phases:
 # ---------------------------------------------------------------------------
 # public API
 # ---------------------------------------------------------------------------
-def _plan_cache_key(N, M, Lb, st, w):
-    return (torch.cuda.current_device(), N, M, Lb, st.tobytes(), w.tobytes())
+_PLAN_POOL: dict = {}
+_POOL_PER_KEY = 2
 
 
-_PLANS: dict = {}
-_PLAN_CACHE_MAX = 4
+class _Lease:
+    """Marks a pooled plan busy for as long as this object is alive."""
 
 
-def _cached_plan(N, M, Lb, steps, weights) -> Plan:
+def _lease_plan(N, M, Lb, steps, weights, owner) -> Plan:
+    """A plan for this geometry that no live owner is using, from the pool
+    (device workspace is allocated once per shape, not per call)."""
+    import weakref
     st, w = normalize_steps(steps, weights)
-    key = _plan_cache_key(N, M, Lb, st, w)
-    p = _PLANS.get(key)
-    if p is None:
-        while len(_PLANS) >= _PLAN_CACHE_MAX:
-            _PLANS.pop(next(iter(_PLANS))).close()
-        p = Plan(N, M, Lb, st, w)
-        _PLANS[key] = p
+    key = (torch.cuda.current_device(), N, M, Lb, st.tobytes(), w.tobytes())
+    pool = _PLAN_POOL.setdefault(key, [])
+    for p in pool:
+        if getattr(p, "_lease", None) is None or p._lease() is None:
+            p._lease = weakref.ref(owner)
+            return p
+    p = Plan(N, M, Lb, st, w)
+    p._lease = weakref.ref(owner)
+    if len(pool) < _POOL_PER_KEY:
+        pool.append(p)
     return p
+
+
+def clear_plan_cache():
+    """Release every pooled plan's device memory."""
+    for pool in _PLAN_POOL.values():
+        for p in pool:
+            p.close()
+    _PLAN_POOL.clear()
 
 
 def _buffer_global(L1, L2, beta):
@@ -362,7 +413,8 @@ def parflex(C, steps, weights, beta, L=None, profile_dir="Profiling_results",
     ph = _Phases(profile_dir is not None)
     ph.mark("gpu_host_to_device_C")
     C_dev = cost_matrix_to_gpu(C)
-    plan = _cached_plan(L1, L2, int(L), steps, weights)
+    lease = _Lease()
+    plan = _lease_plan(L1, L2, int(L), steps, weights, lease)
     ph.mark("stage1_chunk_flexdtw_all_tiles")
     plan.stage1(C_dev)
     ph.mark("propagate_tile_edge_costs_total")
@@ -404,14 +456,21 @@ def run_flexdtw_on_tiles(C, L, steps=None, weights=None, buffer=1,
         if C_dev is not None and tuple(C.shape) != tuple(C_dev.shape):
             raise ValueError("C_dev shape must match C")
     Cd = cost_matrix_to_gpu(C_dev if C_dev is not None else C)
-    plan = Plan(L1, L2, int(L), steps, weights)
+    return _stage1(L1, L2, int(L), steps, weights, profile_dir,
+                   lambda plan: plan.stage1(Cd), _CostSource(C_dev=Cd))
+
+
+def _stage1(L1, L2, Lb, steps, weights, profile_dir, load_and_run, cost):
+    holder = _Lease()
+    plan = _lease_plan(L1, L2, Lb, steps, weights, holder)
     ph = _Phases(profile_dir is not None)
     ph.mark("stage1_chunk_flexdtw_all_tiles")
-    plan.stage1(Cd)
+    load_and_run(plan)
     ph.mark("end")
     ph.finish(profile_dir, "stage1_runtime_breakdown.csv")
-    chunks = ChunksDict(plan, Cd)
-    return chunks, L, plan.n1, plan.n2
+    chunks = ChunksDict(plan, cost)
+    chunks._lease_holder = holder  # the plan stays leased while chunks_dict lives
+    return chunks, Lb, plan.n1, plan.n2
 
 
 def tiled_stage1_from_features(F1, F2, steps=None, weights=None, beta=0.1, L=None,
@@ -422,16 +481,23 @@ def tiled_stage1_from_features(F1, F2, steps=None, weights=None, beta=0.1, L=Non
     _require_gpu(use_gpu)
     if L is None:
         L = DEFAULT_CHUNK_LENGTH
-    C_dev = cost_matrix_from_features_gpu(F1, F2)
+    f1 = _features_to_device(F1)
+    f2 = _features_to_device(F2)
+    if f1.dim() != 2 or f2.dim() != 2 or f1.shape[0] != f2.shape[0]:
+        raise ValueError("features must be (d, frames) with the same d")
     steps = steps if steps is not None else _STD_STEPS
     weights = weights if weights is not None else np.array([1.25, 3.0, 3.0])
     steps_arr = np.array(steps).reshape((-1, 2))
     stage1_params = {"steps": steps_arr, "weights": np.array(weights), "buffer": 1.0}
-    chunks, L_out, n1, n2 = run_flexdtw_on_tiles(None, L, steps, weights, buffer=1,
-                                                 profile_dir=None, use_gpu=True,
-                                                 C_dev=C_dev)
-    N, M = C_dev.shape
-    tiled_result = {
+    N, M = int(f1.shape[1]), int(f2.shape[1])
+    cost = _CostSource(F1=f1, F2=f2)
+
+    def load_and_run(plan):
+        plan.load_features(f1, f2)
+        plan.stage1()
+
+    chunks, L_out, n1, n2 = _stage1(N, M, int(L), steps, weights, None, load_and_run, cost)
+    tiled_result = TiledResult({
         "C_shape": (int(N), int(M)),
         "L_block": L_out,
         "hop": L_out - 1,
@@ -441,8 +507,8 @@ def tiled_stage1_from_features(F1, F2, steps=None, weights=None, beta=0.1, L=Non
         "C": None,
         "stage1_params": stage1_params,
         "chunks_dict": chunks,
-        "C_dev": C_dev,
-    }
+        "C_dev": cost,
+    })
     return None, tiled_result
 
 
@@ -541,9 +607,7 @@ def run_stage2_from_tiled(tiled_result, C=None, beta=0.1, show_fig=False, top_k=
     plan = chunks.plan
     if C is None:
         L1, L2 = tiled_result["C_shape"]
-        C_dev = tiled_result.get("C_dev")
-        if C_dev is None:
-            C_dev = chunks.C_dev
+        C_dev = None  # overlap costs come from the plan's own copy of C
     else:
         L1, L2 = C.shape
         C_dev = cost_matrix_to_gpu(C)
@@ -577,4 +641,5 @@ __all__ = [
     "run_stage2_from_tiled", "run_flexdtw_on_tiles", "flexdtw_chunk_from_global_C",
     "cost_matrix_from_features_gpu", "cost_matrix_to_gpu", "cost_matrix_to_gpu_f32",
     "is_gpu_available", "buffer_global", "ChunksDict", "Stage2Result", "Plan",
+    "TiledResult", "clear_plan_cache",
 ]

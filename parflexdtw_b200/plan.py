@@ -105,17 +105,38 @@ class Plan:
     def host(self, name) -> np.ndarray:
         return self.view(name).cpu().numpy()
 
-    # -- stages ----------------------------------------------------------
-    def stage1(self, C_dev: torch.Tensor, stream=None):
-        lib = L.load()
-        L.check(lib.pfx_stage1(self._h, ct.c_void_p(C_dev.data_ptr()), C_dev.stride(0),
-                               stream or current_stream_ptr()))
+    # -- cost loading ----------------------------------------------------
+    def load_cost(self, C_dev: torch.Tensor, stream=None):
+        """Copy a row-major FP64 cost matrix into the plan's tile-skewed layout."""
+        L.check(L.load().pfx_plan_load_cost(self._h, ct.c_void_p(C_dev.data_ptr()),
+                                            C_dev.stride(0), stream or current_stream_ptr()))
 
-    def propagate(self, C_dev: torch.Tensor, stream=None, snapshot=False):
+    def load_features(self, F1_dev: torch.Tensor, F2_dev: torch.Tensor, stream=None):
+        """Build the cost 1 - L2norm(F1)^T L2norm(F2) straight into the plan's
+        tile-skewed layout (F1: d x N, F2: d x M, FP64, contiguous)."""
+        if F1_dev.shape[0] != F2_dev.shape[0]:
+            raise ValueError("features must share the feature dimension")
+        L.check(L.load().pfx_plan_load_features(
+            self._h, ct.c_void_p(F1_dev.data_ptr()), ct.c_void_p(F2_dev.data_ptr()),
+            int(F1_dev.shape[0]), stream or current_stream_ptr()))
+
+    # -- stages ----------------------------------------------------------
+    @staticmethod
+    def _cptr(C_dev):
+        if C_dev is None:
+            return ct.c_void_p(0), 0
+        return ct.c_void_p(C_dev.data_ptr()), C_dev.stride(0)
+
+    def stage1(self, C_dev: torch.Tensor = None, stream=None):
+        """Stage 1; with ``C_dev`` it is loaded first, else the loaded cost is used."""
+        p, ld = self._cptr(C_dev)
+        L.check(L.load().pfx_stage1(self._h, p, ld, stream or current_stream_ptr()))
+
+    def propagate(self, C_dev: torch.Tensor = None, stream=None, snapshot=False):
         lib = L.load()
         s = stream or current_stream_ptr()
-        L.check(lib.pfx_stage2_propagate(self._h, ct.c_void_p(C_dev.data_ptr()),
-                                         C_dev.stride(0), s))
+        p, ld = self._cptr(C_dev)
+        L.check(lib.pfx_stage2_propagate(self._h, p, ld, s))
         if snapshot:
             L.check(lib.pfx_snapshot_prop(self._h, s))
 
@@ -132,9 +153,9 @@ class Plan:
             i, j, e, x = (int(v) for v in start)
             L.check(lib.pfx_stage2_stitch(self._h, 0, i, j, e, x, s))
 
-    def run(self, C_dev: torch.Tensor, beta, stream=None):
-        L.check(L.load().pfx_parflex_device(self._h, ct.c_void_p(C_dev.data_ptr()),
-                                            C_dev.stride(0), float(beta),
+    def run(self, C_dev: torch.Tensor = None, beta=0.1, stream=None):
+        p, ld = self._cptr(C_dev)
+        L.check(L.load().pfx_parflex_device(self._h, p, ld, float(beta),
                                             stream or current_stream_ptr()))
 
     def result(self, stream=None, raise_no_endpoint=True):

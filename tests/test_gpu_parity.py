@@ -280,3 +280,63 @@ def test_config1_full_size_vs_oracle(oracle_mod):
     ref = oracle_mod.parflex_full(C, spec.steps, spec.weights, spec.beta, spec.L)
     assert best == ref["best_cost"]
     assert same(wp, ref["wp"])
+
+
+# ---------------------------------------------------------------------------
+# tile-skewed cost layout: relayout of a row-major C and the fused features
+# path give the same stage-1 products, for every strip / block regime
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("Lb", [2, 3, 5, 17, 63, 64, 65, 127, 129, 300])
+def test_small_tile_lengths_vs_oracle(Lb, oracle_mod):
+    rng = np.random.default_rng(1000 + Lb)
+    F1, F2 = W.warped_pair(rng, 260, 310, pad_frac=0.1)
+    C = W.cost_matrix_det(F1, F2)
+    ref = oracle_mod.parflex_full(C, STD, [2, 3, 3], 0.1, Lb)
+    plan = pf.Plan(C.shape[0], C.shape[1], Lb, STD, [2, 3, 3])
+    Cd = torch.from_numpy(C).cuda()
+    plan.run(Cd, 0.1)
+    best, end, found, n = plan.result()
+    assert same(plan.host("EDGE_D"), ref["edge_Df"])
+    assert same(plan.host("EDGE_P"), ref["edge_S"])
+    assert same(plan.host("D_ARR"), ref["D_arr"])
+    assert best == ref["best_cost"] and end == ref["best_end"]
+    assert same(plan.path(n).T, ref["wp"])
+
+
+@pytest.mark.parametrize("Lb", [64, 1000, 2500])
+def test_fused_and_relayout_cost_agree(Lb, oracle_mod):
+    rng = np.random.default_rng(77 + Lb)
+    F1, F2 = W.warped_pair(rng, 2600, 2900, pad_frac=0.1)
+    C = W.cost_matrix_det(F1, F2)
+    N, M = C.shape
+    pa = pf.Plan(N, M, Lb, STD, [2, 3, 3])
+    pb = pf.Plan(N, M, Lb, STD, [2, 3, 3])
+    pa.load_features(torch.from_numpy(F1).cuda(), torch.from_numpy(F2).cuda())
+    pb.load_cost(torch.from_numpy(C).cuda())
+    for p in (pa, pb):
+        p.run(None, 0.1)
+    for name in ("EDGE_D", "EDGE_P", "BACKPTR", "EDGE_CF", "D_ARR", "L_ARR"):
+        assert same(pa.host(name), pb.host(name)), name
+    ra, rb = pa.result(), pb.result()
+    assert ra == rb
+    ref = oracle_mod.parflex_full(C, STD, [2, 3, 3], 0.1, Lb)
+    assert ra[0] == ref["best_cost"]
+    assert same(pa.path(ra[3]).T, ref["wp"])
+
+
+def test_plan_reuse_across_pairs(oracle_mod):
+    """One plan, two different cost matrices in a row (no stale state)."""
+    rng = np.random.default_rng(9)
+    pairs = [W.warped_pair(rng, 700, 760, pad_frac=0.1) for _ in range(2)]
+    plan = pf.Plan(700, pairs[0][1].shape[1], 200, STD, [2, 3, 3])
+    for F1, F2 in pairs:
+        if F2.shape[1] != plan.M:
+            F2 = F2[:, :plan.M] if F2.shape[1] > plan.M else np.pad(
+                F2, ((0, 0), (0, plan.M - F2.shape[1])), constant_values=0.1)
+        C = W.cost_matrix_det(F1, F2)
+        plan.load_features(torch.from_numpy(F1).cuda(), torch.from_numpy(F2).cuda())
+        plan.run(None, 0.1)
+        best, end, found, n = plan.result()
+        ref = oracle_mod.parflex_full(C, STD, [2, 3, 3], 0.1, 200)
+        assert best == ref["best_cost"]
+        assert same(plan.path(n).T, ref["wp"])
