@@ -273,19 +273,25 @@ def b200_arm(args, spec):
     alg_bytes = cells * (8 + 0.25)
     achieved = alg_bytes / (ms_s1 / 1e3) / 1e9
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "stage1_traffic.json")
+    tp = os.path.join(ROOT, "profiles", "stage1_traffic.txt")
     if os.path.exists(tp):
+        kv = {}
         with open(tp) as fp:
-            td = json.load(fp)
-        if td.get("workload") == spec.name:
-            traffic = td.get("bytes_per_launch")
-    roofline = {"bound": "hbm", "kernel": "k_stage1_f64", "achieved": achieved,
+            for line in fp:
+                if "=" in line and not line.lstrip().startswith("#"):
+                    a, b = line.split("=", 1)
+                    kv[a.strip()] = b.strip()
+        if kv.get("workload") == spec.name:
+            traffic = float(kv["bytes_per_launch"])
+    roofline = {"bound": "hbm", "kernel": "k_stage1_v3", "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback",
                 "stage1_ms_per_launch": ms_s1,
                 "alg_bytes_per_cell": 8.25,
-                "fp64_dp_cells_per_s": cells / (ms_s1 / 1e3)}
+                "fp64_dp_cells_per_s": cells / (ms_s1 / 1e3),
+                "traffic_source": "profiles/k_stage1_v3_ncu_small.md (dram read+write per "
+                                  "launch, scaled by cells)"}
 
     # --- row-major C input: the relayout into the tile-skewed layout --------
     C_dev = pf.cost_matrix_from_features_gpu(F1, F2)
