@@ -197,6 +197,64 @@ int pfx_flexdtw_tile_noalloc(const double *C, int64_t ldc, int32_t R, int32_t W,
                              int32_t n_steps, double *D, int32_t *P, int8_t *B,
                              void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Batches.  A batch aligns n pairs of feature sequences of uneven lengths
+ * that share steps, weights and feature dimension d (1..16); pair i has its
+ * own shape (N[i], M[i]) and tile length L[i].  It owns, in one device
+ * arena, a plan per pair (pfx_batch_plan), the raw feature inputs, one
+ * pool of tile-skewed cost slabs and the stage-1 tile queues.  Pairs are
+ * packed into "waves" whose cost slabs fit the pool (wave_bytes; 0 = half
+ * of the free device memory); per wave, the cost of every pair is built
+ * from its features, ONE persistent stage-1 launch runs all tiles of all
+ * pairs of the wave (largest first) from a device work queue, and stage 2
+ * of the pairs runs on forked streams.  pfx_batch_run records this whole
+ * sequence once into a CUDA graph and replays it.
+ *
+ * The reference has no batch entry point: its notebooks loop over pairs
+ * calling parflex / tiled_stage1_from_features + run_stage2_from_tiled
+ * (Parflex.py:1466-1547; gpu_flexdtw.py:405-470).  Each pair's result is
+ * that of those calls on the same pair.
+ * ------------------------------------------------------------------------- */
+typedef struct pfx_batch pfx_batch;
+
+/* nw: stage-1 warps per tile CTA (4, 8 or 16; 0 = chosen from the tile
+ * count).  The batch is created on the current CUDA device. */
+int pfx_batch_create(int32_t n, const int64_t *N, const int64_t *M, const int32_t *L,
+                     const int64_t *steps, const double *weights, int32_t n_steps,
+                     int32_t d, int64_t wave_bytes, int32_t nw, pfx_batch **out);
+void pfx_batch_destroy(pfx_batch *batch);
+/* info[0..7] = n, waves, total tiles, DP cells (sum of tile R*W), device
+ * bytes, stage-1 warps per CTA, largest wave's tiles, cost-slab pool bytes. */
+int pfx_batch_info(const pfx_batch *batch, int64_t *info);
+/* Device input buffers of pair i: F1 (d x N[i]) and F2 (d x M[i]),
+ * row-major by feature.  Fill them before pfx_batch_run (any stream, but
+ * ordered before the run). */
+int pfx_batch_features(pfx_batch *batch, int32_t i, double **F1, double **F2);
+/* The plan of pair i (owned by the batch: do not destroy; do not load a
+ * cost into it).  pfx_result / pfx_copy_path / pfx_plan_buffer read pair
+ * i's results after pfx_batch_run. */
+int pfx_batch_plan(pfx_batch *batch, int32_t i, pfx_plan **plan);
+/* Aligns every pair (asynchronous on `stream`).  use_graph = 1 records the
+ * launch sequence into a CUDA graph on the first call (and again when beta
+ * changes) and replays it; 0 launches directly. */
+int pfx_batch_run(pfx_batch *batch, double beta, int32_t use_graph, void *stream);
+/* Device time (ms) of the phases of the last direct (use_graph = 0) run,
+ * summed over waves: ms3[0] cost building from features, ms3[1] the stage-1
+ * launches, ms3[2] stage 2 (end of stage 1 to the join of its streams).
+ * Waits for that run.  No reference counterpart (benchmark hook). */
+int pfx_batch_timing(pfx_batch *batch, double *ms3);
+/* Synchronises `stream` and copies every pair's result to host arrays:
+ * best_cost[n], best_end7[7n] (as in pfx_result), wp_len[n].  Pairs whose
+ * scan found no endpoint have best_end7[7i+6] = 0.  Fails if a stage-1
+ * wait ran out (the whole batch is then invalid). */
+int pfx_batch_results(pfx_batch *batch, void *stream, double *best_cost,
+                      int64_t *best_end7, int64_t *wp_len);
+/* Copies the paths of all pairs into host memory: pair i's K_i x 2 points
+ * start at wp_host + 2*offsets[i] (offsets from the wp_len of
+ * pfx_batch_results; capacity `cap` points in total).  Synchronises. */
+int pfx_batch_copy_paths(pfx_batch *batch, void *stream, int64_t *wp_host,
+                         const int64_t *offsets, int64_t cap);
+
 #ifdef __cplusplus
 }
 #endif

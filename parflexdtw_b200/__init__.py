@@ -2,10 +2,12 @@
 
 The public functions keep the reference's (ishitajain21/ParFlexDTW) API:
 ``parflex``, ``tiled_stage1_from_features``, ``run_stage2_from_tiled``,
-``run_flexdtw_on_tiles`` and ``flexdtw_chunk_from_global_C``.  They run on
+``run_flexdtw_on_tiles`` and ``flexdtw_chunk_from_global_C``; ``parflex_batch``
+aligns many pairs of uneven lengths in one device batch.  They run on
 hand-written sm_100a CUDA kernels behind the C ABI in
 ``include/parflexdtw_b200.h``; there is no CPU path.
 """
+from .batch import Batch, parflex_batch  # noqa: F401
 from .parflex import (  # noqa: F401
     DEFAULT_CHUNK_LENGTH,
     ChunksDict,

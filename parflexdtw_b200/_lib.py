@@ -17,6 +17,7 @@ _i32 = ct.c_int32
 _f64 = ct.c_double
 _vp = ct.c_void_p
 _i64p = ct.POINTER(ct.c_int64)
+_i32p = ct.POINTER(ct.c_int32)
 _f64p = ct.POINTER(ct.c_double)
 
 PFX_OK = 0
@@ -60,6 +61,16 @@ SIGNATURES = [
                                     _vp, _vp]),
     ("pfx_flexdtw_tile_noalloc", ct.c_int, [_vp, _i64, _i32, _i32, _i64p, _f64p, _i32, _vp,
                                             _vp, _vp, _vp]),
+    ("pfx_batch_create", ct.c_int, [_i32, _i64p, _i64p, _i32p, _i64p, _f64p, _i32, _i32, _i64,
+                                    _i32, ct.POINTER(_vp)]),
+    ("pfx_batch_destroy", None, [_vp]),
+    ("pfx_batch_info", ct.c_int, [_vp, _i64p]),
+    ("pfx_batch_features", ct.c_int, [_vp, _i32, ct.POINTER(_vp), ct.POINTER(_vp)]),
+    ("pfx_batch_plan", ct.c_int, [_vp, _i32, ct.POINTER(_vp)]),
+    ("pfx_batch_run", ct.c_int, [_vp, _f64, _i32, _vp]),
+    ("pfx_batch_timing", ct.c_int, [_vp, _f64p]),
+    ("pfx_batch_results", ct.c_int, [_vp, _vp, _f64p, _i64p, _i64p]),
+    ("pfx_batch_copy_paths", ct.c_int, [_vp, _vp, _i64p, _i64p, _i64]),
 ]
 
 _lib = None
@@ -111,6 +122,10 @@ def check(status: int):
 def i64_array(values):
     arr = (ct.c_int64 * len(values))(*[int(v) for v in values])
     return arr
+
+
+def i32_array(values):
+    return (ct.c_int32 * len(values))(*[int(v) for v in values])
 
 
 def f64_array(values):

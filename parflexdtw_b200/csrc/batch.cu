@@ -1,0 +1,489 @@
+// Batches of alignments: many pairs of uneven lengths, one persistent stage-1
+// launch per wave, stage 2 on forked streams, all recorded into a CUDA graph.
+//
+// The reference aligns one pair per call (Parflex.py:1466-1547,
+// gpu_flexdtw.py:405-470); a batch gives every pair exactly the result of
+// those calls.  Device memory: one arena holds every pair's plan buffers
+// (edge tensors, 2-bit backpointers, stage-2 slots), raw and normalised
+// features, the tile queues and the result block; one pool holds the
+// tile-skewed FP64 cost slabs of one wave.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "plan.cuh"
+
+using namespace pfx;
+
+namespace {
+
+constexpr int kSide = 8;  // streams stage 2 of a wave is spread over
+
+struct PairOut {
+    const double* best;
+    const int64_t* best_end;
+    const int64_t* wp_len;
+};
+
+__global__ void k_gather_results(const PairOut* __restrict__ po, int n, int64_t* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const PairOut p = po[i];
+    int64_t* o = out + (int64_t)i * 9;
+    o[0] = __double_as_longlong(*p.best);
+    for (int k = 0; k < 7; ++k) o[1 + k] = p.best_end[k];
+    o[8] = *p.wp_len;
+}
+
+int errf(int status, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    return report_status(status, buf);
+}
+
+size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+}  // namespace
+
+struct pfx_batch {
+    int n = 0, d = 0, nw = 0, device = 0;
+    Geo gq;  // step set and weights; L = largest tile length (ring sizing)
+    std::vector<pfx_plan> plans;
+    char* arena = nullptr;
+    size_t arena_bytes = 0;
+    double* slabs = nullptr;
+    size_t slab_bytes = 0;
+    double* fin = nullptr;  // raw features, pair i at fin_off[i]: F1 (d x N) then F2 (d x M)
+    std::vector<int64_t> fin_off;
+    // waves: pairs of wave w are wave_pairs[wave_first[w] .. wave_first[w+1])
+    std::vector<int> wave_pairs, wave_first;
+    std::vector<int64_t> wave_desc_off, wave_tiles;
+    TileDesc* descs = nullptr;
+    int* heads = nullptr;
+    int32_t* status = nullptr;
+    PairOut* pout = nullptr;
+    int64_t* res = nullptr;  // [n][9]
+    int64_t total_tiles = 0, cells = 0, max_wave_tiles = 0;
+    // streams and graph
+    cudaStream_t cap = nullptr;
+    cudaStream_t side[kSide] = {};
+    cudaEvent_t fork_ev = nullptr;
+    cudaEvent_t join_ev[kSide] = {};
+    cudaGraphExec_t exec = nullptr;
+    double graph_beta = 0.0;
+    int64_t graph_kernels = 0;  // kernel launches recorded in the graph
+    // phase events of the last direct run: per wave, before cost building,
+    // before stage 1, after stage 1, after the stage-2 join
+    std::vector<cudaEvent_t> phase_ev;
+    bool phase_valid = false;
+};
+
+static void batch_free(pfx_batch* b) {
+    if (!b) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(b->device);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    for (int k = 0; k < kSide; ++k) {
+        if (b->side[k]) cudaStreamDestroy(b->side[k]);
+        if (b->join_ev[k]) cudaEventDestroy(b->join_ev[k]);
+    }
+    if (b->fork_ev) cudaEventDestroy(b->fork_ev);
+    for (cudaEvent_t e : b->phase_ev) cudaEventDestroy(e);
+    if (b->cap) cudaStreamDestroy(b->cap);
+    if (b->arena) cudaFree(b->arena);
+    if (b->slabs) cudaFree(b->slabs);
+    cudaSetDevice(cur);
+    delete b;
+}
+
+extern "C" void pfx_batch_destroy(pfx_batch* b) { batch_free(b); }
+
+#define BCK(call)                                                                          \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            const int st_ = errf(PFX_ERR_CUDA, "%s failed: %s (%s:%d)", #call,             \
+                                 cudaGetErrorString(e_), __FILE__, __LINE__);              \
+            return st_;                                                                    \
+        }                                                                                  \
+    } while (0)
+
+extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, const int32_t* L,
+                                const int64_t* steps, const double* weights, int32_t n_steps,
+                                int32_t d, int64_t wave_bytes, int32_t nw, pfx_batch** out) {
+    if (!out || !N || !M || !L || !steps || !weights) return errf(PFX_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (n < 1) return errf(PFX_ERR_ARG, "batch of %d pairs", n);
+    if (d < 1 || d > 16) return errf(PFX_ERR_ARG, "feature dimension %d: the batch takes 1..16", d);
+    if (nw != 0 && nw != 4 && nw != 8 && nw != 16)
+        return errf(PFX_ERR_ARG, "nw=%d: warps per tile must be 4, 8 or 16 (or 0)", nw);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return errf(PFX_ERR_NO_DEVICE, "no CUDA device");
+    pfx_batch* b = new pfx_batch();
+    cudaGetDevice(&b->device);
+    b->n = n;
+    b->d = d;
+    b->plans.resize(n);
+    int st = PFX_OK;
+    int32_t maxL = 0;
+    // pass 1: geometry and byte counts
+    size_t arena = 0;
+    std::vector<size_t> plan_off(n), feat_off(n);
+    std::vector<int64_t> slab(n);
+    for (int i = 0; i < n; ++i) {
+        pfx_plan& p = b->plans[i];
+        memset(&p, 0, sizeof(p));
+        p.arena_mode = 1;
+        if ((st = plan_init(&p, N[i], M[i], L[i], steps, weights, n_steps, nw ? nw : 16))) {
+            batch_free(b);
+            return st;
+        }
+        plan_off[i] = arena;
+        arena += round256(p.bytes);
+        feat_off[i] = arena;
+        arena += round256((size_t)d * (N[i] + M[i]) * 8);
+        slab[i] = (int64_t)p.g.n1 * p.g.n2 * p.skew_stride * 8;
+        maxL = std::max(maxL, p.g.L);
+        b->total_tiles += (int64_t)p.g.n1 * p.g.n2;
+        for (int t = 0; t < p.g.n1 * p.g.n2; ++t) {
+            int64_t r0, c0;
+            int32_t R, W;
+            tile_rect(p.g, t / p.g.n2, t % p.g.n2, &r0, &c0, &R, &W);
+            b->cells += (int64_t)R * W;
+        }
+    }
+    b->gq = b->plans[0].g;
+    b->gq.L = maxL;
+    for (int i = 1; i < n; ++i) {
+        const Geo& g = b->plans[i].g;
+        if (g.S != b->gq.S) { batch_free(b); return errf(PFX_ERR_ARG, "steps differ"); }
+    }
+    // waves: pairs by slab size, largest first, packed in order
+    size_t freeb = 0, totalb = 0;
+    cudaMemGetInfo(&freeb, &totalb);
+    const size_t fin_total = [&] {
+        size_t s = 0;
+        for (int i = 0; i < n; ++i) s += round256((size_t)d * (N[i] + M[i]) * 8);
+        return s;
+    }();
+    const size_t fixed = arena + fin_total + round256(b->total_tiles * sizeof(TileDesc)) + (1 << 20);
+    int64_t budget = wave_bytes;
+    if (budget <= 0) budget = (int64_t)((freeb > fixed ? freeb - fixed : 0) / 2);
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return slab[a] > slab[c]; });
+    if (slab[order[0]] > budget) {
+        batch_free(b);
+        return errf(PFX_ERR_TOO_LARGE, "pair %d needs %lld B of cost slabs; wave budget %lld B",
+                    order[0], (long long)slab[order[0]], (long long)budget);
+    }
+    std::vector<int64_t> pool_off(n);
+    int64_t cur = 0, pool = 0;
+    b->wave_first.push_back(0);
+    for (int q = 0; q < n; ++q) {
+        const int i = order[q];
+        if (cur + slab[i] > budget) {
+            b->wave_first.push_back(q);
+            cur = 0;
+        }
+        pool_off[i] = cur;
+        cur += (slab[i] + 255) & ~(int64_t)255;
+        pool = std::max(pool, cur);
+        b->wave_pairs.push_back(i);
+    }
+    b->wave_first.push_back(n);
+    const int waves = (int)b->wave_first.size() - 1;
+    // stage-1 warps per tile: from the largest wave's tile count
+    for (int w = 0; w < waves; ++w) {
+        int64_t t = 0;
+        for (int q = b->wave_first[w]; q < b->wave_first[w + 1]; ++q) {
+            const Geo& g = b->plans[b->wave_pairs[q]].g;
+            t += (int64_t)g.n1 * g.n2;
+        }
+        b->wave_tiles.push_back(t);
+        b->max_wave_tiles = std::max(b->max_wave_tiles, t);
+    }
+    b->nw = nw ? nw
+               : stage1_queue_warps((int)std::min<int64_t>(b->max_wave_tiles, 1 << 30), maxL,
+                                    num_sms_cur());
+    if (b->nw == 0 || stage1_queue_warps(1, maxL, 1) == 0) {
+        batch_free(b);
+        return errf(PFX_ERR_TOO_LARGE, "L=%d: the stage-1 rings do not fit in shared memory", maxL);
+    }
+    // the remaining arena: raw features, descriptors, heads, status, results
+    const size_t off_fin = arena;
+    arena += fin_total;
+    const size_t off_desc = arena;
+    arena += round256(b->total_tiles * sizeof(TileDesc));
+    const size_t off_heads = arena;
+    arena += round256((size_t)waves * sizeof(int));
+    const size_t off_status = arena;
+    arena += 256;
+    const size_t off_pout = arena;
+    arena += round256((size_t)n * sizeof(PairOut));
+    const size_t off_res = arena;
+    arena += round256((size_t)n * 9 * 8);
+    cudaError_t e = cudaMalloc(&b->arena, arena);
+    if (e == cudaSuccess) e = cudaMemset(b->arena, 0, arena);
+    if (e == cudaSuccess) e = cudaMalloc(&b->slabs, (size_t)pool);
+    if (e != cudaSuccess) {
+        batch_free(b);
+        return errf(PFX_ERR_CUDA, "batch allocation (%zu + %lld B): %s", arena, (long long)pool,
+                    cudaGetErrorString(e));
+    }
+    b->arena_bytes = arena;
+    b->slab_bytes = (size_t)pool;
+    b->fin = reinterpret_cast<double*>(b->arena + off_fin);
+    b->descs = reinterpret_cast<TileDesc*>(b->arena + off_desc);
+    b->heads = reinterpret_cast<int*>(b->arena + off_heads);
+    b->status = reinterpret_cast<int32_t*>(b->arena + off_status);
+    b->pout = reinterpret_cast<PairOut*>(b->arena + off_pout);
+    b->res = reinterpret_cast<int64_t*>(b->arena + off_res);
+    // pass 2: carve the plans
+    b->fin_off.resize(n);
+    std::vector<PairOut> po(n);
+    size_t fo = 0;
+    for (int i = 0; i < n; ++i) {
+        pfx_plan& p = b->plans[i];
+        memset(&p, 0, sizeof(p));
+        p.arena_mode = 2;
+        p.arena = b->arena + plan_off[i];
+        if ((st = plan_init(&p, N[i], M[i], L[i], steps, weights, n_steps, b->nw))) {
+            batch_free(b);
+            return st;
+        }
+        p.feat = reinterpret_cast<double*>(b->arena + feat_off[i]);
+        p.feat_d = d;
+        p.Csk = reinterpret_cast<double*>(reinterpret_cast<char*>(b->slabs) + pool_off[i]);
+        p.cost_loaded = 1;
+        p.s1.status = b->status;
+        b->fin_off[i] = (int64_t)(fo / 8);
+        fo += round256((size_t)d * (N[i] + M[i]) * 8);
+        po[i] = PairOut{p.s2.best, p.s2.best_end, p.s2.wp_len};
+    }
+    // tile queues: per wave, all tiles of its pairs, largest first
+    std::vector<TileDesc> all;
+    all.reserve(b->total_tiles);
+    for (int w = 0; w < waves; ++w) {
+        b->wave_desc_off.push_back((int64_t)all.size());
+        std::vector<TileDesc> wv;
+        for (int q = b->wave_first[w]; q < b->wave_first[w + 1]; ++q) {
+            pfx_plan& p = b->plans[b->wave_pairs[q]];
+            std::vector<TileDesc> pd((size_t)p.g.n1 * p.g.n2);
+            plan_tile_descs(&p, p.Csk, pd.data());
+            // the pair's own queue (pfx_stage1 on the batch plan)
+            e = cudaMemcpy(p.descs, pd.data(), pd.size() * sizeof(TileDesc), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) break;
+            wv.insert(wv.end(), pd.begin(), pd.end());
+        }
+        std::stable_sort(wv.begin(), wv.end(), [](const TileDesc& a, const TileDesc& c) {
+            return (int64_t)a.R * a.W > (int64_t)c.R * c.W;
+        });
+        all.insert(all.end(), wv.begin(), wv.end());
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->descs, all.data(), all.size() * sizeof(TileDesc), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->pout, po.data(), n * sizeof(PairOut), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(b->status, 0, 4);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
+    for (int k = 0; k < kSide && e == cudaSuccess; ++k) {
+        e = cudaStreamCreateWithFlags(&b->side[k], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join_ev[k], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        batch_free(b);
+        return errf(PFX_ERR_CUDA, "batch setup: %s", cudaGetErrorString(e));
+    }
+    *out = b;
+    return PFX_OK;
+}
+
+extern "C" int pfx_batch_info(const pfx_batch* b, int64_t* info) {
+    if (!b || !info) return errf(PFX_ERR_ARG, "null argument");
+    info[0] = b->n;
+    info[1] = (int64_t)b->wave_first.size() - 1;
+    info[2] = b->total_tiles;
+    info[3] = b->cells;
+    info[4] = (int64_t)(b->arena_bytes + b->slab_bytes);
+    info[5] = b->nw;
+    info[6] = b->max_wave_tiles;
+    info[7] = (int64_t)b->slab_bytes;
+    return PFX_OK;
+}
+
+extern "C" int pfx_batch_features(pfx_batch* b, int32_t i, double** F1, double** F2) {
+    if (!b || !F1 || !F2) return errf(PFX_ERR_ARG, "null argument");
+    if (i < 0 || i >= b->n) return errf(PFX_ERR_ARG, "pair %d of %d", i, b->n);
+    *F1 = b->fin + b->fin_off[i];
+    *F2 = *F1 + (int64_t)b->d * b->plans[i].g.N;
+    return PFX_OK;
+}
+
+extern "C" int pfx_batch_plan(pfx_batch* b, int32_t i, pfx_plan** plan) {
+    if (!b || !plan) return errf(PFX_ERR_ARG, "null argument");
+    if (i < 0 || i >= b->n) return errf(PFX_ERR_ARG, "pair %d of %d", i, b->n);
+    *plan = &b->plans[i];
+    return PFX_OK;
+}
+
+// The launch sequence of one batch run, on stream s (captured or direct;
+// `timed` records the phase events, direct runs only).
+static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) {
+    const int waves = (int)b->wave_first.size() - 1;
+    BCK(cudaMemsetAsync(b->heads, 0, (size_t)waves * sizeof(int), s));
+    if (timed && b->phase_ev.empty()) {
+        b->phase_ev.resize((size_t)waves * 4);
+        for (auto& e : b->phase_ev) BCK(cudaEventCreate(&e));
+    }
+    b->phase_valid = false;
+    auto mark = [&](int w, int k) -> cudaError_t {
+        return timed ? cudaEventRecord(b->phase_ev[(size_t)w * 4 + k], s) : cudaSuccess;
+    };
+    int st;
+    for (int w = 0; w < waves; ++w) {
+        const int q0 = b->wave_first[w], q1 = b->wave_first[w + 1];
+        BCK(mark(w, 0));
+        for (int q = q0; q < q1; ++q) {
+            const int i = b->wave_pairs[q];
+            pfx_plan& p = b->plans[i];
+            const double* F1 = b->fin + b->fin_off[i];
+            const double* F2 = F1 + (int64_t)b->d * p.g.N;
+            double* An = p.feat;
+            double* Bn = p.feat + (int64_t)b->d * p.g.N;
+            BCK(launch_l2norm(F1, b->d, p.g.N, An, s));
+            BCK(launch_l2norm(F2, b->d, p.g.M, Bn, s));
+            BCK(launch_cost_skew(An, Bn, b->d, p.g, p.Csk, p.skew_stride, s));
+        }
+        BCK(mark(w, 1));
+        BCK(launch_stage1_queue(b->descs + b->wave_desc_off[w], (int)b->wave_tiles[w], b->heads + w,
+                                b->gq, b->status, b->nw, s));
+        BCK(mark(w, 2));
+        BCK(cudaEventRecord(b->fork_ev, s));
+        const int nside = std::min(kSide, q1 - q0);
+        for (int k = 0; k < nside; ++k) BCK(cudaStreamWaitEvent(b->side[k], b->fork_ev, 0));
+        for (int q = q0; q < q1; ++q) {
+            pfx_plan* p = &b->plans[b->wave_pairs[q]];
+            cudaStream_t ss = b->side[(q - q0) % nside];
+            if ((st = pfx_stage2_propagate(p, nullptr, 0, ss))) return st;
+            if ((st = pfx_stage2_scan(p, beta, ss))) return st;
+            if ((st = pfx_stage2_stitch(p, 1, 0, 0, 0, 0, ss))) return st;
+        }
+        for (int k = 0; k < nside; ++k) {
+            BCK(cudaEventRecord(b->join_ev[k], b->side[k]));
+            BCK(cudaStreamWaitEvent(s, b->join_ev[k], 0));
+        }
+        BCK(mark(w, 3));
+    }
+    b->phase_valid = timed;
+    return PFX_OK;
+}
+
+extern "C" int pfx_batch_run(pfx_batch* b, double beta, int32_t use_graph, void* stream) {
+    if (!b) return errf(PFX_ERR_ARG, "null batch");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!use_graph) return batch_enqueue(b, beta, s, true);
+    if (!b->exec || b->graph_beta != beta) {
+        if (b->exec) {
+            cudaGraphExecDestroy(b->exec);
+            b->exec = nullptr;
+        }
+        // record on the batch's own stream, ordered after work already on `s`
+        BCK(cudaEventRecord(b->fork_ev, s));
+        BCK(cudaStreamWaitEvent(b->cap, b->fork_ev, 0));
+        BCK(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeRelaxed));
+        const int64_t k0 = pfx_kernel_launches();
+        const int st = batch_enqueue(b, beta, b->cap, false);
+        // recorded launches run at each replay: count them there, not here
+        b->graph_kernels = pfx_kernel_launches() - k0;
+        count_launches(-(int)b->graph_kernels);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(b->cap, &graph);
+        if (st) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        if (e != cudaSuccess) return errf(PFX_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        const cudaError_t ei = cudaGraphInstantiate(&b->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ei != cudaSuccess) {
+            b->exec = nullptr;
+            return errf(PFX_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ei));
+        }
+        b->graph_beta = beta;
+    }
+    BCK(cudaGraphLaunch(b->exec, s));
+    count_launches((int)b->graph_kernels);
+    return PFX_OK;
+}
+
+extern "C" int pfx_batch_timing(pfx_batch* b, double* ms3) {
+    if (!b || !ms3) return errf(PFX_ERR_ARG, "null argument");
+    if (!b->phase_valid) return errf(PFX_ERR_ARG, "no direct (use_graph = 0) run to time");
+    const int waves = (int)b->wave_first.size() - 1;
+    BCK(cudaEventSynchronize(b->phase_ev[(size_t)waves * 4 - 1]));
+    ms3[0] = ms3[1] = ms3[2] = 0.0;
+    for (int w = 0; w < waves; ++w) {
+        for (int k = 0; k < 3; ++k) {
+            float t = 0.f;
+            BCK(cudaEventElapsedTime(&t, b->phase_ev[(size_t)w * 4 + k],
+                                     b->phase_ev[(size_t)w * 4 + k + 1]));
+            ms3[k] += t;
+        }
+    }
+    return PFX_OK;
+}
+
+extern "C" int pfx_batch_results(pfx_batch* b, void* stream, double* best_cost, int64_t* best_end7,
+                                 int64_t* wp_len) {
+    if (!b) return errf(PFX_ERR_ARG, "null batch");
+    cudaStream_t s = (cudaStream_t)stream;
+    k_gather_results<<<(b->n + 127) / 128, 128, 0, s>>>(b->pout, b->n, b->res);
+    count_launches(1);
+    BCK(cudaGetLastError());
+    std::vector<int64_t> h((size_t)b->n * 9);
+    int32_t kst = 0;
+    BCK(cudaMemcpyAsync(h.data(), b->res, h.size() * 8, cudaMemcpyDeviceToHost, s));
+    BCK(cudaMemcpyAsync(&kst, b->status, 4, cudaMemcpyDeviceToHost, s));
+    BCK(cudaStreamSynchronize(s));
+    if (kst) {
+        cudaMemsetAsync(b->status, 0, 4, s);
+        return errf(PFX_ERR_CUDA, "stage-1 wavefront wait ran out (status %d); batch invalid", kst);
+    }
+    for (int i = 0; i < b->n; ++i) {
+        const int64_t* r = &h[(size_t)i * 9];
+        if (best_cost) memcpy(&best_cost[i], &r[0], 8);
+        if (best_end7) memcpy(&best_end7[(size_t)i * 7], &r[1], 56);
+        if (wp_len) wp_len[i] = r[8];
+    }
+    return PFX_OK;
+}
+
+extern "C" int pfx_batch_copy_paths(pfx_batch* b, void* stream, int64_t* wp_host,
+                                    const int64_t* offsets, int64_t cap) {
+    if (!b || !wp_host || !offsets) return errf(PFX_ERR_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    std::vector<int64_t> lens(b->n);
+    for (int i = 0; i < b->n; ++i)
+        BCK(cudaMemcpyAsync(&lens[i], b->plans[i].s2.wp_len, 8, cudaMemcpyDeviceToHost, s));
+    BCK(cudaStreamSynchronize(s));
+    for (int i = 0; i < b->n; ++i) {
+        if (offsets[i] < 0 || offsets[i] + lens[i] > cap)
+            return errf(PFX_ERR_ARG, "pair %d: path of %lld points at offset %lld exceeds %lld", i,
+                        (long long)lens[i], (long long)offsets[i], (long long)cap);
+        if (lens[i] > 0)
+            BCK(cudaMemcpyAsync(wp_host + 2 * offsets[i], b->plans[i].s2.wp, (size_t)lens[i] * 16,
+                                cudaMemcpyDeviceToHost, s));
+    }
+    BCK(cudaStreamSynchronize(s));
+    return PFX_OK;
+}

@@ -8,8 +8,9 @@
 #include <string.h>
 
 #include <cmath>
+#include <vector>
 
-#include "common.cuh"
+#include "plan.cuh"
 
 
 
@@ -37,26 +38,6 @@ static int fail(int status, const char* fmt, ...) {
             return fail(PFX_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
                         __FILE__, __LINE__);                                             \
     } while (0)
-
-struct pfx_plan {
-    Geo g;
-    int nw;
-    int device;
-    size_t bytes;
-    S1Out s1;
-    S2Buf s2;
-    double* D_prop;
-    double* L_prop;
-    int64_t n4;  // n1*n2*2*L
-    void* blocks[32];
-    int nblocks;
-    // tile-skewed cost (allocated on first load) and normalised features
-    double* Csk;
-    int64_t skew_stride;  // doubles per tile slab
-    double* feat;         // d*(N+M) doubles
-    int feat_d;
-    int cost_loaded;
-};
 
 static const char* kStatus[] = {"ok",
                                 "invalid argument",
@@ -119,18 +100,18 @@ static int make_geo(int64_t N, int64_t M, int32_t L, const int64_t* steps, const
     return PFX_OK;
 }
 
-static int num_sms_cur() {
+int pfx::num_sms_cur() {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     return sms;
 }
 
-static int check_smem(int32_t L, int nw, bool v3 = false) {
+static int check_smem(int32_t L, int nw) {
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const size_t need = v3 ? stage1_v3_smem_bytes(L, nw, optin) : stage1_smem_bytes_host(L, nw);
+    const size_t need = stage1_smem_bytes_host(L, nw);
     if (need > (size_t)optin)
         return fail(PFX_ERR_TOO_LARGE, "L=%d needs %zu B of shared memory per tile CTA (limit %d)",
                     L, need, optin);
@@ -141,6 +122,16 @@ template <typename T>
 static int plan_alloc(pfx_plan* p, T** ptr, size_t count) {
     void* q = nullptr;
     const size_t bytes = count * sizeof(T) > 0 ? count * sizeof(T) : 16;
+    if (p->arena_mode) {
+        // carve from a caller-owned arena (mode 2) or only count (mode 1)
+        const size_t rounded = (bytes + 255) & ~(size_t)255;
+        *ptr = p->arena_mode == 2 ? reinterpret_cast<T*>(p->arena + p->arena_off) : nullptr;
+        p->arena_off += rounded;
+        p->bytes += rounded;
+        return PFX_OK;
+    }
+    if (p->nblocks >= (int)(sizeof(p->blocks) / sizeof(p->blocks[0])))
+        return fail(PFX_ERR_ARG, "plan buffer table full");
     cudaError_t e = cudaMalloc(&q, bytes);
     if (e != cudaSuccess)
         return fail(PFX_ERR_CUDA, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
@@ -151,7 +142,7 @@ static int plan_alloc(pfx_plan* p, T** ptr, size_t count) {
 }
 
 extern "C" void pfx_plan_destroy(pfx_plan* p) {
-    if (!p) return;
+    if (!p || p->arena_mode == 2) return;  // plans inside a batch belong to the batch
     int cur = 0;
     cudaGetDevice(&cur);
     cudaSetDevice(p->device);
@@ -160,23 +151,20 @@ extern "C" void pfx_plan_destroy(pfx_plan* p) {
     free(p);
 }
 
-extern "C" int pfx_plan_create(int64_t N, int64_t M, int32_t L, const int64_t* steps,
-                               const double* weights, int32_t n_steps, pfx_plan** out) {
-    if (!out || !steps || !weights) return fail(PFX_ERR_ARG, "null argument");
-    *out = nullptr;
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
-        return fail(PFX_ERR_NO_DEVICE, "no CUDA device");
-    pfx_plan* p = (pfx_plan*)calloc(1, sizeof(pfx_plan));
-    if (!p) return fail(PFX_ERR_ARG, "out of host memory");
+// Geometry, warps per tile and every buffer of a plan (cudaMalloc, or the
+// arena selected by p->arena_mode).  The tile-skewed cost slabs and the tile
+// queue are separate (plan_attach_cost).
+int pfx::plan_init(pfx_plan* p, int64_t N, int64_t M, int32_t L, const int64_t* steps,
+                   const double* weights, int32_t n_steps, int nw) {
     int st = make_geo(N, M, L, steps, weights, n_steps, &p->g);
-    if (st) { free(p); return st; }
+    if (st) return st;
     cudaGetDevice(&p->device);
-    p->nw = stage1_pick_warps(p->g, num_sms_cur());
-    if ((st = check_smem(L, p->nw, true))) { free(p); return st; }
-    p->skew_stride = skew_slab_elems(L);
     const Geo& g = p->g;
     const int64_t nt = (int64_t)g.n1 * g.n2;
+    p->nw = nw ? nw : stage1_queue_warps((int)std::min<int64_t>(nt, 1 << 30), L, num_sms_cur());
+    if (p->nw == 0 || stage1_queue_warps(1, L, 1) == 0)
+        return fail(PFX_ERR_TOO_LARGE, "L=%d: the stage-1 rings do not fit in shared memory", L);
+    p->skew_stride = skew_slab_elems(L);
     p->n4 = nt * 2 * g.L;
     const int64_t ms = std::max<int64_t>(std::max(ceil_div64(M, L), ceil_div64(N, L)), 1);
     p->s2.max_segs = (int32_t)ms;
@@ -184,12 +172,9 @@ extern "C" int pfx_plan_create(int64_t N, int64_t M, int32_t L, const int64_t* s
     double* eD;
     int32_t* eP;
     uint32_t* Bw;
-#define PA(ptr, n)                                            \
-    do {                                                      \
-        if ((st = plan_alloc(p, ptr, (size_t)(n)))) {         \
-            pfx_plan_destroy(p);                              \
-            return st;                                        \
-        }                                                     \
+#define PA(ptr, n)                                                 \
+    do {                                                           \
+        if ((st = plan_alloc(p, ptr, (size_t)(n)))) return st;     \
     } while (0)
     PA(&eD, p->n4);
     PA(&eP, p->n4);
@@ -221,11 +206,60 @@ extern "C" int pfx_plan_create(int64_t N, int64_t M, int32_t L, const int64_t* s
     PA(&p->s2.wp, 101 * p->s2.seg_cap * 2);
     PA(&p->s2.wp_len, 1);
     PA(&p->s1.status, 1);
+    PA(&p->descs, nt);
+    PA(&p->head, 1);
 #undef PA
+    if (p->arena_mode) return PFX_OK;  // arenas are zeroed by their owner
     CK(cudaMemset(p->s2.best_end, 0, 7 * sizeof(int64_t)));
     CK(cudaMemset(p->s2.chain_len, 0, sizeof(int32_t)));
     CK(cudaMemset(p->s2.wp_len, 0, sizeof(int64_t)));
     CK(cudaMemset(p->s1.status, 0, sizeof(int32_t)));
+    return PFX_OK;
+}
+
+// Tile descriptors of plan p with cost slabs at Csk, in queue order (largest
+// tile first, then row-major tile index).
+void pfx::plan_tile_descs(const pfx_plan* p, const double* Csk, TileDesc* out) {
+    const Geo& g = p->g;
+    const int nt = g.n1 * g.n2;
+    std::vector<int> order(nt);
+    for (int t = 0; t < nt; ++t) order[t] = t;
+    auto area = [&](int t) {
+        int64_t r0, c0;
+        int32_t R, W;
+        tile_rect(g, t / g.n2, t % g.n2, &r0, &c0, &R, &W);
+        return (int64_t)R * W;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return area(a) > area(b); });
+    for (int q = 0; q < nt; ++q) {
+        const int t = order[q];
+        int64_t r0, c0;
+        TileDesc d;
+        memset(&d, 0, sizeof(d));
+        tile_rect(g, t / g.n2, t % g.n2, &r0, &c0, &d.R, &d.W);
+        d.Csk = Csk + (int64_t)t * p->skew_stride;
+        d.Bw = p->s1.Bw + (int64_t)t * g.b_words;
+        d.eD = p->s1.edge_D + (int64_t)t * 2 * g.L;
+        d.eP = p->s1.edge_P + (int64_t)t * 2 * g.L;
+        d.L = g.L;
+        out[q] = d;
+    }
+}
+
+extern "C" int pfx_plan_create(int64_t N, int64_t M, int32_t L, const int64_t* steps,
+                               const double* weights, int32_t n_steps, pfx_plan** out) {
+    if (!out || !steps || !weights) return fail(PFX_ERR_ARG, "null argument");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(PFX_ERR_NO_DEVICE, "no CUDA device");
+    pfx_plan* p = (pfx_plan*)calloc(1, sizeof(pfx_plan));
+    if (!p) return fail(PFX_ERR_ARG, "out of host memory");
+    int st = plan_init(p, N, M, L, steps, weights, n_steps, 0);
+    if (st) {
+        pfx_plan_destroy(p);
+        return st;
+    }
     *out = p;
     return PFX_OK;
 }
@@ -273,9 +307,16 @@ static int check_ldc(const pfx_plan* p, const double* C, int64_t ldc) {
     return PFX_OK;
 }
 
+// Cost slabs (allocated on first use unless a batch attached its own) and
+// the plan's tile queue pointing at them.
 static int ensure_cost_buffer(pfx_plan* p) {
     if (p->Csk) return PFX_OK;
-    return plan_alloc(p, &p->Csk, (size_t)p->g.n1 * p->g.n2 * p->skew_stride);
+    int st = plan_alloc(p, &p->Csk, (size_t)p->g.n1 * p->g.n2 * p->skew_stride);
+    if (st) return st;
+    std::vector<TileDesc> d((size_t)p->g.n1 * p->g.n2);
+    plan_tile_descs(p, p->Csk, d.data());
+    CK(cudaMemcpy(p->descs, d.data(), d.size() * sizeof(TileDesc), cudaMemcpyHostToDevice));
+    return PFX_OK;
 }
 
 extern "C" int pfx_plan_load_cost(pfx_plan* p, const double* C, int64_t ldc, void* stream) {
@@ -316,9 +357,8 @@ extern "C" int pfx_stage1(pfx_plan* p, const double* C, int64_t ldc, void* strea
     if (C && (st = pfx_plan_load_cost(p, C, ldc, stream))) return st;
     if (!p->cost_loaded) return fail(PFX_ERR_ARG, "no cost matrix loaded into the plan");
     cudaStream_t s = (cudaStream_t)stream;
-    CK(launch_fill(p->s1.edge_D, p->n4, HUGE_VAL, s));
-    CK(cudaMemsetAsync(p->s1.edge_P, 0, (size_t)p->n4 * 4, s));
-    CK(launch_stage1_v3(p->Csk, p->skew_stride, p->g, p->s1, p->nw, s));
+    CK(cudaMemsetAsync(p->head, 0, sizeof(int), s));
+    CK(launch_stage1_queue(p->descs, p->g.n1 * p->g.n2, p->head, p->g, p->s1.status, p->nw, s));
     return PFX_OK;
 }
 

@@ -121,6 +121,18 @@ struct S1Out {
     int32_t* status;  // set non-zero by a kernel whose bounded wait ran out, or null
 };
 
+// One stage-1 work item: a tile of one alignment, with the addresses of its
+// inputs and outputs (the stage-1 kernel claims these from a device queue).
+struct TileDesc {
+    const double* Csk;  // tile-skewed cost slab
+    uint32_t* Bw;       // packed backpointers
+    double* eD;         // [2][L] D on the top / right edge
+    int32_t* eP;        // [2][L] start encodings on the edges
+    int32_t R, W;       // tile rows / columns
+    int32_t L;          // edge-array stride (the alignment's tile length)
+    int32_t pad;
+};
+
 // Status word values written by kernels.
 constexpr int32_t kStatusWaitTimeout = 1;
 
@@ -160,9 +172,13 @@ int parse_step_kinds(const int64_t* steps, const double* weights, int32_t n, Geo
 void count_launches(int n);
 
 // Launchers (stage1_f64.cu, stage1_v3.cu, layout.cu, stage2.cu, cost.cu).
-cudaError_t launch_stage1_v3(const double* Csk, int64_t skew_stride, const Geo& g, const S1Out& o,
-                             int nw, cudaStream_t st);
-size_t stage1_v3_smem_bytes(int32_t L, int nw, int smem_limit);
+// Stage-1 queue kernel over `ntiles` descriptors (all sharing the step set and
+// weights of g; tiles at most g.L x g.L); `*head` must be 0 at launch; nw in
+// {4, 8, 16} warps per tile.
+cudaError_t launch_stage1_queue(const TileDesc* descs, int ntiles, int* head, const Geo& g,
+                                int32_t* status, int nw, cudaStream_t st);
+// Smallest valid warps-per-tile choice heuristic for `ntiles` tiles of length L.
+int stage1_queue_warps(int ntiles, int32_t L, int num_sms);
 cudaError_t launch_relayout_skew(const double* C, int64_t ldc, const Geo& g, double* Csk,
                                  int64_t skew_stride, cudaStream_t st);
 cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Geo& g, double* Csk,

@@ -1,0 +1,41 @@
+// Plan object behind the opaque pfx_plan handle of the C ABI, shared by the
+// single-alignment entry points (capi.cu) and the batch (batch.cu).
+#pragma once
+
+#include "common.cuh"
+
+struct pfx_plan {
+    pfx::Geo g;
+    int nw;  // warps per tile CTA of the stage-1 kernel
+    int device;
+    size_t bytes;
+    pfx::S1Out s1;
+    pfx::S2Buf s2;
+    double* D_prop;
+    double* L_prop;
+    int64_t n4;  // n1*n2*2*L
+    void* blocks[40];
+    int nblocks;
+    // tile-skewed cost (allocated on first load, or attached by a batch) and
+    // normalised features
+    double* Csk;
+    int64_t skew_stride;  // doubles per tile slab
+    double* feat;         // d*(N+M) doubles
+    int feat_d;
+    int cost_loaded;
+    // stage-1 tile queue of this plan (descriptors in queue order) and its head
+    pfx::TileDesc* descs;
+    int* head;
+    // arena allocation: 0 = cudaMalloc per buffer, 1 = count bytes only,
+    // 2 = carve from `arena`
+    int arena_mode;
+    char* arena;
+    size_t arena_off;
+};
+
+namespace pfx {
+int plan_init(pfx_plan* p, int64_t N, int64_t M, int32_t L, const int64_t* steps,
+              const double* weights, int32_t n_steps, int nw);
+void plan_tile_descs(const pfx_plan* p, const double* Csk, TileDesc* out);
+int num_sms_cur();
+}  // namespace pfx

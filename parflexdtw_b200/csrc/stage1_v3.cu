@@ -16,12 +16,20 @@
 //
 // Lane 0 takes rows 64k-2 and 64k-1 (the previous strip's lane 31) from a
 // per-warp shared-memory ring indexed by (strip start + column) mod RB.
-// Strips start `lag` (>= 80) steps apart.  Warps do not use CTA barriers:
-// each publishes the global step it has completed (release store by lane 31,
-// the ring writer) and, before a block, waits (acquire, bounded) until its
-// producer has written everything the block reads and its consumer has read
-// every slot the block overwrites.  A wait that runs out sets the status word
-// and the warp returns, and so, in turn, do the warps that wait on it.
+// Strips start `lag` (>= 80) steps apart.  Inside a tile warps do not use CTA
+// barriers: each publishes the global step it has completed (release store by
+// lane 31, the ring writer) and, before a block, waits (acquire, bounded)
+// until its producer has written everything the block reads and its consumer
+// has read every slot the block overwrites.  A wait that runs out sets the
+// status word and the CTA's abort flag; every warp then leaves the tile at its
+// next wait and the CTA stops claiming tiles.
+//
+// Work queue.  The kernel is persistent: each CTA claims tile descriptors
+// (cost slab, output addresses, shape) from a device queue with one atomic
+// per tile, so the tiles of one alignment or of a whole batch of alignments
+// of uneven sizes run in one launch.  Queues are ordered largest tile first.
+// A CTA barrier separates consecutive tiles of a CTA (rings and progress
+// words are reset there).
 //
 // Selection.  Every cell first takes a branch-free, division-free comparison
 // of the three candidates (cross products with a 2^-48 relative margin, see
@@ -31,6 +39,7 @@
 // IEEE division.  Only blocks touching a tile boundary ("edge" blocks) pay
 // for the bounds tests and the edge-row stores.  The cost queue runs two
 // steps ahead.
+#include <algorithm>
 #include <cuda/atomic>
 
 #include "common.cuh"
@@ -157,7 +166,7 @@ __device__ __forceinline__ void run_block(const Geo& g, Wave& st, const Rings& r
                                           const double2* __restrict__ Cs, int span, int tau0,
                                           int k, int R, int W, int lane, int prev_base,
                                           int mine_base, int rmask, int Tb, int lag,
-                                          const S1Out& out, int tile, int nP) {
+                                          const TileDesc& td, int nP) {
     const unsigned F = 0xffffffffu;
     const double w_last = g.S == 1 ? g.w[0] : (g.S == 2 ? g.w[1] : g.w[2]);
     const int rA = 64 * k + 2 * lane, rB = rA + 1;
@@ -229,16 +238,16 @@ __device__ __forceinline__ void run_block(const Geo& g, Wave& st, const Rings& r
                 }
             }
             if (EDGE) {
-                double* eD = out.edge_D + (int64_t)tile * 2 * g.L;
-                int32_t* eP = out.edge_P + (int64_t)tile * 2 * g.L;
+                double* eD = td.eD;
+                int32_t* eP = td.eP;
                 if (actA && (rA == 0 || cA == 0)) { oAD = cc.x; oAP = 0; codeA = 0; }
                 if (actB && cB == 0) { oBD = cc.y; oBP = 0; codeB = 0; }
                 if (!actA) { oAD = 0.0; oAP = 0; codeA = 0; }
                 if (!actB) { oBD = 0.0; oBP = 0; codeB = 0; }
                 if (actA && rA == R - 1) { eD[cA] = oAD; eP[cA] = oAP; }
                 if (actB && rB == R - 1) { eD[cB] = oBD; eP[cB] = oBP; }
-                if (actA && cA == W - 1) { eD[g.L + rA] = oAD; eP[g.L + rA] = oAP; }
-                if (actB && cB == W - 1) { eD[g.L + rB] = oBD; eP[g.L + rB] = oBP; }
+                if (actA && cA == W - 1) { eD[td.L + rA] = oAD; eP[td.L + rA] = oAP; }
+                if (actB && cB == W - 1) { eD[td.L + rB] = oBD; eP[td.L + rB] = oBP; }
             }
             if (lane == 31) {
                 if (actA) {
@@ -263,15 +272,18 @@ __device__ __forceinline__ void run_block(const Geo& g, Wave& st, const Rings& r
         }
     }
     if (rA < R) {
-        uint2* Bt = reinterpret_cast<uint2*>(out.Bw + (int64_t)tile * g.b_words);
+        uint2* Bt = reinterpret_cast<uint2*>(td.Bw);
         Bt[((int64_t)k * nP + (tau0 >> 4)) * 32 + lane] = make_uint2(bitsA, bitsB);
     }
 }
 
-__device__ __forceinline__ bool wait_progress(int* p, int target) {
+// Bounded wait until progress word *p reaches target; gives up early when
+// another warp of the CTA has already given up (*abort set).
+__device__ __forceinline__ bool wait_progress(int* p, int target, const volatile int* abort) {
     cuda::atomic_ref<int, cuda::thread_scope_block> a(*p);
     for (int it = 0; it < kSpinLimit; ++it) {
         if (a.load(cuda::memory_order_acquire) >= target) return true;
+        if (*abort) return false;
         __nanosleep(32);
     }
     return false;
@@ -292,73 +304,98 @@ __host__ __device__ inline int ring_len(int lag, int nw, int smem_limit) {
 }
 
 template <int NW, bool STD>
-__global__ void __launch_bounds__(NW * 32, 1)
-    k_stage1_v3(const double* __restrict__ Csk, const int64_t skew_stride, const Geo g,
-                const S1Out out, const int RBmax) {
+__global__ void __launch_bounds__(NW * 32, 16 / NW)
+    k_stage1_v3(const TileDesc* __restrict__ descs, const int ntiles, int* __restrict__ head,
+                const Geo g, int32_t* __restrict__ status, const int RB) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int tile = (int)blockIdx.x;
-    const int ti = tile / g.n2, tj = tile % g.n2;
-    int64_t r0, c0;
-    int32_t R, W;
-    tile_rect(g, ti, tj, &r0, &c0, &R, &W);
-    const Sched2 sc = make_sched2(R, W, NW);
-    const int lag = sc.lag;
-    const int RB = RBmax;  // >= lag - 29 for every tile (checked on the host for L x L)
     Rings rg;
     rg.AD = reinterpret_cast<double*>(smem_raw);
     rg.BD = rg.AD + NW * RB;
     rg.AP = reinterpret_cast<int*>(rg.BD + NW * RB);
     rg.BP = rg.AP + NW * RB;
     int* prog = rg.BP + NW * RB;
-    if (threadIdx.x < NW) prog[threadIdx.x] = 0;
-    __syncthreads();
-
+    __shared__ TileDesc td;
+    __shared__ Sched2 s_sc;  // schedule of the current tile (read from smem, not held in registers)
+    __shared__ int s_item, s_abort, s_ttot;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int prevw = (warp + NW - 1) % NW, nextw = (warp + 1) % NW;
-    const int Ttot = (sc.nS - 1) * lag + sc.span;
-    const double2* Ct = reinterpret_cast<const double2*>(Csk + (int64_t)tile * skew_stride);
+    if (threadIdx.x == 0) s_abort = 0;
     cuda::atomic_ref<int, cuda::thread_scope_block> my_prog(prog[warp]);
-
-    Wave st;
-    st.aD1 = st.aD2 = st.aD3 = st.bD1 = st.bD2 = st.xpD = 0.0;
-    st.aP1 = st.aP2 = st.aP3 = st.bP1 = st.bP2 = st.xpP = 0;
-#pragma unroll
-    for (int q = 0; q < 2; ++q) st.q[q] = make_double2(0.0, 0.0);
-
-    for (int Tb = 0; Tb < Ttot; Tb += kBlk) {
-        int k = -1;
-        if (Tb >= warp * lag) {
-            const int j = (Tb - warp * lag) / (NW * lag);
-            const int kk = warp + j * NW;
-            if (kk < sc.nS && Tb < kk * lag + sc.span) k = kk;
-        }
-        if (k >= 0) {
-            int failed = 0;
-            if (lane == 0) {
-                // producer (strip k-1) has written every ring slot this block reads
-                if (k >= 1 && !wait_progress(prog + prevw, Tb - lag + 78)) failed = 1;
-                // consumer (strip k+1) has read every slot this block overwrites
-                if (!failed && k + 1 < sc.nS && !wait_progress(prog + nextw, Tb + lag - RB - 45))
-                    failed = 1;
-                if (failed && out.status) atomicExch(out.status, kStatusWaitTimeout);
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int it = atomicAdd(head, 1);
+            s_item = it;
+            if (it < ntiles) {
+                td = descs[it];
+                s_sc = make_sched2(td.R, td.W, NW);
+                s_ttot = (s_sc.nS - 1) * s_sc.lag + s_sc.span;
             }
-            if (__shfl_sync(0xffffffffu, failed, 0)) return;
-            const int tau0 = Tb - k * lag;
-            const double2* Cs = Ct + (int64_t)k * sc.span * 32 + lane;
-            if (tau0 == 0) {
-#pragma unroll
-                for (int q = 0; q < 2; ++q) st.q[q] = __ldcs(Cs + q * 32);
-            }
-            const bool interior = k >= 1 && k <= sc.nS - 2 && tau0 >= 80 && tau0 + 17 <= W;
-            if (interior)
-                run_block<false, STD>(g, st, rg, Cs, sc.span, tau0, k, R, W, lane, prevw * RB,
-                                      warp * RB, RB - 1, Tb, lag, out, tile, sc.nP);
-            else
-                run_block<true, STD>(g, st, rg, Cs, sc.span, tau0, k, R, W, lane, prevw * RB,
-                                     warp * RB, RB - 1, Tb, lag, out, tile, sc.nP);
         }
-        __syncwarp();
-        if (lane == 31) my_prog.store(Tb + kBlk, cuda::memory_order_release);
+        if (threadIdx.x < NW) prog[threadIdx.x] = 0;
+        __syncthreads();
+        if (s_item >= ntiles || s_abort) return;
+        {
+            // edge rows past the tile's extent stay +inf / 0 (the DP writes the rest)
+            double* eD = td.eD;
+            int32_t* eP = td.eP;
+            for (int i = threadIdx.x; i < 2 * td.L; i += NW * 32) {
+                eD[i] = CUDART_INF;
+                eP[i] = 0;
+            }
+        }
+        __syncthreads();
+        const int32_t R = td.R, W = td.W;
+        const Sched2& sc = s_sc;
+        const int lag = sc.lag;
+        const int Ttot = s_ttot;
+        const double2* Ct = reinterpret_cast<const double2*>(td.Csk);
+
+        Wave st;
+        st.aD1 = st.aD2 = st.aD3 = st.bD1 = st.bD2 = st.xpD = 0.0;
+        st.aP1 = st.aP2 = st.aP3 = st.bP1 = st.bP2 = st.xpP = 0;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) st.q[q] = make_double2(0.0, 0.0);
+
+        for (int Tb = 0; Tb < Ttot; Tb += kBlk) {
+            int k = -1;
+            if (Tb >= warp * lag) {
+                const int j = (Tb - warp * lag) / (NW * lag);
+                const int kk = warp + j * NW;
+                if (kk < sc.nS && Tb < kk * lag + sc.span) k = kk;
+            }
+            if (k >= 0) {
+                int failed = 0;
+                if (lane == 0) {
+                    // producer (strip k-1) has written every ring slot this block reads
+                    if (k >= 1 && !wait_progress(prog + prevw, Tb - lag + 78, &s_abort)) failed = 1;
+                    // consumer (strip k+1) has read every slot this block overwrites
+                    if (!failed && k + 1 < sc.nS &&
+                        !wait_progress(prog + nextw, Tb + lag - RB - 45, &s_abort))
+                        failed = 1;
+                    if (failed) {
+                        if (status) atomicExch(status, kStatusWaitTimeout);
+                        s_abort = 1;
+                    }
+                }
+                if (__shfl_sync(0xffffffffu, failed, 0)) break;  // to the tile barrier
+                const int tau0 = Tb - k * lag;
+                const double2* Cs = Ct + (int64_t)k * sc.span * 32 + lane;
+                if (tau0 == 0) {
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) st.q[q] = __ldcs(Cs + q * 32);
+                }
+                const bool interior = k >= 1 && k <= sc.nS - 2 && tau0 >= 80 && tau0 + 17 <= W;
+                if (interior)
+                    run_block<false, STD>(g, st, rg, Cs, sc.span, tau0, k, R, W, lane, prevw * RB,
+                                          warp * RB, RB - 1, Tb, lag, td, sc.nP);
+                else
+                    run_block<true, STD>(g, st, rg, Cs, sc.span, tau0, k, R, W, lane, prevw * RB,
+                                         warp * RB, RB - 1, Tb, lag, td, sc.nP);
+            }
+            __syncwarp();
+            if (lane == 31) my_prog.store(Tb + kBlk, cuda::memory_order_release);
+        }
+        __syncthreads();  // every warp is done with this tile's rings and descriptor
     }
 }
 
@@ -369,6 +406,20 @@ static int smem_optin() {
     return v;
 }
 
+static int smem_per_sm() {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    return v;
+}
+
+// Shared memory budget per CTA when 16/NW CTAs share an SM.
+static int cta_budget(int nw) {
+    const int per_cta = smem_per_sm() / (16 / nw) - 2048;  // static smem and reserve
+    const int optin = smem_optin();
+    return per_cta < optin ? per_cta : optin;
+}
+
 size_t stage1_v3_smem_bytes(int32_t L, int nw, int smem_limit) {
     const Sched2 s = make_sched2(L, L, nw);
     const int rb = ring_len(s.lag, nw, smem_limit);
@@ -376,10 +427,21 @@ size_t stage1_v3_smem_bytes(int32_t L, int nw, int smem_limit) {
     return (size_t)nw * rb * (2 * sizeof(double) + 2 * sizeof(int)) + nw * sizeof(int);
 }
 
+int stage1_queue_warps(int ntiles, int32_t L, int num_sms) {
+    // fewer warps per tile fill the strip pipeline better (utilisation ~
+    // strips / (strips - 1 + warps)) but need several tiles per SM
+    const int budget16 = cta_budget(16);
+    if ((int64_t)ntiles >= 4LL * num_sms && stage1_v3_smem_bytes(L, 4, cta_budget(4)) < (1u << 30))
+        return 4;
+    if ((int64_t)ntiles >= 2LL * num_sms && stage1_v3_smem_bytes(L, 8, cta_budget(8)) < (1u << 30))
+        return 8;
+    return stage1_v3_smem_bytes(L, 16, budget16) < (1u << 30) ? 16 : 0;
+}
+
 template <int NW, bool STD>
-static cudaError_t launch_v3_t(const double* Csk, int64_t stride, const Geo& g, const S1Out& o,
-                               cudaStream_t st) {
-    const int limit = smem_optin();
+static cudaError_t launch_q_t(const TileDesc* descs, int ntiles, int* head, const Geo& g,
+                              int32_t* status, cudaStream_t st) {
+    const int limit = cta_budget(NW);
     const Sched2 s = make_sched2(g.L, g.L, NW);
     const int rb = ring_len(s.lag, NW, limit);
     if (rb == 0) return cudaErrorInvalidValue;
@@ -387,19 +449,34 @@ static cudaError_t launch_v3_t(const double* Csk, int64_t stride, const Geo& g, 
     cudaError_t e = cudaFuncSetAttribute(k_stage1_v3<NW, STD>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_stage1_v3<NW, STD><<<g.n1 * g.n2, NW * 32, smem, st>>>(Csk, stride, g, o, rb);
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage1_v3<NW, STD>, NW * 32,
+                                                      smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    const int grid = (int)std::min<int64_t>((int64_t)sms * per_sm, ntiles);
+    if (grid <= 0) return cudaSuccess;
+    k_stage1_v3<NW, STD><<<grid, NW * 32, smem, st>>>(descs, ntiles, head, g, status, rb);
     count_launches(1);
     return cudaGetLastError();
 }
 
-cudaError_t launch_stage1_v3(const double* Csk, int64_t skew_stride, const Geo& g, const S1Out& o,
-                             int nw, cudaStream_t st) {
+cudaError_t launch_stage1_queue(const TileDesc* descs, int ntiles, int* head, const Geo& g,
+                                int32_t* status, int nw, cudaStream_t st) {
     const bool std_steps = g.S == 3 && g.kind[0] == 0 && g.kind[1] == 1 && g.kind[2] == 2;
-    if (std_steps)
-        return nw == 16 ? launch_v3_t<16, true>(Csk, skew_stride, g, o, st)
-                        : launch_v3_t<8, true>(Csk, skew_stride, g, o, st);
-    return nw == 16 ? launch_v3_t<16, false>(Csk, skew_stride, g, o, st)
-                    : launch_v3_t<8, false>(Csk, skew_stride, g, o, st);
+    switch (nw) {
+        case 4:
+            return std_steps ? launch_q_t<4, true>(descs, ntiles, head, g, status, st)
+                             : launch_q_t<4, false>(descs, ntiles, head, g, status, st);
+        case 8:
+            return std_steps ? launch_q_t<8, true>(descs, ntiles, head, g, status, st)
+                             : launch_q_t<8, false>(descs, ntiles, head, g, status, st);
+        default:
+            return std_steps ? launch_q_t<16, true>(descs, ntiles, head, g, status, st)
+                             : launch_q_t<16, false>(descs, ntiles, head, g, status, st);
+    }
 }
 
 }  // namespace pfx

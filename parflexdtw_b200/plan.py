@@ -74,6 +74,23 @@ class Plan:
          self.warps) = (int(x) for x in info)
         self.device = torch.cuda.current_device()
 
+    @classmethod
+    def borrow(cls, handle, owner, N, M, Lb, steps, weights):
+        """A Plan over a handle owned by ``owner`` (a batch): not destroyed
+        here, and ``owner`` stays alive while the Plan does."""
+        self = cls.__new__(cls)
+        self.steps, self.weights = normalize_steps(steps, weights)
+        self.N, self.M, self.L = int(N), int(M), int(Lb)
+        self._h = handle
+        self._owner = owner
+        self._fin = weakref.finalize(self, lambda: None)
+        info = (ct.c_int64 * 8)()
+        L.check(L.load().pfx_plan_info(handle, info))
+        (self.n1, self.n2, _, self.hop, self.S, self.b_words, self.device_bytes,
+         self.warps) = (int(x) for x in info)
+        self.device = owner.device
+        return self
+
     @property
     def handle(self):
         return self._h

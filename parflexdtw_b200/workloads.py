@@ -171,7 +171,56 @@ CONFIG1 = PairSpec("chroma12_pair_30000x36000_L4000_fp64", 30000, 36000, 4000,
 NCU_SMALL = PairSpec("chroma12_pair_8000x9600_L4000_fp64", 8000, 9600, 4000,
                      pad_frac=0.0)
 
-WORKLOADS = {"config0": CONFIG0, "config1": CONFIG1, "ncu_small": NCU_SMALL}
+
+
+class BatchSpec:
+    """Named batch workload: ``n_pairs`` pairs with N ~ U(n_lo, n_hi) and
+    M = N x U(ratio_lo, ratio_hi) through the warp model of ``warped_pair``;
+    tile length per pair from ``L_choices`` (the autotuner picks per length
+    bucket when more than one is given)."""
+
+    def __init__(self, name, n_pairs, n_lo, n_hi, ratio_lo=0.7, ratio_hi=1.4,
+                 L_choices=(1000, 2000), pad_frac=0.0, d=12, noise=0.05,
+                 weights=(2.0, 3.0, 3.0), beta=0.1, seed=0):
+        self.name = name
+        self.n_pairs = n_pairs
+        self.n_lo, self.n_hi = n_lo, n_hi
+        self.ratio_lo, self.ratio_hi = ratio_lo, ratio_hi
+        self.L_choices = tuple(int(x) for x in L_choices)
+        self.pad_frac = pad_frac
+        self.d = d
+        self.noise = noise
+        self.steps = ((1, 1), (1, 2), (2, 1))
+        self.weights = tuple(float(w) for w in weights)
+        self.beta = beta
+        self.seed = seed
+
+    def describe(self):
+        return {"workload": self.name, "pairs": self.n_pairs,
+                "N_range": [self.n_lo, self.n_hi],
+                "M_over_N": [self.ratio_lo, self.ratio_hi],
+                "L_choices": list(self.L_choices), "d": self.d,
+                "weights": list(self.weights), "beta": self.beta, "seed": self.seed}
+
+
+def make_batch(spec: BatchSpec, seed_offset: int = 0):
+    """Generate the ``n_pairs`` (F1, F2) pairs of a batch spec."""
+    rng = np.random.default_rng(spec.seed + seed_offset)
+    out = []
+    for _ in range(spec.n_pairs):
+        n = int(rng.integers(spec.n_lo, spec.n_hi + 1))
+        m = int(round(n * rng.uniform(spec.ratio_lo, spec.ratio_hi)))
+        out.append(warped_pair(rng, n, m, d=spec.d, noise=spec.noise,
+                               pad_frac=spec.pad_frac))
+    return out
+
+
+# 256 pairs, N ~ U(2000, 20000), M = N x U(0.7, 1.4), 12-d chroma-like
+# features, L in {1000, 2000} per length bucket, FP64 DP.
+BATCH256 = BatchSpec("chroma12_batch256_N2000-20000_fp64", 256, 2000, 20000)
+
+WORKLOADS = {"config0": CONFIG0, "config1": CONFIG1, "ncu_small": NCU_SMALL,
+             "batch256": BATCH256}
 
 
 def make_pair(spec: PairSpec):

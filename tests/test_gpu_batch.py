@@ -1,0 +1,153 @@
+"""Batched alignment (pfx_batch_* / parflex_batch) vs the C oracle.
+
+Every pair of a batch must give exactly what the single-pair path and the
+oracle give for it (bit-exact best cost, endpoint and path), whatever the
+wave packing, the warps per tile, graph replay or direct launch.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover - CPU container
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import parflexdtw_b200 as pf  # noqa: E402
+from parflexdtw_b200 import workloads as W  # noqa: E402
+from parflexdtw_b200.autotune import Autotuner  # noqa: E402
+from parflexdtw_b200.batch import Batch  # noqa: E402
+
+STD = [(1, 1), (1, 2), (2, 1)]
+WTS = [2.0, 3.0, 3.0]
+
+
+def same(a, b):
+    return np.array_equal(np.asarray(a), np.asarray(b), equal_nan=True)
+
+
+def _pairs(seed, sizes, pad=0.1):
+    rng = np.random.default_rng(seed)
+    return [W.warped_pair(rng, n, m, pad_frac=pad) for n, m in sizes]
+
+
+SIZES = [(700, 900), (1500, 1200), (333, 410), (1200, 1700), (90, 120), (2100, 2000)]
+LS = [128, 300, 64, 500, 17, 256]
+
+
+@pytest.fixture(scope="module")
+def reference(oracle_mod):
+    pairs = _pairs(1, SIZES)
+    refs = [oracle_mod.parflex_full(W.cost_matrix_det(F1, F2), STD, WTS, 0.1, Lb)
+            for (F1, F2), Lb in zip(pairs, LS)]
+    return pairs, refs
+
+
+def _check(b, refs):
+    best, end, lens = b.results()
+    paths = b.paths(lens)
+    for i, ref in enumerate(refs):
+        assert best[i] == ref["best_cost"], i
+        assert tuple(end[i, :6]) == tuple(ref["best_end"]), i
+        assert end[i, 6] == 1
+        assert same(paths[i].T, ref["wp"]), i
+
+
+@pytest.mark.parametrize("warps", [4, 8, 16])
+def test_batch_one_wave_vs_oracle(reference, warps):
+    pairs, refs = reference
+    b = Batch([(p[0].shape[1], p[1].shape[1]) for p in pairs], LS, STD, WTS, 12, warps=warps)
+    assert b.waves == 1 and b.warps == warps
+    b.load(pairs)
+    b.run(0.1)
+    _check(b, refs)
+    # graph replay on fresh features gives the same answers again
+    b.run(0.1)
+    _check(b, refs)
+    b.close()
+
+
+def test_batch_waves_and_direct_launch(reference):
+    pairs, refs = reference
+    shapes = [(p[0].shape[1], p[1].shape[1]) for p in pairs]
+    b = Batch(shapes, LS, STD, WTS, 12, wave_bytes=56 << 20, warps=4)
+    assert b.waves >= 2
+    b.load(pairs)
+    b.run(0.1, use_graph=False)
+    _check(b, refs)
+    b.run(0.1, use_graph=True)
+    _check(b, refs)
+    b.close()
+
+
+def test_batch_beta_change_rerecords(oracle_mod):
+    pairs = _pairs(2, [(800, 950), (640, 600)])
+    C = [W.cost_matrix_det(F1, F2) for F1, F2 in pairs]
+    b = Batch([(p[0].shape[1], p[1].shape[1]) for p in pairs], 200, STD, WTS, 12)
+    b.load(pairs)
+    for beta in (0.1, 0.3, 0.1):
+        b.run(beta)
+        best, end, lens = b.results()
+        paths = b.paths(lens)
+        for i in range(2):
+            ref = oracle_mod.parflex_full(C[i], STD, WTS, beta, 200)
+            assert best[i] == ref["best_cost"]
+            assert same(paths[i].T, ref["wp"])
+    b.close()
+
+
+def test_batch_plan_views_match_single_pair(reference, oracle_mod):
+    """Stage-2 intermediates of a pair inside a batch equal the oracle's."""
+    pairs, refs = reference
+    b = Batch([(p[0].shape[1], p[1].shape[1]) for p in pairs], LS, STD, WTS, 12)
+    b.load(pairs)
+    b.run(0.1)
+    torch.cuda.synchronize()
+    for i in (0, 3):
+        p = b.plan(i)
+        assert same(p.host("D_ARR"), refs[i]["D_arr"])
+        assert same(p.host("L_ARR"), refs[i]["L_arr"])
+        bc, be, found, n = p.result()
+        assert bc == refs[i]["best_cost"] and found
+    b.close()
+
+
+def test_parflex_batch_api_matches_parflex(reference):
+    pairs, refs = reference
+    out = pf.parflex_batch(pairs, STD, WTS, 0.1, L=LS)
+    for (best, wp), ref, (F1, F2), Lb in zip(out, refs, pairs, LS):
+        assert best == ref["best_cost"]
+        assert same(wp, ref["wp"])
+        b1, wp1 = pf.parflex(W.cost_matrix_det(F1, F2), STD, WTS, 0.1, L=Lb, profile_dir=None)
+        assert b1 == best and same(wp1, wp)
+
+
+def test_autotuner_picks_candidates_and_stays_exact(oracle_mod):
+    sizes = [(900, 1000), (1000, 1300), (5000, 4500), (4200, 5200)]
+    pairs = _pairs(3, sizes)
+    t = Autotuner(candidates_L=(250, 500), candidates_warps=(4, 16), probe_pairs=2,
+                  bucket_edges=(3000,), repeats=1)
+    Ls, warps = t.choose([(p[0].shape[1], p[1].shape[1]) for p in pairs], STD, WTS, 12)
+    assert set(Ls) <= {250, 500} and warps in (4, 16)
+    assert Ls[0] == Ls[1] and Ls[2] == Ls[3]  # one choice per bucket
+    assert len(t.log) == 8  # 2 buckets x 2 L x 2 warps probes
+    out = pf.parflex_batch(pairs, STD, WTS, 0.1, tuner=t)
+    for (best, wp), (F1, F2), Lb in zip(out, pairs, Ls):
+        ref = oracle_mod.parflex_full(W.cost_matrix_det(F1, F2), STD, WTS, 0.1, Lb)
+        assert best == ref["best_cost"]
+        assert same(wp, ref["wp"])
+
+
+def test_batch_errors():
+    with pytest.raises(ValueError):
+        Batch([(100, 100)], 100, STD, WTS, 17)  # d > 16
+    with pytest.raises(ValueError):
+        Batch([(100, 100)], 100, STD, WTS, 12, warps=5)
+    with pytest.raises(ValueError):
+        Batch([(100, 100)], 100, [(1, 1), (3, 1)], [1, 1], 12)
+    b = Batch([(100, 120)], 50, STD, WTS, 12)
+    with pytest.raises(ValueError):
+        b.load([(np.zeros((12, 99)), np.zeros((12, 120)))])
+    b.close()
+    with pytest.raises(ValueError):
+        pf.parflex_batch([np.zeros((10, 10))], STD, WTS, 0.1, L=8)
