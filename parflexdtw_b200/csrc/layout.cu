@@ -31,13 +31,11 @@ __device__ __forceinline__ void write_skewed(const double* __restrict__ S, doubl
 
 constexpr int kRegionThreads = 512;
 
-template <bool FEAT>
-__global__ void __launch_bounds__(kRegionThreads) k_region_skew(const double* __restrict__ C, int64_t ldc,
-                                                     const double* __restrict__ An,
-                                                     const double* __restrict__ Bn, int d,
-                                                     const Geo g, double* __restrict__ Csk,
-                                                     int64_t stride) {
-    extern __shared__ __align__(16) double S[];  // [64][kWinStride] (+ features)
+__global__ void __launch_bounds__(kRegionThreads) k_region_skew(const double* __restrict__ C,
+                                                               int64_t ldc, const Geo g,
+                                                               double* __restrict__ Csk,
+                                                               int64_t stride) {
+    extern __shared__ __align__(16) double S[];  // [64][kWinStride]
     // blockIdx.x enumerates (tile, step chunk) pairs, blockIdx.y the strip
     const int nchunk = ceil_div32(make_sched2(g.L, g.L, 1).span, kTC);
     const int tile = (int)(blockIdx.x / nchunk), k = blockIdx.y;
@@ -49,89 +47,120 @@ __global__ void __launch_bounds__(kRegionThreads) k_region_skew(const double* __
     const Sched2 sc = make_sched2(R, W, 1);
     if (k >= sc.nS || ts >= sc.span) return;
     const int col0 = ts - 63;  // tile-local column of window column 0
-    if (!FEAT) {
-        // 40 elements per thread, issued as independent loads before the stores
-        constexpr int kPer = 64 * kWinStride / kRegionThreads;
-        double v[kPer];
+    // 40 elements per thread, issued as independent loads before the stores
+    constexpr int kPer = 64 * kWinStride / kRegionThreads;
+    double v[kPer];
 #pragma unroll
-        for (int u = 0; u < kPer; ++u) {
-            const int q = threadIdx.x + u * kRegionThreads;
-            const int rho = q / kWinStride, x = q % kWinStride;
-            const int r = 64 * k + rho, c = col0 + x;
-            v[u] = (r < R && c >= 0 && c < W) ? __ldcs(C + (r0 + r) * ldc + c0 + c) : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < kPer; ++u) S[threadIdx.x + u * kRegionThreads] = v[u];
-    } else {
-        double* sA = S + 64 * kWinStride;        // [kMaxFeat][64]
-        double* sB = sA + kMaxFeat * 64;         // [kMaxFeat][kWinStride]
-        for (int q = threadIdx.x; q < d * 64; q += blockDim.x) {
-            const int f = q / 64, rho = q % 64;
-            const int r = 64 * k + rho;
-            sA[f * 64 + rho] = r < R ? An[(int64_t)f * g.N + r0 + r] : 0.0;
-        }
-        for (int q = threadIdx.x; q < d * kWinStride; q += blockDim.x) {
-            const int f = q / kWinStride, x = q % kWinStride;
-            const int c = col0 + x;
-            sB[f * kWinStride + x] = (c >= 0 && c < W) ? Bn[(int64_t)f * g.M + c0 + c] : 0.0;
-        }
-        __syncthreads();
-        // 4 rows x 5 window columns (stride XB, so neighbouring threads read
-        // neighbouring columns) per thread and pass: 1024 micro-tiles
-        constexpr int XB = kWinStride / 5;  // 64
-        for (int q = threadIdx.x; q < 16 * XB; q += blockDim.x) {
-            const int rg = q / XB, xg = q % XB;
-            double acc[4][5];
-#pragma unroll
-            for (int f = 0; f < kMaxFeat; ++f) {
-                if (f >= d) break;
-                double a[4], b[5];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) a[u] = sA[f * 64 + rg * 4 + u];
-#pragma unroll
-                for (int v = 0; v < 5; ++v) b[v] = sB[f * kWinStride + xg + XB * v];
-#pragma unroll
-                for (int u = 0; u < 4; ++u)
-#pragma unroll
-                    for (int v = 0; v < 5; ++v)
-                        acc[u][v] = f == 0 ? __dmul_rn(a[u], b[v])
-                                           : __dadd_rn(acc[u][v], __dmul_rn(a[u], b[v]));
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int rho = rg * 4 + u, r = 64 * k + rho;
-#pragma unroll
-                for (int v = 0; v < 5; ++v) {
-                    const int x = xg + XB * v, c = col0 + x;
-                    S[rho * kWinStride + x] =
-                        (r < R && c >= 0 && c < W) ? __dsub_rn(1.0, acc[u][v]) : 0.0;
-                }
-            }
-        }
+    for (int u = 0; u < kPer; ++u) {
+        const int q = threadIdx.x + u * kRegionThreads;
+        const int rho = q / kWinStride, x = q % kWinStride;
+        const int r = 64 * k + rho, c = col0 + x;
+        v[u] = (r < R && c >= 0 && c < W) ? __ldcs(C + (r0 + r) * ldc + c0 + c) : 0.0;
     }
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) S[threadIdx.x + u * kRegionThreads] = v[u];
     __syncthreads();
     write_skewed(S, Csk + (int64_t)tile * stride, sc.span, k, ts);
 }
 
-static size_t region_smem(bool feat) {
-    size_t b = (size_t)64 * kWinStride * sizeof(double);
-    if (feat) b += (size_t)kMaxFeat * (64 + kWinStride) * sizeof(double);
-    return b;
+// ---------------------------------------------------------------------------
+// Cost from features straight into the skewed layout.  Lane l of a warp owns
+// rows 64k + 2l (A) and 64k + 2l + 1 (B) of strip k -- the stage-1 mapping --
+// with their d features in registers, and produces 8 consecutive steps
+// tau per pass: A = (64k+2l, tau-2l), B = (64k+2l+1, tau-2l-1), stored as one
+// 16-byte (A, B) pair per lane and step, so a warp writes 512 contiguous bytes
+// per step.  B's column at tau is A's column at tau-1: one pass reads 9
+// column vectors for 16 cells.  Column features of the CTA's window are
+// staged in shared memory split by column parity; at one instruction every
+// lane reads the same parity at consecutive half-indices (conflict-free).
+constexpr int kCT = 256;                // steps per CTA
+constexpr int kCV = 8;                  // steps per register pass
+constexpr int kCostThreads = 256;       // 8 warps x 32 steps
+constexpr int kCX = kCT + 66;           // window columns (x = c - ts + 64), even
+constexpr int kCH = kCX / 2;            // per parity
+
+template <int DMAX>
+__global__ void __launch_bounds__(kCostThreads, 2)
+    k_cost_skew(const double* __restrict__ An, const double* __restrict__ Bn, const int d,
+                const Geo g, double* __restrict__ Csk, const int64_t stride) {
+    extern __shared__ __align__(16) double sB[];  // [d][2][kCH]
+    const int nchunk = ceil_div32(make_sched2(g.L, g.L, 1).span, kCT);
+    const int tile = (int)(blockIdx.x / nchunk), k = blockIdx.y;
+    const int ts = (int)(blockIdx.x % nchunk) * kCT;
+    int64_t r0, c0;
+    int32_t R, W;
+    tile_rect(g, tile / g.n2, tile % g.n2, &r0, &c0, &R, &W);
+    const int span = ceil_div32(W + kStripRows - 1, kBlk) * kBlk;
+    const int nS = ceil_div32(R, kStripRows);
+    if (k >= nS || ts >= span) return;
+    for (int q = threadIdx.x; q < d * kCX; q += kCostThreads) {
+        const int f = q / kCX, x = q - f * kCX;
+        const int c = ts - 64 + x;
+        sB[(f * 2 + (x & 1)) * kCH + (x >> 1)] =
+            (c >= 0 && c < W) ? __ldg(Bn + (int64_t)f * g.M + c0 + c) : 0.0;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int rA = 64 * k + 2 * lane, rB = rA + 1;
+    double aA[DMAX], aB[DMAX];
+#pragma unroll
+    for (int f = 0; f < DMAX; ++f) {
+        aA[f] = (f < d && rA < R) ? __ldg(An + (int64_t)f * g.N + r0 + rA) : 0.0;
+        aB[f] = (f < d && rB < R) ? __ldg(An + (int64_t)f * g.N + r0 + rB) : 0.0;
+    }
+    __syncthreads();
+    double2* out = reinterpret_cast<double2*>(Csk + (int64_t)tile * stride) + (int64_t)k * span * 32 + lane;
+#pragma unroll 1
+    for (int blk = 0; blk < 32 / kCV; ++blk) {
+        const int t0 = ts + 32 * warp + kCV * blk;  // warp-uniform
+        if (t0 >= span) break;
+        // A's column at t0 + v is window x = t0 - ts + 64 - 2*lane + v (even at v = 0);
+        // b[j] holds x = xA0 - 1 + j, j = 0..8 (B at v uses b[v], A uses b[v + 1])
+        const int h0 = ((t0 - ts + 64) >> 1) - lane;  // half-index of xA0
+        double accA[kCV], accB[kCV];
+#pragma unroll
+        for (int f = 0; f < DMAX; ++f) {
+            if (f >= d) break;
+            const double* se = sB + (f * 2) * kCH;  // even x
+            const double* so = se + kCH;             // odd x
+            double b[kCV + 1];
+#pragma unroll
+            for (int j = 0; j <= kCV; ++j) {
+                // x = 2*h0 - 1 + j: odd for even j (half-index h0 - 1 + j/2), even for odd j
+                b[j] = (j & 1) ? se[h0 + (j >> 1)] : so[h0 - 1 + (j >> 1)];
+            }
+#pragma unroll
+            for (int v = 0; v < kCV; ++v) {
+                const double pA = __dmul_rn(aA[f], b[v + 1]);
+                const double pB = __dmul_rn(aB[f], b[v]);
+                accA[v] = f == 0 ? pA : __dadd_rn(accA[v], pA);
+                accB[v] = f == 0 ? pB : __dadd_rn(accB[v], pB);
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < kCV; ++v) {
+            const int tau = t0 + v;
+            if (tau < span) {
+                const int cA = tau - 2 * lane, cB = cA - 1;
+                const double vA = (rA < R && cA >= 0 && cA < W) ? __dsub_rn(1.0, accA[v]) : 0.0;
+                const double vB = (rB < R && cB >= 0 && cB < W) ? __dsub_rn(1.0, accB[v]) : 0.0;
+                __stcs(out + (int64_t)tau * 32, make_double2(vA, vB));
+            }
+        }
+    }
 }
 
-static dim3 region_grid(const Geo& g) {
+static dim3 region_grid(const Geo& g, int per_cta) {
     const Sched2 s = make_sched2(g.L, g.L, 1);
-    return dim3((unsigned)(ceil_div32(s.span, kTC) * (int64_t)g.n1 * g.n2), (unsigned)s.nS, 1);
+    return dim3((unsigned)(ceil_div32(s.span, per_cta) * (int64_t)g.n1 * g.n2), (unsigned)s.nS, 1);
 }
 
 cudaError_t launch_relayout_skew(const double* C, int64_t ldc, const Geo& g, double* Csk,
                                  int64_t stride, cudaStream_t st) {
-    const size_t smem = region_smem(false);
-    cudaError_t e = cudaFuncSetAttribute(k_region_skew<false>,
+    const size_t smem = (size_t)64 * kWinStride * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(k_region_skew,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_region_skew<false><<<region_grid(g), kRegionThreads, smem, st>>>(C, ldc, nullptr, nullptr, 0, g, Csk,
-                                                           stride);
+    k_region_skew<<<region_grid(g, kTC), kRegionThreads, smem, st>>>(C, ldc, g, Csk, stride);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -139,11 +168,13 @@ cudaError_t launch_relayout_skew(const double* C, int64_t ldc, const Geo& g, dou
 cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Geo& g, double* Csk,
                              int64_t stride, cudaStream_t st) {
     if (d < 1 || d > kMaxFeat) return cudaErrorInvalidValue;
-    const size_t smem = region_smem(true);
-    cudaError_t e = cudaFuncSetAttribute(k_region_skew<true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    k_region_skew<true><<<region_grid(g), kRegionThreads, smem, st>>>(nullptr, 0, An, Bn, d, g, Csk, stride);
+    const size_t smem = (size_t)d * kCX * sizeof(double);
+    if (d == 12) {
+        k_cost_skew<12><<<region_grid(g, kCT), kCostThreads, smem, st>>>(An, Bn, d, g, Csk, stride);
+    } else {
+        k_cost_skew<kMaxFeat><<<region_grid(g, kCT), kCostThreads, smem, st>>>(An, Bn, d, g, Csk,
+                                                                             stride);
+    }
     count_launches(1);
     return cudaGetLastError();
 }
