@@ -45,6 +45,12 @@ typedef enum pfx_status {
 
 typedef struct pfx_plan pfx_plan;
 
+/* DP precision of a plan.  PFX_FP64: the plain form, bit-exact with the
+ * reference.  PFX_FP32: the chosen form -- FP32 cost (from a BF16 tensor-core
+ * GEMM when built from features) and FP32 stage-1 DP; stage 2 stays FP64 on
+ * the exactly widened FP32 edge values.  No reference counterpart. */
+typedef enum pfx_precision { PFX_FP64 = 0, PFX_FP32 = 1 } pfx_precision;
+
 /* Human-readable status and the calling thread's last error detail. */
 const char *pfx_status_string(int status);
 const char *pfx_last_error(void);
@@ -69,6 +75,10 @@ int64_t pfx_kernel_launches(void);
  * ------------------------------------------------------------------------- */
 int pfx_plan_create(int64_t N, int64_t M, int32_t L, const int64_t *steps,
                     const double *weights, int32_t n_steps, pfx_plan **out);
+/* pfx_plan_create with a precision (pfx_precision). */
+int pfx_plan_create_ex(int64_t N, int64_t M, int32_t L, const int64_t *steps,
+                       const double *weights, int32_t n_steps, int32_t precision,
+                       pfx_plan **out);
 void pfx_plan_destroy(pfx_plan *plan);
 
 /* info[0..7] = n1, n2, L, hop, n_steps, b_words_per_tile, device_bytes,
@@ -91,7 +101,14 @@ typedef enum pfx_buffer_id {
     PFX_BUF_SEG_NORM = 11,/* f64 [2][max_segs] per-segment best cost/length               */
     PFX_BUF_SEG_META = 12,/* i64 [2][max_segs][6] ci cj edge idx grow gcol (-1 = none)    */
     PFX_BUF_D_PROP = 13,  /* f64 [n1][n2][2][L] snapshot before overlap sync (pfx_snapshot_prop) */
-    PFX_BUF_L_PROP = 14
+    PFX_BUF_L_PROP = 14,
+    PFX_BUF_COST = 15,    /* f64 (f32 in the FP32 form) [n1*n2][strips][span][64]: the
+                             tile-skewed cost slabs; element (k, tau, rho) of a tile is
+                             C[r0 + 64k + rho][c0 + tau - rho], 0 outside the tile;
+                             span = 16 * ceil((W + 63) / 16) of that tile, slab stride
+                             that of an L x L tile */
+    PFX_BUF_FEAT_BF16 = 16 /* bf16 [N + M][Kp] FP32 form: the L2-normalised features
+                             the tensor-core cost GEMM read (rows of F1, then F2) */
 } pfx_buffer_id;
 int pfx_plan_buffer(pfx_plan *plan, int which, void **ptr, int64_t *nbytes);
 
@@ -110,6 +127,18 @@ int pfx_plan_buffer(pfx_plan *plan, int which, void **ptr, int64_t *nbytes);
 int pfx_plan_load_cost(pfx_plan *plan, const double *C, int64_t ldc, void *stream);
 int pfx_plan_load_features(pfx_plan *plan, const double *F1, const double *F2,
                            int32_t d, void *stream);
+/* FP32 plans: loads an FP32 row-major C (pfx_plan_load_cost on an FP32 plan
+ * takes an FP64 C and rounds it to FP32).  Stage 2 of an FP32 plan always
+ * reads the overlap costs from this FP32 copy. */
+int pfx_plan_load_cost_f32(pfx_plan *plan, const float *C, int64_t ldc, void *stream);
+/* FP32 plans: the chosen-form cost from features (F1 d x N, F2 d x M, FP64,
+ * row-major by feature, 1 <= d <= 256): each frame is L2-normalised in FP64
+ * and rounded to bf16, and C = 1 - A^T B is one BF16 x BF16 -> FP32
+ * tensor-core GEMM (tcgen05, TMEM accumulator) whose epilogue writes the FP32
+ * tile-skewed slabs directly.  Replaces cost_matrix_from_features_gpu
+ * (gpu_flexdtw.py:95-109) in the FP32 form. */
+int pfx_plan_load_features_bf16(pfx_plan *plan, const double *F1, const double *F2,
+                                int32_t d, void *stream);
 
 /* Stage 1: FlexDTW on every tile (run_flexdtw_on_tiles, Parflex.py:376-469;
  * GPU variant flexdtw_chunk_from_global_C, gpu_flexdtw.py:288-402).  Writes D

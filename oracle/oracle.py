@@ -18,6 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 
 _f64p = ct.POINTER(ct.c_double)
+_f32p = ct.POINTER(ct.c_float)
 _i64p = ct.POINTER(ct.c_int64)
 _i32p = ct.POINTER(ct.c_int32)
 _u8p = ct.POINTER(ct.c_uint8)
@@ -61,6 +62,13 @@ def lib():
                                      _i64p, _f64p, ct.c_int, ct.c_double,
                                      ct.c_int64, ct.c_int, ct.c_int,
                                      ct.POINTER(_Result)]
+        L.oracle_parflex2.restype = ct.c_int
+        L.oracle_parflex2.argtypes = [_f64p, ct.c_int64, ct.c_int64, ct.c_int64,
+                                      _i64p, _f64p, ct.c_int, ct.c_double,
+                                      ct.c_int64, ct.c_int, ct.c_int, ct.c_int,
+                                      ct.POINTER(_Result)]
+        L.oracle_tile_dp_f32.argtypes = [_f32p, ct.c_int64, ct.c_int64, ct.c_int64,
+                                         _i64p, _f64p, ct.c_int, _f32p, _i32p, _i8p]
         L.oracle_free.argtypes = [ct.POINTER(_Result)]
         L.oracle_result_size.restype = ct.c_int64
         L.oracle_tile_dp.argtypes = [_f64p, ct.c_int64, ct.c_int64, ct.c_int64,
@@ -91,8 +99,11 @@ def _steps_weights(steps, weights):
     return st, w
 
 
-def flexdtw(C, steps, weights, buffer=1):
-    """``FlexDTW.flexdtw`` restated: returns (best_cost, wp, D, P, B)."""
+def flexdtw(C, steps, weights, buffer=1, fp32=False):
+    """``FlexDTW.flexdtw`` restated: returns (best_cost, wp, D, P, B).
+
+    ``fp32``: the FP32 form (C rounded to FP32, DP values in FP32; D is
+    returned widened to FP64)."""
     C = np.ascontiguousarray(C, dtype=np.float64)
     R, W = C.shape
     st, w = _steps_weights(steps, weights)
@@ -100,8 +111,15 @@ def flexdtw(C, steps, weights, buffer=1):
     P = np.empty((R, W), np.int32)
     B = np.empty((R, W), np.int8)
     L = lib()
-    L.oracle_tile_dp(_ptr(C, _f64p), W, R, W, _ptr(st, _i64p), _ptr(w, _f64p),
-                     st.shape[0], _ptr(D, _f64p), _ptr(P, _i32p), _ptr(B, _i8p))
+    if fp32:
+        Cf = np.ascontiguousarray(C, dtype=np.float32)
+        Df = np.empty((R, W), np.float32)
+        L.oracle_tile_dp_f32(_ptr(Cf, _f32p), W, R, W, _ptr(st, _i64p), _ptr(w, _f64p),
+                             st.shape[0], _ptr(Df, _f32p), _ptr(P, _i32p), _ptr(B, _i8p))
+        D[...] = Df
+    else:
+        L.oracle_tile_dp(_ptr(C, _f64p), W, R, W, _ptr(st, _i64p), _ptr(w, _f64p),
+                         st.shape[0], _ptr(D, _f64p), _ptr(P, _i32p), _ptr(B, _i8p))
     br, bc = ct.c_int64(), ct.c_int64()
     best = L.oracle_find_best_endpoint(_ptr(D, _f64p), _ptr(P, _i32p), R, W,
                                        int(buffer), ct.byref(br), ct.byref(bc))
@@ -118,20 +136,24 @@ def _arr(p, n, dtype):
     return np.ctypeslib.as_array(p, shape=(n,)).astype(dtype, copy=True)
 
 
-def parflex_full(C, steps, weights, beta, L, threads=0, tile_wp=False):
+def parflex_full(C, steps, weights, beta, L, threads=0, tile_wp=False, fp32=False):
     """Run the restated ParFlex and return every intermediate as numpy arrays.
 
-    Raises ``ValueError`` with the reference's wording when no endpoint is
-    found (``Parflex.py:1285-1286``).
+    ``fp32``: the FP32 form -- C rounded to FP32 and the tile DP in FP32,
+    stage 2 in FP64 on the widened values.  Raises ``ValueError`` with the
+    reference's wording when no endpoint is found (``Parflex.py:1285-1286``).
     """
     C = np.ascontiguousarray(C, dtype=np.float64)
+    if fp32:
+        C = C.astype(np.float32).astype(np.float64)
     N, M = C.shape
     st, w = _steps_weights(steps, weights)
     res = _Result()
     lb = lib()
-    rc = lb.oracle_parflex(_ptr(C, _f64p), N, M, M, _ptr(st, _i64p),
-                           _ptr(w, _f64p), st.shape[0], float(beta), int(L),
-                           int(threads), int(bool(tile_wp)), ct.byref(res))
+    rc = lb.oracle_parflex2(_ptr(C, _f64p), N, M, M, _ptr(st, _i64p),
+                            _ptr(w, _f64p), st.shape[0], float(beta), int(L),
+                            int(threads), int(bool(tile_wp)), int(bool(fp32)),
+                            ct.byref(res))
     try:
         if rc == -2:
             raise ValueError("Stage 2: No valid endpoint found on global "

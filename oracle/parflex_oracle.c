@@ -24,6 +24,13 @@
  *
  * Arithmetic is IEEE FP64 with no contraction (compile with
  * -ffp-contract=off), matching Numba's non-fastmath code for the DP.
+ *
+ * The FP32 form (oracle_tile_dp_f32, oracle_parflex2 with fp32 = 1) is the
+ * same recurrence with every DP value in FP32 -- cost, accumulated cost,
+ * path cost and the quotient path cost / path length -- and the weights
+ * rounded to FP32; stage 2 then runs in FP64 on the exactly widened FP32
+ * edge values.  It has no counterpart in the reference: it defines the
+ * device's FP32 DP, which the tests hold to it bit for bit.
  * Parity of this restatement is pinned by tests/test_oracle_golden.py
  * against fixtures produced by the reference itself
  * (tests/golden/make_golden.py).
@@ -82,6 +89,57 @@ void oracle_tile_dp(const double *C, int64_t ldc, int64_t R, int64_t W,
                 continue;
             }
             D[row * W + col] = D[bestr * W + bestc] + cval * weights[minidx];
+            B[row * W + col] = (int8_t)minidx;
+            if (bestr == 0)
+                P[row * W + col] = (int32_t)bestc;
+            else if (bestc == 0)
+                P[row * W + col] = (int32_t)(-bestr);
+            else
+                P[row * W + col] = P[bestr * W + bestc];
+        }
+    }
+}
+
+/* FP32 form of oracle_tile_dp (same recurrence, FP32 values). */
+void oracle_tile_dp_f32(const float *C, int64_t ldc, int64_t R, int64_t W,
+                        const int64_t *steps, const double *weights, int S,
+                        float *D, int32_t *P, int8_t *B)
+{
+    float w[ORACLE_MAX_STEPS];
+    for (int s = 0; s < S; ++s) w[s] = (float)weights[s];
+    memset(D, 0, sizeof(float) * (size_t)(R * W));
+    memset(P, 0, sizeof(int32_t) * (size_t)(R * W));
+    memset(B, 0, (size_t)(R * W));
+    for (int64_t c = 0; c < W; ++c) D[c] = C[c];
+    for (int64_t r = 0; r < R; ++r) D[r * W] = C[r * ldc];
+    for (int64_t row = 1; row < R; ++row) {
+        for (int64_t col = 1; col < W; ++col) {
+            const float cval = C[row * ldc + col];
+            float mincost = INFINITY;
+            int minidx = -1;
+            int64_t bestr = -1, bestc = -1;
+            for (int s = 0; s < S; ++s) {
+                int64_t pr = row - steps[2 * s], pc = col - steps[2 * s + 1];
+                if (pr >= 0 && pc >= 0) {
+                    float pathcost = D[pr * W + pc] + cval * w[s];
+                    int64_t pp = P[pr * W + pc];
+                    int64_t mdist = (pp >= 0) ? row + (col - pp) : (row + pp) + col;
+                    float cpm = pathcost / (float)mdist;
+                    if (cpm < mincost) {
+                        mincost = cpm;
+                        minidx = s;
+                        bestr = pr;
+                        bestc = pc;
+                    }
+                }
+            }
+            if (minidx < 0) {
+                D[row * W + col] = D[R * W - 1] + cval * w[S - 1];
+                B[row * W + col] = -1;
+                P[row * W + col] = P[R * W - 1];
+                continue;
+            }
+            D[row * W + col] = D[bestr * W + bestc] + cval * w[minidx];
             B[row * W + col] = (int8_t)minidx;
             if (bestr == 0)
                 P[row * W + col] = (int32_t)bestc;
@@ -214,7 +272,7 @@ void oracle_free(oracle_result *o)
 /* Stage 1 (Parflex.py:376-469) + edge tensors (Parflex.py:509-564). */
 static int stage1(oracle_result *o, const double *C, int64_t ldc,
                   const int64_t *steps, const double *weights, int S,
-                  int threads, int want_tile_wp)
+                  int threads, int want_tile_wp, int fp32)
 {
     const int64_t nt = o->n1 * o->n2, L = o->L;
     int failed = 0;
@@ -227,9 +285,11 @@ static int stage1(oracle_result *o, const double *C, int64_t ldc,
     {
         double *D = (double *)malloc(sizeof(double) * (size_t)(L * L));
         int32_t *P = (int32_t *)malloc(sizeof(int32_t) * (size_t)(L * L));
+        float *Cf = fp32 ? (float *)malloc(sizeof(float) * (size_t)(L * L)) : NULL;
+        float *Df = fp32 ? (float *)malloc(sizeof(float) * (size_t)(L * L)) : NULL;
         int64_t *wpbuf = want_tile_wp ?
             (int64_t *)malloc(sizeof(int64_t) * (size_t)(4 * L + 8)) : NULL;
-        if (!D || !P || (want_tile_wp && !wpbuf)) {
+        if (!D || !P || (want_tile_wp && !wpbuf) || (fp32 && (!Cf || !Df))) {
 #pragma omp atomic write
             failed = 1;
         }
@@ -246,7 +306,15 @@ static int stage1(oracle_result *o, const double *C, int64_t ldc,
                 continue;
             }
             const double *Ct = C + s1 * ldc + s2;
-            oracle_tile_dp(Ct, ldc, R, W, steps, weights, S, D, P, B);
+            if (fp32) {
+                /* C holds FP32 values; the DP runs in FP32, D is widened */
+                for (int64_t r = 0; r < R; ++r)
+                    for (int64_t c = 0; c < W; ++c) Cf[r * W + c] = (float)Ct[r * ldc + c];
+                oracle_tile_dp_f32(Cf, W, R, W, steps, weights, S, Df, P, B);
+                for (int64_t q = 0; q < R * W; ++q) D[q] = (double)Df[q];
+            } else {
+                oracle_tile_dp(Ct, ldc, R, W, steps, weights, S, D, P, B);
+            }
             o->tile_B[t] = B;
             if (want_tile_wp) {
                 int64_t br, bc;
@@ -274,7 +342,7 @@ static int stage1(oracle_result *o, const double *C, int64_t ldc,
                 }
             }
         }
-        free(D); free(P); free(wpbuf);
+        free(D); free(P); free(Cf); free(Df); free(wpbuf);
     }
     return failed ? -1 : 0;
 }
@@ -700,10 +768,10 @@ static void scan_edges(oracle_result *o, int64_t buf)
 /* Full ParFlex on a host cost matrix (Parflex.py:1510-1547), keeping every
  * intermediate for the tests.  Returns 0, or -1 on allocation failure, or
  * -2 when stage 2 finds no endpoint (the reference raises ValueError). */
-int oracle_parflex(const double *C, int64_t N, int64_t M, int64_t ldc,
-                   const int64_t *steps, const double *weights, int S,
-                   double beta, int64_t L, int threads, int want_tile_wp,
-                   oracle_result *o)
+int oracle_parflex2(const double *C, int64_t N, int64_t M, int64_t ldc,
+                    const int64_t *steps, const double *weights, int S,
+                    double beta, int64_t L, int threads, int want_tile_wp,
+                    int fp32, oracle_result *o)
 {
     memset(o, 0, sizeof(*o));
     if (N < 2 || M < 2 || L < 2 || S < 1 || S > ORACLE_MAX_STEPS) return -3;
@@ -745,7 +813,7 @@ int oracle_parflex(const double *C, int64_t N, int64_t M, int64_t ldc,
         o->D_prop[q] = INFINITY;
         o->L_prop[q] = INFINITY;
     }
-    if (stage1(o, C, ldc, steps, weights, S, threads, want_tile_wp)) return -1;
+    if (stage1(o, C, ldc, steps, weights, S, threads, want_tile_wp, fp32)) return -1;
     build_valid_mask(o);
     propagate(o);
     memcpy(o->D_arr, o->D_prop, sizeof(double) * (size_t)n4);
@@ -762,6 +830,15 @@ int oracle_parflex(const double *C, int64_t N, int64_t M, int64_t ldc,
                               o->best_end[4], o->best_end[5], o->wp,
                               o->tile_order, &o->n_stitch);
     return 0;
+}
+
+int oracle_parflex(const double *C, int64_t N, int64_t M, int64_t ldc,
+                   const int64_t *steps, const double *weights, int S,
+                   double beta, int64_t L, int threads, int want_tile_wp,
+                   oracle_result *o)
+{
+    return oracle_parflex2(C, N, M, ldc, steps, weights, S, beta, L, threads,
+                           want_tile_wp, 0, o);
 }
 
 /* Size of oracle_result, so the Python side can check its struct layout. */

@@ -28,11 +28,14 @@ PFX_ERR_NO_ENDPOINT = 4
 PFX_ERR_TOO_LARGE = 5
 PFX_ERR_NO_DEVICE = 6
 
+PFX_FP64 = 0
+PFX_FP32 = 1
+
 NO_ENDPOINT_MSG = "Stage 2: No valid endpoint found on global top/right edges."
 
 BUF = dict(EDGE_D=0, EDGE_P=1, BACKPTR=2, EDGE_CF=3, VALID=4, D_ARR=5, L_ARR=6,
            TOP_D=7, TOP_L=8, RIGHT_D=9, RIGHT_L=10, SEG_NORM=11, SEG_META=12,
-           D_PROP=13, L_PROP=14)
+           D_PROP=13, L_PROP=14, COST=15, FEAT_BF16=16)
 
 # (name, restype, argtypes) for every exported symbol of the header
 SIGNATURES = [
@@ -41,11 +44,15 @@ SIGNATURES = [
     ("pfx_version", ct.c_int, []),
     ("pfx_kernel_launches", ct.c_int64, []),
     ("pfx_plan_create", ct.c_int, [_i64, _i64, _i32, _i64p, _f64p, _i32, ct.POINTER(_vp)]),
+    ("pfx_plan_create_ex", ct.c_int, [_i64, _i64, _i32, _i64p, _f64p, _i32, _i32,
+                                      ct.POINTER(_vp)]),
     ("pfx_plan_destroy", None, [_vp]),
     ("pfx_plan_info", ct.c_int, [_vp, _i64p]),
     ("pfx_plan_buffer", ct.c_int, [_vp, ct.c_int, ct.POINTER(_vp), _i64p]),
     ("pfx_plan_load_cost", ct.c_int, [_vp, _vp, _i64, _vp]),
     ("pfx_plan_load_features", ct.c_int, [_vp, _vp, _vp, _i32, _vp]),
+    ("pfx_plan_load_cost_f32", ct.c_int, [_vp, _vp, _i64, _vp]),
+    ("pfx_plan_load_features_bf16", ct.c_int, [_vp, _vp, _vp, _i32, _vp]),
     ("pfx_stage1", ct.c_int, [_vp, _vp, _i64, _vp]),
     ("pfx_stage2_propagate", ct.c_int, [_vp, _vp, _i64, _vp]),
     ("pfx_snapshot_prop", ct.c_int, [_vp, _vp]),

@@ -142,7 +142,7 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
         pfx_plan& p = b->plans[i];
         memset(&p, 0, sizeof(p));
         p.arena_mode = 1;
-        if ((st = plan_init(&p, N[i], M[i], L[i], steps, weights, n_steps, nw ? nw : 16))) {
+        if ((st = plan_init(&p, N[i], M[i], L[i], steps, weights, n_steps, nw ? nw : 16, 0))) {
             batch_free(b);
             return st;
         }
@@ -150,7 +150,7 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
         arena += round256(p.bytes);
         feat_off[i] = arena;
         arena += round256((size_t)d * (N[i] + M[i]) * 8);
-        slab[i] = (int64_t)p.g.n1 * p.g.n2 * p.skew_stride * 8;
+        slab[i] = plan_slab_bytes(&p);
         maxL = std::max(maxL, p.g.L);
         b->total_tiles += (int64_t)p.g.n1 * p.g.n2;
         for (int t = 0; t < p.g.n1 * p.g.n2; ++t) {
@@ -256,13 +256,13 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
         memset(&p, 0, sizeof(p));
         p.arena_mode = 2;
         p.arena = b->arena + plan_off[i];
-        if ((st = plan_init(&p, N[i], M[i], L[i], steps, weights, n_steps, b->nw))) {
+        if ((st = plan_init(&p, N[i], M[i], L[i], steps, weights, n_steps, b->nw, 0))) {
             batch_free(b);
             return st;
         }
         p.feat = reinterpret_cast<double*>(b->arena + feat_off[i]);
         p.feat_d = d;
-        p.Csk = reinterpret_cast<double*>(reinterpret_cast<char*>(b->slabs) + pool_off[i]);
+        p.Csk = reinterpret_cast<char*>(b->slabs) + pool_off[i];
         p.cost_loaded = 1;
         p.s1.status = b->status;
         b->fin_off[i] = (int64_t)(fo / 8);
@@ -362,11 +362,11 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
             double* Bn = p.feat + (int64_t)b->d * p.g.N;
             BCK(launch_l2norm(F1, b->d, p.g.N, An, s));
             BCK(launch_l2norm(F2, b->d, p.g.M, Bn, s));
-            BCK(launch_cost_skew(An, Bn, b->d, p.g, p.Csk, p.skew_stride, s));
+            BCK(launch_cost_skew(An, Bn, b->d, p.g, static_cast<double*>(p.Csk), p.skew_stride, s));
         }
         BCK(mark(w, 1));
         BCK(launch_stage1_queue(b->descs + b->wave_desc_off[w], (int)b->wave_tiles[w], b->heads + w,
-                                b->gq, b->status, b->nw, s));
+                                b->gq, b->status, b->nw, false, s));
         BCK(mark(w, 2));
         BCK(cudaEventRecord(b->fork_ev, s));
         const int nside = std::min(kSide, q1 - q0);

@@ -155,9 +155,10 @@ extern "C" void pfx_plan_destroy(pfx_plan* p) {
 // arena selected by p->arena_mode).  The tile-skewed cost slabs and the tile
 // queue are separate (plan_attach_cost).
 int pfx::plan_init(pfx_plan* p, int64_t N, int64_t M, int32_t L, const int64_t* steps,
-                   const double* weights, int32_t n_steps, int nw) {
+                   const double* weights, int32_t n_steps, int nw, int fp32) {
     int st = make_geo(N, M, L, steps, weights, n_steps, &p->g);
     if (st) return st;
+    p->fp32 = fp32 ? 1 : 0;
     cudaGetDevice(&p->device);
     const Geo& g = p->g;
     const int64_t nt = (int64_t)g.n1 * g.n2;
@@ -219,7 +220,7 @@ int pfx::plan_init(pfx_plan* p, int64_t N, int64_t M, int32_t L, const int64_t* 
 
 // Tile descriptors of plan p with cost slabs at Csk, in queue order (largest
 // tile first, then row-major tile index).
-void pfx::plan_tile_descs(const pfx_plan* p, const double* Csk, TileDesc* out) {
+void pfx::plan_tile_descs(const pfx_plan* p, const void* Csk, TileDesc* out) {
     const Geo& g = p->g;
     const int nt = g.n1 * g.n2;
     std::vector<int> order(nt);
@@ -237,7 +238,7 @@ void pfx::plan_tile_descs(const pfx_plan* p, const double* Csk, TileDesc* out) {
         TileDesc d;
         memset(&d, 0, sizeof(d));
         tile_rect(g, t / g.n2, t % g.n2, &r0, &c0, &d.R, &d.W);
-        d.Csk = Csk + (int64_t)t * p->skew_stride;
+        d.Csk = static_cast<const char*>(Csk) + (int64_t)t * p->skew_stride * (p->fp32 ? 4 : 8);
         d.Bw = p->s1.Bw + (int64_t)t * g.b_words;
         d.eD = p->s1.edge_D + (int64_t)t * 2 * g.L;
         d.eP = p->s1.edge_P + (int64_t)t * 2 * g.L;
@@ -248,14 +249,22 @@ void pfx::plan_tile_descs(const pfx_plan* p, const double* Csk, TileDesc* out) {
 
 extern "C" int pfx_plan_create(int64_t N, int64_t M, int32_t L, const int64_t* steps,
                                const double* weights, int32_t n_steps, pfx_plan** out) {
+    return pfx_plan_create_ex(N, M, L, steps, weights, n_steps, PFX_FP64, out);
+}
+
+extern "C" int pfx_plan_create_ex(int64_t N, int64_t M, int32_t L, const int64_t* steps,
+                                  const double* weights, int32_t n_steps, int32_t precision,
+                                  pfx_plan** out) {
     if (!out || !steps || !weights) return fail(PFX_ERR_ARG, "null argument");
+    if (precision != PFX_FP64 && precision != PFX_FP32)
+        return fail(PFX_ERR_ARG, "precision %d: PFX_FP64 (0) or PFX_FP32 (1)", precision);
     *out = nullptr;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(PFX_ERR_NO_DEVICE, "no CUDA device");
     pfx_plan* p = (pfx_plan*)calloc(1, sizeof(pfx_plan));
     if (!p) return fail(PFX_ERR_ARG, "out of host memory");
-    int st = plan_init(p, N, M, L, steps, weights, n_steps, 0);
+    int st = plan_init(p, N, M, L, steps, weights, n_steps, 0, precision == PFX_FP32);
     if (st) {
         pfx_plan_destroy(p);
         return st;
@@ -296,6 +305,16 @@ extern "C" int pfx_plan_buffer(pfx_plan* p, int which, void** ptr, int64_t* nbyt
         case PFX_BUF_SEG_META: *ptr = p->s2.seg_meta; *nbytes = 12 * ms * 8; break;
         case PFX_BUF_D_PROP: *ptr = p->D_prop; *nbytes = n4 * 8; break;
         case PFX_BUF_L_PROP: *ptr = p->L_prop; *nbytes = n4 * 8; break;
+        case PFX_BUF_FEAT_BF16:
+            if (!p->fbf) return fail(PFX_ERR_ARG, "no bf16 features in the plan");
+            *ptr = p->fbf;
+            *nbytes = (p->g.N + p->g.M) * p->fbf_kp * 2;
+            break;
+        case PFX_BUF_COST:
+            if (!p->Csk) return fail(PFX_ERR_ARG, "no cost loaded into the plan");
+            *ptr = p->Csk;
+            *nbytes = plan_slab_bytes(p);
+            break;
         default: return fail(PFX_ERR_ARG, "unknown buffer id %d", which);
     }
     return PFX_OK;
@@ -311,8 +330,10 @@ static int check_ldc(const pfx_plan* p, const double* C, int64_t ldc) {
 // the plan's tile queue pointing at them.
 static int ensure_cost_buffer(pfx_plan* p) {
     if (p->Csk) return PFX_OK;
-    int st = plan_alloc(p, &p->Csk, (size_t)p->g.n1 * p->g.n2 * p->skew_stride);
+    char* slabs = nullptr;
+    int st = plan_alloc(p, &slabs, (size_t)plan_slab_bytes(p));
     if (st) return st;
+    p->Csk = slabs;
     std::vector<TileDesc> d((size_t)p->g.n1 * p->g.n2);
     plan_tile_descs(p, p->Csk, d.data());
     CK(cudaMemcpy(p->descs, d.data(), d.size() * sizeof(TileDesc), cudaMemcpyHostToDevice));
@@ -324,7 +345,25 @@ extern "C" int pfx_plan_load_cost(pfx_plan* p, const double* C, int64_t ldc, voi
     int st = check_ldc(p, C, ldc);
     if (st) return st;
     if ((st = ensure_cost_buffer(p))) return st;
-    CK(launch_relayout_skew(C, ldc, p->g, p->Csk, p->skew_stride, (cudaStream_t)stream));
+    if (p->fp32)
+        CK(launch_relayout_skew_f32(C, nullptr, ldc, p->g, static_cast<float*>(p->Csk),
+                                    p->skew_stride, (cudaStream_t)stream));
+    else
+        CK(launch_relayout_skew(C, ldc, p->g, static_cast<double*>(p->Csk), p->skew_stride,
+                                (cudaStream_t)stream));
+    p->cost_loaded = 1;
+    return PFX_OK;
+}
+
+extern "C" int pfx_plan_load_cost_f32(pfx_plan* p, const float* C, int64_t ldc, void* stream) {
+    if (!p) return fail(PFX_ERR_ARG, "null plan");
+    if (!p->fp32) return fail(PFX_ERR_ARG, "pfx_plan_load_cost_f32 needs an FP32 plan");
+    if (!C) return fail(PFX_ERR_ARG, "null cost matrix");
+    if (ldc < p->g.M) return fail(PFX_ERR_ARG, "ldc=%lld < M=%lld", (long long)ldc, (long long)p->g.M);
+    int st;
+    if ((st = ensure_cost_buffer(p))) return st;
+    CK(launch_relayout_skew_f32(nullptr, C, ldc, p->g, static_cast<float*>(p->Csk),
+                                p->skew_stride, (cudaStream_t)stream));
     p->cost_loaded = 1;
     return PFX_OK;
 }
@@ -332,6 +371,7 @@ extern "C" int pfx_plan_load_cost(pfx_plan* p, const double* C, int64_t ldc, voi
 extern "C" int pfx_plan_load_features(pfx_plan* p, const double* F1, const double* F2, int32_t d,
                                       void* stream) {
     if (!p || !F1 || !F2) return fail(PFX_ERR_ARG, "null argument");
+    if (p->fp32) return fail(PFX_ERR_ARG, "FP32 plans build their cost with pfx_plan_load_features_bf16");
     if (d < 1 || d > 16)
         return fail(PFX_ERR_ARG, "feature dimension %d: the fused cost layout takes 1..16", d);
     int st;
@@ -346,7 +386,34 @@ extern "C" int pfx_plan_load_features(pfx_plan* p, const double* F1, const doubl
     double* Bn = p->feat + (int64_t)d * p->g.N;
     CK(launch_l2norm(F1, d, p->g.N, An, s));
     CK(launch_l2norm(F2, d, p->g.M, Bn, s));
-    CK(launch_cost_skew(An, Bn, d, p->g, p->Csk, p->skew_stride, s));
+    CK(launch_cost_skew(An, Bn, d, p->g, static_cast<double*>(p->Csk), p->skew_stride, s));
+    p->cost_loaded = 1;
+    return PFX_OK;
+}
+
+extern "C" int pfx_plan_load_features_bf16(pfx_plan* p, const double* F1, const double* F2,
+                                           int32_t d, void* stream) {
+    if (!p || !F1 || !F2) return fail(PFX_ERR_ARG, "null argument");
+    if (!p->fp32) return fail(PFX_ERR_ARG, "pfx_plan_load_features_bf16 needs an FP32 plan");
+    if (d < 1 || d > 256)
+        return fail(PFX_ERR_ARG, "feature dimension %d: the tensor-core cost takes 1..256", d);
+    const int kp = (d + 63) / 64 * 64;
+    int st;
+    if ((st = ensure_cost_buffer(p))) return st;
+    if (p->fbf && p->fbf_kp < kp) return fail(PFX_ERR_ARG, "feature dimension grew");
+    if (!p->fbf) {
+        char* q = nullptr;
+        if ((st = plan_alloc(p, &q, (size_t)(p->g.N + p->g.M) * kp * 2))) return st;
+        p->fbf = q;
+        p->fbf_kp = kp;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    char* A = static_cast<char*>(p->fbf);
+    char* B = A + (size_t)p->g.N * p->fbf_kp * 2;
+    CK(launch_features_bf16(F1, d, p->g.N, p->fbf_kp, A, s));
+    CK(launch_features_bf16(F2, d, p->g.M, p->fbf_kp, B, s));
+    CK(launch_gemm_cost_skew(A, B, p->fbf_kp, p->g, static_cast<float*>(p->Csk), p->skew_stride,
+                             p->s1.status, s));
     p->cost_loaded = 1;
     return PFX_OK;
 }
@@ -358,21 +425,25 @@ extern "C" int pfx_stage1(pfx_plan* p, const double* C, int64_t ldc, void* strea
     if (!p->cost_loaded) return fail(PFX_ERR_ARG, "no cost matrix loaded into the plan");
     cudaStream_t s = (cudaStream_t)stream;
     CK(cudaMemsetAsync(p->head, 0, sizeof(int), s));
-    CK(launch_stage1_queue(p->descs, p->g.n1 * p->g.n2, p->head, p->g, p->s1.status, p->nw, s));
+    CK(launch_stage1_queue(p->descs, p->g.n1 * p->g.n2, p->head, p->g, p->s1.status, p->nw,
+                           p->fp32 != 0, s));
     return PFX_OK;
 }
 
 extern "C" int pfx_stage2_propagate(pfx_plan* p, const double* C, int64_t ldc, void* stream) {
     if (!p) return fail(PFX_ERR_ARG, "null plan");
     Geo g = p->g;
-    if (C) {
+    if (C && !p->fp32) {
         int st = check_ldc(p, C, ldc);
         if (st) return st;
         g.ldc = ldc;
     } else if (!p->cost_loaded) {
         return fail(PFX_ERR_ARG, "no cost matrix loaded into the plan");
     }
-    CK(launch_stage2(C, p->Csk, p->skew_stride, g, p->s2, (cudaStream_t)stream));
+    // the FP32 form reads overlap costs from its own FP32 slabs (the values
+    // its DP used), never from an FP64 C
+    CK(launch_stage2(p->fp32 ? nullptr : C, p->Csk, p->skew_stride, p->fp32 != 0, g, p->s2,
+                     (cudaStream_t)stream));
     return PFX_OK;
 }
 
@@ -429,7 +500,7 @@ extern "C" int pfx_result(pfx_plan* p, void* stream, double* best_cost, int64_t*
     CK(cudaStreamSynchronize(s));
     if (kst) {
         cudaMemsetAsync(p->s1.status, 0, 4, s);
-        return fail(PFX_ERR_CUDA, "stage-1 wavefront wait ran out (status %d); results invalid",
+        return fail(PFX_ERR_CUDA, "a bounded device wait ran out (status %d: 1 stage-1 wavefront, 2 cost GEMM); results invalid",
                     kst);
     }
     if (best_cost) *best_cost = b;

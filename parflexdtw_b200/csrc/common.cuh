@@ -124,7 +124,7 @@ struct S1Out {
 // One stage-1 work item: a tile of one alignment, with the addresses of its
 // inputs and outputs (the stage-1 kernel claims these from a device queue).
 struct TileDesc {
-    const double* Csk;  // tile-skewed cost slab
+    const void* Csk;    // tile-skewed cost slab (FP64, or FP32 in the FP32 form)
     uint32_t* Bw;       // packed backpointers
     double* eD;         // [2][L] D on the top / right edge
     int32_t* eP;        // [2][L] start encodings on the edges
@@ -176,11 +176,20 @@ void count_launches(int n);
 // weights of g; tiles at most g.L x g.L); `*head` must be 0 at launch; nw in
 // {4, 8, 16} warps per tile.
 cudaError_t launch_stage1_queue(const TileDesc* descs, int ntiles, int* head, const Geo& g,
-                                int32_t* status, int nw, cudaStream_t st);
+                                int32_t* status, int nw, bool fp32, cudaStream_t st);
 // Smallest valid warps-per-tile choice heuristic for `ntiles` tiles of length L.
 int stage1_queue_warps(int ntiles, int32_t L, int num_sms);
 cudaError_t launch_relayout_skew(const double* C, int64_t ldc, const Geo& g, double* Csk,
                                  int64_t skew_stride, cudaStream_t st);
+// FP32 form cost from features (gemm_bf16.cu): bf16 rows of L2-normalised
+// features, then 1 - A B^T on the tensor cores into FP32 skewed slabs.
+cudaError_t launch_features_bf16(const double* F, int d, int64_t n, int Kp, void* out,
+                                 cudaStream_t st);
+cudaError_t launch_gemm_cost_skew(const void* Abf, const void* Bbf, int Kp, const Geo& g,
+                                  float* Csk, int64_t stride, int32_t* status, cudaStream_t st);
+// FP32 slabs from a row-major FP64 (rounded) or FP32 C (exactly one non-null).
+cudaError_t launch_relayout_skew_f32(const double* C64, const float* C32, int64_t ldc,
+                                     const Geo& g, float* Csk, int64_t stride, cudaStream_t st);
 cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Geo& g, double* Csk,
                              int64_t skew_stride, cudaStream_t st);
 cudaError_t launch_l2norm(const double* F, int d, int64_t n, double* out, cudaStream_t st);
@@ -189,8 +198,8 @@ cudaError_t launch_stage1(const double* C, const Geo& g, const S1Out& o, int til
 size_t stage1_smem_bytes_host(int32_t L, int nw);
 int stage1_pick_warps(const Geo& g, int num_sms);
 cudaError_t launch_fill(double* p, int64_t n, double v, cudaStream_t st);
-cudaError_t launch_stage2(const double* C, const double* Csk, int64_t skew_stride, const Geo& g,
-                          const S2Buf& b, cudaStream_t st);
+cudaError_t launch_stage2(const double* C, const void* Csk, int64_t skew_stride, bool f32,
+                          const Geo& g, const S2Buf& b, cudaStream_t st);
 cudaError_t launch_sync_scan(const Geo& g, const S2Buf& b, int64_t buf, cudaStream_t st);
 cudaError_t launch_stitch(const Geo& g, const S2Buf& b, cudaStream_t st, int from_best,
                           int64_t si, int64_t sj, int64_t se, int64_t sx);

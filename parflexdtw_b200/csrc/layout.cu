@@ -19,7 +19,8 @@ constexpr int kWinStride = kTC + 64;   // window columns (TC + 63 used, 1 pad); 
                                        // diagonal read stride 319 is odd: conflict-free
 constexpr int kMaxFeat = 16;           // features staged in shared memory
 
-__device__ __forceinline__ void write_skewed(const double* __restrict__ S, double* __restrict__ Cs,
+template <typename T>
+__device__ __forceinline__ void write_skewed(const T* __restrict__ S, T* __restrict__ Cs,
                                              int span, int k, int ts) {
     const int nt = (span - ts) < kTC ? (span - ts) : kTC;
     for (int q = threadIdx.x; q < nt * 64; q += blockDim.x) {
@@ -31,11 +32,14 @@ __device__ __forceinline__ void write_skewed(const double* __restrict__ S, doubl
 
 constexpr int kRegionThreads = 512;
 
-__global__ void __launch_bounds__(kRegionThreads) k_region_skew(const double* __restrict__ C,
+// Row-major C (Tin) -> skewed slabs (Tout; FP64 -> FP32 rounds to nearest).
+template <typename Tin, typename Tout>
+__global__ void __launch_bounds__(kRegionThreads) k_region_skew(const Tin* __restrict__ C,
                                                                int64_t ldc, const Geo g,
-                                                               double* __restrict__ Csk,
+                                                               Tout* __restrict__ Csk,
                                                                int64_t stride) {
-    extern __shared__ __align__(16) double S[];  // [64][kWinStride]
+    extern __shared__ __align__(16) unsigned char S_raw[];
+    Tout* S = reinterpret_cast<Tout*>(S_raw);  // [64][kWinStride]
     // blockIdx.x enumerates (tile, step chunk) pairs, blockIdx.y the strip
     const int nchunk = ceil_div32(make_sched2(g.L, g.L, 1).span, kTC);
     const int tile = (int)(blockIdx.x / nchunk), k = blockIdx.y;
@@ -49,13 +53,13 @@ __global__ void __launch_bounds__(kRegionThreads) k_region_skew(const double* __
     const int col0 = ts - 63;  // tile-local column of window column 0
     // 40 elements per thread, issued as independent loads before the stores
     constexpr int kPer = 64 * kWinStride / kRegionThreads;
-    double v[kPer];
+    Tout v[kPer];
 #pragma unroll
     for (int u = 0; u < kPer; ++u) {
         const int q = threadIdx.x + u * kRegionThreads;
         const int rho = q / kWinStride, x = q % kWinStride;
         const int r = 64 * k + rho, c = col0 + x;
-        v[u] = (r < R && c >= 0 && c < W) ? __ldcs(C + (r0 + r) * ldc + c0 + c) : 0.0;
+        v[u] = (r < R && c >= 0 && c < W) ? (Tout)__ldcs(C + (r0 + r) * ldc + c0 + c) : (Tout)0;
     }
 #pragma unroll
     for (int u = 0; u < kPer; ++u) S[threadIdx.x + u * kRegionThreads] = v[u];
@@ -154,15 +158,27 @@ static dim3 region_grid(const Geo& g, int per_cta) {
     return dim3((unsigned)(ceil_div32(s.span, per_cta) * (int64_t)g.n1 * g.n2), (unsigned)s.nS, 1);
 }
 
-cudaError_t launch_relayout_skew(const double* C, int64_t ldc, const Geo& g, double* Csk,
-                                 int64_t stride, cudaStream_t st) {
-    const size_t smem = (size_t)64 * kWinStride * sizeof(double);
-    cudaError_t e = cudaFuncSetAttribute(k_region_skew,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+template <typename Tin, typename Tout>
+static cudaError_t relayout_t(const Tin* C, int64_t ldc, const Geo& g, Tout* Csk, int64_t stride,
+                              cudaStream_t st) {
+    const size_t smem = (size_t)64 * kWinStride * sizeof(Tout);
+    auto kern = k_region_skew<Tin, Tout>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
     if (e != cudaSuccess) return e;
-    k_region_skew<<<region_grid(g, kTC), kRegionThreads, smem, st>>>(C, ldc, g, Csk, stride);
+    kern<<<region_grid(g, kTC), kRegionThreads, smem, st>>>(C, ldc, g, Csk, stride);
     count_launches(1);
     return cudaGetLastError();
+}
+
+cudaError_t launch_relayout_skew(const double* C, int64_t ldc, const Geo& g, double* Csk,
+                                 int64_t stride, cudaStream_t st) {
+    return relayout_t(C, ldc, g, Csk, stride, st);
+}
+
+cudaError_t launch_relayout_skew_f32(const double* C64, const float* C32, int64_t ldc,
+                                     const Geo& g, float* Csk, int64_t stride, cudaStream_t st) {
+    return C32 ? relayout_t(C32, ldc, g, Csk, stride, st) : relayout_t(C64, ldc, g, Csk, stride, st);
 }
 
 cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Geo& g, double* Csk,

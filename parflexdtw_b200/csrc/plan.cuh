@@ -18,10 +18,13 @@ struct pfx_plan {
     int nblocks;
     // tile-skewed cost (allocated on first load, or attached by a batch) and
     // normalised features
-    double* Csk;
-    int64_t skew_stride;  // doubles per tile slab
+    void* Csk;            // FP64 slabs, or FP32 in the FP32 form
+    int64_t skew_stride;  // elements per tile slab
+    int fp32;             // 1: FP32 form (FP32 cost slabs and stage-1 DP)
     double* feat;         // d*(N+M) doubles
     int feat_d;
+    void* fbf;            // FP32 form: bf16 features, [N + M][fbf_kp]
+    int fbf_kp;
     int cost_loaded;
     // stage-1 tile queue of this plan (descriptors in queue order) and its head
     pfx::TileDesc* descs;
@@ -35,7 +38,10 @@ struct pfx_plan {
 
 namespace pfx {
 int plan_init(pfx_plan* p, int64_t N, int64_t M, int32_t L, const int64_t* steps,
-              const double* weights, int32_t n_steps, int nw);
-void plan_tile_descs(const pfx_plan* p, const double* Csk, TileDesc* out);
+              const double* weights, int32_t n_steps, int nw, int fp32);
+void plan_tile_descs(const pfx_plan* p, const void* Csk, TileDesc* out);
+inline int64_t plan_slab_bytes(const pfx_plan* p) {
+    return (int64_t)p->g.n1 * p->g.n2 * p->skew_stride * (p->fp32 ? 4 : 8);
+}
 int num_sms_cur();
 }  // namespace pfx

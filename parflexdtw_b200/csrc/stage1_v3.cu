@@ -50,6 +50,16 @@ namespace pfx {
 
 constexpr int kSpinLimit = 1 << 22;
 
+// IEEE arithmetic of the DP's value type (FP64 plain form, FP32 chosen form),
+// rounded to nearest, never contracted.
+__device__ __forceinline__ double addr(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float addr(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double mulr(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mulr(float a, float b) { return __fmul_rn(a, b); }
+template <typename T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
 // Exact RN(b/nd) < RN(a/md) (nd, md positive integers), per lane, no warp
 // collectives.  Division only when the cross products cannot decide.
 __device__ __forceinline__ bool qless_exact(double b, double nd, double a, double md) {
@@ -65,24 +75,38 @@ __device__ __forceinline__ bool qless_exact(double b, double nd, double a, doubl
     return __ddiv_rn(b, nd) < __ddiv_rn(a, md);
 }
 
+// FP32 form: RN32(b/nd) < RN32(a/md).  The cross products of two FP32 values
+// and two integers below 2^24 are exact in FP64, so their difference has the
+// sign of the exact comparison: <= 0 decides "not less"; a relative margin of
+// 2^-21 (two FP32 roundings are at most 2^-24 each) decides "less"; in
+// between the two IEEE divisions decide.
+__device__ __forceinline__ bool qless_exact(float b, float nd, float a, float md) {
+    const double U = __dmul_rn((double)b, (double)md);
+    const double V = __dmul_rn((double)a, (double)nd);
+    const double diff = __dadd_rn(V, -U);
+    if (diff <= 0.0) return false;
+    if (diff > __dmul_rn(__dadd_rn(fabs(U), fabs(V)), 0x1p-21)) return true;
+    return __fdiv_rn(b, nd) < __fdiv_rn(a, md);
+}
+
 // Exact selection of one cell with r, c >= 1 (generic steps, any position).
-template <bool STD, bool ALLIN>
-__device__ __forceinline__ void select_exact(const Geo& g, double w_last, int r, int c, double rc,
-                                          double cval, double x1D, int x1P, double x2D, int x2P,
-                                          double x3D, int x3P, double& oD, int& oP, int& code) {
+template <bool STD, bool ALLIN, typename T>
+__device__ __forceinline__ void select_exact(const Geo& g, T w_last, int r, int c, T rc, T cval,
+                                          T x1D, int x1P, T x2D, int x2P, T x3D, int x3P, T& oD,
+                                          int& oP, int& code) {
     int bs = -1, bk = 0, bP = 0;
-    double bA = 0.0, bM = 1.0;
+    T bA = 0, bM = 1;
 #pragma unroll
     for (int s = 0; s < 3; ++s) {
         if (!STD && s >= g.S) continue;
         const int kd = STD ? s : g.kind[s];
         const bool inb = ALLIN || kd == 0 || (kd == 1 ? c >= 2 : r >= 2);
         if (!inb) continue;
-        const double pD = kd == 0 ? x1D : (kd == 1 ? x2D : x3D);
+        const T pD = kd == 0 ? x1D : (kd == 1 ? x2D : x3D);
         const int pP = kd == 0 ? x1P : (kd == 1 ? x2P : x3P);
-        const double a = __dadd_rn(pD, __dmul_rn(cval, g.w[s]));
-        const double md = __dadd_rn(rc, -fabs((double)pP));
-        const bool take = bs < 0 ? a < CUDART_INF : qless_exact(a, md, bA, bM);
+        const T a = addr(pD, mulr(cval, (T)g.w[s]));
+        const T md = addr(rc, -fabs((T)pP));
+        const bool take = bs < 0 ? a < (T)CUDART_INF : qless_exact(a, md, bA, bM);
         if (take) {
             bs = s;
             bk = kd;
@@ -93,7 +117,7 @@ __device__ __forceinline__ void select_exact(const Geo& g, double w_last, int r,
     }
     if (bs < 0) {
         // reference: D[-1,-1] (still 0) + C * w[-1], P[-1,-1] (0), B = -1
-        oD = __dadd_rn(0.0, __dmul_rn(cval, w_last));
+        oD = addr((T)0, mulr(cval, w_last));
         oP = 0;
         code = 3;
     } else {
@@ -148,47 +172,88 @@ __device__ __forceinline__ bool select_fast_std(const Geo& g, int r, int c, doub
     return a0 < CUDART_INF && ok1 && ok2;
 }
 
+// FP32 form of select_fast_std: FP32 path costs, exact FP64 cross products
+// (see the FP32 qless_exact) for the two comparisons.
+template <bool EDGE>
+__device__ __forceinline__ bool select_fast_std(const Geo& g, int r, int c, float rc, float cval,
+                                                float x1D, int x1P, float x2D, int x2P,
+                                                float x3D, int x3P, float& oD, int& oP,
+                                                int& code) {
+    const float a0 = __fadd_rn(x1D, __fmul_rn(cval, (float)g.w[0]));
+    const float a1 = __fadd_rn(x2D, __fmul_rn(cval, (float)g.w[1]));
+    const float a2 = __fadd_rn(x3D, __fmul_rn(cval, (float)g.w[2]));
+    const float m0 = __fadd_rn(rc, -fabsf((float)x1P));
+    const float m1 = __fadd_rn(rc, -fabsf((float)x2P));
+    const float m2 = __fadd_rn(rc, -fabsf((float)x3P));
+    const bool in1 = !EDGE || c >= 2, in2 = !EDGE || r >= 2;
+    const double U1 = __dmul_rn((double)a1, (double)m0), V1 = __dmul_rn((double)a0, (double)m1);
+    const double d1 = __dadd_rn(V1, -U1);
+    const double t1 = __dmul_rn(__dadd_rn(fabs(U1), fabs(V1)), 0x1p-21);
+    const bool win1 = in1 && d1 > t1;
+    const bool ok1 = !in1 || d1 > t1 || d1 <= 0.0;
+    const float bA = win1 ? a1 : a0, bM = win1 ? m1 : m0;
+    const double U2 = __dmul_rn((double)a2, (double)bM), V2 = __dmul_rn((double)bA, (double)m2);
+    const double d2 = __dadd_rn(V2, -U2);
+    const double t2 = __dmul_rn(__dadd_rn(fabs(U2), fabs(V2)), 0x1p-21);
+    const bool win2 = in2 && d2 > t2;
+    const bool ok2 = !in2 || d2 > t2 || d2 <= 0.0;
+    oD = win2 ? a2 : bA;
+    const int inh = win2 ? x3P : (win1 ? x2P : x1P);
+    code = win2 ? 2 : (win1 ? 1 : 0);
+    if (EDGE) {
+        const int pr = r - (win2 ? 2 : 1);
+        const int pcn = c - (win1 && !win2 ? 2 : 1);
+        oP = pr == 0 ? pcn : (pcn == 0 ? -pr : inh);
+    } else {
+        oP = inh;
+    }
+    return a0 < CUDART_INF_F && a1 < CUDART_INF_F && a2 < CUDART_INF_F && ok1 && ok2;
+}
+
+template <typename T>
 struct Wave {
-    double aD1, aD2, aD3, bD1, bD2, xpD;  // own A outputs 1..3 steps ago, own B 1..2 ago,
-    int aP1, aP2, aP3, bP1, bP2, xpP;     // lane i-1's B received one step ago
-    double2 q[2];                          // cost queue, step tau in slot tau & 1
+    T aD1, aD2, aD3, bD1, bD2, xpD;  // own A outputs 1..3 steps ago, own B 1..2 ago,
+    int aP1, aP2, aP3, bP1, bP2, xpP;  // lane i-1's B received one step ago
+    typename Vec2<T>::type q[2];     // cost queue, step tau in slot tau & 1
 };
 
+template <typename T>
 struct Rings {
-    double* AD;  // [NW][RB] row 64k+62 of each warp's strips
-    double* BD;  // row 64k+63
+    T* AD;  // [NW][RB] row 64k+62 of each warp's strips
+    T* BD;  // row 64k+63
     int* AP;
     int* BP;
 };
 
-template <bool EDGE, bool STD>
-__device__ __forceinline__ void run_block(const Geo& g, Wave& st, const Rings& rg,
-                                          const double2* __restrict__ Cs, int span, int tau0,
-                                          int k, int R, int W, int lane, int prev_base,
-                                          int mine_base, int rmask, int Tb, int lag,
-                                          const TileDesc& td, int nP) {
+template <bool EDGE, bool STD, typename T>
+__device__ __forceinline__ void run_block(const Geo& g, Wave<T>& st, const Rings<T>& rg,
+                                          const typename Vec2<T>::type* __restrict__ Cs,
+                                          int span, int tau0, int k, int R, int W, int lane,
+                                          int prev_base, int mine_base, int rmask, int Tb,
+                                          int lag, const TileDesc& td, int nP) {
+    using V2 = typename Vec2<T>::type;
     const unsigned F = 0xffffffffu;
-    const double w_last = g.S == 1 ? g.w[0] : (g.S == 2 ? g.w[1] : g.w[2]);
+    const T w_last = (T)(g.S == 1 ? g.w[0] : (g.S == 2 ? g.w[1] : g.w[2]));
     const int rA = 64 * k + 2 * lane, rB = rA + 1;
     uint32_t bitsA = 0, bitsB = 0;
-    const double rc0 = (double)(64 * k + tau0);
+    const T rc0 = (T)(64 * k + tau0);
 #pragma unroll 1
     for (int tq = 0; tq < kBlk; tq += 2) {
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
             const int t = tq + u;
             const int tau = tau0 + t;
-            const double rc = __dadd_rn(rc0, (double)t);
-            const double2 cc = st.q[u & 1];
+            const T rc = addr(rc0, (T)t);
+            const V2 cc = st.q[u & 1];
             if (tau + 2 < span) st.q[u & 1] = __ldcs(Cs + (int64_t)(tau + 2) * 32);
-            double x1D = __shfl_up_sync(F, st.bD2, 1);
+            T x1D = __shfl_up_sync(F, st.bD2, 1);
             int x1P = __shfl_up_sync(F, st.bP2, 1);
-            double x3D = __shfl_up_sync(F, st.aD3, 1);
+            T x3D = __shfl_up_sync(F, st.aD3, 1);
             int x3P = __shfl_up_sync(F, st.aP3, 1);
             {
                 // every lane reads the same slot (a broadcast); lane 0 keeps it
                 const int rs = prev_base + ((Tb + t - lag - 1) & rmask);
-                const double rBD = rg.BD[rs], rAD = rg.AD[rs];
+                const T rBD = rg.BD[rs], rAD = rg.AD[rs];
                 const int rBP = rg.BP[rs], rAP = rg.AP[rs];
                 if (lane == 0) {
                     x1D = rBD;
@@ -197,10 +262,10 @@ __device__ __forceinline__ void run_block(const Geo& g, Wave& st, const Rings& r
                     x3P = rAP;
                 }
             }
-            const double x2D = st.xpD;
+            const T x2D = st.xpD;
             const int x2P = st.xpP;
             const int cA = tau - 2 * lane, cB = cA - 1;
-            double oAD, oBD;
+            T oAD, oBD;
             int oAP, oBP, codeA, codeB;
             bool actA = true, actB = true;
             bool okA, okB;
@@ -242,12 +307,13 @@ __device__ __forceinline__ void run_block(const Geo& g, Wave& st, const Rings& r
                 int32_t* eP = td.eP;
                 if (actA && (rA == 0 || cA == 0)) { oAD = cc.x; oAP = 0; codeA = 0; }
                 if (actB && cB == 0) { oBD = cc.y; oBP = 0; codeB = 0; }
-                if (!actA) { oAD = 0.0; oAP = 0; codeA = 0; }
-                if (!actB) { oBD = 0.0; oBP = 0; codeB = 0; }
-                if (actA && rA == R - 1) { eD[cA] = oAD; eP[cA] = oAP; }
-                if (actB && rB == R - 1) { eD[cB] = oBD; eP[cB] = oBP; }
-                if (actA && cA == W - 1) { eD[td.L + rA] = oAD; eP[td.L + rA] = oAP; }
-                if (actB && cB == W - 1) { eD[td.L + rB] = oBD; eP[td.L + rB] = oBP; }
+                if (!actA) { oAD = 0; oAP = 0; codeA = 0; }
+                if (!actB) { oBD = 0; oBP = 0; codeB = 0; }
+                // edges are FP64 for stage 2 (exact widening in the FP32 form)
+                if (actA && rA == R - 1) { eD[cA] = (double)oAD; eP[cA] = oAP; }
+                if (actB && rB == R - 1) { eD[cB] = (double)oBD; eP[cB] = oBP; }
+                if (actA && cA == W - 1) { eD[td.L + rA] = (double)oAD; eP[td.L + rA] = oAP; }
+                if (actB && cB == W - 1) { eD[td.L + rB] = (double)oBD; eP[td.L + rB] = oBP; }
             }
             if (lane == 31) {
                 if (actA) {
@@ -292,24 +358,26 @@ __device__ __forceinline__ bool wait_progress(int* p, int target, const volatile
 // Ring length: the largest power of two whose rings fit the shared-memory
 // limit, capped at the first power of two >= lag + 64 (enough slack that the
 // pairwise waits rarely block); at least lag - 29 (one block of slack).
-__host__ __device__ inline int ring_len(int lag, int nw, int smem_limit) {
+// `vbytes` is the size of a DP value (8 for FP64, 4 for FP32).
+__host__ __device__ inline int ring_len(int lag, int nw, int smem_limit, int vbytes) {
     int cap = 16;
     while (cap * 2 <= lag + 64) cap *= 2;
     if (cap < lag + 64) cap *= 2;
     int fit = 16;
-    const int per = nw * (2 * (int)sizeof(double) + 2 * (int)sizeof(int));
+    const int per = nw * (2 * vbytes + 2 * (int)sizeof(int));
     while ((fit * 2) * per + nw * (int)sizeof(int) <= smem_limit) fit *= 2;
     const int rb = cap < fit ? cap : fit;
     return rb >= lag - 29 ? rb : 0;
 }
 
-template <int NW, bool STD>
+template <int NW, bool STD, typename T>
 __global__ void __launch_bounds__(NW * 32, 16 / NW)
     k_stage1_v3(const TileDesc* __restrict__ descs, const int ntiles, int* __restrict__ head,
                 const Geo g, int32_t* __restrict__ status, const int RB) {
+    using V2 = typename Vec2<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Rings rg;
-    rg.AD = reinterpret_cast<double*>(smem_raw);
+    Rings<T> rg;
+    rg.AD = reinterpret_cast<T*>(smem_raw);
     rg.BD = rg.AD + NW * RB;
     rg.AP = reinterpret_cast<int*>(rg.BD + NW * RB);
     rg.BP = rg.AP + NW * RB;
@@ -348,13 +416,13 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW)
         const Sched2& sc = s_sc;
         const int lag = sc.lag;
         const int Ttot = s_ttot;
-        const double2* Ct = reinterpret_cast<const double2*>(td.Csk);
+        const V2* Ct = reinterpret_cast<const V2*>(td.Csk);
 
-        Wave st;
-        st.aD1 = st.aD2 = st.aD3 = st.bD1 = st.bD2 = st.xpD = 0.0;
+        Wave<T> st;
+        st.aD1 = st.aD2 = st.aD3 = st.bD1 = st.bD2 = st.xpD = 0;
         st.aP1 = st.aP2 = st.aP3 = st.bP1 = st.bP2 = st.xpP = 0;
 #pragma unroll
-        for (int q = 0; q < 2; ++q) st.q[q] = make_double2(0.0, 0.0);
+        for (int q = 0; q < 2; ++q) st.q[q].x = st.q[q].y = 0;
 
         for (int Tb = 0; Tb < Ttot; Tb += kBlk) {
             int k = -1;
@@ -379,7 +447,7 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW)
                 }
                 if (__shfl_sync(0xffffffffu, failed, 0)) break;  // to the tile barrier
                 const int tau0 = Tb - k * lag;
-                const double2* Cs = Ct + (int64_t)k * sc.span * 32 + lane;
+                const V2* Cs = Ct + (int64_t)k * sc.span * 32 + lane;
                 if (tau0 == 0) {
 #pragma unroll
                     for (int q = 0; q < 2; ++q) st.q[q] = __ldcs(Cs + q * 32);
@@ -420,63 +488,70 @@ static int cta_budget(int nw) {
     return per_cta < optin ? per_cta : optin;
 }
 
-size_t stage1_v3_smem_bytes(int32_t L, int nw, int smem_limit) {
+static size_t smem_bytes(int32_t L, int nw, int smem_limit, int vbytes) {
     const Sched2 s = make_sched2(L, L, nw);
-    const int rb = ring_len(s.lag, nw, smem_limit);
+    const int rb = ring_len(s.lag, nw, smem_limit, vbytes);
     if (rb == 0) return (size_t)1 << 30;  // does not fit
-    return (size_t)nw * rb * (2 * sizeof(double) + 2 * sizeof(int)) + nw * sizeof(int);
+    return (size_t)nw * rb * (2 * vbytes + 2 * sizeof(int)) + nw * sizeof(int);
 }
 
 int stage1_queue_warps(int ntiles, int32_t L, int num_sms) {
     // fewer warps per tile fill the strip pipeline better (utilisation ~
-    // strips / (strips - 1 + warps)) but need several tiles per SM
-    const int budget16 = cta_budget(16);
-    if ((int64_t)ntiles >= 4LL * num_sms && stage1_v3_smem_bytes(L, 4, cta_budget(4)) < (1u << 30))
+    // strips / (strips - 1 + warps)) but need several tiles per SM; the
+    // FP64 rings are the larger, so they decide what fits
+    if ((int64_t)ntiles >= 4LL * num_sms && smem_bytes(L, 4, cta_budget(4), 8) < (1u << 30))
         return 4;
-    if ((int64_t)ntiles >= 2LL * num_sms && stage1_v3_smem_bytes(L, 8, cta_budget(8)) < (1u << 30))
+    if ((int64_t)ntiles >= 2LL * num_sms && smem_bytes(L, 8, cta_budget(8), 8) < (1u << 30))
         return 8;
-    return stage1_v3_smem_bytes(L, 16, budget16) < (1u << 30) ? 16 : 0;
+    return smem_bytes(L, 16, cta_budget(16), 8) < (1u << 30) ? 16 : 0;
 }
 
-template <int NW, bool STD>
+template <int NW, bool STD, typename T>
 static cudaError_t launch_q_t(const TileDesc* descs, int ntiles, int* head, const Geo& g,
                               int32_t* status, cudaStream_t st) {
     const int limit = cta_budget(NW);
     const Sched2 s = make_sched2(g.L, g.L, NW);
-    const int rb = ring_len(s.lag, NW, limit);
+    const int rb = ring_len(s.lag, NW, limit, (int)sizeof(T));
     if (rb == 0) return cudaErrorInvalidValue;
-    const size_t smem = stage1_v3_smem_bytes(g.L, NW, limit);
-    cudaError_t e = cudaFuncSetAttribute(k_stage1_v3<NW, STD>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = smem_bytes(g.L, NW, limit, (int)sizeof(T));
+    auto kern = k_stage1_v3<NW, STD, T>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage1_v3<NW, STD>, NW * 32,
-                                                      smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NW * 32, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     const int grid = (int)std::min<int64_t>((int64_t)sms * per_sm, ntiles);
     if (grid <= 0) return cudaSuccess;
-    k_stage1_v3<NW, STD><<<grid, NW * 32, smem, st>>>(descs, ntiles, head, g, status, rb);
+    kern<<<grid, NW * 32, smem, st>>>(descs, ntiles, head, g, status, rb);
     count_launches(1);
     return cudaGetLastError();
 }
 
-cudaError_t launch_stage1_queue(const TileDesc* descs, int ntiles, int* head, const Geo& g,
-                                int32_t* status, int nw, cudaStream_t st) {
+template <typename T>
+static cudaError_t launch_q_type(const TileDesc* descs, int ntiles, int* head, const Geo& g,
+                                 int32_t* status, int nw, cudaStream_t st) {
     const bool std_steps = g.S == 3 && g.kind[0] == 0 && g.kind[1] == 1 && g.kind[2] == 2;
     switch (nw) {
         case 4:
-            return std_steps ? launch_q_t<4, true>(descs, ntiles, head, g, status, st)
-                             : launch_q_t<4, false>(descs, ntiles, head, g, status, st);
+            return std_steps ? launch_q_t<4, true, T>(descs, ntiles, head, g, status, st)
+                             : launch_q_t<4, false, T>(descs, ntiles, head, g, status, st);
         case 8:
-            return std_steps ? launch_q_t<8, true>(descs, ntiles, head, g, status, st)
-                             : launch_q_t<8, false>(descs, ntiles, head, g, status, st);
+            return std_steps ? launch_q_t<8, true, T>(descs, ntiles, head, g, status, st)
+                             : launch_q_t<8, false, T>(descs, ntiles, head, g, status, st);
         default:
-            return std_steps ? launch_q_t<16, true>(descs, ntiles, head, g, status, st)
-                             : launch_q_t<16, false>(descs, ntiles, head, g, status, st);
+            return std_steps ? launch_q_t<16, true, T>(descs, ntiles, head, g, status, st)
+                             : launch_q_t<16, false, T>(descs, ntiles, head, g, status, st);
     }
+}
+
+cudaError_t launch_stage1_queue(const TileDesc* descs, int ntiles, int* head, const Geo& g,
+                                int32_t* status, int nw, bool fp32, cudaStream_t st) {
+    return fp32 ? launch_q_type<float>(descs, ntiles, head, g, status, nw, st)
+                : launch_q_type<double>(descs, ntiles, head, g, status, nw, st);
 }
 
 }  // namespace pfx

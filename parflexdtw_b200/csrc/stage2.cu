@@ -35,9 +35,10 @@ __global__ void k_fill_f64(double* p, int64_t n, double v) {
 
 // Edge tensors + valid mask (Parflex.py:509-564, 347-373, 582-624) -------
 // C: row-major cost (leading dimension g.ldc), or null to read the tile-skewed
-// copy Csk (per-tile stride `skew_stride`).
-__global__ void k_edges(const double* __restrict__ C, const double* __restrict__ Csk,
-                        int64_t skew_stride, const Geo g, S2Buf b) {
+// copy Csk (per-tile stride `skew_stride` elements; FP32 elements when `f32`,
+// widened exactly to FP64).
+__global__ void k_edges(const double* __restrict__ C, const void* __restrict__ Csk,
+                        int64_t skew_stride, bool f32, const Geo g, S2Buf b) {
     const int64_t total = (int64_t)g.n1 * g.n2 * 2 * g.L;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
          q += (int64_t)gridDim.x * blockDim.x) {
@@ -54,8 +55,10 @@ __global__ void k_edges(const double* __restrict__ C, const double* __restrict__
         const int32_t s = b.edge_P[q];
         int32_t sr, sc;
         decode_start(s, &sr, &sc);
+        const int64_t si = t * skew_stride + skew_index(W, sr, sc);
         b.edge_Cf[q] = C ? C[(r0 + sr) * g.ldc + c0 + sc]
-                         : Csk[t * skew_stride + skew_index(W, sr, sc)];
+                         : (f32 ? (double)static_cast<const float*>(Csk)[si]
+                                : static_cast<const double*>(Csk)[si]);
         // mandatory slots: whole top edge of the last tile row, whole right
         // edge of the last tile column, and both ends of every edge
         const bool last = e == 0 ? (i == g.n1 - 1) : (j == g.n2 - 1);
@@ -489,8 +492,8 @@ cudaError_t launch_fill(double* p, int64_t n, double v, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_stage2(const double* C, const double* Csk, int64_t skew_stride, const Geo& g,
-                          const S2Buf& b, cudaStream_t st) {
+cudaError_t launch_stage2(const double* C, const void* Csk, int64_t skew_stride, bool f32,
+                          const Geo& g, const S2Buf& b, cudaStream_t st) {
     const int64_t nslots = (int64_t)g.n1 * g.n2 * 2 * g.L;
     cudaError_t e;
     if ((e = cudaMemsetAsync(b.valid, 0, (size_t)nslots, st)) != cudaSuccess) return e;
@@ -499,7 +502,7 @@ cudaError_t launch_stage2(const double* C, const double* Csk, int64_t skew_strid
     {
         int64_t blocks = (nslots + 255) / 256;
         if (blocks > 8192) blocks = 8192;
-        k_edges<<<(int)blocks, 256, 0, st>>>(C, Csk, skew_stride, g, b);
+        k_edges<<<(int)blocks, 256, 0, st>>>(C, Csk, skew_stride, f32, g, b);
         count_launches(1);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }

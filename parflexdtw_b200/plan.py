@@ -14,14 +14,16 @@ import torch
 
 from . import _lib as L
 
-_DT = {"f64": ("<f8", torch.float64, 8), "i32": ("<i4", torch.int32, 4),
+_DT = {"f64": ("<f8", torch.float64, 8), "f32": ("<f4", torch.float32, 4),
+       "i32": ("<i4", torch.int32, 4), "bf16": ("<u2", torch.uint16, 2),
        "u32": ("<u4", torch.int32, 4), "u8": ("|u1", torch.uint8, 1),
        "i64": ("<i8", torch.int64, 8)}
 
 _BUF_DTYPE = {"EDGE_D": "f64", "EDGE_P": "i32", "BACKPTR": "u32", "EDGE_CF": "f64",
               "VALID": "u8", "D_ARR": "f64", "L_ARR": "f64", "TOP_D": "f64",
               "TOP_L": "f64", "RIGHT_D": "f64", "RIGHT_L": "f64", "SEG_NORM": "f64",
-              "SEG_META": "i64", "D_PROP": "f64", "L_PROP": "f64"}
+              "SEG_META": "i64", "D_PROP": "f64", "L_PROP": "f64", "COST": "f64",
+              "FEAT_BF16": "bf16"}
 
 
 class _DevView:
@@ -53,8 +55,11 @@ def _free_plan(handle):
 class Plan:
     """Geometry + device workspace for an N x M cost matrix with tile length L."""
 
-    def __init__(self, N, M, Lb, steps, weights):
+    def __init__(self, N, M, Lb, steps, weights, precision="fp64"):
         lib = L.load()
+        if precision not in ("fp64", "fp32"):
+            raise ValueError("precision must be 'fp64' or 'fp32'")
+        self.precision = precision
         if not torch.cuda.is_available():
             raise RuntimeError("parflexdtw_b200 needs a CUDA device")
         torch.cuda.init()
@@ -63,9 +68,11 @@ class Plan:
         self.weights = w
         self.N, self.M, self.L = int(N), int(M), int(Lb)
         h = ct.c_void_p()
-        L.check(lib.pfx_plan_create(self.N, self.M, self.L,
-                                    L.i64_array(st.reshape(-1)),
-                                    L.f64_array(w), st.shape[0], ct.byref(h)))
+        L.check(lib.pfx_plan_create_ex(self.N, self.M, self.L,
+                                       L.i64_array(st.reshape(-1)),
+                                       L.f64_array(w), st.shape[0],
+                                       L.PFX_FP32 if precision == "fp32" else L.PFX_FP64,
+                                       ct.byref(h)))
         self._h = h
         self._fin = weakref.finalize(self, _free_plan, h)
         info = (ct.c_int64 * 8)()
@@ -79,6 +86,7 @@ class Plan:
         """A Plan over a handle owned by ``owner`` (a batch): not destroyed
         here, and ``owner`` stays alive while the Plan does."""
         self = cls.__new__(cls)
+        self.precision = getattr(owner, "precision", "fp64")
         self.steps, self.weights = normalize_steps(steps, weights)
         self.N, self.M, self.L = int(N), int(M), int(Lb)
         self._h = handle
@@ -103,7 +111,10 @@ class Plan:
         lib = L.load()
         ptr, nb = ct.c_void_p(), ct.c_int64()
         L.check(lib.pfx_plan_buffer(self._h, L.BUF[name], ct.byref(ptr), ct.byref(nb)))
-        typestr, tdt, size = _DT[_BUF_DTYPE[name]]
+        kind = _BUF_DTYPE[name]
+        if name == "COST" and self.precision == "fp32":
+            kind = "f32"
+        typestr, tdt, size = _DT[kind]
         n = nb.value // size
         shape = (n,)
         s4 = (self.n1, self.n2, 2, self.L)
@@ -114,26 +125,71 @@ class Plan:
             shape = (2, n // 2)
         elif name == "SEG_META":
             shape = (2, n // 12, 6)
+        elif name == "FEAT_BF16":
+            shape = (self.N + self.M, n // (self.N + self.M))
         t = torch.as_tensor(_DevView(ptr.value, shape, typestr),
                             device=f"cuda:{self.device}")
+        if kind == "bf16":
+            t = t.view(torch.bfloat16)
         t._pfx_owner = self  # keep the plan alive while the view lives
         return t
 
     def host(self, name) -> np.ndarray:
         return self.view(name).cpu().numpy()
 
+    def cost_matrix(self) -> np.ndarray:
+        """The loaded cost as an N x M host array, read back from the
+        tile-skewed slabs (FP64, or FP32 in the FP32 form)."""
+        slab = self.host("COST")
+        spanL = -(-(self.L + 63) // 16) * 16
+        nSL = -(-self.L // 64)
+        stride = nSL * spanL * 64
+        out = np.zeros((self.N, self.M), dtype=slab.dtype)
+        for t in range(self.n1 * self.n2):
+            i, j = divmod(t, self.n2)
+            r0, c0 = i * self.hop, j * self.hop
+            R, W = min(self.L, self.N - r0), min(self.L, self.M - c0)
+            span = -(-(W + 63) // 16) * 16
+            nS = -(-R // 64)
+            sl = slab[t * stride:t * stride + nS * span * 64].reshape(nS, span, 64)
+            r = np.arange(R)
+            k, rho = r // 64, r % 64
+            c = np.arange(W)
+            out[r0:r0 + R, c0:c0 + W] = sl[k[:, None], c[None, :] + rho[:, None], rho[:, None]]
+        return out
+
     # -- cost loading ----------------------------------------------------
     def load_cost(self, C_dev: torch.Tensor, stream=None):
-        """Copy a row-major FP64 cost matrix into the plan's tile-skewed layout."""
-        L.check(L.load().pfx_plan_load_cost(self._h, ct.c_void_p(C_dev.data_ptr()),
-                                            C_dev.stride(0), stream or current_stream_ptr()))
+        """Copy a row-major cost matrix into the plan's tile-skewed layout
+        (FP64; an FP32 plan also takes an FP32 matrix, and rounds an FP64
+        one to FP32)."""
+        if C_dev.stride(1) != 1:
+            raise ValueError("cost matrix rows must be contiguous")
+        lib = L.load()
+        s = stream or current_stream_ptr()
+        if C_dev.dtype == torch.float32:
+            L.check(lib.pfx_plan_load_cost_f32(self._h, ct.c_void_p(C_dev.data_ptr()),
+                                               C_dev.stride(0), s))
+        elif C_dev.dtype == torch.float64:
+            L.check(lib.pfx_plan_load_cost(self._h, ct.c_void_p(C_dev.data_ptr()),
+                                           C_dev.stride(0), s))
+        else:
+            raise ValueError(f"cost matrix dtype {C_dev.dtype}: float64 or float32")
 
     def load_features(self, F1_dev: torch.Tensor, F2_dev: torch.Tensor, stream=None):
         """Build the cost 1 - L2norm(F1)^T L2norm(F2) straight into the plan's
-        tile-skewed layout (F1: d x N, F2: d x M, FP64, contiguous)."""
+        tile-skewed layout (F1: d x N, F2: d x M, FP64, contiguous).  FP32
+        plans build it on the tensor cores from bf16 features."""
+        for F, n in ((F1_dev, self.N), (F2_dev, self.M)):
+            if F.dim() != 2 or F.shape[1] != n or F.dtype != torch.float64 or \
+                    not F.is_contiguous() or not F.is_cuda:
+                raise ValueError(f"features must be contiguous FP64 CUDA tensors of shape "
+                                 f"(d, {n}); got {tuple(F.shape)} {F.dtype}")
         if F1_dev.shape[0] != F2_dev.shape[0]:
             raise ValueError("features must share the feature dimension")
-        L.check(L.load().pfx_plan_load_features(
+        fn = L.load().pfx_plan_load_features_bf16 if self.precision == "fp32" else \
+            L.load().pfx_plan_load_features
+        L.check(fn(
             self._h, ct.c_void_p(F1_dev.data_ptr()), ct.c_void_p(F2_dev.data_ptr()),
             int(F1_dev.shape[0]), stream or current_stream_ptr()))
 
