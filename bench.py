@@ -565,6 +565,230 @@ def batch_arm(args, spec):
         dist.destroy_process_group()
 
 
+PREC_METRIC = ("DP cells/s and pairs/s (ParFlex batch, FP32 chosen form: bf16 tensor-core "
+               "cost + FP32 DP, against the FP64 plain form)")
+
+
+def _batch_run_timed(b, beta, steps, warmup, uuid=None):
+    """Phase times of one direct run, then `steps` graph replays timed with
+    CUDA events (after `warmup`); returns (ms_total, phases, clocks)."""
+    import torch
+    b.run(beta, use_graph=False)
+    phases = b.timing()
+    for _ in range(warmup):
+        b.run(beta)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk = ClockSampler(uuid) if uuid else None
+    if clk:
+        clk.__enter__()
+    e0.record()
+    for _ in range(steps):
+        b.run(beta)
+    e1.record()
+    torch.cuda.synchronize()
+    if clk:
+        clk.__exit__(None, None, None)
+    return e0.elapsed_time(e1), phases, (clk.summary() if clk else None)
+
+
+def precision_reference_arm(args, spec):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    sample = W.make_precision_batch(spec, n_pairs=args.ref_pairs)
+    Cs = [W.cost_matrix_host(F1, F2) for F1, F2 in sample]
+    times, cells = [], 0
+    for s in range(args.warmup + args.steps):
+        _, cells, t = _oracle_on_sample(spec, Cs, [spec.L] * len(Cs), threads)
+        if s >= args.warmup:
+            times.append(t[0])
+    tot = sum(times)
+    v = cells * len(times) / tot
+    line = {
+        "impl": "reference", "metric": PREC_METRIC, "value": v, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(spec.describe(), parallelism="replicas"),
+        "pairs_per_s": len(Cs) * len(times) / tot,
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"the first {len(Cs)} pairs ({cells} tile cells, L={spec.L}) "
+                                   f"per step, FP64 (the reference's arithmetic), all stages, "
+                                   f"cost matrix built outside the timed region"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def precision_arm(args, spec):
+    import torch
+    import torch.distributed as dist
+
+    import parflexdtw_b200 as pf
+    from parflexdtw_b200 import _lib
+    from parflexdtw_b200 import precision as PR
+    from parflexdtw_b200.batch import Batch
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    lib = _lib.load()
+    t0 = time.perf_counter()
+    pairs = W.make_precision_batch(spec, seed_offset=1000 * rank, n_pairs=args.pairs)
+    gen_s = time.perf_counter() - t0
+    shapes = [(F1.shape[1], F2.shape[1]) for F1, F2 in pairs]
+    n = len(pairs)
+
+    # --- FP32 chosen form -------------------------------------------------
+    b32 = Batch(shapes, spec.L, spec.steps, spec.weights, spec.d, precision="fp32")
+    cells = b32.cells
+    b32.load(pairs)
+    if ws > 1:
+        dist.barrier()
+    launches0 = lib.pfx_kernel_launches()
+    ms32, ph32, clk = _batch_run_timed(b32, spec.beta, args.steps, args.warmup, uuid)
+    launches = lib.pfx_kernel_launches() - launches0
+    if ws > 1:
+        t = torch.tensor([ms32], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms32 = float(t.item())
+    best32, end32, lens32 = b32.results()
+    paths32 = b32.paths(lens32)
+    # e2e: pinned host features in, results and paths out, every step
+    pinned = [(torch.from_numpy(F1).pin_memory(), torch.from_numpy(F2).pin_memory())
+              for F1, F2 in pairs]
+    h2d = sum(a.numel() * 8 + c.numel() * 8 for a, c in pinned)
+    e2e_ms, d2h = [], 0
+    for s in range(1 + args.e2e_steps):
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        b32.load(pinned)
+        b32.run(spec.beta)
+        bb, ee, ll = b32.results()
+        pp = b32.paths(ll)
+        c.record()
+        torch.cuda.synchronize()
+        if s:
+            e2e_ms.append(a.elapsed_time(c))
+        d2h = 8 * 9 * n + 16 * int(ll.sum())
+        assert np.array_equal(bb, best32), "FP32 form not deterministic"
+    del pinned
+    info32 = {"waves": b32.waves, "tiles": b32.tiles, "warps_per_tile": b32.warps,
+              "device_bytes": b32.device_bytes}
+    b32.close()
+    torch.cuda.empty_cache()
+
+    # --- FP64 plain form on the same pairs ---------------------------------
+    b64 = Batch(shapes, spec.L, spec.steps, spec.weights, spec.d, precision="fp64")
+    b64.load(pairs)
+    ms64, ph64, _ = _batch_run_timed(b64, spec.beta, args.plain_steps, 1)
+    if ws > 1:
+        t = torch.tensor([ms64], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms64 = float(t.item())
+    best64, end64, lens64 = b64.results()
+    paths64 = b64.paths(lens64)
+    b64.close()
+    torch.cuda.empty_cache()
+
+    value32 = cells * ws * args.steps / (ms32 / 1e3)
+    value64 = cells * ws * args.plain_steps / (ms64 / 1e3)
+
+    line = None
+    if rank == 0:
+        t1 = time.perf_counter()
+        prec = PR.compare_results(pairs, best32, paths32, best64, paths64, spec.steps,
+                                  spec.weights, end32[:, 6], end64[:, 6])
+        # cost-matrix error on sample pairs (both forms' slabs)
+        cmax, csum, ccnt = 0.0, 0.0, 0
+        for F1, F2 in pairs[:args.cerr_pairs]:
+            N, M = F1.shape[1], F2.shape[1]
+            p32 = pf.Plan(N, M, spec.L, spec.steps, spec.weights, precision="fp32")
+            p64 = pf.Plan(N, M, spec.L, spec.steps, spec.weights)
+            f1, f2 = torch.from_numpy(F1).to(dev), torch.from_numpy(F2).to(dev)
+            p32.load_features(f1, f2)
+            p64.load_features(f1, f2)
+            mx, sm, ct = PR.cost_error(p32, p64)
+            cmax, csum, ccnt = max(cmax, mx), csum + sm, ccnt + ct
+            p32.close()
+            p64.close()
+        prec.update({"C_abs_err_max": cmax, "C_abs_err_mean": csum / max(ccnt, 1),
+                     "C_err_pairs": min(args.cerr_pairs, n),
+                     "report_seconds": time.perf_counter() - t1})
+        cpu = None
+        parity = None
+        if not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            sample = pairs[:args.ref_pairs]
+            Cs = [pf.cost_matrix_from_features_gpu(F1, F2).cpu().numpy() for F1, F2 in sample]
+            refs, scells, t = _oracle_on_sample(spec, Cs, [spec.L] * len(Cs), threads)
+            cpu = {"value": scells / t[0], "unit": UNIT, "cores": threads, "kind": "port",
+                   "pairs_per_s": len(Cs) / t[0],
+                   "sample": f"the first {len(Cs)} pairs ({scells} tile cells), FP64, all "
+                             f"stages, cost matrix built outside the timing",
+                   "seconds": t[0]}
+            parity = {"pairs_checked": len(refs),
+                      "fp64_plain_best_cost_equal": bool(all(
+                          r["best_cost"] == best64[i] for i, r in enumerate(refs))),
+                      "fp64_plain_path_equal": bool(all(
+                          np.array_equal(r["wp"], paths64[i].T) for i, r in enumerate(refs)))}
+            del Cs
+        peak, peak_kind = load_peaks()
+        s1 = ph32[1]
+        roofline = {
+            "bound": "hbm", "kernel": "k_stage1_v3<.., float> (FP32 DP, tile queue)",
+            "achieved": cells * 4.25 / (s1 / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+            "frac": cells * 4.25 / (s1 / 1e3) / 1e9 / peak,
+            "traffic": None, "alg_bytes_per_cell": 4.25,
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+            if peak_kind == "measured" else "fallback",
+            "stage1_ms": s1, "cost_gemm_ms": ph32[0], "stage2_ms": ph32[2],
+            "fp32_dp_cells_per_s": cells / (s1 / 1e3),
+            "gemm": {"kernel": "k_gemm_cost_skew (tcgen05 BF16 -> FP32, TMA, skew epilogue)",
+                     "bound": "hbm", "alg_bytes_per_cell": 4.0,
+                     "achieved_GBps": cells * 4.0 / (ph32[0] / 1e3) / 1e9,
+                     "tensor_TFLOPs": 2.0 * spec.d * cells * 1.5 / (ph32[0] / 1e3) / 1e12,
+                     "note": "time includes the bf16 feature conversion kernels; FLOPs "
+                             "count the 1.5x column overlap the kernel computes"},
+        }
+        cfg = dict(spec.describe())
+        cfg.update({"pairs_run": n, "cells_per_step": cells, "generation_seconds": gen_s,
+                    "parallelism": "replicas", "input": "features resident in HBM; the "
+                    "timed step builds the cost", "l2": "slabs larger than L2 (no flush "
+                    "needed)", "fp32_batch": info32})
+        line = {
+            "metric": PREC_METRIC, "value": value32, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 cost / f32 DP", "data": "synthetic", "config": cfg,
+            "pairs_per_s": ws * n * args.steps / (ms32 / 1e3),
+            "plain_fp64": {"value": value64, "unit": UNIT, "steps": args.plain_steps,
+                           "ms_per_step": ms64 / args.plain_steps,
+                           "pairs_per_s": ws * n * args.plain_steps / (ms64 / 1e3),
+                           "phases_ms": {"cost": ph64[0], "stage1": ph64[1], "stage2": ph64[2]}},
+            "speedup_fp32_over_fp64": value32 / value64,
+            "precision": prec,
+            "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": {"value": cells * ws * len(e2e_ms) / (sum(e2e_ms) / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "steps": len(e2e_ms), "ms_per_step": sum(e2e_ms) / len(e2e_ms),
+                    "api": "Batch.load (pinned host features) + run + results + paths"},
+            "gpu_launches": int(launches), "clocks": clk, "parity": parity,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -576,9 +800,20 @@ def main():
     ap.add_argument("--ref-tile-rows", type=int, default=2)
     ap.add_argument("--ref-batch-cells", type=float, default=3e9,
                     help="batch workloads: tile cells of the leading pairs the CPU times")
+    ap.add_argument("--pairs", type=int, default=None,
+                    help="precision workload: run only the first PAIRS pairs")
+    ap.add_argument("--plain-steps", type=int, default=1,
+                    help="precision workload: timed steps of the FP64 plain form")
+    ap.add_argument("--cerr-pairs", type=int, default=16,
+                    help="precision workload: pairs whose full cost matrices are compared")
+    ap.add_argument("--ref-pairs", type=int, default=8,
+                    help="precision workload: pairs the CPU oracle times")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     spec = W.WORKLOADS[args.workload]
+    if isinstance(spec, W.PrecisionSpec):
+        (precision_reference_arm if args.impl == "reference" else precision_arm)(args, spec)
+        return
     batch = isinstance(spec, W.BatchSpec)
     if args.impl == "reference":
         (batch_reference_arm if batch else reference_arm)(args, spec)

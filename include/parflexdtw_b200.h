@@ -121,7 +121,7 @@ int pfx_plan_buffer(pfx_plan *plan, int which, void **ptr, int64_t *nbytes);
  * index, so one wavefront step of a warp reads 512 contiguous bytes; about
  * 1.03x the size of C).  From a row-major C (leading dimension ldc), or
  * directly from features: F1 d x N and F2 d x M row-major by feature (the
- * (d, frames) layout), 1 <= d <= 16, giving 1 - L2norm(F1)^T L2norm(F2) with
+ * (d, frames) layout), any d >= 1, giving 1 - L2norm(F1)^T L2norm(F2) with
  * the same fixed-order FP64 sum as pfx_cost_matrix_f64
  * (cost_matrix_from_features_gpu, gpu_flexdtw.py:95-109; Parflex.py:1470). */
 int pfx_plan_load_cost(pfx_plan *plan, const double *C, int64_t ldc, void *stream);
@@ -228,7 +228,9 @@ int pfx_flexdtw_tile_noalloc(const double *C, int64_t ldc, int32_t R, int32_t W,
 
 /* ---------------------------------------------------------------------------
  * Batches.  A batch aligns n pairs of feature sequences of uneven lengths
- * that share steps, weights and feature dimension d (1..16); pair i has its
+ * that share steps, weights, feature dimension d and DP precision
+ * (pfx_precision; the FP32 form takes d <= 256 and builds its cost on the
+ * tensor cores as pfx_plan_load_features_bf16 does); pair i has its
  * own shape (N[i], M[i]) and tile length L[i].  It owns, in one device
  * arena, a plan per pair (pfx_batch_plan), the raw feature inputs, one
  * pool of tile-skewed cost slabs and the stage-1 tile queues.  Pairs are
@@ -250,7 +252,8 @@ typedef struct pfx_batch pfx_batch;
  * count).  The batch is created on the current CUDA device. */
 int pfx_batch_create(int32_t n, const int64_t *N, const int64_t *M, const int32_t *L,
                      const int64_t *steps, const double *weights, int32_t n_steps,
-                     int32_t d, int64_t wave_bytes, int32_t nw, pfx_batch **out);
+                     int32_t d, int64_t wave_bytes, int32_t nw, int32_t precision,
+                     pfx_batch **out);
 void pfx_batch_destroy(pfx_batch *batch);
 /* info[0..7] = n, waves, total tiles, DP cells (sum of tile R*W), device
  * bytes, stage-1 warps per CTA, largest wave's tiles, cost-slab pool bytes. */

@@ -69,7 +69,7 @@ SIGNATURES = [
     ("pfx_flexdtw_tile_noalloc", ct.c_int, [_vp, _i64, _i32, _i32, _i64p, _f64p, _i32, _vp,
                                             _vp, _vp, _vp]),
     ("pfx_batch_create", ct.c_int, [_i32, _i64p, _i64p, _i32p, _i64p, _f64p, _i32, _i32, _i64,
-                                    _i32, ct.POINTER(_vp)]),
+                                    _i32, _i32, ct.POINTER(_vp)]),
     ("pfx_batch_destroy", None, [_vp]),
     ("pfx_batch_info", ct.c_int, [_vp, _i64p]),
     ("pfx_batch_features", ct.c_int, [_vp, _i32, ct.POINTER(_vp), ct.POINTER(_vp)]),

@@ -11,7 +11,8 @@ chroma-like features) with CUDA events for every candidate and keeps the
 fastest per bucket; the batch then runs all pairs in one launch per wave
 with the warps choice of the bucket holding most of the cells.
 
-Results are cached per (device, bucket, steps, weights, d) in memory and,
+Results are cached per (device, bucket, steps, weights, d, precision) in
+memory and,
 when ``cache_path`` is given, in a JSON file.
 """
 from __future__ import annotations
@@ -50,20 +51,20 @@ class Autotuner:
     def bucket(self, N, M) -> int:
         return int(np.searchsorted(self.bucket_edges, min(N, M), side="right"))
 
-    def _key(self, b, steps, weights, d):
+    def _key(self, b, steps, weights, d, precision):
         name = torch.cuda.get_device_name() if torch.cuda.is_available() else "none"
         st = np.asarray(steps, dtype=np.int64).reshape(-1).tolist()
         w = np.asarray(weights, dtype=np.float64).reshape(-1).tolist()
-        return f"{name}|b{b}|{st}|{w}|d{d}"
+        return f"{name}|b{b}|{st}|{w}|d{d}|{precision}"
 
-    def _probe(self, shapes, Lb, warps, steps, weights, d, beta=0.1):
+    def _probe(self, shapes, Lb, warps, steps, weights, d, precision, beta=0.1):
         """Milliseconds per pair of one batch run (graph replay, after warm-up),
         or None when the configuration does not fit."""
         rng = np.random.default_rng(self.seed)
         pairs = [warped_pair(rng, n, m, d=d) for n, m in shapes]
         shapes = [(p[0].shape[1], p[1].shape[1]) for p in pairs]
         try:
-            b = Batch(shapes, Lb, steps, weights, d, warps=warps)
+            b = Batch(shapes, Lb, steps, weights, d, warps=warps, precision=precision)
         except ValueError:
             return None
         try:
@@ -80,13 +81,13 @@ class Autotuner:
         finally:
             b.close()
 
-    def tune_bucket(self, shapes, steps, weights, d):
+    def tune_bucket(self, shapes, steps, weights, d, precision="fp64"):
         """(L, warps) with the least time per pair for these shapes."""
         sel = shapes[:self.probe_pairs]
         best = None
         for Lb in self.candidates_L:
             for w in self.candidates_warps:
-                ms = self._probe(sel, Lb, w, steps, weights, d)
+                ms = self._probe(sel, Lb, w, steps, weights, d, precision)
                 self.log.append((self.bucket(*sel[0]), Lb, w, ms))
                 if ms is not None and (best is None or ms < best[2]):
                     best = (Lb, w, ms)
@@ -94,7 +95,7 @@ class Autotuner:
             raise ValueError("no tile length / warps candidate fits these shapes")
         return best[0], best[1]
 
-    def choose(self, shapes, steps, weights, d):
+    def choose(self, shapes, steps, weights, d, precision="fp64"):
         """Per-pair tile lengths and one warps-per-tile value for a batch."""
         groups = {}
         for i, (n, m) in enumerate(shapes):
@@ -102,18 +103,18 @@ class Autotuner:
         Ls = [0] * len(shapes)
         cells = {}
         for b, idx in groups.items():
-            key = self._key(b, steps, weights, d)
+            key = self._key(b, steps, weights, d, precision)
             if key not in self.table:
                 # representative probe shapes: spread over the bucket's pairs
                 pick = [shapes[i] for i in idx[::max(1, len(idx) // self.probe_pairs)]]
-                self.table[key] = self.tune_bucket(pick, steps, weights, d)
+                self.table[key] = self.tune_bucket(pick, steps, weights, d, precision)
                 self._save()
             Lb, w = self.table[key]
             for i in idx:
                 Ls[i] = Lb
             cells[b] = sum(shapes[i][0] * shapes[i][1] for i in idx)
         main = max(cells, key=cells.get)
-        warps = self.table[self._key(main, steps, weights, d)][1]
+        warps = self.table[self._key(main, steps, weights, d, precision)][1]
         return Ls, warps
 
     def _save(self):

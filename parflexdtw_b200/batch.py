@@ -38,8 +38,12 @@ class Batch:
     fixed at creation; features are loaded and the batch re-run any number
     of times (the CUDA graph is recorded on the first run)."""
 
-    def __init__(self, shapes, L_per_pair, steps, weights, d, wave_bytes=0, warps=0):
+    def __init__(self, shapes, L_per_pair, steps, weights, d, wave_bytes=0, warps=0,
+                 precision="fp64"):
         lib = _lib.load()
+        if precision not in ("fp64", "fp32"):
+            raise ValueError("precision must be 'fp64' or 'fp32'")
+        self.precision = precision
         if not torch.cuda.is_available():
             raise RuntimeError("parflexdtw_b200 needs a CUDA device")
         torch.cuda.init()
@@ -58,7 +62,8 @@ class Batch:
         _lib.check(lib.pfx_batch_create(
             n, _lib.i64_array([s[0] for s in self.shapes]), _lib.i64_array([s[1] for s in self.shapes]),
             _lib.i32_array(self.L), _lib.i64_array(st.reshape(-1)), _lib.f64_array(w), st.shape[0],
-            self.d, int(wave_bytes), int(warps), ct.byref(h)))
+            self.d, int(wave_bytes), int(warps),
+            _lib.PFX_FP32 if precision == "fp32" else _lib.PFX_FP64, ct.byref(h)))
         self._h = h
         self._fin = weakref.finalize(self, _free_batch, h)
         info = (ct.c_int64 * 8)()
@@ -155,13 +160,14 @@ def _split_pair(pair):
 
 
 def parflex_batch(pairs, steps, weights, beta, L=None, wave_bytes=0, warps=0,
-                  use_graph=True, errors="raise", tuner=None):
+                  use_graph=True, errors="raise", tuner=None, precision="fp64"):
     """ParFlex on every (F1, F2) feature pair of ``pairs`` in one device batch.
 
     Same argument conventions as ``parflex`` (features are d x frames, the
     cost is 1 - L2norm(F1)^T L2norm(F2) as in tiled_stage1_from_features).
     ``L``: one tile length for all pairs, one per pair, or None to let the
-    autotuner pick per length bucket.  Returns a list with, per pair,
+    autotuner pick per length bucket.  ``precision="fp32"`` runs the FP32
+    form (bf16 tensor-core cost, FP32 DP; d <= 256).  Returns a list with, per pair,
     ``(best_cost, wp[2, K])``.  A pair whose scan finds no endpoint raises the
     reference's ValueError (``errors="raise"``) or yields None
     (``errors="none"``).
@@ -180,11 +186,12 @@ def parflex_batch(pairs, steps, weights, beta, L=None, wave_bytes=0, warps=0,
     if L is None:
         from .autotune import default_tuner
         t = tuner or default_tuner()
-        Ls, w = t.choose(shapes, steps, weights, d)
+        Ls, w = t.choose(shapes, steps, weights, d, precision=precision)
         warps = warps or w
     else:
         Ls = L
-    b = Batch(shapes, Ls, steps, weights, d, wave_bytes=wave_bytes, warps=warps)
+    b = Batch(shapes, Ls, steps, weights, d, wave_bytes=wave_bytes, warps=warps,
+              precision=precision)
     b.load(feats)
     b.run(beta, use_graph=use_graph)
     best, end, lens = b.results()

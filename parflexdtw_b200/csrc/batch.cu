@@ -52,7 +52,7 @@ size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
 }  // namespace
 
 struct pfx_batch {
-    int n = 0, d = 0, nw = 0, device = 0;
+    int n = 0, d = 0, nw = 0, device = 0, fp32 = 0, kp = 0;
     Geo gq;  // step set and weights; L = largest tile length (ring sizing)
     std::vector<pfx_plan> plans;
     char* arena = nullptr;
@@ -117,11 +117,21 @@ extern "C" void pfx_batch_destroy(pfx_batch* b) { batch_free(b); }
 
 extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, const int32_t* L,
                                 const int64_t* steps, const double* weights, int32_t n_steps,
-                                int32_t d, int64_t wave_bytes, int32_t nw, pfx_batch** out) {
+                                int32_t d, int64_t wave_bytes, int32_t nw, int32_t precision,
+                                pfx_batch** out) {
     if (!out || !N || !M || !L || !steps || !weights) return errf(PFX_ERR_ARG, "null argument");
     *out = nullptr;
     if (n < 1) return errf(PFX_ERR_ARG, "batch of %d pairs", n);
-    if (d < 1 || d > 16) return errf(PFX_ERR_ARG, "feature dimension %d: the batch takes 1..16", d);
+    if (precision != PFX_FP64 && precision != PFX_FP32)
+        return errf(PFX_ERR_ARG, "precision %d: PFX_FP64 (0) or PFX_FP32 (1)", precision);
+    const int fp32 = precision == PFX_FP32;
+    if (d < 1 || (fp32 && d > 256))
+        return errf(PFX_ERR_ARG, "feature dimension %d (the FP32 form takes 1..256)", d);
+    const int kp = (d + 63) / 64 * 64;
+    // per pair: normalised FP64 features, or the bf16 rows of the FP32 form
+    auto feat_bytes = [&](int64_t n_, int64_t m_) {
+        return fp32 ? (size_t)(n_ + m_) * kp * 2 : (size_t)d * (n_ + m_) * 8;
+    };
     if (nw != 0 && nw != 4 && nw != 8 && nw != 16)
         return errf(PFX_ERR_ARG, "nw=%d: warps per tile must be 4, 8 or 16 (or 0)", nw);
     int ndev = 0;
@@ -131,6 +141,8 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
     cudaGetDevice(&b->device);
     b->n = n;
     b->d = d;
+    b->fp32 = fp32;
+    b->kp = kp;
     b->plans.resize(n);
     int st = PFX_OK;
     int32_t maxL = 0;
@@ -142,14 +154,14 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
         pfx_plan& p = b->plans[i];
         memset(&p, 0, sizeof(p));
         p.arena_mode = 1;
-        if ((st = plan_init(&p, N[i], M[i], L[i], steps, weights, n_steps, nw ? nw : 16, 0))) {
+        if ((st = plan_init(&p, N[i], M[i], L[i], steps, weights, n_steps, nw ? nw : 16, fp32))) {
             batch_free(b);
             return st;
         }
         plan_off[i] = arena;
         arena += round256(p.bytes);
         feat_off[i] = arena;
-        arena += round256((size_t)d * (N[i] + M[i]) * 8);
+        arena += round256(feat_bytes(N[i], M[i]));
         slab[i] = plan_slab_bytes(&p);
         maxL = std::max(maxL, p.g.L);
         b->total_tiles += (int64_t)p.g.n1 * p.g.n2;
@@ -256,12 +268,17 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
         memset(&p, 0, sizeof(p));
         p.arena_mode = 2;
         p.arena = b->arena + plan_off[i];
-        if ((st = plan_init(&p, N[i], M[i], L[i], steps, weights, n_steps, b->nw, 0))) {
+        if ((st = plan_init(&p, N[i], M[i], L[i], steps, weights, n_steps, b->nw, fp32))) {
             batch_free(b);
             return st;
         }
-        p.feat = reinterpret_cast<double*>(b->arena + feat_off[i]);
-        p.feat_d = d;
+        if (fp32) {
+            p.fbf = b->arena + feat_off[i];
+            p.fbf_kp = kp;
+        } else {
+            p.feat = reinterpret_cast<double*>(b->arena + feat_off[i]);
+            p.feat_d = d;
+        }
         p.Csk = reinterpret_cast<char*>(b->slabs) + pool_off[i];
         p.cost_loaded = 1;
         p.s1.status = b->status;
@@ -358,15 +375,25 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
             pfx_plan& p = b->plans[i];
             const double* F1 = b->fin + b->fin_off[i];
             const double* F2 = F1 + (int64_t)b->d * p.g.N;
-            double* An = p.feat;
-            double* Bn = p.feat + (int64_t)b->d * p.g.N;
-            BCK(launch_l2norm(F1, b->d, p.g.N, An, s));
-            BCK(launch_l2norm(F2, b->d, p.g.M, Bn, s));
-            BCK(launch_cost_skew(An, Bn, b->d, p.g, static_cast<double*>(p.Csk), p.skew_stride, s));
+            if (b->fp32) {
+                char* A = static_cast<char*>(p.fbf);
+                char* B = A + (size_t)p.g.N * b->kp * 2;
+                BCK(launch_features_bf16(F1, b->d, p.g.N, b->kp, A, s));
+                BCK(launch_features_bf16(F2, b->d, p.g.M, b->kp, B, s));
+                BCK(launch_gemm_cost_skew(A, B, b->kp, p.g, static_cast<float*>(p.Csk),
+                                          p.skew_stride, b->status, s));
+            } else {
+                double* An = p.feat;
+                double* Bn = p.feat + (int64_t)b->d * p.g.N;
+                BCK(launch_l2norm(F1, b->d, p.g.N, An, s));
+                BCK(launch_l2norm(F2, b->d, p.g.M, Bn, s));
+                BCK(launch_cost_skew(An, Bn, b->d, p.g, static_cast<double*>(p.Csk),
+                                     p.skew_stride, s));
+            }
         }
         BCK(mark(w, 1));
         BCK(launch_stage1_queue(b->descs + b->wave_desc_off[w], (int)b->wave_tiles[w], b->heads + w,
-                                b->gq, b->status, b->nw, false, s));
+                                b->gq, b->status, b->nw, b->fp32 != 0, s));
         BCK(mark(w, 2));
         BCK(cudaEventRecord(b->fork_ev, s));
         const int nside = std::min(kSide, q1 - q0);

@@ -372,8 +372,7 @@ extern "C" int pfx_plan_load_features(pfx_plan* p, const double* F1, const doubl
                                       void* stream) {
     if (!p || !F1 || !F2) return fail(PFX_ERR_ARG, "null argument");
     if (p->fp32) return fail(PFX_ERR_ARG, "FP32 plans build their cost with pfx_plan_load_features_bf16");
-    if (d < 1 || d > 16)
-        return fail(PFX_ERR_ARG, "feature dimension %d: the fused cost layout takes 1..16", d);
+    if (d < 1) return fail(PFX_ERR_ARG, "feature dimension %d", d);
     int st;
     if ((st = ensure_cost_buffer(p))) return st;
     if (p->feat && p->feat_d < d) return fail(PFX_ERR_ARG, "feature dimension grew");

@@ -153,6 +153,78 @@ __global__ void __launch_bounds__(kCostThreads, 2)
     }
 }
 
+// Any feature dimension: the same mapping with 64 steps per CTA (one
+// 8-step pass per warp), the features taken 16 at a time (columns staged per
+// chunk, rows re-read per chunk) while the 16 sums of a lane stay in
+// registers, so the fixed summation order f = 0, 1, ..., d-1 is kept.
+constexpr int kCT2 = 64;
+constexpr int kCX2 = kCT2 + 66;
+constexpr int kCH2 = kCX2 / 2;
+
+__global__ void __launch_bounds__(kCostThreads, 2)
+    k_cost_skew_chunked(const double* __restrict__ An, const double* __restrict__ Bn, const int d,
+                        const Geo g, double* __restrict__ Csk, const int64_t stride) {
+    __shared__ __align__(16) double sB[kMaxFeat * kCX2];  // [16][2][kCH2]
+    const int nchunk = ceil_div32(make_sched2(g.L, g.L, 1).span, kCT2);
+    const int tile = (int)(blockIdx.x / nchunk), k = blockIdx.y;
+    const int ts = (int)(blockIdx.x % nchunk) * kCT2;
+    int64_t r0, c0;
+    int32_t R, W;
+    tile_rect(g, tile / g.n2, tile % g.n2, &r0, &c0, &R, &W);
+    const int span = ceil_div32(W + kStripRows - 1, kBlk) * kBlk;
+    const int nS = ceil_div32(R, kStripRows);
+    if (k >= nS || ts >= span) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int rA = 64 * k + 2 * lane, rB = rA + 1;
+    const int t0 = ts + kCV * warp;  // this warp's 8 steps
+    const int h0 = ((t0 - ts + 64) >> 1) - lane;
+    double accA[kCV], accB[kCV];
+    for (int f0 = 0; f0 < d; f0 += kMaxFeat) {
+        const int nf = d - f0 < kMaxFeat ? d - f0 : kMaxFeat;
+        __syncthreads();  // the previous chunk's columns are consumed
+        for (int q = threadIdx.x; q < nf * kCX2; q += kCostThreads) {
+            const int f = q / kCX2, x = q - f * kCX2;
+            const int c = ts - 64 + x;
+            sB[(f * 2 + (x & 1)) * kCH2 + (x >> 1)] =
+                (c >= 0 && c < W) ? __ldg(Bn + (int64_t)(f0 + f) * g.M + c0 + c) : 0.0;
+        }
+        __syncthreads();
+        if (t0 < span) {
+#pragma unroll 4
+            for (int f = 0; f < nf; ++f) {
+                const double aA = rA < R ? __ldg(An + (int64_t)(f0 + f) * g.N + r0 + rA) : 0.0;
+                const double aB = rB < R ? __ldg(An + (int64_t)(f0 + f) * g.N + r0 + rB) : 0.0;
+                const double* se = sB + (f * 2) * kCH2;
+                const double* so = se + kCH2;
+                double b[kCV + 1];
+#pragma unroll
+                for (int j = 0; j <= kCV; ++j)
+                    b[j] = (j & 1) ? se[h0 + (j >> 1)] : so[h0 - 1 + (j >> 1)];
+                const bool first = f0 + f == 0;
+#pragma unroll
+                for (int v = 0; v < kCV; ++v) {
+                    const double pA = __dmul_rn(aA, b[v + 1]);
+                    const double pB = __dmul_rn(aB, b[v]);
+                    accA[v] = first ? pA : __dadd_rn(accA[v], pA);
+                    accB[v] = first ? pB : __dadd_rn(accB[v], pB);
+                }
+            }
+        }
+    }
+    if (t0 >= span) return;
+    double2* out = reinterpret_cast<double2*>(Csk + (int64_t)tile * stride) + (int64_t)k * span * 32 + lane;
+#pragma unroll
+    for (int v = 0; v < kCV; ++v) {
+        const int tau = t0 + v;
+        if (tau < span) {
+            const int cA = tau - 2 * lane, cB = cA - 1;
+            const double vA = (rA < R && cA >= 0 && cA < W) ? __dsub_rn(1.0, accA[v]) : 0.0;
+            const double vB = (rB < R && cB >= 0 && cB < W) ? __dsub_rn(1.0, accB[v]) : 0.0;
+            __stcs(out + (int64_t)tau * 32, make_double2(vA, vB));
+        }
+    }
+}
+
 static dim3 region_grid(const Geo& g, int per_cta) {
     const Sched2 s = make_sched2(g.L, g.L, 1);
     return dim3((unsigned)(ceil_div32(s.span, per_cta) * (int64_t)g.n1 * g.n2), (unsigned)s.nS, 1);
@@ -183,7 +255,13 @@ cudaError_t launch_relayout_skew_f32(const double* C64, const float* C32, int64_
 
 cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Geo& g, double* Csk,
                              int64_t stride, cudaStream_t st) {
-    if (d < 1 || d > kMaxFeat) return cudaErrorInvalidValue;
+    if (d < 1) return cudaErrorInvalidValue;
+    if (d > kMaxFeat) {
+        k_cost_skew_chunked<<<region_grid(g, kCT2), kCostThreads, 0, st>>>(An, Bn, d, g, Csk,
+                                                                          stride);
+        count_launches(1);
+        return cudaGetLastError();
+    }
     const size_t smem = (size_t)d * kCX * sizeof(double);
     if (d == 12) {
         k_cost_skew<12><<<region_grid(g, kCT), kCostThreads, smem, st>>>(An, Bn, d, g, Csk, stride);

@@ -219,8 +219,52 @@ def make_batch(spec: BatchSpec, seed_offset: int = 0):
 # features, L in {1000, 2000} per length bucket, FP64 DP.
 BATCH256 = BatchSpec("chroma12_batch256_N2000-20000_fp64", 256, 2000, 20000)
 
+
+
+class PrecisionSpec:
+    """Named precision workload: ``n_pairs`` pairs with N, M ~ U(lo, hi)
+    independently; each pair from one ``d``-dimensional Gaussian latent
+    sequence (F1 = its L2-normalised frames, F2 = F1 under the warp model
+    plus N(0, noise) noise, re-normalised); one tile length ``L``."""
+
+    def __init__(self, name, n_pairs, lo, hi, d=128, noise=0.1, L=1000,
+                 weights=(2.0, 3.0, 3.0), beta=0.1, seed=0):
+        self.name = name
+        self.n_pairs = n_pairs
+        self.lo, self.hi = lo, hi
+        self.d = d
+        self.noise = noise
+        self.L = L
+        self.steps = ((1, 1), (1, 2), (2, 1))
+        self.weights = tuple(float(w) for w in weights)
+        self.beta = beta
+        self.seed = seed
+
+    def describe(self):
+        return {"workload": self.name, "pairs": self.n_pairs, "N_range": [self.lo, self.hi],
+                "M_range": [self.lo, self.hi], "d": self.d, "latent": "gaussian",
+                "noise": self.noise, "L": self.L, "weights": list(self.weights),
+                "beta": self.beta, "seed": self.seed}
+
+
+def make_precision_batch(spec: PrecisionSpec, seed_offset: int = 0, n_pairs=None):
+    """Generate the (F1, F2) pairs of a precision spec (the first ``n_pairs``)."""
+    rng = np.random.default_rng(spec.seed + seed_offset)
+    out = []
+    for _ in range(spec.n_pairs if n_pairs is None else n_pairs):
+        n = int(rng.integers(spec.lo, spec.hi + 1))
+        m = int(rng.integers(spec.lo, spec.hi + 1))
+        out.append(warped_pair(rng, n, m, d=spec.d, noise=spec.noise, latent="gaussian"))
+    return out
+
+
+# 2048 pairs, N, M ~ U(1000, 8000), 128-d Gaussian latents, L = 1000: the FP32
+# form (bf16 tensor-core cost, FP32 DP) against the FP64 plain form.
+PRECISION2048 = PrecisionSpec("gauss128_batch2048_N1000-8000_L1000_fp32_vs_fp64", 2048,
+                              1000, 8000)
+
 WORKLOADS = {"config0": CONFIG0, "config1": CONFIG1, "ncu_small": NCU_SMALL,
-             "batch256": BATCH256}
+             "batch256": BATCH256, "precision2048": PRECISION2048}
 
 
 def make_pair(spec: PairSpec):

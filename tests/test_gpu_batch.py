@@ -138,9 +138,48 @@ def test_autotuner_picks_candidates_and_stays_exact(oracle_mod):
         assert same(wp, ref["wp"])
 
 
+def test_batch_fp64_wide_features_vs_oracle(oracle_mod):
+    """d > 16: the FP64 cost sums the features 16 at a time, same order."""
+    sizes = [(500, 640), (800, 700), (300, 350)]
+    rng = np.random.default_rng(9)
+    pairs = [W.warped_pair(rng, n, m, d=40, noise=0.1, latent="gaussian") for n, m in sizes]
+    b = Batch([(p[0].shape[1], p[1].shape[1]) for p in pairs], 200, STD, WTS, 40)
+    b.load(pairs)
+    b.run(0.1)
+    refs = [oracle_mod.parflex_full(W.cost_matrix_det(F1, F2), STD, WTS, 0.1, 200)
+            for F1, F2 in pairs]
+    _check(b, refs)
+    assert same(b.plan(1).cost_matrix(), W.cost_matrix_det(*pairs[1]))
+    b.close()
+
+
+def test_batch_fp32_vs_oracle(oracle_mod):
+    """FP32 form batch: per pair, the oracle's FP32 form on the device's own
+    tensor-core cost; also equal to the single-pair FP32 plan."""
+    sizes = [(900, 1100), (1500, 1300), (400, 380), (2200, 2000)]
+    rng = np.random.default_rng(10)
+    pairs = [W.warped_pair(rng, n, m, d=128, noise=0.1, latent="gaussian") for n, m in sizes]
+    shapes = [(p[0].shape[1], p[1].shape[1]) for p in pairs]
+    b = Batch(shapes, [300, 500, 128, 1000], STD, WTS, 128, precision="fp32", warps=8)
+    b.load(pairs)
+    b.run(0.1)
+    torch.cuda.synchronize()
+    refs = [oracle_mod.parflex_full(b.plan(i).cost_matrix().astype(np.float64), STD, WTS, 0.1,
+                                    b.L[i], fp32=True) for i in range(b.n)]
+    _check(b, refs)
+    p = pf.Plan(shapes[3][0], shapes[3][1], 1000, STD, WTS, precision="fp32")
+    p.load_features(torch.from_numpy(pairs[3][0]).cuda(), torch.from_numpy(pairs[3][1]).cuda())
+    p.run(None, 0.1)
+    best, end, found, n = p.result()
+    assert best == refs[3]["best_cost"]
+    b.close()
+
+
 def test_batch_errors():
     with pytest.raises(ValueError):
-        Batch([(100, 100)], 100, STD, WTS, 17)  # d > 16
+        Batch([(100, 100)], 100, STD, WTS, 0)  # no features
+    with pytest.raises(ValueError):
+        Batch([(100, 100)], 100, STD, WTS, 300, precision="fp32")  # beyond the GEMM's K
     with pytest.raises(ValueError):
         Batch([(100, 100)], 100, STD, WTS, 12, warps=5)
     with pytest.raises(ValueError):
