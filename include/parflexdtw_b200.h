@@ -140,6 +140,16 @@ int pfx_plan_load_cost_f32(pfx_plan *plan, const float *C, int64_t ldc, void *st
 int pfx_plan_load_features_bf16(pfx_plan *plan, const double *F1, const double *F2,
                                 int32_t d, void *stream);
 
+/* Restricts cost building (load_cost / load_features*), stage 1 and the
+ * stage-2 overlap gather to the tiles set in mask[n1*n2] (row-major tile
+ * index; device memory when on_device, else host); tiles outside it keep
+ * +inf edge costs, so no stage-2 path crosses them.  mask NULL lifts the
+ * restriction.  The masked tile queue is built on the device (no host
+ * round trip when on_device).  Used by the learned tile-pruning proposer;
+ * no reference counterpart. */
+int pfx_plan_set_tile_mask(pfx_plan *plan, const uint8_t *mask, int32_t on_device,
+                           void *stream);
+
 /* Stage 1: FlexDTW on every tile (run_flexdtw_on_tiles, Parflex.py:376-469;
  * GPU variant flexdtw_chunk_from_global_C, gpu_flexdtw.py:288-402).  Writes D
  * and S on tile edges and the packed backpointers.  C non-null: loads it

@@ -392,7 +392,8 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
             }
         }
         BCK(mark(w, 1));
-        BCK(launch_stage1_queue(b->descs + b->wave_desc_off[w], (int)b->wave_tiles[w], b->heads + w,
+        BCK(launch_stage1_queue(b->descs + b->wave_desc_off[w], (int)b->wave_tiles[w], nullptr,
+                                b->heads + w,
                                 b->gq, b->status, b->nw, b->fp32 != 0, s));
         BCK(mark(w, 2));
         BCK(cudaEventRecord(b->fork_ev, s));

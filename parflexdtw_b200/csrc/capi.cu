@@ -209,6 +209,9 @@ int pfx::plan_init(pfx_plan* p, int64_t N, int64_t M, int32_t L, const int64_t* 
     PA(&p->s1.status, 1);
     PA(&p->descs, nt);
     PA(&p->head, 1);
+    PA(&p->tile_mask, nt);
+    PA(&p->descs_sub, nt);
+    PA(&p->nsub, 1);
 #undef PA
     if (p->arena_mode) return PFX_OK;  // arenas are zeroed by their owner
     CK(cudaMemset(p->s2.best_end, 0, 7 * sizeof(int64_t)));
@@ -243,6 +246,7 @@ void pfx::plan_tile_descs(const pfx_plan* p, const void* Csk, TileDesc* out) {
         d.eD = p->s1.edge_D + (int64_t)t * 2 * g.L;
         d.eP = p->s1.edge_P + (int64_t)t * 2 * g.L;
         d.L = g.L;
+        d.tile = t;
         out[q] = d;
     }
 }
@@ -340,6 +344,31 @@ static int ensure_cost_buffer(pfx_plan* p) {
     return PFX_OK;
 }
 
+static const uint8_t* active_mask(const pfx_plan* p) {
+    return p->mask_active ? p->tile_mask : nullptr;
+}
+
+extern "C" int pfx_plan_set_tile_mask(pfx_plan* p, const uint8_t* mask, int32_t on_device,
+                                      void* stream) {
+    if (!p) return fail(PFX_ERR_ARG, "null plan");
+    if (!mask) {
+        p->mask_active = 0;
+        p->s2.tile_mask = nullptr;
+        return PFX_OK;
+    }
+    int st;
+    if ((st = ensure_cost_buffer(p))) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nt = p->g.n1 * p->g.n2;
+    CK(cudaMemcpyAsync(p->tile_mask, mask, (size_t)nt,
+                       on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    if (!on_device) CK(cudaStreamSynchronize(s));  // the host array may go away
+    CK(launch_compact_descs(p->descs, nt, p->tile_mask, p->descs_sub, p->nsub, s));
+    p->mask_active = 1;
+    p->s2.tile_mask = p->tile_mask;
+    return PFX_OK;
+}
+
 extern "C" int pfx_plan_load_cost(pfx_plan* p, const double* C, int64_t ldc, void* stream) {
     if (!p) return fail(PFX_ERR_ARG, "null plan");
     int st = check_ldc(p, C, ldc);
@@ -347,10 +376,10 @@ extern "C" int pfx_plan_load_cost(pfx_plan* p, const double* C, int64_t ldc, voi
     if ((st = ensure_cost_buffer(p))) return st;
     if (p->fp32)
         CK(launch_relayout_skew_f32(C, nullptr, ldc, p->g, static_cast<float*>(p->Csk),
-                                    p->skew_stride, (cudaStream_t)stream));
+                                    p->skew_stride, (cudaStream_t)stream, active_mask(p)));
     else
         CK(launch_relayout_skew(C, ldc, p->g, static_cast<double*>(p->Csk), p->skew_stride,
-                                (cudaStream_t)stream));
+                                (cudaStream_t)stream, active_mask(p)));
     p->cost_loaded = 1;
     return PFX_OK;
 }
@@ -363,7 +392,7 @@ extern "C" int pfx_plan_load_cost_f32(pfx_plan* p, const float* C, int64_t ldc, 
     int st;
     if ((st = ensure_cost_buffer(p))) return st;
     CK(launch_relayout_skew_f32(nullptr, C, ldc, p->g, static_cast<float*>(p->Csk),
-                                p->skew_stride, (cudaStream_t)stream));
+                                p->skew_stride, (cudaStream_t)stream, active_mask(p)));
     p->cost_loaded = 1;
     return PFX_OK;
 }
@@ -385,7 +414,8 @@ extern "C" int pfx_plan_load_features(pfx_plan* p, const double* F1, const doubl
     double* Bn = p->feat + (int64_t)d * p->g.N;
     CK(launch_l2norm(F1, d, p->g.N, An, s));
     CK(launch_l2norm(F2, d, p->g.M, Bn, s));
-    CK(launch_cost_skew(An, Bn, d, p->g, static_cast<double*>(p->Csk), p->skew_stride, s));
+    CK(launch_cost_skew(An, Bn, d, p->g, static_cast<double*>(p->Csk), p->skew_stride, s,
+                        active_mask(p)));
     p->cost_loaded = 1;
     return PFX_OK;
 }
@@ -412,7 +442,7 @@ extern "C" int pfx_plan_load_features_bf16(pfx_plan* p, const double* F1, const 
     CK(launch_features_bf16(F1, d, p->g.N, p->fbf_kp, A, s));
     CK(launch_features_bf16(F2, d, p->g.M, p->fbf_kp, B, s));
     CK(launch_gemm_cost_skew(A, B, p->fbf_kp, p->g, static_cast<float*>(p->Csk), p->skew_stride,
-                             p->s1.status, s));
+                             p->s1.status, s, active_mask(p)));
     p->cost_loaded = 1;
     return PFX_OK;
 }
@@ -424,8 +454,16 @@ extern "C" int pfx_stage1(pfx_plan* p, const double* C, int64_t ldc, void* strea
     if (!p->cost_loaded) return fail(PFX_ERR_ARG, "no cost matrix loaded into the plan");
     cudaStream_t s = (cudaStream_t)stream;
     CK(cudaMemsetAsync(p->head, 0, sizeof(int), s));
-    CK(launch_stage1_queue(p->descs, p->g.n1 * p->g.n2, p->head, p->g, p->s1.status, p->nw,
-                           p->fp32 != 0, s));
+    if (p->mask_active) {
+        // tiles outside the mask keep +inf edges and start 0
+        CK(launch_fill(p->s1.edge_D, p->n4, HUGE_VAL, s));
+        CK(cudaMemsetAsync(p->s1.edge_P, 0, (size_t)p->n4 * 4, s));
+        CK(launch_stage1_queue(p->descs_sub, p->g.n1 * p->g.n2, p->nsub, p->head, p->g,
+                               p->s1.status, p->nw, p->fp32 != 0, s));
+    } else {
+        CK(launch_stage1_queue(p->descs, p->g.n1 * p->g.n2, nullptr, p->head, p->g,
+                               p->s1.status, p->nw, p->fp32 != 0, s));
+    }
     return PFX_OK;
 }
 

@@ -130,7 +130,7 @@ struct TileDesc {
     int32_t* eP;        // [2][L] start encodings on the edges
     int32_t R, W;       // tile rows / columns
     int32_t L;          // edge-array stride (the alignment's tile length)
-    int32_t pad;
+    int32_t tile;       // tile index within its alignment (row-major)
 };
 
 // Status word values written by kernels.
@@ -161,6 +161,7 @@ struct S2Buf {
     int64_t seg_cap;
     int64_t* wp;         // [K][2] final path, start first
     int64_t* wp_len;     // [1]
+    const uint8_t* tile_mask;  // [n1*n2] tiles stage 1 ran on (null: all)
 };
 
 // Records `msg` as the calling thread's last error and returns `status`.
@@ -175,23 +176,33 @@ void count_launches(int n);
 // Stage-1 queue kernel over `ntiles` descriptors (all sharing the step set and
 // weights of g; tiles at most g.L x g.L); `*head` must be 0 at launch; nw in
 // {4, 8, 16} warps per tile.
-cudaError_t launch_stage1_queue(const TileDesc* descs, int ntiles, int* head, const Geo& g,
-                                int32_t* status, int nw, bool fp32, cudaStream_t st);
+// `ntiles_dev` (nullable): the queue length read on the device (at most ntiles).
+cudaError_t launch_stage1_queue(const TileDesc* descs, int ntiles, const int* ntiles_dev,
+                                int* head, const Geo& g, int32_t* status, int nw, bool fp32,
+                                cudaStream_t st);
+// Keeps the descriptors whose tile is set in `mask`, in order; *count = kept.
+cudaError_t launch_compact_descs(const TileDesc* in, int n, const uint8_t* mask, TileDesc* out,
+                                 int* count, cudaStream_t st);
 // Smallest valid warps-per-tile choice heuristic for `ntiles` tiles of length L.
 int stage1_queue_warps(int ntiles, int32_t L, int num_sms);
+// Cost-building launchers take an optional tile mask (null: all tiles);
+// masked-out tiles' slabs are left untouched.
 cudaError_t launch_relayout_skew(const double* C, int64_t ldc, const Geo& g, double* Csk,
-                                 int64_t skew_stride, cudaStream_t st);
+                                 int64_t skew_stride, cudaStream_t st,
+                                 const uint8_t* mask = nullptr);
 // FP32 form cost from features (gemm_bf16.cu): bf16 rows of L2-normalised
 // features, then 1 - A B^T on the tensor cores into FP32 skewed slabs.
 cudaError_t launch_features_bf16(const double* F, int d, int64_t n, int Kp, void* out,
                                  cudaStream_t st);
 cudaError_t launch_gemm_cost_skew(const void* Abf, const void* Bbf, int Kp, const Geo& g,
-                                  float* Csk, int64_t stride, int32_t* status, cudaStream_t st);
+                                  float* Csk, int64_t stride, int32_t* status, cudaStream_t st,
+                                  const uint8_t* mask = nullptr);
 // FP32 slabs from a row-major FP64 (rounded) or FP32 C (exactly one non-null).
 cudaError_t launch_relayout_skew_f32(const double* C64, const float* C32, int64_t ldc,
-                                     const Geo& g, float* Csk, int64_t stride, cudaStream_t st);
+                                     const Geo& g, float* Csk, int64_t stride, cudaStream_t st,
+                                     const uint8_t* mask = nullptr);
 cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Geo& g, double* Csk,
-                             int64_t skew_stride, cudaStream_t st);
+                             int64_t skew_stride, cudaStream_t st, const uint8_t* mask = nullptr);
 cudaError_t launch_l2norm(const double* F, int d, int64_t n, double* out, cudaStream_t st);
 cudaError_t launch_stage1(const double* C, const Geo& g, const S1Out& o, int tile0, int ntiles,
                           int nw, bool full, cudaStream_t st);

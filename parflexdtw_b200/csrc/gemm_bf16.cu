@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
     k_gemm_cost_skew(const __grid_constant__ CUtensorMap mapA,
                      const __grid_constant__ CUtensorMap mapB, const Geo g,
                      float* __restrict__ Csk, const int64_t stride,
-                     int32_t* __restrict__ status) {
+                     int32_t* __restrict__ status, const uint8_t* __restrict__ mask) {
     extern __shared__ __align__(1024) unsigned char gsm_raw[];
     // operands (1024-byte aligned atoms), later reused as the skew stage
     unsigned char* base = reinterpret_cast<unsigned char*>(
@@ -125,6 +125,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
     q /= ncb;
     const int kk = q % nkk;
     const int tile = q / nkk;
+    if (mask && !mask[tile]) return;  // uniform over the CTA
     int64_t r0, c0;
     int32_t R, W;
     tile_rect(g, tile / g.n2, tile % g.n2, &r0, &c0, &R, &W);
@@ -323,7 +324,7 @@ size_t gemm_cost_smem_bytes(int Kp) {
 
 template <int KB>
 static cudaError_t gemm_t(const CUtensorMap& ma, const CUtensorMap& mb, const Geo& g, float* Csk,
-                          int64_t stride, int32_t* status, cudaStream_t st) {
+                          int64_t stride, int32_t* status, cudaStream_t st, const uint8_t* mask) {
     const size_t smem = gemm_cost_smem_bytes(64 * KB);
     auto kern = k_gemm_cost_skew<KB>;
     cudaError_t e =
@@ -333,22 +334,23 @@ static cudaError_t gemm_t(const CUtensorMap& ma, const CUtensorMap& mb, const Ge
     const int64_t nblk =
         (int64_t)g.n1 * g.n2 * ((s.nS + 1) / 2) * ceil_div32(s.span, kGSteps);
     if (nblk > 0x7fffffffLL) return cudaErrorInvalidValue;
-    kern<<<(unsigned)nblk, kGThreads, smem, st>>>(ma, mb, g, Csk, stride, status);
+    kern<<<(unsigned)nblk, kGThreads, smem, st>>>(ma, mb, g, Csk, stride, status, mask);
     count_launches(1);
     return cudaGetLastError();
 }
 
 cudaError_t launch_gemm_cost_skew(const void* Abf, const void* Bbf, int Kp, const Geo& g,
-                                  float* Csk, int64_t stride, int32_t* status, cudaStream_t st) {
+                                  float* Csk, int64_t stride, int32_t* status, cudaStream_t st,
+                                  const uint8_t* mask) {
     if (Kp % 64 || Kp < 64 || Kp > 256) return cudaErrorInvalidValue;
     CUtensorMap ma, mb;
     if (!make_map(&ma, Abf, g.N, Kp, kGRows) || !make_map(&mb, Bbf, g.M, Kp, kGCols))
         return cudaErrorInvalidValue;
     switch (Kp / 64) {
-        case 1: return gemm_t<1>(ma, mb, g, Csk, stride, status, st);
-        case 2: return gemm_t<2>(ma, mb, g, Csk, stride, status, st);
-        case 3: return gemm_t<3>(ma, mb, g, Csk, stride, status, st);
-        default: return gemm_t<4>(ma, mb, g, Csk, stride, status, st);
+        case 1: return gemm_t<1>(ma, mb, g, Csk, stride, status, st, mask);
+        case 2: return gemm_t<2>(ma, mb, g, Csk, stride, status, st, mask);
+        case 3: return gemm_t<3>(ma, mb, g, Csk, stride, status, st, mask);
+        default: return gemm_t<4>(ma, mb, g, Csk, stride, status, st, mask);
     }
 }
 

@@ -37,13 +37,15 @@ template <typename Tin, typename Tout>
 __global__ void __launch_bounds__(kRegionThreads) k_region_skew(const Tin* __restrict__ C,
                                                                int64_t ldc, const Geo g,
                                                                Tout* __restrict__ Csk,
-                                                               int64_t stride) {
+                                                               int64_t stride,
+                                                               const uint8_t* __restrict__ mask) {
     extern __shared__ __align__(16) unsigned char S_raw[];
     Tout* S = reinterpret_cast<Tout*>(S_raw);  // [64][kWinStride]
     // blockIdx.x enumerates (tile, step chunk) pairs, blockIdx.y the strip
     const int nchunk = ceil_div32(make_sched2(g.L, g.L, 1).span, kTC);
     const int tile = (int)(blockIdx.x / nchunk), k = blockIdx.y;
     const int ts = (int)(blockIdx.x % nchunk) * kTC;
+    if (mask && !mask[tile]) return;
     const int ti = tile / g.n2, tj = tile % g.n2;
     int64_t r0, c0;
     int32_t R, W;
@@ -86,11 +88,13 @@ constexpr int kCH = kCX / 2;            // per parity
 template <int DMAX>
 __global__ void __launch_bounds__(kCostThreads, 2)
     k_cost_skew(const double* __restrict__ An, const double* __restrict__ Bn, const int d,
-                const Geo g, double* __restrict__ Csk, const int64_t stride) {
+                const Geo g, double* __restrict__ Csk, const int64_t stride,
+                const uint8_t* __restrict__ mask) {
     extern __shared__ __align__(16) double sB[];  // [d][2][kCH]
     const int nchunk = ceil_div32(make_sched2(g.L, g.L, 1).span, kCT);
     const int tile = (int)(blockIdx.x / nchunk), k = blockIdx.y;
     const int ts = (int)(blockIdx.x % nchunk) * kCT;
+    if (mask && !mask[tile]) return;
     int64_t r0, c0;
     int32_t R, W;
     tile_rect(g, tile / g.n2, tile % g.n2, &r0, &c0, &R, &W);
@@ -163,11 +167,13 @@ constexpr int kCH2 = kCX2 / 2;
 
 __global__ void __launch_bounds__(kCostThreads, 2)
     k_cost_skew_chunked(const double* __restrict__ An, const double* __restrict__ Bn, const int d,
-                        const Geo g, double* __restrict__ Csk, const int64_t stride) {
+                        const Geo g, double* __restrict__ Csk, const int64_t stride,
+                        const uint8_t* __restrict__ mask) {
     __shared__ __align__(16) double sB[kMaxFeat * kCX2];  // [16][2][kCH2]
     const int nchunk = ceil_div32(make_sched2(g.L, g.L, 1).span, kCT2);
     const int tile = (int)(blockIdx.x / nchunk), k = blockIdx.y;
     const int ts = (int)(blockIdx.x % nchunk) * kCT2;
+    if (mask && !mask[tile]) return;
     int64_t r0, c0;
     int32_t R, W;
     tile_rect(g, tile / g.n2, tile % g.n2, &r0, &c0, &R, &W);
@@ -232,42 +238,45 @@ static dim3 region_grid(const Geo& g, int per_cta) {
 
 template <typename Tin, typename Tout>
 static cudaError_t relayout_t(const Tin* C, int64_t ldc, const Geo& g, Tout* Csk, int64_t stride,
-                              cudaStream_t st) {
+                              cudaStream_t st, const uint8_t* mask) {
     const size_t smem = (size_t)64 * kWinStride * sizeof(Tout);
     auto kern = k_region_skew<Tin, Tout>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<region_grid(g, kTC), kRegionThreads, smem, st>>>(C, ldc, g, Csk, stride);
+    kern<<<region_grid(g, kTC), kRegionThreads, smem, st>>>(C, ldc, g, Csk, stride, mask);
     count_launches(1);
     return cudaGetLastError();
 }
 
 cudaError_t launch_relayout_skew(const double* C, int64_t ldc, const Geo& g, double* Csk,
-                                 int64_t stride, cudaStream_t st) {
-    return relayout_t(C, ldc, g, Csk, stride, st);
+                                 int64_t stride, cudaStream_t st, const uint8_t* mask) {
+    return relayout_t(C, ldc, g, Csk, stride, st, mask);
 }
 
 cudaError_t launch_relayout_skew_f32(const double* C64, const float* C32, int64_t ldc,
-                                     const Geo& g, float* Csk, int64_t stride, cudaStream_t st) {
-    return C32 ? relayout_t(C32, ldc, g, Csk, stride, st) : relayout_t(C64, ldc, g, Csk, stride, st);
+                                     const Geo& g, float* Csk, int64_t stride, cudaStream_t st,
+                                     const uint8_t* mask) {
+    return C32 ? relayout_t(C32, ldc, g, Csk, stride, st, mask)
+               : relayout_t(C64, ldc, g, Csk, stride, st, mask);
 }
 
 cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Geo& g, double* Csk,
-                             int64_t stride, cudaStream_t st) {
+                             int64_t stride, cudaStream_t st, const uint8_t* mask) {
     if (d < 1) return cudaErrorInvalidValue;
     if (d > kMaxFeat) {
         k_cost_skew_chunked<<<region_grid(g, kCT2), kCostThreads, 0, st>>>(An, Bn, d, g, Csk,
-                                                                          stride);
+                                                                          stride, mask);
         count_launches(1);
         return cudaGetLastError();
     }
     const size_t smem = (size_t)d * kCX * sizeof(double);
     if (d == 12) {
-        k_cost_skew<12><<<region_grid(g, kCT), kCostThreads, smem, st>>>(An, Bn, d, g, Csk, stride);
+        k_cost_skew<12><<<region_grid(g, kCT), kCostThreads, smem, st>>>(An, Bn, d, g, Csk, stride,
+                                                                         mask);
     } else {
         k_cost_skew<kMaxFeat><<<region_grid(g, kCT), kCostThreads, smem, st>>>(An, Bn, d, g, Csk,
-                                                                             stride);
+                                                                             stride, mask);
     }
     count_launches(1);
     return cudaGetLastError();

@@ -29,6 +29,11 @@ struct pfx_plan {
     // stage-1 tile queue of this plan (descriptors in queue order) and its head
     pfx::TileDesc* descs;
     int* head;
+    // tile mask (pfx_plan_set_tile_mask): the masked queue and its device length
+    uint8_t* tile_mask;
+    pfx::TileDesc* descs_sub;
+    int* nsub;
+    int mask_active;
     // arena allocation: 0 = cudaMalloc per buffer, 1 = count bytes only,
     // 2 = carve from `arena`
     int arena_mode;

@@ -372,8 +372,9 @@ __host__ __device__ inline int ring_len(int lag, int nw, int smem_limit, int vby
 
 template <int NW, bool STD, typename T>
 __global__ void __launch_bounds__(NW * 32, 16 / NW)
-    k_stage1_v3(const TileDesc* __restrict__ descs, const int ntiles, int* __restrict__ head,
-                const Geo g, int32_t* __restrict__ status, const int RB) {
+    k_stage1_v3(const TileDesc* __restrict__ descs, const int ntiles_max,
+                const int* __restrict__ ntiles_dev, int* __restrict__ head, const Geo g,
+                int32_t* __restrict__ status, const int RB) {
     using V2 = typename Vec2<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Rings<T> rg;
@@ -387,6 +388,7 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW)
     __shared__ int s_item, s_abort, s_ttot;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int prevw = (warp + NW - 1) % NW, nextw = (warp + 1) % NW;
+    const int ntiles = ntiles_dev ? min(*ntiles_dev, ntiles_max) : ntiles_max;
     if (threadIdx.x == 0) s_abort = 0;
     cuda::atomic_ref<int, cuda::thread_scope_block> my_prog(prog[warp]);
     for (;;) {
@@ -507,8 +509,8 @@ int stage1_queue_warps(int ntiles, int32_t L, int num_sms) {
 }
 
 template <int NW, bool STD, typename T>
-static cudaError_t launch_q_t(const TileDesc* descs, int ntiles, int* head, const Geo& g,
-                              int32_t* status, cudaStream_t st) {
+static cudaError_t launch_q_t(const TileDesc* descs, int ntiles, const int* ntiles_dev, int* head,
+                              const Geo& g, int32_t* status, cudaStream_t st) {
     const int limit = cta_budget(NW);
     const Sched2 s = make_sched2(g.L, g.L, NW);
     const int rb = ring_len(s.lag, NW, limit, (int)sizeof(T));
@@ -526,32 +528,72 @@ static cudaError_t launch_q_t(const TileDesc* descs, int ntiles, int* head, cons
     if (per_sm < 1) per_sm = 1;
     const int grid = (int)std::min<int64_t>((int64_t)sms * per_sm, ntiles);
     if (grid <= 0) return cudaSuccess;
-    kern<<<grid, NW * 32, smem, st>>>(descs, ntiles, head, g, status, rb);
+    kern<<<grid, NW * 32, smem, st>>>(descs, ntiles, ntiles_dev, head, g, status, rb);
     count_launches(1);
     return cudaGetLastError();
 }
 
 template <typename T>
-static cudaError_t launch_q_type(const TileDesc* descs, int ntiles, int* head, const Geo& g,
-                                 int32_t* status, int nw, cudaStream_t st) {
+static cudaError_t launch_q_type(const TileDesc* descs, int ntiles, const int* nd, int* head,
+                                 const Geo& g, int32_t* status, int nw, cudaStream_t st) {
     const bool std_steps = g.S == 3 && g.kind[0] == 0 && g.kind[1] == 1 && g.kind[2] == 2;
     switch (nw) {
         case 4:
-            return std_steps ? launch_q_t<4, true, T>(descs, ntiles, head, g, status, st)
-                             : launch_q_t<4, false, T>(descs, ntiles, head, g, status, st);
+            return std_steps ? launch_q_t<4, true, T>(descs, ntiles, nd, head, g, status, st)
+                             : launch_q_t<4, false, T>(descs, ntiles, nd, head, g, status, st);
         case 8:
-            return std_steps ? launch_q_t<8, true, T>(descs, ntiles, head, g, status, st)
-                             : launch_q_t<8, false, T>(descs, ntiles, head, g, status, st);
+            return std_steps ? launch_q_t<8, true, T>(descs, ntiles, nd, head, g, status, st)
+                             : launch_q_t<8, false, T>(descs, ntiles, nd, head, g, status, st);
         default:
-            return std_steps ? launch_q_t<16, true, T>(descs, ntiles, head, g, status, st)
-                             : launch_q_t<16, false, T>(descs, ntiles, head, g, status, st);
+            return std_steps ? launch_q_t<16, true, T>(descs, ntiles, nd, head, g, status, st)
+                             : launch_q_t<16, false, T>(descs, ntiles, nd, head, g, status, st);
     }
 }
 
-cudaError_t launch_stage1_queue(const TileDesc* descs, int ntiles, int* head, const Geo& g,
-                                int32_t* status, int nw, bool fp32, cudaStream_t st) {
-    return fp32 ? launch_q_type<float>(descs, ntiles, head, g, status, nw, st)
-                : launch_q_type<double>(descs, ntiles, head, g, status, nw, st);
+cudaError_t launch_stage1_queue(const TileDesc* descs, int ntiles, const int* ntiles_dev,
+                                int* head, const Geo& g, int32_t* status, int nw, bool fp32,
+                                cudaStream_t st) {
+    return fp32 ? launch_q_type<float>(descs, ntiles, ntiles_dev, head, g, status, nw, st)
+                : launch_q_type<double>(descs, ntiles, ntiles_dev, head, g, status, nw, st);
+}
+
+// Order-preserving compaction of a tile queue by a tile mask (one CTA: a
+// block-wide prefix count per chunk of 1024 descriptors).
+__global__ void __launch_bounds__(1024) k_compact_descs(const TileDesc* __restrict__ in, int n,
+                                                        const uint8_t* __restrict__ mask,
+                                                        TileDesc* __restrict__ out,
+                                                        int* __restrict__ count) {
+    __shared__ int warp_sums[32];
+    __shared__ int base;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int c0 = 0; c0 < n; c0 += 1024) {
+        const int i = c0 + (int)threadIdx.x;
+        const bool keep = i < n && mask[in[i].tile];
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        const int before = __popc(bal & ((1u << lane) - 1u));
+        if (lane == 0) warp_sums[warp] = __popc(bal);
+        __syncthreads();
+        int off = 0;
+        for (int w = 0; w < warp; ++w) off += warp_sums[w];
+        if (keep) out[base + off + before] = in[i];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int tot = 0;
+            for (int w = 0; w < 32; ++w) tot += warp_sums[w];
+            base += tot;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *count = base;
+}
+
+cudaError_t launch_compact_descs(const TileDesc* in, int n, const uint8_t* mask, TileDesc* out,
+                                 int* count, cudaStream_t st) {
+    k_compact_descs<<<1, 1024, 0, st>>>(in, n, mask, out, count);
+    count_launches(1);
+    return cudaGetLastError();
 }
 
 }  // namespace pfx

@@ -56,9 +56,12 @@ __global__ void k_edges(const double* __restrict__ C, const void* __restrict__ C
         int32_t sr, sc;
         decode_start(s, &sr, &sc);
         const int64_t si = t * skew_stride + skew_index(W, sr, sc);
-        b.edge_Cf[q] = C ? C[(r0 + sr) * g.ldc + c0 + sc]
-                         : (f32 ? (double)static_cast<const float*>(Csk)[si]
-                                : static_cast<const double*>(Csk)[si]);
+        // a tile stage 1 skipped has no cost slab: its edges are +inf anyway
+        b.edge_Cf[q] = (b.tile_mask && !b.tile_mask[t])
+                           ? 0.0
+                           : (C ? C[(r0 + sr) * g.ldc + c0 + sc]
+                                : (f32 ? (double)static_cast<const float*>(Csk)[si]
+                                       : static_cast<const double*>(Csk)[si]));
         // mandatory slots: whole top edge of the last tile row, whole right
         // edge of the last tile column, and both ends of every edge
         const bool last = e == 0 ? (i == g.n1 - 1) : (j == g.n2 - 1);

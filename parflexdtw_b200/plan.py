@@ -193,6 +193,26 @@ class Plan:
             self._h, ct.c_void_p(F1_dev.data_ptr()), ct.c_void_p(F2_dev.data_ptr()),
             int(F1_dev.shape[0]), stream or current_stream_ptr()))
 
+    def set_tile_mask(self, mask=None, stream=None):
+        """Restrict cost building and stage 1 to the tiles set in ``mask``
+        ((n1, n2) bool/uint8, host array or CUDA tensor); None lifts it."""
+        lib = L.load()
+        s = stream or current_stream_ptr()
+        if mask is None:
+            L.check(lib.pfx_plan_set_tile_mask(self._h, None, 0, s))
+            return
+        if isinstance(mask, torch.Tensor) and mask.is_cuda:
+            m = mask.to(torch.uint8).contiguous()
+            if m.numel() != self.n1 * self.n2:
+                raise ValueError("mask must have n1 * n2 entries")
+            L.check(lib.pfx_plan_set_tile_mask(self._h, ct.c_void_p(m.data_ptr()), 1, s))
+            self._mask_keep = m
+        else:
+            m = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8).reshape(-1))
+            if m.size != self.n1 * self.n2:
+                raise ValueError("mask must have n1 * n2 entries")
+            L.check(lib.pfx_plan_set_tile_mask(self._h, m.ctypes.data_as(ct.c_void_p), 0, s))
+
     # -- stages ----------------------------------------------------------
     @staticmethod
     def _cptr(C_dev):
