@@ -81,6 +81,11 @@ int pfx_plan_create_ex(int64_t N, int64_t M, int32_t L, const int64_t *steps,
                        pfx_plan **out);
 void pfx_plan_destroy(pfx_plan *plan);
 
+/* Stage-1 warps per tile CTA (4, 8 or 16; the plan picks one from its tile
+ * count).  A masked run with few tiles is faster with 16.  No reference
+ * counterpart. */
+int pfx_plan_set_warps(pfx_plan *plan, int32_t nw);
+
 /* info[0..7] = n1, n2, L, hop, n_steps, b_words_per_tile, device_bytes,
  * stage-1 warps per CTA. */
 int pfx_plan_info(const pfx_plan *plan, int64_t *info);
@@ -296,6 +301,55 @@ int pfx_batch_results(pfx_batch *batch, void *stream, double *best_cost,
  * pfx_batch_results; capacity `cap` points in total).  Synchronises. */
 int pfx_batch_copy_paths(pfx_batch *batch, void *stream, int64_t *wp_host,
                          const int64_t *offsets, int64_t cap);
+
+/* ---------------------------------------------------------------------------
+ * Learned tile proposer (no reference counterpart).  A 3-layer CNN reads
+ * the 16x average-pooled cost matrix and scores the tiles the optimal path
+ * crosses; stage 1 then runs only on proposed tiles (pfx_plan_set_tile_mask)
+ * and the full-tile method is the fallback.  These are its hand-written
+ * inference and training kernels; images are one sample, [C][H][W], FP32
+ * unless a *_bf16 flag selects bf16 activation storage (FP32 arithmetic).
+ * All pointers are device memory; all calls are asynchronous on `stream`.
+ * ------------------------------------------------------------------------- */
+/* out (d x P, P = ceil(n / pool)): per block of `pool` frames, the mean of
+ * the L2-normalised frames of F (d x n, FP64, row-major by feature). */
+int pfx_pool_features(const double *F, int32_t d, int64_t n, int32_t pool, float *out,
+                      void *stream);
+/* out (P1 x P2) = 1 - A^T B for A (d x P1), B (d x P2), P1 <= 65535: with
+ * pooled features, the block means of the cost matrix. */
+int pfx_pooled_cost(const float *A, const float *B, int32_t d, int64_t P1, int64_t P2,
+                    float *out, void *stream);
+/* y (Cout x Ho x Wo) = act(conv3x3(x) + b), zero padding 1, stride 1 or 2,
+ * Ho = (H - 1) / stride + 1; w is [Cout][Cin][3][3]; act = ReLU if relu. */
+int pfx_conv3x3_forward(const void *x, int32_t x_bf16, int32_t Cin, int32_t H, int32_t W,
+                        const float *w, const float *b, int32_t Cout, int32_t stride,
+                        int32_t relu, void *y, int32_t y_bf16, void *stream);
+/* Backward of pfx_conv3x3_forward (FP32, Cout <= 64): from dy (gradient at y)
+ * and the forward's x and y: dx (overwritten; may be NULL), dw and db
+ * (accumulated). */
+int pfx_conv3x3_backward(const float *x, int32_t Cin, int32_t H, int32_t W, const float *w,
+                         int32_t Cout, int32_t stride, const float *y, int32_t relu,
+                         const float *dy, float *dx, float *dw, float *db, void *stream);
+/* score[t] = max of the logit map (H x W, `fpp` frames per pixel) over the
+ * region of tile t of an N x M alignment cut with tile length L and hop;
+ * argmax[t] = the flat pixel index of that max (lowest on ties). */
+int pfx_tile_max(const float *logits, int32_t H, int32_t W, int32_t n1, int32_t n2,
+                 int64_t hop, int64_t L, int64_t N, int64_t M, int32_t fpp, float *score,
+                 int32_t *argmax, void *stream);
+/* Weighted BCE with logits over n tiles: *loss += mean loss, dscore = its
+ * gradient (positives weighted by pos_weight). */
+int pfx_tile_bce(const float *score, const uint8_t *label, int32_t n, float pos_weight,
+                 float *loss, float *dscore, void *stream);
+/* dlogits[argmax[t]] += dscore[t] (dlogits zeroed by the caller). */
+int pfx_tile_max_backward(const float *dscore, const int32_t *argmax, int32_t n,
+                          float *dlogits, void *stream);
+/* One Adam update (bias-corrected, step >= 1) of n parameters. */
+int pfx_adam_step(float *param, const float *grad, float *m, float *v, int64_t n, float lr,
+                  float beta1, float beta2, float eps, int32_t step, void *stream);
+/* mask[t] = 1 if some tile within Chebyshev distance `dilation` of t has
+ * score > threshold. */
+int pfx_tile_mask_from_scores(const float *score, int32_t n1, int32_t n2, float threshold,
+                              int32_t dilation, uint8_t *mask, void *stream);
 
 #ifdef __cplusplus
 }

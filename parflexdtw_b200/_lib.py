@@ -48,6 +48,7 @@ SIGNATURES = [
                                       ct.POINTER(_vp)]),
     ("pfx_plan_destroy", None, [_vp]),
     ("pfx_plan_info", ct.c_int, [_vp, _i64p]),
+    ("pfx_plan_set_warps", ct.c_int, [_vp, _i32]),
     ("pfx_plan_buffer", ct.c_int, [_vp, ct.c_int, ct.POINTER(_vp), _i64p]),
     ("pfx_plan_load_cost", ct.c_int, [_vp, _vp, _i64, _vp]),
     ("pfx_plan_load_features", ct.c_int, [_vp, _vp, _vp, _i32, _vp]),
@@ -79,6 +80,19 @@ SIGNATURES = [
     ("pfx_batch_timing", ct.c_int, [_vp, _f64p]),
     ("pfx_batch_results", ct.c_int, [_vp, _vp, _f64p, _i64p, _i64p]),
     ("pfx_batch_copy_paths", ct.c_int, [_vp, _vp, _i64p, _i64p, _i64]),
+    ("pfx_pool_features", ct.c_int, [_vp, _i32, _i64, _i32, _vp, _vp]),
+    ("pfx_pooled_cost", ct.c_int, [_vp, _vp, _i32, _i64, _i64, _vp, _vp]),
+    ("pfx_conv3x3_forward", ct.c_int, [_vp, _i32, _i32, _i32, _i32, _vp, _vp, _i32, _i32, _i32,
+                                       _vp, _i32, _vp]),
+    ("pfx_conv3x3_backward", ct.c_int, [_vp, _i32, _i32, _i32, _vp, _i32, _i32, _vp, _i32, _vp,
+                                        _vp, _vp, _vp, _vp]),
+    ("pfx_tile_max", ct.c_int, [_vp, _i32, _i32, _i32, _i32, _i64, _i64, _i64, _i64, _i32, _vp,
+                                _vp, _vp]),
+    ("pfx_tile_bce", ct.c_int, [_vp, _vp, _i32, ct.c_float, _vp, _vp, _vp]),
+    ("pfx_tile_max_backward", ct.c_int, [_vp, _vp, _i32, _vp, _vp]),
+    ("pfx_adam_step", ct.c_int, [_vp, _vp, _vp, _vp, _i64, ct.c_float, ct.c_float, ct.c_float,
+                                 ct.c_float, _i32, _vp]),
+    ("pfx_tile_mask_from_scores", ct.c_int, [_vp, _i32, _i32, ct.c_float, _i32, _vp, _vp]),
 ]
 
 _lib = None

@@ -277,6 +277,16 @@ extern "C" int pfx_plan_create_ex(int64_t N, int64_t M, int32_t L, const int64_t
     return PFX_OK;
 }
 
+extern "C" int pfx_plan_set_warps(pfx_plan* p, int32_t nw) {
+    if (!p) return fail(PFX_ERR_ARG, "null plan");
+    if (nw != 4 && nw != 8 && nw != 16) return fail(PFX_ERR_ARG, "nw=%d: 4, 8 or 16", nw);
+    if (stage1_queue_warps(1, p->g.L, 1) == 0 ||
+        (nw != 16 && stage1_queue_warps(1 << 30, p->g.L, 1) > nw))
+        return fail(PFX_ERR_TOO_LARGE, "L=%d: rings of %d warps do not fit", p->g.L, nw);
+    p->nw = nw;
+    return PFX_OK;
+}
+
 extern "C" int pfx_plan_info(const pfx_plan* p, int64_t* info) {
     if (!p || !info) return fail(PFX_ERR_ARG, "null argument");
     info[0] = p->g.n1;

@@ -1,0 +1,496 @@
+// Learned tile proposer: the kernels of a small CNN that reads a 16x
+// average-pooled cost matrix and scores which L x L tiles the optimal path
+// crosses (inference and training: forward, backward, Adam).  No reference
+// counterpart; the full-tile method stays the fallback and the judge.
+//
+// Images are one sample, channels-first [C][H][W], FP32 in training; in
+// inference the activations between layers may be stored in bf16 (FP32
+// arithmetic).  Convolutions are 3x3, zero padding 1, stride 1 or 2.
+//
+// Pooled cost: 16-frame block means of the L2-normalised features give the
+// block mean of C exactly in real arithmetic (C is bilinear in the two
+// frames: mean_{r,c}(1 - a_r . b_c) = 1 - mean(a) . mean(b)), so the pooled
+// map costs one small (P1 x d) x (d x P2) product instead of the full C.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+namespace pfx {
+
+__device__ __forceinline__ float ld_act(const float* p) { return *p; }
+__device__ __forceinline__ float ld_act(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+__device__ __forceinline__ void st_act(float* p, float v) { *p = v; }
+__device__ __forceinline__ void st_act(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+
+// F (d x n, FP64, row-major by feature) -> out (d x P, FP32): per block of
+// `pool` frames the mean of the L2-normalised frames (last block: the frames
+// it has).
+__global__ void k_pool_features(const double* __restrict__ F, int d, int64_t n, int pool,
+                                float* __restrict__ out, int64_t P) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    const int64_t i0 = p * pool, i1 = min(n, i0 + pool);
+    for (int f = 0; f < d; ++f) {
+        double s = 0.0;
+        for (int64_t i = i0; i < i1; ++i) {
+            double ss = 0.0;
+            for (int g = 0; g < d; ++g) {
+                const double x = F[(int64_t)g * n + i];
+                ss += x * x;
+            }
+            const double nr = sqrt(ss);
+            s += nr > 0.0 ? F[(int64_t)f * n + i] / nr : 0.0;
+        }
+        out[(int64_t)f * P + p] = (float)(s / (double)(i1 - i0));
+    }
+}
+
+// out[i][j] = 1 - sum_f A[f][i] B[f][j]   (A: d x P1, B: d x P2)
+__global__ void k_pooled_cost(const float* __restrict__ A, const float* __restrict__ B, int d,
+                              int64_t P1, int64_t P2, float* __restrict__ out) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t i = blockIdx.y;
+    if (j >= P2) return;
+    float acc = 0.f;
+    for (int f = 0; f < d; ++f) acc = fmaf(A[(int64_t)f * P1 + i], B[(int64_t)f * P2 + j], acc);
+    out[i * P2 + j] = 1.f - acc;
+}
+
+// --------------------------------------------------------------------------
+// 3x3 convolution, forward.  A CTA computes a 16 x 16 tile of output pixels
+// for up to 32 output channels; per input channel the input patch and that
+// channel's weights ([tap][co], read 4 at a time) are staged in shared
+// memory.  y = act(conv(x) + b), act = ReLU or identity.
+constexpr int kCvT = 16;   // output tile edge
+constexpr int kCvCo = 32;  // output channels per CTA
+
+template <int S, typename Tin, typename Tout>
+__global__ void __launch_bounds__(kCvT * kCvT)
+    k_conv3x3_fwd(const Tin* __restrict__ x, int Cin, int H, int W, const float* __restrict__ w,
+                  const float* __restrict__ b, int Cout, int Ho, int Wo, int relu,
+                  Tout* __restrict__ y) {
+    constexpr int PT = (kCvT - 1) * S + 3;  // input patch edge
+    __shared__ float patch[PT * PT];
+    __shared__ __align__(16) float ws[9 * kCvCo];
+    const int ox0 = blockIdx.x * kCvT, oy0 = blockIdx.y * kCvT, co0 = blockIdx.z * kCvCo;
+    const int tx = threadIdx.x % kCvT, ty = threadIdx.x / kCvT;
+    const int ox = ox0 + tx, oy = oy0 + ty;
+    const int nco = min(kCvCo, Cout - co0);
+    float acc[kCvCo];
+#pragma unroll
+    for (int c = 0; c < kCvCo; ++c) acc[c] = 0.f;
+    const int ix0 = ox0 * S - 1, iy0 = oy0 * S - 1;
+    for (int ci = 0; ci < Cin; ++ci) {
+        __syncthreads();
+        for (int q = threadIdx.x; q < PT * PT; q += kCvT * kCvT) {
+            const int py = q / PT, px = q % PT;
+            const int iy = iy0 + py, ix = ix0 + px;
+            patch[q] = (iy >= 0 && iy < H && ix >= 0 && ix < W)
+                           ? ld_act(x + ((int64_t)ci * H + iy) * W + ix)
+                           : 0.f;
+        }
+        for (int q = threadIdx.x; q < 9 * kCvCo; q += kCvT * kCvT) {
+            const int tap = q / kCvCo, c = q % kCvCo;
+            ws[q] = c < nco ? w[((int64_t)(co0 + c) * Cin + ci) * 9 + tap] : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int tap = 0; tap < 9; ++tap) {
+            const float xv = patch[(ty * S + tap / 3) * PT + tx * S + tap % 3];
+            const float4* w4 = reinterpret_cast<const float4*>(ws + tap * kCvCo);
+#pragma unroll
+            for (int c4 = 0; c4 < kCvCo / 4; ++c4) {
+                const float4 wv = w4[c4];
+                acc[4 * c4 + 0] = fmaf(wv.x, xv, acc[4 * c4 + 0]);
+                acc[4 * c4 + 1] = fmaf(wv.y, xv, acc[4 * c4 + 1]);
+                acc[4 * c4 + 2] = fmaf(wv.z, xv, acc[4 * c4 + 2]);
+                acc[4 * c4 + 3] = fmaf(wv.w, xv, acc[4 * c4 + 3]);
+            }
+        }
+    }
+    if (ox >= Wo || oy >= Ho) return;
+#pragma unroll
+    for (int c = 0; c < kCvCo; ++c) {
+        if (c < nco) {
+            float v = acc[c] + b[co0 + c];
+            if (relu) v = fmaxf(v, 0.f);
+            st_act(y + ((int64_t)(co0 + c) * Ho + oy) * Wo + ox, v);
+        }
+    }
+}
+
+// Gradient at the conv output before the activation: dz = dy * (y > 0) for
+// ReLU layers, dy otherwise.
+__device__ __forceinline__ float dz_at(const float* dy, const float* y, int relu, int64_t i) {
+    return relu ? (y[i] > 0.f ? dy[i] : 0.f) : dy[i];
+}
+
+// Backward, data: dx[ci][iy][ix] = sum_{co, tap} w[co][ci][tap] dz[co][oy][ox]
+// over the outputs whose window covers (iy, ix).  One thread per input pixel.
+template <int S>
+__global__ void k_conv3x3_bwd_data(const float* __restrict__ w, int Cin, int H, int W, int Cout,
+                                   int Ho, int Wo, const float* __restrict__ y,
+                                   const float* __restrict__ dy, int relu, float* __restrict__ dx) {
+    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (q >= (int64_t)Cin * H * W) return;
+    const int ix = (int)(q % W), iy = (int)((q / W) % H), ci = (int)(q / ((int64_t)W * H));
+    float acc = 0.f;
+    for (int ky = 0; ky < 3; ++ky) {
+        const int ty = iy + 1 - ky;  // = oy * S
+        if (ty < 0 || ty % S) continue;
+        const int oy = ty / S;
+        if (oy >= Ho) continue;
+        for (int kx = 0; kx < 3; ++kx) {
+            const int tx = ix + 1 - kx;
+            if (tx < 0 || tx % S) continue;
+            const int ox = tx / S;
+            if (ox >= Wo) continue;
+            for (int co = 0; co < Cout; ++co) {
+                const int64_t oi = ((int64_t)co * Ho + oy) * Wo + ox;
+                acc = fmaf(w[((int64_t)co * Cin + ci) * 9 + ky * 3 + kx], dz_at(dy, y, relu, oi),
+                           acc);
+            }
+        }
+    }
+    dx[q] = acc;
+}
+
+// Backward, weights and bias: dw[co][ci][tap] += sum_pixels dz * x, db[co] +=
+// sum dz.  A CTA takes a 16 x 16 output tile and a chunk of 8 input
+// channels; per-CTA partial sums go to global memory with atomics.
+constexpr int kWgCi = 8;
+
+template <int S>
+__global__ void __launch_bounds__(256)
+    k_conv3x3_bwd_weight(const float* __restrict__ x, int Cin, int H, int W, int Cout, int Ho,
+                         int Wo, const float* __restrict__ y, const float* __restrict__ dy,
+                         int relu, float* __restrict__ dw, float* __restrict__ db) {
+    constexpr int PT = (kCvT - 1) * S + 3;
+    extern __shared__ float sm[];
+    float* dz = sm;                          // [Cout][256]
+    float* patch = sm + Cout * kCvT * kCvT;  // [kWgCi][PT*PT]
+    const int ox0 = blockIdx.x * kCvT, oy0 = blockIdx.y * kCvT, ci0 = blockIdx.z * kWgCi;
+    const int nci = min(kWgCi, Cin - ci0);
+    for (int q = threadIdx.x; q < Cout * kCvT * kCvT; q += 256) {
+        const int co = q / (kCvT * kCvT), p = q % (kCvT * kCvT);
+        const int ox = ox0 + p % kCvT, oy = oy0 + p / kCvT;
+        dz[q] = (ox < Wo && oy < Ho) ? dz_at(dy, y, relu, ((int64_t)co * Ho + oy) * Wo + ox) : 0.f;
+    }
+    const int ix0 = ox0 * S - 1, iy0 = oy0 * S - 1;
+    for (int q = threadIdx.x; q < nci * PT * PT; q += 256) {
+        const int c = q / (PT * PT), r = q % (PT * PT);
+        const int iy = iy0 + r / PT, ix = ix0 + r % PT;
+        patch[q] = (iy >= 0 && iy < H && ix >= 0 && ix < W)
+                       ? x[((int64_t)(ci0 + c) * H + iy) * W + ix]
+                       : 0.f;
+    }
+    __syncthreads();
+    const int ncomb = Cout * nci * 9;
+    for (int cmb = threadIdx.x; cmb < ncomb; cmb += 256) {
+        const int tap = cmb % 9, c = (cmb / 9) % nci, co = cmb / (9 * nci);
+        const int ky = tap / 3, kx = tap % 3;
+        const float* dzc = dz + co * kCvT * kCvT;
+        const float* pc = patch + c * PT * PT;
+        float acc = 0.f;
+        for (int p = 0; p < kCvT * kCvT; ++p) {
+            const int py = p / kCvT, px = p % kCvT;
+            acc = fmaf(dzc[p], pc[(py * S + ky) * PT + px * S + kx], acc);
+        }
+        atomicAdd(dw + ((int64_t)co * Cin + ci0 + c) * 9 + tap, acc);
+    }
+    if (blockIdx.z == 0) {
+        for (int co = threadIdx.x; co < Cout; co += 256) {
+            float acc = 0.f;
+            for (int p = 0; p < kCvT * kCvT; ++p) acc += dz[co * kCvT * kCvT + p];
+            atomicAdd(db + co, acc);
+        }
+    }
+}
+
+// Tile scores: the max logit over each tile's region of the logit map
+// (`fpp` frames per logit pixel); argmax = flat pixel index (ties: lowest).
+__global__ void __launch_bounds__(256)
+    k_tile_max(const float* __restrict__ logits, int H, int W, int n1, int n2, int64_t hop,
+               int64_t L, int64_t N, int64_t M, int fpp, float* __restrict__ score,
+               int32_t* __restrict__ argmax) {
+    const int t = blockIdx.x;
+    if (t >= n1 * n2) return;
+    const int i = t / n2, j = t % n2;
+    const int64_t r0 = i * hop, c0 = j * hop;
+    const int64_t r1 = r0 + L < N ? r0 + L : N, c1 = c0 + L < M ? c0 + L : M;
+    const int64_t ya = r0 / fpp, yb = (r1 + fpp - 1) / fpp;
+    const int64_t xa = c0 / fpp, xb = (c1 + fpp - 1) / fpp;
+    const int y0 = (int)(ya < H - 1 ? ya : H - 1), y1 = (int)(yb < H ? yb : H);
+    const int x0 = (int)(xa < W - 1 ? xa : W - 1), x1 = (int)(xb < W ? xb : W);
+    const int h = max(y1 - y0, 1), wd = max(x1 - x0, 1);
+    float best = -INFINITY;
+    int bi = y0 * W + x0;
+    for (int q = threadIdx.x; q < h * wd; q += blockDim.x) {
+        const int idx = (y0 + q / wd) * W + x0 + q % wd;
+        const float v = logits[idx];
+        if (v > best || (v == best && idx < bi)) {
+            best = v;
+            bi = idx;
+        }
+    }
+    __shared__ float sv[256];
+    __shared__ int si[256];
+    sv[threadIdx.x] = best;
+    si[threadIdx.x] = bi;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            const float v = sv[threadIdx.x + s];
+            const int ix = si[threadIdx.x + s];
+            if (v > sv[threadIdx.x] || (v == sv[threadIdx.x] && ix < si[threadIdx.x])) {
+                sv[threadIdx.x] = v;
+                si[threadIdx.x] = ix;
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        score[t] = sv[0];
+        argmax[t] = si[0];
+    }
+}
+
+// Weighted binary cross-entropy with logits: loss += sum_t w_t * l_t / n,
+// dscore_t = w_t * (sigmoid(s_t) - y_t) / n, w_t = pos_weight for positives.
+__global__ void k_tile_bce(const float* __restrict__ s, const uint8_t* __restrict__ label, int n,
+                           float pos_weight, float* __restrict__ loss, float* __restrict__ ds) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.f;
+    if (t < n) {
+        const float x = s[t], yv = label[t] ? 1.f : 0.f;
+        const float wt = label[t] ? pos_weight : 1.f;
+        // log(1 + exp(-|x|)) + max(x, 0) - x*y: the stable form
+        l = wt * (log1pf(expf(-fabsf(x))) + fmaxf(x, 0.f) - x * yv) / n;
+        const float sg = 1.f / (1.f + expf(-x));
+        ds[t] = wt * (sg - yv) / n;
+    }
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, l);
+}
+
+__global__ void k_tile_max_bwd(const float* __restrict__ ds, const int32_t* __restrict__ argmax,
+                               int n, float* __restrict__ dlogits) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) atomicAdd(dlogits + argmax[t], ds[t]);
+}
+
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, int64_t n, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// mask = dilate(score > threshold) by `dil` tiles (Chebyshev distance).
+__global__ void k_tile_mask(const float* __restrict__ score, int n1, int n2, float thr, int dil,
+                            uint8_t* __restrict__ mask) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n1 * n2) return;
+    const int i = t / n2, j = t % n2;
+    uint8_t on = 0;
+    for (int a = max(0, i - dil); a <= min(n1 - 1, i + dil) && !on; ++a)
+        for (int b = max(0, j - dil); b <= min(n2 - 1, j + dil); ++b)
+            if (score[a * n2 + b] > thr) {
+                on = 1;
+                break;
+            }
+    mask[t] = on;
+}
+
+// ---------------------------------------------------------------- launchers
+static unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+cudaError_t cnn_pool_features(const double* F, int d, int64_t n, int pool, float* out,
+                              cudaStream_t st) {
+    const int64_t P = (n + pool - 1) / pool;
+    if (P <= 0) return cudaSuccess;
+    k_pool_features<<<blocks_for(P, 128), 128, 0, st>>>(F, d, n, pool, out, P);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t cnn_pooled_cost(const float* A, const float* B, int d, int64_t P1, int64_t P2,
+                            float* out, cudaStream_t st) {
+    if (P1 <= 0 || P2 <= 0) return cudaSuccess;
+    k_pooled_cost<<<dim3(blocks_for(P2, 256), (unsigned)P1), 256, 0, st>>>(A, B, d, P1, P2, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+template <int S, typename Tin, typename Tout>
+static cudaError_t conv_fwd_t(const void* x, int Cin, int H, int W, const float* w, const float* b,
+                              int Cout, int relu, void* y, cudaStream_t st) {
+    const int Ho = (H - 1) / S + 1, Wo = (W - 1) / S + 1;
+    const dim3 grid(blocks_for(Wo, kCvT), blocks_for(Ho, kCvT), blocks_for(Cout, kCvCo));
+    k_conv3x3_fwd<S, Tin, Tout><<<grid, kCvT * kCvT, 0, st>>>(
+        static_cast<const Tin*>(x), Cin, H, W, w, b, Cout, Ho, Wo, relu, static_cast<Tout*>(y));
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+// in_bf16 / out_bf16: activation storage types (FP32 otherwise).
+cudaError_t cnn_conv_forward(const void* x, int in_bf16, int Cin, int H, int W, const float* w,
+                             const float* b, int Cout, int stride, int relu, void* y,
+                             int out_bf16, cudaStream_t st) {
+    using bf = __nv_bfloat16;
+#define PFX_CONV(S)                                                                             \
+    if (in_bf16 && out_bf16) return conv_fwd_t<S, bf, bf>(x, Cin, H, W, w, b, Cout, relu, y, st); \
+    if (in_bf16) return conv_fwd_t<S, bf, float>(x, Cin, H, W, w, b, Cout, relu, y, st);          \
+    if (out_bf16) return conv_fwd_t<S, float, bf>(x, Cin, H, W, w, b, Cout, relu, y, st);         \
+    return conv_fwd_t<S, float, float>(x, Cin, H, W, w, b, Cout, relu, y, st);
+    if (stride == 1) {
+        PFX_CONV(1)
+    }
+    PFX_CONV(2)
+#undef PFX_CONV
+}
+
+cudaError_t cnn_conv_backward(const float* x, int Cin, int H, int W, const float* w, int Cout,
+                              int stride, const float* y, int relu, const float* dy, float* dx,
+                              float* dw, float* db, cudaStream_t st) {
+    const int Ho = (H - 1) / stride + 1, Wo = (W - 1) / stride + 1;
+    if (dx) {
+        const int64_t n = (int64_t)Cin * H * W;
+        if (stride == 1)
+            k_conv3x3_bwd_data<1><<<blocks_for(n, 256), 256, 0, st>>>(w, Cin, H, W, Cout, Ho, Wo,
+                                                                     y, dy, relu, dx);
+        else
+            k_conv3x3_bwd_data<2><<<blocks_for(n, 256), 256, 0, st>>>(w, Cin, H, W, Cout, Ho, Wo,
+                                                                     y, dy, relu, dx);
+        count_launches(1);
+    }
+    const dim3 grid(blocks_for(Wo, kCvT), blocks_for(Ho, kCvT), blocks_for(Cin, kWgCi));
+    const int PT = (kCvT - 1) * stride + 3;
+    const size_t smem = ((size_t)Cout * kCvT * kCvT + (size_t)kWgCi * PT * PT) * sizeof(float);
+    cudaError_t e;
+    if (stride == 1) {
+        e = cudaFuncSetAttribute(k_conv3x3_bwd_weight<1>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_conv3x3_bwd_weight<1><<<grid, 256, smem, st>>>(x, Cin, H, W, Cout, Ho, Wo, y, dy, relu,
+                                                         dw, db);
+    } else {
+        e = cudaFuncSetAttribute(k_conv3x3_bwd_weight<2>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_conv3x3_bwd_weight<2><<<grid, 256, smem, st>>>(x, Cin, H, W, Cout, Ho, Wo, y, dy, relu,
+                                                         dw, db);
+    }
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+}  // namespace pfx
+
+// ------------------------------------------------------------------ C ABI
+using namespace pfx;
+
+#define PFX_CNN_RET(expr)                                                                  \
+    do {                                                                                   \
+        const cudaError_t e_ = (expr);                                                     \
+        if (e_ != cudaSuccess) return report_status(PFX_ERR_CUDA, cudaGetErrorString(e_)); \
+        return PFX_OK;                                                                     \
+    } while (0)
+
+#define PFX_CNN_LAUNCHED()                                                                 \
+    do {                                                                                   \
+        count_launches(1);                                                                 \
+        PFX_CNN_RET(cudaGetLastError());                                                   \
+    } while (0)
+
+extern "C" int pfx_pool_features(const double* F, int32_t d, int64_t n, int32_t pool, float* out,
+                                 void* stream) {
+    if (!F || !out || d < 1 || n < 1 || pool < 1)
+        return report_status(PFX_ERR_ARG, "pfx_pool_features: bad argument");
+    PFX_CNN_RET(cnn_pool_features(F, d, n, pool, out, (cudaStream_t)stream));
+}
+
+extern "C" int pfx_pooled_cost(const float* A, const float* B, int32_t d, int64_t P1, int64_t P2,
+                               float* out, void* stream) {
+    if (!A || !B || !out || d < 1 || P1 < 1 || P2 < 1 || P1 > 65535)
+        return report_status(PFX_ERR_ARG, "pfx_pooled_cost: bad argument (P1 <= 65535)");
+    PFX_CNN_RET(cnn_pooled_cost(A, B, d, P1, P2, out, (cudaStream_t)stream));
+}
+
+extern "C" int pfx_conv3x3_forward(const void* x, int32_t x_bf16, int32_t Cin, int32_t H,
+                                   int32_t W, const float* w, const float* b, int32_t Cout,
+                                   int32_t stride, int32_t relu, void* y, int32_t y_bf16,
+                                   void* stream) {
+    if (!x || !w || !b || !y || Cin < 1 || Cout < 1 || H < 1 || W < 1 ||
+        (stride != 1 && stride != 2) || (int64_t)H * W > (1LL << 31) / 64)
+        return report_status(PFX_ERR_ARG, "pfx_conv3x3_forward: bad argument");
+    PFX_CNN_RET(cnn_conv_forward(x, x_bf16, Cin, H, W, w, b, Cout, stride, relu, y, y_bf16,
+                                 (cudaStream_t)stream));
+}
+
+extern "C" int pfx_conv3x3_backward(const float* x, int32_t Cin, int32_t H, int32_t W,
+                                    const float* w, int32_t Cout, int32_t stride, const float* y,
+                                    int32_t relu, const float* dy, float* dx, float* dw, float* db,
+                                    void* stream) {
+    if (!x || !w || !y || !dy || !dw || !db || Cin < 1 || Cout < 1 || Cout > 64 || H < 1 ||
+        W < 1 || (stride != 1 && stride != 2))
+        return report_status(PFX_ERR_ARG, "pfx_conv3x3_backward: bad argument");
+    PFX_CNN_RET(cnn_conv_backward(x, Cin, H, W, w, Cout, stride, y, relu, dy, dx, dw, db,
+                                  (cudaStream_t)stream));
+}
+
+extern "C" int pfx_tile_max(const float* logits, int32_t H, int32_t W, int32_t n1, int32_t n2,
+                            int64_t hop, int64_t L, int64_t N, int64_t M, int32_t fpp,
+                            float* score, int32_t* argmax, void* stream) {
+    if (!logits || !score || !argmax || n1 < 1 || n2 < 1 || fpp < 1 || H < 1 || W < 1 ||
+        hop < 1 || L < 2)
+        return report_status(PFX_ERR_ARG, "pfx_tile_max: bad argument");
+    k_tile_max<<<(unsigned)(n1 * n2), 256, 0, (cudaStream_t)stream>>>(logits, H, W, n1, n2, hop,
+                                                                     L, N, M, fpp, score, argmax);
+    PFX_CNN_LAUNCHED();
+}
+
+extern "C" int pfx_tile_bce(const float* score, const uint8_t* label, int32_t n, float pos_weight,
+                            float* loss, float* dscore, void* stream) {
+    if (!score || !label || !loss || !dscore || n < 1)
+        return report_status(PFX_ERR_ARG, "pfx_tile_bce: bad argument");
+    k_tile_bce<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(score, label, n, pos_weight,
+                                                                    loss, dscore);
+    PFX_CNN_LAUNCHED();
+}
+
+extern "C" int pfx_tile_max_backward(const float* dscore, const int32_t* argmax, int32_t n,
+                                     float* dlogits, void* stream) {
+    if (!dscore || !argmax || !dlogits || n < 1)
+        return report_status(PFX_ERR_ARG, "pfx_tile_max_backward: bad argument");
+    k_tile_max_bwd<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(dscore, argmax, n,
+                                                                        dlogits);
+    PFX_CNN_LAUNCHED();
+}
+
+extern "C" int pfx_adam_step(float* param, const float* grad, float* m, float* v, int64_t n,
+                             float lr, float beta1, float beta2, float eps, int32_t step,
+                             void* stream) {
+    if (!param || !grad || !m || !v || n < 1 || step < 1)
+        return report_status(PFX_ERR_ARG, "pfx_adam_step: bad argument");
+    const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
+    k_adam<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(param, grad, m, v, n, lr, beta1,
+                                                                beta2, eps, c1, c2);
+    PFX_CNN_LAUNCHED();
+}
+
+extern "C" int pfx_tile_mask_from_scores(const float* score, int32_t n1, int32_t n2,
+                                         float threshold, int32_t dilation, uint8_t* mask,
+                                         void* stream) {
+    if (!score || !mask || n1 < 1 || n2 < 1 || dilation < 0)
+        return report_status(PFX_ERR_ARG, "pfx_tile_mask_from_scores: bad argument");
+    k_tile_mask<<<blocks_for((int64_t)n1 * n2, 256), 256, 0, (cudaStream_t)stream>>>(
+        score, n1, n2, threshold, dilation, mask);
+    PFX_CNN_LAUNCHED();
+}

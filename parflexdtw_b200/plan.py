@@ -193,6 +193,11 @@ class Plan:
             self._h, ct.c_void_p(F1_dev.data_ptr()), ct.c_void_p(F2_dev.data_ptr()),
             int(F1_dev.shape[0]), stream or current_stream_ptr()))
 
+    def set_warps(self, nw):
+        """Stage-1 warps per tile CTA (4, 8 or 16)."""
+        L.check(L.load().pfx_plan_set_warps(self._h, int(nw)))
+        self.warps = int(nw)
+
     def set_tile_mask(self, mask=None, stream=None):
         """Restrict cost building and stage 1 to the tiles set in ``mask``
         ((n1, n2) bool/uint8, host array or CUDA tensor); None lifts it."""

@@ -1,0 +1,270 @@
+"""Learned tile pruning: a small CNN proposes which L x L tiles the optimal
+path crosses, stage 1 runs only on those (and a ring around them), and the
+full-tile method is the fallback.
+
+The network reads the cost matrix average-pooled 16x16 (from 16-frame means
+of the normalised features: the pooled map of a bilinear cost, no full C):
+
+    conv3x3(1 -> 32, stride 2) + ReLU
+    conv3x3(32 -> 32, stride 2) + ReLU
+    conv3x3(32 -> 1, stride 1)           -> logits, 64 frames per pixel
+
+A tile's score is the max logit over its region.  Training (hand-written
+forward / backward / Adam kernels of csrc/cnn.cu, driven from here) uses
+labels that the full method itself produces: a tile is positive when the
+stitched path of the full-tile FP64 run has a point in it.  Inference keeps
+the tiles scoring above a threshold, dilated by one tile; when the pruned
+run's path reaches a tile next to a pruned one (or no endpoint qualifies) the
+full-tile method runs instead.  No counterpart in the reference.
+
+torch supplies device memory only; every computation is a library kernel.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+import numpy as np
+import torch
+
+from . import _lib
+from .plan import Plan, current_stream_ptr
+
+POOL = 16
+CH = 32
+STRIDES = (2, 2, 1)
+FPP = POOL * STRIDES[0] * STRIDES[1]  # frames per logit pixel
+DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data",
+                               "proposer_L2000.npz")
+
+
+def _p(t):
+    return ct.c_void_p(t.data_ptr()) if t is not None else ct.c_void_p(0)
+
+
+def tiles_on_path(wp, N, M, L):
+    """(n1, n2) uint8: tiles holding a point of the path wp ((K, 2) or (2, K))."""
+    wp = np.asarray(wp)
+    if wp.shape[0] == 2 and wp.shape[1] != 2:
+        wp = wp.T
+    hop = L - 1
+    n1, n2 = -(-(N - 1) // hop), -(-(M - 1) // hop)
+    lab = np.zeros((n1, n2), np.uint8)
+    r, c = wp[:, 0], wp[:, 1]
+    for di in (0, -1):  # a point on an overlap row belongs to both tiles
+        i = np.clip(r // hop + di, 0, n1 - 1)
+        okr = (r >= i * hop) & (r < i * hop + L)
+        for dj in (0, -1):
+            j = np.clip(c // hop + dj, 0, n2 - 1)
+            ok = okr & (c >= j * hop) & (c < j * hop + L)
+            lab[i[ok], j[ok]] = 1
+    return lab
+
+
+class TileProposer:
+    """The proposal network: parameters on the device, kernels from the C ABI."""
+
+    NAMES = ("w1", "b1", "w2", "b2", "w3", "b3")
+
+    def __init__(self, params=None, threshold=0.0, seed=0, device=None):
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None
+                                   else device)
+        self.threshold = float(threshold)
+        if params is None:
+            g = torch.Generator().manual_seed(seed)
+            shapes = {"w1": (CH, 1, 3, 3), "w2": (CH, CH, 3, 3), "w3": (1, CH, 3, 3)}
+            params = {}
+            for k, shp in shapes.items():
+                fan_in = shp[1] * 9
+                params[k] = torch.randn(shp, generator=g) * np.sqrt(2.0 / fan_in)
+            params["b1"] = torch.zeros(CH)
+            params["b2"] = torch.zeros(CH)
+            params["b3"] = torch.full((1,), -2.0)
+        self.params = {k: torch.as_tensor(np.asarray(params[k]), dtype=torch.float32)
+                       .to(self.device).contiguous() for k in self.NAMES}
+
+    # -- persistence -------------------------------------------------------
+    def save(self, path, **meta):
+        np.savez(path, threshold=self.threshold,
+                 **{k: v.cpu().numpy() for k, v in self.params.items()}, **meta)
+
+    @classmethod
+    def load(cls, path=DEFAULT_WEIGHTS):
+        z = np.load(path)
+        return cls({k: z[k] for k in cls.NAMES}, threshold=float(z["threshold"]))
+
+    # -- building blocks ---------------------------------------------------
+    @staticmethod
+    def pooled_cost(f1, f2):
+        """16x average-pooled cost matrix (P1 x P2, FP32) of device features
+        (d x N, d x M, FP64)."""
+        lib = _lib.load()
+        s = current_stream_ptr()
+        d, N = f1.shape
+        M = f2.shape[1]
+        P1, P2 = -(-N // POOL), -(-M // POOL)
+        A = torch.empty((d, P1), dtype=torch.float32, device=f1.device)
+        B = torch.empty((d, P2), dtype=torch.float32, device=f1.device)
+        out = torch.empty((P1, P2), dtype=torch.float32, device=f1.device)
+        _lib.check(lib.pfx_pool_features(_p(f1), d, N, POOL, _p(A), s))
+        _lib.check(lib.pfx_pool_features(_p(f2), d, M, POOL, _p(B), s))
+        _lib.check(lib.pfx_pooled_cost(_p(A), _p(B), d, P1, P2, _p(out), s))
+        return out
+
+    def forward(self, pooled, keep=False, bf16=False):
+        """Logits (H3 x W3) of one pooled map; with keep, also the layer
+        inputs and outputs for backward.  bf16: store the hidden activations
+        in bf16 (inference)."""
+        lib = _lib.load()
+        s = current_stream_ptr()
+        H, W = pooled.shape
+        x = pooled.contiguous()
+        acts = [x]
+        cin = 1
+        layers = ((self.params["w1"], self.params["b1"], CH, STRIDES[0], 1),
+                  (self.params["w2"], self.params["b2"], CH, STRIDES[1], 1),
+                  (self.params["w3"], self.params["b3"], 1, STRIDES[2], 0))
+        x_bf = 0
+        for li, (w, b, cout, st, relu) in enumerate(layers):
+            Ho, Wo = (H - 1) // st + 1, (W - 1) // st + 1
+            y_bf = 1 if (bf16 and li < 2) else 0
+            y = torch.empty((cout, Ho, Wo), dtype=torch.bfloat16 if y_bf else torch.float32,
+                            device=pooled.device)
+            _lib.check(lib.pfx_conv3x3_forward(_p(x), x_bf, cin, H, W, _p(w), _p(b), cout, st,
+                                               relu, _p(y), y_bf, s))
+            acts.append(y)
+            x, x_bf, cin, H, W = y, y_bf, cout, Ho, Wo
+        logits = x.reshape(H, W)
+        return (logits, acts) if keep else logits
+
+    @staticmethod
+    def tile_scores(logits, N, M, L):
+        lib = _lib.load()
+        hop = L - 1
+        n1, n2 = -(-(N - 1) // hop), -(-(M - 1) // hop)
+        H, W = logits.shape
+        score = torch.empty(n1 * n2, dtype=torch.float32, device=logits.device)
+        arg = torch.empty(n1 * n2, dtype=torch.int32, device=logits.device)
+        _lib.check(lib.pfx_tile_max(_p(logits), H, W, n1, n2, hop, L, N, M, FPP, _p(score),
+                                    _p(arg), current_stream_ptr()))
+        return score, arg, (n1, n2)
+
+    def propose(self, pooled, N, M, L, threshold=None, dilation=1):
+        """Device uint8 mask (n1 x n2) of the tiles to run, and the scores."""
+        logits = self.forward(pooled, bf16=True)
+        score, _, (n1, n2) = self.tile_scores(logits, N, M, L)
+        mask = torch.empty(n1 * n2, dtype=torch.uint8, device=pooled.device)
+        thr = self.threshold if threshold is None else float(threshold)
+        _lib.check(_lib.load().pfx_tile_mask_from_scores(_p(score), n1, n2, thr, int(dilation),
+                                                         _p(mask), current_stream_ptr()))
+        return mask.reshape(n1, n2), score.reshape(n1, n2)
+
+    # -- training ------------------------------------------------------------
+    def init_optimizer(self):
+        self.opt = {k: (torch.zeros_like(v), torch.zeros_like(v)) for k, v in self.params.items()}
+        self.opt_step = 0
+
+    def gradients(self, pooled, label, N, M, L, pos_weight):
+        """(loss, grads dict) for one map and its (n1, n2) tile labels."""
+        lib = _lib.load()
+        s = current_stream_ptr()
+        logits, acts = self.forward(pooled, keep=True)
+        score, arg, (n1, n2) = self.tile_scores(logits, N, M, L)
+        lab = torch.as_tensor(np.ascontiguousarray(label, dtype=np.uint8).reshape(-1),
+                              device=pooled.device)
+        loss = torch.zeros(1, dtype=torch.float32, device=pooled.device)
+        dscore = torch.empty_like(score)
+        _lib.check(lib.pfx_tile_bce(_p(score), _p(lab), n1 * n2, float(pos_weight), _p(loss),
+                                    _p(dscore), s))
+        dy = torch.zeros_like(logits)
+        _lib.check(lib.pfx_tile_max_backward(_p(dscore), _p(arg), n1 * n2, _p(dy), s))
+        grads = {k: torch.zeros_like(v) for k, v in self.params.items()}
+        layers = ((1, CH, STRIDES[0], 1), (CH, CH, STRIDES[1], 1), (CH, 1, STRIDES[2], 0))
+        dy = dy.reshape(1, *logits.shape)
+        for li in (2, 1, 0):
+            cin, cout, st, relu = layers[li]
+            x, y = acts[li], acts[li + 1]
+            H, W = x.shape[-2:]
+            dx = torch.empty((cin, H, W), dtype=torch.float32, device=x.device) if li else None
+            _lib.check(lib.pfx_conv3x3_backward(
+                _p(x), cin, H, W, _p(self.params[f"w{li + 1}"]), cout, st, _p(y), relu, _p(dy),
+                _p(dx), _p(grads[f"w{li + 1}"]), _p(grads[f"b{li + 1}"]), s))
+            dy = dx
+        return loss, grads
+
+    def step(self, grads, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
+        lib = _lib.load()
+        s = current_stream_ptr()
+        self.opt_step += 1
+        for k, p in self.params.items():
+            m, v = self.opt[k]
+            _lib.check(lib.pfx_adam_step(_p(p), _p(grads[k]), _p(m), _p(v), p.numel(), lr, b1,
+                                         b2, eps, self.opt_step, s))
+
+
+def _needs_fallback(wp, mask, N, M, L):
+    """True when the path has a point in a tile that has a pruned neighbour
+    (8-neighbourhood): it may have been cut off there."""
+    path_tiles = tiles_on_path(wp, N, M, L).astype(bool)
+    m = np.asarray(mask, bool)
+    n1, n2 = m.shape
+    p = np.pad(~m, 1, constant_values=False)
+    near = np.zeros_like(m)
+    for di in range(3):
+        for dj in range(3):
+            near |= p[di:di + n1, dj:dj + n2]
+    return bool(np.any(path_tiles & near))
+
+
+def parflex_pruned(F1, F2, steps, weights, beta, L, proposer=None, threshold=None,
+                   dilation=1, precision="fp64", plan=None, warps=None):
+    """ParFlex from features with learned tile pruning.
+
+    Returns ``(best_cost, wp[2, K], info)``; ``info`` has the tile counts, the
+    skipped fraction and whether the full-tile fallback ran (and why).
+    """
+    from .parflex import _features_to_device
+    f1 = _features_to_device(F1)
+    f2 = _features_to_device(F2)
+    N, M = int(f1.shape[1]), int(f2.shape[1])
+    if proposer is None:
+        proposer = TileProposer.load()
+    own = plan is None
+    if own:
+        plan = Plan(N, M, L, steps, weights, precision=precision)
+    pooled = proposer.pooled_cost(f1, f2)
+    mask, _ = proposer.propose(pooled, N, M, L, threshold, dilation)
+    m_host = mask.cpu().numpy()
+    kept = int(m_host.sum())
+    total = plan.n1 * plan.n2
+    info = {"tiles_total": total, "tiles_run": kept, "skipped_fraction": 1 - kept / total,
+            "fallback": False, "reason": None}
+    full_warps = plan.warps
+    best = wp = None
+    if kept:
+        plan.set_tile_mask(mask)
+        if warps or kept < 2 * 148:
+            plan.set_warps(warps or 16)
+        plan.load_features(f1, f2)
+        plan.run(None, beta)
+        try:
+            best, end, found, n = plan.result()
+            wp = plan.path(n)
+            if _needs_fallback(wp, m_host, N, M, L):
+                info.update(fallback=True, reason="path next to a pruned tile")
+        except ValueError:
+            info.update(fallback=True, reason="no endpoint among proposed tiles")
+    else:
+        info.update(fallback=True, reason="no tile proposed")
+    if info["fallback"]:
+        plan.set_tile_mask(None)
+        plan.set_warps(full_warps)
+        plan.load_features(f1, f2)
+        plan.run(None, beta)
+        best, end, found, n = plan.result()
+        wp = plan.path(n)
+        info["tiles_run"] = kept + total
+    else:
+        plan.set_tile_mask(None)
+        plan.set_warps(full_warps)
+    return best, np.ascontiguousarray(wp.T), info

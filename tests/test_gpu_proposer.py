@@ -1,0 +1,198 @@
+"""Learned tile proposer: its hand-written kernels against the numpy oracle
+(oracle/cnn_oracle.py), and the tile-masked alignment against the full one.
+
+Tolerances (FP32 kernels against FP64 numpy): forward values and gradients
+within 1e-4 of the largest magnitude of the compared array; tile scores and
+their argmax exact (the oracle is fed the device's own logits); bf16
+activation storage within 3e-2.  Masked runs: bit-exact against the
+unmasked run whenever the mask holds every tile the full path uses.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover - CPU container
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import parflexdtw_b200 as pf  # noqa: E402
+from parflexdtw_b200 import _lib, workloads as W  # noqa: E402
+from parflexdtw_b200.prune import (FPP, TileProposer, _needs_fallback, _p,  # noqa: E402
+                                   tiles_on_path)
+from oracle import cnn_oracle as CO  # noqa: E402
+
+STD = [(1, 1), (1, 2), (2, 1)]
+WTS = [2.0, 3.0, 3.0]
+TOL = 1e-4
+
+
+def close(a, b, tol=TOL):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    scale = max(np.abs(b).max(), 1e-30)
+    return np.abs(a - b).max() <= tol * scale
+
+
+def test_pooled_cost_vs_oracle():
+    rng = np.random.default_rng(0)
+    F1, F2 = W.warped_pair(rng, 1003, 1210)
+    f1, f2 = torch.from_numpy(F1).cuda(), torch.from_numpy(F2).cuda()
+    got = TileProposer.pooled_cost(f1, f2).cpu().numpy()
+    ref = CO.pooled_cost(CO.pool_features(F1, 16), CO.pool_features(F2, 16))
+    assert got.shape == ref.shape == (63, 76)
+    assert np.abs(got - ref).max() < 1e-5
+    # the pooled map is the block mean of the full cost matrix
+    C = W.cost_matrix_det(F1, F2)
+    assert abs(got[3, 5] - C[48:64, 80:96].mean()) < 1e-5
+
+
+@pytest.mark.parametrize("cin,cout,stride,relu,H,W", [(1, 32, 2, 1, 37, 51), (32, 32, 2, 1, 19, 23),
+                                                      (32, 1, 1, 0, 17, 30), (3, 5, 1, 1, 16, 16)])
+def test_conv_forward_backward_vs_oracle(cin, cout, stride, relu, H, W):
+    rng = np.random.default_rng(cin * 100 + cout)
+    x = rng.standard_normal((cin, H, W)).astype(np.float32)
+    w = (rng.standard_normal((cout, cin, 3, 3)) * 0.3).astype(np.float32)
+    b = (rng.standard_normal(cout) * 0.1).astype(np.float32)
+    xd, wd, bd = (torch.from_numpy(a).cuda() for a in (x, w, b))
+    Ho, Wo = (H - 1) // stride + 1, (W - 1) // stride + 1
+    y = torch.empty((cout, Ho, Wo), dtype=torch.float32, device="cuda")
+    lib = _lib.load()
+    s = pf.plan.current_stream_ptr()
+    _lib.check(lib.pfx_conv3x3_forward(_p(xd), 0, cin, H, W, _p(wd), _p(bd), cout, stride, relu,
+                                       _p(y), 0, s))
+    yref = CO.conv3x3(x, w, b, stride, relu)
+    assert close(y.cpu().numpy(), yref)
+    dy = rng.standard_normal(yref.shape).astype(np.float32)
+    dyd = torch.from_numpy(dy).cuda()
+    dx = torch.empty_like(xd)
+    dw = torch.zeros_like(wd)
+    db = torch.zeros_like(bd)
+    _lib.check(lib.pfx_conv3x3_backward(_p(xd), cin, H, W, _p(wd), cout, stride, _p(y), relu,
+                                        _p(dyd), _p(dx), _p(dw), _p(db), s))
+    rdx, rdw, rdb = CO.conv3x3_backward(x, w, stride, y.cpu().numpy(), relu, dy)
+    assert close(dx.cpu().numpy(), rdx)
+    assert close(dw.cpu().numpy(), rdw)
+    assert close(db.cpu().numpy(), rdb)
+    # bf16 storage of the output (inference)
+    yb = torch.empty((cout, Ho, Wo), dtype=torch.bfloat16, device="cuda")
+    _lib.check(lib.pfx_conv3x3_forward(_p(xd), 0, cin, H, W, _p(wd), _p(bd), cout, stride, relu,
+                                       _p(yb), 1, s))
+    assert close(yb.float().cpu().numpy(), yref, 3e-2)
+
+
+def test_network_gradients_vs_oracle():
+    """Loss and every parameter gradient of the whole proposer (three convs,
+    tile max, weighted BCE) against the numpy chain on the same input."""
+    rng = np.random.default_rng(3)
+    F1, F2 = W.warped_pair(rng, 2600, 3100, pad_frac=0.1)
+    N, M, L = F1.shape[1], F2.shape[1], 500
+    net = TileProposer(seed=1)
+    pooled = net.pooled_cost(torch.from_numpy(F1).cuda(), torch.from_numpy(F2).cuda())
+    hop = L - 1
+    n1, n2 = -(-(N - 1) // hop), -(-(M - 1) // hop)
+    label = (rng.random((n1, n2)) < 0.3).astype(np.uint8)
+    loss, grads = net.gradients(pooled, label, N, M, L, pos_weight=3.0)
+    P = {k: v.cpu().numpy().astype(np.float64) for k, v in net.params.items()}
+    x0 = pooled.cpu().numpy()[None].astype(np.float64)
+    a1 = CO.conv3x3(x0, P["w1"], P["b1"], 2, 1)
+    a2 = CO.conv3x3(a1, P["w2"], P["b2"], 2, 1)
+    a3 = CO.conv3x3(a2, P["w3"], P["b3"], 1, 0)
+    logits = net.forward(pooled).cpu().numpy()
+    assert close(logits, a3[0])
+    score, arg = CO.tile_max(logits, n1, n2, hop, L, N, M, FPP)
+    s_dev, a_dev, _ = net.tile_scores(net.forward(pooled), N, M, L)
+    assert np.array_equal(s_dev.cpu().numpy(), score.astype(np.float32))
+    assert np.array_equal(a_dev.cpu().numpy(), arg)
+    rl, ds = CO.bce(score, label.reshape(-1), 3.0)
+    assert abs(float(loss.item()) - rl) <= 1e-5 * abs(rl)
+    d3 = np.zeros_like(a3[0]).reshape(-1)
+    np.add.at(d3, arg, ds)
+    d3 = d3.reshape(1, *a3.shape[1:])
+    dx2, dw3, db3 = CO.conv3x3_backward(a2, P["w3"], 1, a3, 0, d3)
+    dx1, dw2, db2 = CO.conv3x3_backward(a1, P["w2"], 2, a2, 1, dx2)
+    _, dw1, db1 = CO.conv3x3_backward(x0, P["w1"], 2, a1, 1, dx1)
+    for k, ref in (("w3", dw3), ("b3", db3), ("w2", dw2), ("b2", db2), ("w1", dw1), ("b1", db1)):
+        assert close(grads[k].cpu().numpy(), ref, 1e-3), k
+
+
+def test_adam_and_training_lower_the_loss():
+    rng = np.random.default_rng(5)
+    pairs = [W.warped_pair(rng, n, int(n * 1.1), pad_frac=0.1) for n in (2500, 3300)]
+    net = TileProposer(seed=2)
+    net.init_optimizer()
+    data = []
+    for F1, F2 in pairs:
+        N, M = F1.shape[1], F2.shape[1]
+        best, wp = pf.parflex(W.cost_matrix_det(F1, F2), STD, WTS, 0.1, L=400, profile_dir=None)
+        data.append((net.pooled_cost(torch.from_numpy(F1).cuda(), torch.from_numpy(F2).cuda()),
+                     tiles_on_path(wp, N, M, 400), N, M))
+    losses = []
+    for ep in range(30):
+        tot = 0.0
+        for pooled, lab, N, M in data:
+            loss, g = net.gradients(pooled, lab, N, M, 400, pos_weight=4.0)
+            net.step(g, lr=3e-3)
+            tot += float(loss.item())
+        losses.append(tot)
+    assert losses[-1] < 0.7 * losses[0], losses[::5]
+    # one Adam update against its formula
+    p = torch.tensor([1.0, -2.0], device="cuda")
+    gr = torch.tensor([0.5, 0.25], device="cuda")
+    m = torch.zeros(2, device="cuda")
+    v = torch.zeros(2, device="cuda")
+    _lib.check(_lib.load().pfx_adam_step(_p(p), _p(gr), _p(m), _p(v), 2, 0.1, 0.9, 0.999, 1e-8, 1,
+                                         pf.plan.current_stream_ptr()))
+    ref = np.array([1.0, -2.0]) - 0.1 * np.sign([0.5, 0.25])
+    assert np.abs(p.cpu().numpy() - ref).max() < 1e-6
+
+
+def test_tile_mask_with_full_tiles_is_exact():
+    rng = np.random.default_rng(7)
+    F1, F2 = W.warped_pair(rng, 3000, 3400, pad_frac=0.1)
+    N, M, L = F1.shape[1], F2.shape[1], 400
+    f1, f2 = torch.from_numpy(F1).cuda(), torch.from_numpy(F2).cuda()
+    plan = pf.Plan(N, M, L, STD, WTS)
+    plan.load_features(f1, f2)
+    plan.run(None, 0.1)
+    best, end, _, n = plan.result()
+    wp = plan.path(n)
+    D_full = plan.host("D_ARR")
+    # all tiles set: identical to the unmasked run
+    plan.set_tile_mask(np.ones((plan.n1, plan.n2), np.uint8))
+    plan.load_features(f1, f2)
+    plan.run(None, 0.1)
+    b2, e2, _, n2 = plan.result()
+    assert b2 == best and e2 == end and np.array_equal(plan.path(n2), wp)
+    assert np.array_equal(plan.host("D_ARR"), D_full)
+    # the path's tiles and a ring of one tile: same path, fewer tiles
+    lab = tiles_on_path(wp, N, M, L).astype(bool)
+    ring = np.pad(lab, 1)
+    dil = np.zeros_like(lab)
+    for di in range(3):
+        for dj in range(3):
+            dil |= ring[di:di + lab.shape[0], dj:dj + lab.shape[1]]
+    assert dil.sum() < lab.size
+    for mask in (dil, torch.from_numpy(dil.astype(np.uint8)).cuda()):
+        plan.set_tile_mask(mask)
+        plan.set_warps(16)
+        plan.load_features(f1, f2)
+        plan.run(None, 0.1)
+        b3, e3, _, n3 = plan.result()
+        assert b3 == best and e3 == end and np.array_equal(plan.path(n3), wp)
+        assert not _needs_fallback(plan.path(n3), dil, N, M, L)
+    plan.set_tile_mask(None)
+
+
+def test_parflex_pruned_equals_full_and_falls_back():
+    rng = np.random.default_rng(8)
+    F1, F2 = W.warped_pair(rng, 4200, 4600, pad_frac=0.1)
+    C = W.cost_matrix_det(F1, F2)
+    best, wp = pf.parflex(C, STD, WTS, 0.1, L=500, profile_dir=None)
+    # an untrained network proposes little: the fallback must give the full path
+    net = TileProposer(seed=4)
+    b1, wp1, info = pf.parflex_pruned(F1, F2, STD, WTS, 0.1, 500, proposer=net, threshold=50.0)
+    assert info["fallback"] and b1 == best and np.array_equal(wp1, wp)
+    # a threshold that keeps everything: no fallback, same result
+    b2, wp2, info2 = pf.parflex_pruned(F1, F2, STD, WTS, 0.1, 500, proposer=net, threshold=-1e30)
+    assert not info2["fallback"] and info2["tiles_run"] == info2["tiles_total"]
+    assert b2 == best and np.array_equal(wp2, wp)
