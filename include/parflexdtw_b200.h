@@ -319,6 +319,9 @@ int pfx_pool_features(const double *F, int32_t d, int64_t n, int32_t pool, float
  * pooled features, the block means of the cost matrix. */
 int pfx_pooled_cost(const float *A, const float *B, int32_t d, int64_t P1, int64_t P2,
                     float *out, void *stream);
+/* In place: x <- (x - row mean - column mean + mean) / std over the
+ * P1 x P2 map (the proposer's input).  scratch: P1 + P2 + 2 floats. */
+int pfx_pooled_center(float *x, int64_t P1, int64_t P2, float *scratch, void *stream);
 /* y (Cout x Ho x Wo) = act(conv3x3(x) + b), zero padding 1, stride 1 or 2,
  * Ho = (H - 1) / stride + 1; w is [Cout][Cin][3][3]; act = ReLU if relu. */
 int pfx_conv3x3_forward(const void *x, int32_t x_bf16, int32_t Cin, int32_t H, int32_t W,

@@ -27,6 +27,12 @@ def pooled_cost(A, B):
     return 1.0 - np.asarray(A, np.float64).T @ np.asarray(B, np.float64)
 
 
+def center(P):
+    P = np.asarray(P, np.float64)
+    X = P - P.mean(axis=1, keepdims=True) - P.mean(axis=0, keepdims=True) + P.mean()
+    return X / np.sqrt(np.mean(X * X))
+
+
 def _taps(xp, ky, kx, stride, Ho, Wo):
     return xp[:, ky:ky + stride * (Ho - 1) + 1:stride, kx:kx + stride * (Wo - 1) + 1:stride]
 

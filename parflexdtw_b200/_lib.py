@@ -82,6 +82,7 @@ SIGNATURES = [
     ("pfx_batch_copy_paths", ct.c_int, [_vp, _vp, _i64p, _i64p, _i64]),
     ("pfx_pool_features", ct.c_int, [_vp, _i32, _i64, _i32, _vp, _vp]),
     ("pfx_pooled_cost", ct.c_int, [_vp, _vp, _i32, _i64, _i64, _vp, _vp]),
+    ("pfx_pooled_center", ct.c_int, [_vp, _i64, _i64, _vp, _vp]),
     ("pfx_conv3x3_forward", ct.c_int, [_vp, _i32, _i32, _i32, _i32, _vp, _vp, _i32, _i32, _i32,
                                        _vp, _i32, _vp]),
     ("pfx_conv3x3_backward", ct.c_int, [_vp, _i32, _i32, _i32, _vp, _i32, _i32, _vp, _i32, _vp,

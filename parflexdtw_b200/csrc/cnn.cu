@@ -56,6 +56,71 @@ __global__ void k_pooled_cost(const float* __restrict__ A, const float* __restri
     out[i * P2 + j] = 1.f - acc;
 }
 
+// Double centring and standardisation of a P1 x P2 map, in place:
+// x <- (x - rowmean - colmean + mean) / std.  Removes the per-block offsets
+// that a whole row or column of the pooled cost shares, leaving the
+// diagonal ridge of the alignment.  sc: [P1 + P2 + 2] floats of scratch.
+__global__ void k_row_mean(const float* __restrict__ x, int64_t P1, int64_t P2,
+                           float* __restrict__ rm) {
+    const int64_t i = blockIdx.x;
+    float s = 0.f;
+    for (int64_t j = threadIdx.x; j < P2; j += blockDim.x) s += x[i * P2 + j];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    __shared__ float ws[32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += ws[w];
+        rm[i] = t / (float)P2;
+    }
+}
+
+__global__ void k_col_mean(const float* __restrict__ x, int64_t P1, int64_t P2,
+                           float* __restrict__ cm) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= P2) return;
+    float s = 0.f;
+    for (int64_t i = 0; i < P1; ++i) s += x[i * P2 + j];
+    cm[j] = s / (float)P1;
+}
+
+// sc[P1 + P2] = grand mean (mean of the row means), sc[P1 + P2 + 1] = 0
+__global__ void k_grand_mean(float* __restrict__ sc, int64_t P1, int64_t P2) {
+    float s = 0.f;
+    for (int64_t i = threadIdx.x; i < P1; i += blockDim.x) s += sc[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    __shared__ float ws[32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += ws[w];
+        sc[P1 + P2] = t / (float)P1;
+        sc[P1 + P2 + 1] = 0.f;
+    }
+}
+
+__global__ void k_center(float* __restrict__ x, int64_t P1, int64_t P2, float* __restrict__ sc) {
+    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    float v = 0.f;
+    if (q < P1 * P2) {
+        const int64_t i = q / P2, j = q % P2;
+        v = x[q] - sc[i] - sc[P1 + j] + sc[P1 + P2];
+        x[q] = v;
+    }
+    float s = v * v;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(sc + P1 + P2 + 1, s);
+}
+
+__global__ void k_scale(float* __restrict__ x, int64_t n, const float* __restrict__ ss) {
+    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const float var = *ss / (float)n;
+    x[q] = var > 0.f ? x[q] * rsqrtf(var) : 0.f;
+}
+
 // --------------------------------------------------------------------------
 // 3x3 convolution, forward.  A CTA computes a 16 x 16 tile of output pixels
 // for up to 32 output channels; per input channel the input patch and that
@@ -421,6 +486,21 @@ extern "C" int pfx_pooled_cost(const float* A, const float* B, int32_t d, int64_
     if (!A || !B || !out || d < 1 || P1 < 1 || P2 < 1 || P1 > 65535)
         return report_status(PFX_ERR_ARG, "pfx_pooled_cost: bad argument (P1 <= 65535)");
     PFX_CNN_RET(cnn_pooled_cost(A, B, d, P1, P2, out, (cudaStream_t)stream));
+}
+
+extern "C" int pfx_pooled_center(float* x, int64_t P1, int64_t P2, float* scratch,
+                                 void* stream) {
+    if (!x || !scratch || P1 < 1 || P2 < 1)
+        return report_status(PFX_ERR_ARG, "pfx_pooled_center: bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t n = P1 * P2;
+    k_row_mean<<<(unsigned)P1, 256, 0, st>>>(x, P1, P2, scratch);
+    k_col_mean<<<blocks_for(P2, 256), 256, 0, st>>>(x, P1, P2, scratch + P1);
+    k_grand_mean<<<1, 1024, 0, st>>>(scratch, P1, P2);
+    k_center<<<blocks_for(n, 256), 256, 0, st>>>(x, P1, P2, scratch);
+    k_scale<<<blocks_for(n, 256), 256, 0, st>>>(x, n, scratch + P1 + P2 + 1);
+    count_launches(5);
+    PFX_CNN_RET(cudaGetLastError());
 }
 
 extern "C" int pfx_conv3x3_forward(const void* x, int32_t x_bf16, int32_t Cin, int32_t H,

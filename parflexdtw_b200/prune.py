@@ -3,7 +3,8 @@ path crosses, stage 1 runs only on those (and a ring around them), and the
 full-tile method is the fallback.
 
 The network reads the cost matrix average-pooled 16x16 (from 16-frame means
-of the normalised features: the pooled map of a bilinear cost, no full C):
+of the normalised features: the pooled map of a bilinear cost, no full C),
+double centred (row and column means removed) and standardised:
 
     conv3x3(1 -> 32, stride 2) + ReLU
     conv3x3(32 -> 32, stride 2) + ReLU
@@ -95,9 +96,10 @@ class TileProposer:
 
     # -- building blocks ---------------------------------------------------
     @staticmethod
-    def pooled_cost(f1, f2):
+    def pooled_cost(f1, f2, center=True):
         """16x average-pooled cost matrix (P1 x P2, FP32) of device features
-        (d x N, d x M, FP64)."""
+        (d x N, d x M, FP64); with center (the network's input), double
+        centred and standardised (pfx_pooled_center)."""
         lib = _lib.load()
         s = current_stream_ptr()
         d, N = f1.shape
@@ -109,6 +111,9 @@ class TileProposer:
         _lib.check(lib.pfx_pool_features(_p(f1), d, N, POOL, _p(A), s))
         _lib.check(lib.pfx_pool_features(_p(f2), d, M, POOL, _p(B), s))
         _lib.check(lib.pfx_pooled_cost(_p(A), _p(B), d, P1, P2, _p(out), s))
+        if center:
+            sc = torch.empty(P1 + P2 + 2, dtype=torch.float32, device=f1.device)
+            _lib.check(lib.pfx_pooled_center(_p(out), P1, P2, _p(sc), s))
         return out
 
     def forward(self, pooled, keep=False, bf16=False):

@@ -37,13 +37,15 @@ def test_pooled_cost_vs_oracle():
     rng = np.random.default_rng(0)
     F1, F2 = W.warped_pair(rng, 1003, 1210)
     f1, f2 = torch.from_numpy(F1).cuda(), torch.from_numpy(F2).cuda()
-    got = TileProposer.pooled_cost(f1, f2).cpu().numpy()
+    got = TileProposer.pooled_cost(f1, f2, center=False).cpu().numpy()
     ref = CO.pooled_cost(CO.pool_features(F1, 16), CO.pool_features(F2, 16))
     assert got.shape == ref.shape == (63, 76)
     assert np.abs(got - ref).max() < 1e-5
     # the pooled map is the block mean of the full cost matrix
     C = W.cost_matrix_det(F1, F2)
     assert abs(got[3, 5] - C[48:64, 80:96].mean()) < 1e-5
+    cen = TileProposer.pooled_cost(f1, f2).cpu().numpy()
+    assert np.abs(cen - CO.center(ref)).max() < 1e-3
 
 
 @pytest.mark.parametrize("cin,cout,stride,relu,H,W", [(1, 32, 2, 1, 37, 51), (32, 32, 2, 1, 19, 23),
