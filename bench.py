@@ -789,6 +789,171 @@ def precision_arm(args, spec):
         dist.destroy_process_group()
 
 
+PRUNE_METRIC = ("DP cells/s and pairs/s (ParFlex, learned tile pruning + FP64 DP vs the "
+                "full-tile FP64 form; cells counted on the full tiling)")
+
+
+def prune_reference_arm(args, spec):
+    """CPU restatement on the first tile rows of the first pair."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import build_oracle, oracle
+    build_oracle.build()
+    threads = os.cpu_count() or 1
+    rng_pairs = W.make_batch(W.BatchSpec("x", 1, spec.n_lo, spec.n_hi, pad_frac=spec.pad_frac,
+                                         seed=spec.seed))
+    F1, F2 = rng_pairs[0]
+    Lb = spec.L_choices[0]
+    rows = min(F1.shape[1], args.ref_tile_rows * (Lb - 1) + 1)
+    C = W.cost_matrix_host(F1[:, :rows], F2)
+    cells, n1, n2 = tile_cells(C.shape[0], C.shape[1], Lb)
+    times = []
+    for s_ in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        oracle.parflex_full(C, spec.steps, spec.weights, spec.beta, Lb, threads=threads)
+        if s_ >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    v = cells * len(times) / tot
+    line = {
+        "impl": "reference", "metric": PRUNE_METRIC, "value": v, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(spec.describe(), parallelism="replicas"),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"the first {n1} tile rows of the first pair ({C.shape[0]} x "
+                                   f"{C.shape[1]}, {cells} cells) per step, full tiling, FP64"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def prune_arm(args, spec):
+    import torch
+    import torch.distributed as dist
+
+    import parflexdtw_b200 as pf
+    from parflexdtw_b200 import _lib
+    from parflexdtw_b200.prune import TileProposer
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    lib = _lib.load()
+    Lb = spec.L_choices[0]
+    n_pairs = args.pairs or spec.n_pairs
+    t0 = time.perf_counter()
+    spec_r = W.BatchSpec(spec.name, n_pairs, spec.n_lo, spec.n_hi, pad_frac=spec.pad_frac,
+                         seed=spec.seed + 1000 * rank)
+    pairs = W.make_batch(spec_r)
+    gen_s = time.perf_counter() - t0
+    net = TileProposer.load()
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    def run_pair(F1, F2, reps):
+        """(plain ms, pruned ms, cells, results) of one pair; features resident."""
+        N, M = F1.shape[1], F2.shape[1]
+        f1, f2 = torch.from_numpy(F1).to(dev), torch.from_numpy(F2).to(dev)
+        plan = pf.Plan(N, M, Lb, spec.steps, spec.weights)
+        cells = tile_cells(N, M, Lb)[0]
+        out = []
+        for _ in range(reps):
+            a, b = ev(), ev()
+            torch.cuda.synchronize()
+            a.record()
+            plan.load_features(f1, f2)
+            plan.run(None, spec.beta)
+            b.record()
+            best, end, _, n = plan.result()
+            wp = plan.path(n)
+            c, d_ = ev(), ev()
+            torch.cuda.synchronize()
+            c.record()
+            bp, wpp, info = pf.parflex_pruned(f1, f2, spec.steps, spec.weights, spec.beta, Lb,
+                                              proposer=net, plan=plan)
+            d_.record()
+            torch.cuda.synchronize()
+            out.append((a.elapsed_time(b), c.elapsed_time(d_), best, wp, bp, wpp, info))
+        plan.close()
+        del f1, f2
+        return cells, out
+
+    # warm-up on the first pair
+    run_pair(*pairs[0], max(1, args.warmup))
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    plain_ms = pruned_ms = 0.0
+    cells_tot = 0
+    agree = fallbacks = 0
+    reasons = {}
+    skipped, run_tiles, all_tiles = [], 0, 0
+    launches0 = lib.pfx_kernel_launches()
+    with ClockSampler(uuid) as clk:
+        for step in range(args.steps):
+            for F1, F2 in pairs:
+                cells, res = run_pair(F1, F2, 1)
+                pms, qms, best, wp, bp, wpp, info = res[0]
+                plain_ms += pms
+                pruned_ms += qms
+                cells_tot += cells
+                if step == 0:
+                    agree += int(bp == best and np.array_equal(wpp, wp.T))
+                    fallbacks += int(info["fallback"])
+                    if info["fallback"]:
+                        reasons[info["reason"]] = reasons.get(info["reason"], 0) + 1
+                    skipped.append(info["skipped_fraction"])
+                    run_tiles += info["tiles_run"]
+                    all_tiles += info["tiles_total"]
+    launches = lib.pfx_kernel_launches() - launches0
+    if ws > 1:
+        t = torch.tensor([plain_ms, pruned_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        plain_ms, pruned_ms = (float(x) for x in t.tolist())
+    v_pruned = cells_tot * ws / (pruned_ms / 1e3)
+    v_plain = cells_tot * ws / (plain_ms / 1e3)
+    if rank == 0:
+        line = {
+            "metric": PRUNE_METRIC, "value": v_pruned, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": pruned_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(spec.describe(), pairs_run=n_pairs, cells_per_step=cells_tot // args.steps,
+                           generation_seconds=gen_s, parallelism="replicas",
+                           input="features resident in HBM; each timed pair builds its cost",
+                           timing="CUDA events around each pair's full call (host checks of "
+                                  "the proposer mask and the fallback included); plan "
+                                  "allocation outside", l2="cost slabs larger than L2"),
+            "pairs_per_s": ws * n_pairs * args.steps / (pruned_ms / 1e3),
+            "plain_fp64_full_tiles": {"value": v_plain, "unit": UNIT,
+                                      "ms_per_step": plain_ms / args.steps,
+                                      "pairs_per_s": ws * n_pairs * args.steps / (plain_ms / 1e3)},
+            "speedup_over_plain": v_pruned / v_plain,
+            "pruning": {"tiles_skipped_fraction_mean": float(np.mean(skipped)),
+                        "tiles_run_fraction_incl_fallbacks": run_tiles / all_tiles,
+                        "fallback_rate": fallbacks / n_pairs,
+                        "fallback_reasons": reasons,
+                        "exact_path_agreement_rate": agree / n_pairs,
+                        "proposer": "3 conv layers, 32 channels, bf16 activations, "
+                                    "parflexdtw_b200/data/proposer_L2000.npz",
+                        "threshold": net.threshold, "dilation_tiles": 1},
+            "gpu_launches": int(launches), "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -811,6 +976,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     spec = W.WORKLOADS[args.workload]
+    if isinstance(spec, W.PruneSpec):
+        (prune_reference_arm if args.impl == "reference" else prune_arm)(args, spec)
+        return
     if isinstance(spec, W.PrecisionSpec):
         (precision_reference_arm if args.impl == "reference" else precision_arm)(args, spec)
         return

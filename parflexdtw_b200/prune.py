@@ -15,8 +15,8 @@ forward / backward / Adam kernels of csrc/cnn.cu, driven from here) uses
 labels that the full method itself produces: a tile is positive when the
 stitched path of the full-tile FP64 run has a point in it.  Inference keeps
 the tiles scoring above a threshold, dilated by one tile; when the pruned
-run's path reaches a tile next to a pruned one (or no endpoint qualifies) the
-full-tile method runs instead.  No counterpart in the reference.
+run's path comes within 64 to 128 cells of a pruned tile (or no endpoint
+qualifies) the full-tile method runs instead.  No counterpart in the reference.
 
 torch supplies device memory only; every computation is a library kernel.
 """
@@ -207,18 +207,32 @@ class TileProposer:
                                          b2, eps, self.opt_step, s))
 
 
-def _needs_fallback(wp, mask, N, M, L):
-    """True when the path has a point in a tile that has a pruned neighbour
-    (8-neighbourhood): it may have been cut off there."""
-    path_tiles = tiles_on_path(wp, N, M, L).astype(bool)
+FALLBACK_MARGIN = 64  # cells
+
+
+def _needs_fallback(wp, mask, N, M, L, margin=FALLBACK_MARGIN):
+    """True when the path comes within about `margin` cells of a pruned
+    tile's cells: there it may have been cut off, and the full-tile method
+    decides.  Works on a grid of margin x margin cell blocks; a block counts
+    as pruned when any of its cells lies in a pruned tile, and that map is
+    dilated by one block (so the distance tested is margin to 2 margin)."""
+    wp = np.asarray(wp)
+    if wp.shape[0] == 2 and wp.shape[1] != 2:
+        wp = wp.T
     m = np.asarray(mask, bool)
-    n1, n2 = m.shape
-    p = np.pad(~m, 1, constant_values=False)
-    near = np.zeros_like(m)
+    if m.all():
+        return False
+    hop, B = L - 1, int(margin)
+    nb1, nb2 = -(-N // B), -(-M // B)
+    pm = np.zeros((nb1 + 2, nb2 + 2), bool)  # one block of border for the dilation
+    for i, j in np.argwhere(~m):
+        pm[1 + i * hop // B:2 + min(N - 1, i * hop + L - 1) // B,
+           1 + j * hop // B:2 + min(M - 1, j * hop + L - 1) // B] = True
+    near = np.zeros((nb1, nb2), bool)
     for di in range(3):
         for dj in range(3):
-            near |= p[di:di + n1, dj:dj + n2]
-    return bool(np.any(path_tiles & near))
+            near |= pm[di:di + nb1, dj:dj + nb2]
+    return bool(near[wp[:, 0] // B, wp[:, 1] // B].any())
 
 
 def parflex_pruned(F1, F2, steps, weights, beta, L, proposer=None, threshold=None,
@@ -256,7 +270,7 @@ def parflex_pruned(F1, F2, steps, weights, beta, L, proposer=None, threshold=Non
             best, end, found, n = plan.result()
             wp = plan.path(n)
             if _needs_fallback(wp, m_host, N, M, L):
-                info.update(fallback=True, reason="path next to a pruned tile")
+                info.update(fallback=True, reason="path near a pruned tile")
         except ValueError:
             info.update(fallback=True, reason="no endpoint among proposed tiles")
     else:

@@ -263,8 +263,20 @@ def make_precision_batch(spec: PrecisionSpec, seed_offset: int = 0, n_pairs=None
 PRECISION2048 = PrecisionSpec("gauss128_batch2048_N1000-8000_L1000_fp32_vs_fp64", 2048,
                               1000, 8000)
 
+
+
+class PruneSpec(BatchSpec):
+    """Named learned-pruning workload: long pairs aligned one at a time with
+    the full-tile FP64 method and with the tile proposer."""
+
+
+# 64 pairs, N ~ U(40000, 60000), M = N x U(0.7, 1.4), 12-d chroma-like
+# features with 0-10 % unrelated padding per end, L = 2000.
+PRUNE64 = PruneSpec("chroma12_pairs64_N40000-60000_L2000_pruned", 64, 40000, 60000,
+                    L_choices=(2000,), pad_frac=0.10)
+
 WORKLOADS = {"config0": CONFIG0, "config1": CONFIG1, "ncu_small": NCU_SMALL,
-             "batch256": BATCH256, "precision2048": PRECISION2048}
+             "batch256": BATCH256, "precision2048": PRECISION2048, "prune64": PRUNE64}
 
 
 def make_pair(spec: PairSpec):
