@@ -281,6 +281,14 @@ int pfx_batch_features(pfx_batch *batch, int32_t i, double **F1, double **F2);
  * cost into it).  pfx_result / pfx_copy_path / pfx_plan_buffer read pair
  * i's results after pfx_batch_run. */
 int pfx_batch_plan(pfx_batch *batch, int32_t i, pfx_plan **plan);
+/* Restricts every pair to the tiles set in its mask (masks: the pairs' n1*n2
+ * masks concatenated in pair order; device memory when on_device): cost
+ * slabs are built and stage 1 runs only there (the pool now holds only
+ * those slabs, so waves are repacked), other tiles keep +inf edges.  For the
+ * learned tile proposer; synchronises `stream`; invalidates the recorded
+ * graph.  No reference counterpart. */
+int pfx_batch_set_masks(pfx_batch *batch, const uint8_t *masks, int32_t on_device,
+                        void *stream);
 /* Aligns every pair (asynchronous on `stream`).  use_graph = 1 records the
  * launch sequence into a CUDA graph on the first call (and again when beta
  * changes) and replays it; 0 launches directly. */

@@ -8,7 +8,7 @@ hand-written sm_100a CUDA kernels behind the C ABI in
 ``include/parflexdtw_b200.h``; there is no CPU path.
 """
 from .batch import Batch, parflex_batch  # noqa: F401
-from .prune import TileProposer, parflex_pruned  # noqa: F401
+from .prune import PrunedBatch, TileProposer, parflex_pruned  # noqa: F401
 from .parflex import (  # noqa: F401
     DEFAULT_CHUNK_LENGTH,
     ChunksDict,

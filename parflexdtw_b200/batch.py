@@ -108,6 +108,17 @@ class Batch:
                                      f"{tuple(dst.shape)}")
                 dst.copy_(t, non_blocking=non_blocking)
 
+    def set_masks(self, masks, stream=None):
+        """Restrict each pair to its tile mask (a CUDA uint8 tensor holding
+        the pairs' (n1, n2) masks concatenated in pair order)."""
+        m = masks.to(torch.uint8).contiguous()
+        _lib.check(_lib.load().pfx_batch_set_masks(self._h, ct.c_void_p(m.data_ptr()), 1,
+                                                   stream or current_stream_ptr()))
+        info = (ct.c_int64 * 8)()
+        _lib.check(_lib.load().pfx_batch_info(self._h, info))
+        self.waves = int(info[1])
+        self.masked = True
+
     def run(self, beta, use_graph=True, stream=None):
         """Aligns every pair (asynchronous on the current stream)."""
         _lib.check(_lib.load().pfx_batch_run(self._h, float(beta), 1 if use_graph else 0,

@@ -78,6 +78,7 @@ struct pfx_batch {
     cudaGraphExec_t exec = nullptr;
     double graph_beta = 0.0;
     int64_t graph_kernels = 0;  // kernel launches recorded in the graph
+    int masked = 0;             // pfx_batch_set_masks: only masked-in tiles run
     // phase events of the last direct run: per wave, before cost building,
     // before stage 1, after stage 1, after the stage-2 join
     std::vector<cudaEvent_t> phase_ev;
@@ -236,7 +237,7 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
     const size_t off_desc = arena;
     arena += round256(b->total_tiles * sizeof(TileDesc));
     const size_t off_heads = arena;
-    arena += round256((size_t)waves * sizeof(int));
+    arena += round256((size_t)n * sizeof(int));  // up to one wave per pair
     const size_t off_status = arena;
     arena += 256;
     const size_t off_pout = arena;
@@ -325,6 +326,106 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
     return PFX_OK;
 }
 
+extern "C" int pfx_batch_set_masks(pfx_batch* b, const uint8_t* masks, int32_t on_device,
+                                   void* stream) {
+    if (!b || !masks) return errf(PFX_ERR_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n = b->n;
+    std::vector<int64_t> moff(n + 1, 0);
+    for (int i = 0; i < n; ++i)
+        moff[i + 1] = moff[i] + (int64_t)b->plans[i].g.n1 * b->plans[i].g.n2;
+    std::vector<uint8_t> m((size_t)moff[n]);
+    if (on_device) {
+        BCK(cudaMemcpyAsync(m.data(), masks, m.size(), cudaMemcpyDeviceToHost, s));
+        BCK(cudaStreamSynchronize(s));
+    } else {
+        memcpy(m.data(), masks, m.size());
+    }
+    // slots: kept tiles numbered in tile order; slab bytes per pair
+    std::vector<std::vector<int32_t>> slots(n);
+    std::vector<int64_t> bytes(n);
+    for (int i = 0; i < n; ++i) {
+        const pfx_plan& p = b->plans[i];
+        const int nt = p.g.n1 * p.g.n2;
+        slots[i].assign(nt, -1);
+        int kept = 0;
+        for (int t = 0; t < nt; ++t)
+            if (m[moff[i] + t]) slots[i][t] = kept++;
+        bytes[i] = (((int64_t)kept * p.skew_stride * (p.fp32 ? 4 : 8)) + 255) & ~(int64_t)255;
+    }
+    // waves over the existing slab pool, largest first
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return bytes[a] > bytes[c]; });
+    if (bytes[order[0]] > (int64_t)b->slab_bytes)
+        return errf(PFX_ERR_TOO_LARGE, "pair %d needs %lld B of cost slabs; pool %zu B", order[0],
+                    (long long)bytes[order[0]], b->slab_bytes);
+    std::vector<int> wave_pairs, wave_first{0};
+    std::vector<int64_t> off(n);
+    int64_t cur = 0;
+    for (int q = 0; q < n; ++q) {
+        const int i = order[q];
+        if (cur + bytes[i] > (int64_t)b->slab_bytes) {
+            wave_first.push_back(q);
+            cur = 0;
+        }
+        off[i] = cur;
+        cur += bytes[i];
+        wave_pairs.push_back(i);
+    }
+    wave_first.push_back(n);
+    // plans: slab base, slot map, mask; queues of the kept tiles
+    std::vector<TileDesc> all;
+    std::vector<int64_t> wdo, wt;
+    const int waves = (int)wave_first.size() - 1;
+    for (int w = 0; w < waves; ++w) {
+        wdo.push_back((int64_t)all.size());
+        std::vector<TileDesc> wv;
+        for (int q = wave_first[w]; q < wave_first[w + 1]; ++q) {
+            const int i = wave_pairs[q];
+            pfx_plan& p = b->plans[i];
+            p.Csk = reinterpret_cast<char*>(b->slabs) + off[i];
+            const int nt = p.g.n1 * p.g.n2;
+            BCK(cudaMemcpy(p.tile_slot, slots[i].data(), (size_t)nt * 4, cudaMemcpyHostToDevice));
+            BCK(cudaMemcpy(p.tile_mask, m.data() + moff[i], (size_t)nt, cudaMemcpyHostToDevice));
+            std::vector<TileDesc> pd((size_t)nt);
+            plan_tile_descs(&p, p.Csk, pd.data(), slots[i].data());
+            // the pair's own queue keeps every tile (pfx_stage1 compacts it by the mask)
+            BCK(cudaMemcpy(p.descs, pd.data(), pd.size() * sizeof(TileDesc),
+                           cudaMemcpyHostToDevice));
+            BCK(launch_compact_descs(p.descs, nt, p.tile_mask, p.descs_sub, p.nsub, 0));
+            for (const TileDesc& d : pd)
+                if (slots[i][d.tile] >= 0) wv.push_back(d);
+            p.mask_active = 1;
+            p.s2.tile_slot = p.tile_slot;
+        }
+        std::stable_sort(wv.begin(), wv.end(), [](const TileDesc& a, const TileDesc& c) {
+            return (int64_t)a.R * a.W > (int64_t)c.R * c.W;
+        });
+        wt.push_back((int64_t)wv.size());
+        all.insert(all.end(), wv.begin(), wv.end());
+    }
+    if (!all.empty())
+        BCK(cudaMemcpy(b->descs, all.data(), all.size() * sizeof(TileDesc),
+                       cudaMemcpyHostToDevice));
+    BCK(cudaDeviceSynchronize());
+    b->wave_pairs = wave_pairs;
+    b->wave_first = wave_first;
+    b->wave_desc_off = wdo;
+    b->wave_tiles = wt;
+    b->max_wave_tiles = 0;
+    for (int64_t x : wt) b->max_wave_tiles = std::max(b->max_wave_tiles, x);
+    b->masked = 1;
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    for (cudaEvent_t e : b->phase_ev) cudaEventDestroy(e);
+    b->phase_ev.clear();
+    b->phase_valid = false;
+    return PFX_OK;
+}
+
 extern "C" int pfx_batch_info(const pfx_batch* b, int64_t* info) {
     if (!b || !info) return errf(PFX_ERR_ARG, "null argument");
     info[0] = b->n;
@@ -375,20 +476,26 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
             pfx_plan& p = b->plans[i];
             const double* F1 = b->fin + b->fin_off[i];
             const double* F2 = F1 + (int64_t)b->d * p.g.N;
+            const int32_t* slot = b->masked ? p.tile_slot : nullptr;
             if (b->fp32) {
                 char* A = static_cast<char*>(p.fbf);
                 char* B = A + (size_t)p.g.N * b->kp * 2;
                 BCK(launch_features_bf16(F1, b->d, p.g.N, b->kp, A, s));
                 BCK(launch_features_bf16(F2, b->d, p.g.M, b->kp, B, s));
                 BCK(launch_gemm_cost_skew(A, B, b->kp, p.g, static_cast<float*>(p.Csk),
-                                          p.skew_stride, b->status, s));
+                                          p.skew_stride, b->status, s, slot));
             } else {
                 double* An = p.feat;
                 double* Bn = p.feat + (int64_t)b->d * p.g.N;
                 BCK(launch_l2norm(F1, b->d, p.g.N, An, s));
                 BCK(launch_l2norm(F2, b->d, p.g.M, Bn, s));
                 BCK(launch_cost_skew(An, Bn, b->d, p.g, static_cast<double*>(p.Csk),
-                                     p.skew_stride, s));
+                                     p.skew_stride, s, slot));
+            }
+            if (b->masked) {
+                // skipped tiles keep +inf edges and start 0 for stage 2
+                BCK(launch_fill(p.s1.edge_D, p.n4, HUGE_VAL, s));
+                BCK(cudaMemsetAsync(p.s1.edge_P, 0, (size_t)p.n4 * 4, s));
             }
         }
         BCK(mark(w, 1));

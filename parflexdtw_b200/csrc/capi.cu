@@ -210,6 +210,7 @@ int pfx::plan_init(pfx_plan* p, int64_t N, int64_t M, int32_t L, const int64_t* 
     PA(&p->descs, nt);
     PA(&p->head, 1);
     PA(&p->tile_mask, nt);
+    PA(&p->tile_slot, nt);
     PA(&p->descs_sub, nt);
     PA(&p->nsub, 1);
 #undef PA
@@ -223,7 +224,8 @@ int pfx::plan_init(pfx_plan* p, int64_t N, int64_t M, int32_t L, const int64_t* 
 
 // Tile descriptors of plan p with cost slabs at Csk, in queue order (largest
 // tile first, then row-major tile index).
-void pfx::plan_tile_descs(const pfx_plan* p, const void* Csk, TileDesc* out) {
+void pfx::plan_tile_descs(const pfx_plan* p, const void* Csk, TileDesc* out,
+                          const int32_t* slot) {
     const Geo& g = p->g;
     const int nt = g.n1 * g.n2;
     std::vector<int> order(nt);
@@ -241,7 +243,9 @@ void pfx::plan_tile_descs(const pfx_plan* p, const void* Csk, TileDesc* out) {
         TileDesc d;
         memset(&d, 0, sizeof(d));
         tile_rect(g, t / g.n2, t % g.n2, &r0, &c0, &d.R, &d.W);
-        d.Csk = static_cast<const char*>(Csk) + (int64_t)t * p->skew_stride * (p->fp32 ? 4 : 8);
+        const int64_t slab = slot ? slot[t] : t;
+        d.Csk = slab < 0 ? nullptr
+                         : static_cast<const char*>(Csk) + slab * p->skew_stride * (p->fp32 ? 4 : 8);
         d.Bw = p->s1.Bw + (int64_t)t * g.b_words;
         d.eD = p->s1.edge_D + (int64_t)t * 2 * g.L;
         d.eP = p->s1.edge_P + (int64_t)t * 2 * g.L;
@@ -354,8 +358,8 @@ static int ensure_cost_buffer(pfx_plan* p) {
     return PFX_OK;
 }
 
-static const uint8_t* active_mask(const pfx_plan* p) {
-    return p->mask_active ? p->tile_mask : nullptr;
+static const int32_t* active_mask(const pfx_plan* p) {
+    return p->mask_active ? p->tile_slot : nullptr;
 }
 
 extern "C" int pfx_plan_set_tile_mask(pfx_plan* p, const uint8_t* mask, int32_t on_device,
@@ -363,7 +367,7 @@ extern "C" int pfx_plan_set_tile_mask(pfx_plan* p, const uint8_t* mask, int32_t 
     if (!p) return fail(PFX_ERR_ARG, "null plan");
     if (!mask) {
         p->mask_active = 0;
-        p->s2.tile_mask = nullptr;
+        p->s2.tile_slot = nullptr;
         return PFX_OK;
     }
     int st;
@@ -374,8 +378,10 @@ extern "C" int pfx_plan_set_tile_mask(pfx_plan* p, const uint8_t* mask, int32_t 
                        on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
     if (!on_device) CK(cudaStreamSynchronize(s));  // the host array may go away
     CK(launch_compact_descs(p->descs, nt, p->tile_mask, p->descs_sub, p->nsub, s));
+    // a plan keeps every tile's slab in place: slot = tile where set, -1 elsewhere
+    CK(launch_mask_slots(p->tile_mask, nt, p->tile_slot, s));
     p->mask_active = 1;
-    p->s2.tile_mask = p->tile_mask;
+    p->s2.tile_slot = p->tile_slot;
     return PFX_OK;
 }
 

@@ -161,7 +161,8 @@ struct S2Buf {
     int64_t seg_cap;
     int64_t* wp;         // [K][2] final path, start first
     int64_t* wp_len;     // [1]
-    const uint8_t* tile_mask;  // [n1*n2] tiles stage 1 ran on (null: all)
+    const int32_t* tile_slot;  // [n1*n2] cost slab of each tile, -1 where stage 1
+                               // skipped the tile (null: slab = tile index)
 };
 
 // Records `msg` as the calling thread's last error and returns `status`.
@@ -180,29 +181,31 @@ void count_launches(int n);
 cudaError_t launch_stage1_queue(const TileDesc* descs, int ntiles, const int* ntiles_dev,
                                 int* head, const Geo& g, int32_t* status, int nw, bool fp32,
                                 cudaStream_t st);
+// slot[t] = mask[t] ? t : -1.
+cudaError_t launch_mask_slots(const uint8_t* mask, int n, int32_t* slot, cudaStream_t st);
 // Keeps the descriptors whose tile is set in `mask`, in order; *count = kept.
 cudaError_t launch_compact_descs(const TileDesc* in, int n, const uint8_t* mask, TileDesc* out,
                                  int* count, cudaStream_t st);
 // Smallest valid warps-per-tile choice heuristic for `ntiles` tiles of length L.
 int stage1_queue_warps(int ntiles, int32_t L, int num_sms);
-// Cost-building launchers take an optional tile mask (null: all tiles);
-// masked-out tiles' slabs are left untouched.
+// Cost-building launchers take an optional slot map: tile t's slab is slab
+// slot[t] of Csk, and tiles with slot[t] < 0 are skipped (null: slab = t).
 cudaError_t launch_relayout_skew(const double* C, int64_t ldc, const Geo& g, double* Csk,
                                  int64_t skew_stride, cudaStream_t st,
-                                 const uint8_t* mask = nullptr);
+                                 const int32_t* slot = nullptr);
 // FP32 form cost from features (gemm_bf16.cu): bf16 rows of L2-normalised
 // features, then 1 - A B^T on the tensor cores into FP32 skewed slabs.
 cudaError_t launch_features_bf16(const double* F, int d, int64_t n, int Kp, void* out,
                                  cudaStream_t st);
 cudaError_t launch_gemm_cost_skew(const void* Abf, const void* Bbf, int Kp, const Geo& g,
                                   float* Csk, int64_t stride, int32_t* status, cudaStream_t st,
-                                  const uint8_t* mask = nullptr);
+                                  const int32_t* slot = nullptr);
 // FP32 slabs from a row-major FP64 (rounded) or FP32 C (exactly one non-null).
 cudaError_t launch_relayout_skew_f32(const double* C64, const float* C32, int64_t ldc,
                                      const Geo& g, float* Csk, int64_t stride, cudaStream_t st,
-                                     const uint8_t* mask = nullptr);
+                                     const int32_t* slot = nullptr);
 cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Geo& g, double* Csk,
-                             int64_t skew_stride, cudaStream_t st, const uint8_t* mask = nullptr);
+                             int64_t skew_stride, cudaStream_t st, const int32_t* slot = nullptr);
 cudaError_t launch_l2norm(const double* F, int d, int64_t n, double* out, cudaStream_t st);
 cudaError_t launch_stage1(const double* C, const Geo& g, const S1Out& o, int tile0, int ntiles,
                           int nw, bool full, cudaStream_t st);

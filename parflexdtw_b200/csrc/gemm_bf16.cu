@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
     k_gemm_cost_skew(const __grid_constant__ CUtensorMap mapA,
                      const __grid_constant__ CUtensorMap mapB, const Geo g,
                      float* __restrict__ Csk, const int64_t stride,
-                     int32_t* __restrict__ status, const uint8_t* __restrict__ mask) {
+                     int32_t* __restrict__ status, const int32_t* __restrict__ slot) {
     extern __shared__ __align__(1024) unsigned char gsm_raw[];
     // operands (1024-byte aligned atoms), later reused as the skew stage
     unsigned char* base = reinterpret_cast<unsigned char*>(
@@ -125,7 +125,8 @@ __global__ void __launch_bounds__(kGThreads, 1)
     q /= ncb;
     const int kk = q % nkk;
     const int tile = q / nkk;
-    if (mask && !mask[tile]) return;  // uniform over the CTA
+    const int slab = slot ? slot[tile] : tile;  // slab index; < 0: tile skipped
+    if (slab < 0) return;  // uniform over the CTA
     int64_t r0, c0;
     int32_t R, W;
     tile_rect(g, tile / g.n2, tile % g.n2, &r0, &c0, &R, &W);
@@ -245,7 +246,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
     }
     if (s_fail) return;
     // skewed rows out: 32 lanes x float2 = 256 contiguous bytes per (strip, step)
-    float2* out = reinterpret_cast<float2*>(Csk + (int64_t)tile * stride);
+    float2* out = reinterpret_cast<float2*>(Csk + (int64_t)slab * stride);
 #pragma unroll 4
     for (int i = threadIdx.x; i < 2 * kGSteps * 32; i += kGThreads) {
         const int s = i / (kGSteps * 32);
@@ -324,7 +325,7 @@ size_t gemm_cost_smem_bytes(int Kp) {
 
 template <int KB>
 static cudaError_t gemm_t(const CUtensorMap& ma, const CUtensorMap& mb, const Geo& g, float* Csk,
-                          int64_t stride, int32_t* status, cudaStream_t st, const uint8_t* mask) {
+                          int64_t stride, int32_t* status, cudaStream_t st, const int32_t* slot) {
     const size_t smem = gemm_cost_smem_bytes(64 * KB);
     auto kern = k_gemm_cost_skew<KB>;
     cudaError_t e =
@@ -334,23 +335,23 @@ static cudaError_t gemm_t(const CUtensorMap& ma, const CUtensorMap& mb, const Ge
     const int64_t nblk =
         (int64_t)g.n1 * g.n2 * ((s.nS + 1) / 2) * ceil_div32(s.span, kGSteps);
     if (nblk > 0x7fffffffLL) return cudaErrorInvalidValue;
-    kern<<<(unsigned)nblk, kGThreads, smem, st>>>(ma, mb, g, Csk, stride, status, mask);
+    kern<<<(unsigned)nblk, kGThreads, smem, st>>>(ma, mb, g, Csk, stride, status, slot);
     count_launches(1);
     return cudaGetLastError();
 }
 
 cudaError_t launch_gemm_cost_skew(const void* Abf, const void* Bbf, int Kp, const Geo& g,
                                   float* Csk, int64_t stride, int32_t* status, cudaStream_t st,
-                                  const uint8_t* mask) {
+                                  const int32_t* slot) {
     if (Kp % 64 || Kp < 64 || Kp > 256) return cudaErrorInvalidValue;
     CUtensorMap ma, mb;
     if (!make_map(&ma, Abf, g.N, Kp, kGRows) || !make_map(&mb, Bbf, g.M, Kp, kGCols))
         return cudaErrorInvalidValue;
     switch (Kp / 64) {
-        case 1: return gemm_t<1>(ma, mb, g, Csk, stride, status, st, mask);
-        case 2: return gemm_t<2>(ma, mb, g, Csk, stride, status, st, mask);
-        case 3: return gemm_t<3>(ma, mb, g, Csk, stride, status, st, mask);
-        default: return gemm_t<4>(ma, mb, g, Csk, stride, status, st, mask);
+        case 1: return gemm_t<1>(ma, mb, g, Csk, stride, status, st, slot);
+        case 2: return gemm_t<2>(ma, mb, g, Csk, stride, status, st, slot);
+        case 3: return gemm_t<3>(ma, mb, g, Csk, stride, status, st, slot);
+        default: return gemm_t<4>(ma, mb, g, Csk, stride, status, st, slot);
     }
 }
 

@@ -38,14 +38,15 @@ __global__ void __launch_bounds__(kRegionThreads) k_region_skew(const Tin* __res
                                                                int64_t ldc, const Geo g,
                                                                Tout* __restrict__ Csk,
                                                                int64_t stride,
-                                                               const uint8_t* __restrict__ mask) {
+                                                               const int32_t* __restrict__ slot) {
     extern __shared__ __align__(16) unsigned char S_raw[];
     Tout* S = reinterpret_cast<Tout*>(S_raw);  // [64][kWinStride]
     // blockIdx.x enumerates (tile, step chunk) pairs, blockIdx.y the strip
     const int nchunk = ceil_div32(make_sched2(g.L, g.L, 1).span, kTC);
     const int tile = (int)(blockIdx.x / nchunk), k = blockIdx.y;
     const int ts = (int)(blockIdx.x % nchunk) * kTC;
-    if (mask && !mask[tile]) return;
+    const int slab = slot ? slot[tile] : tile;  // slab index; < 0: tile skipped
+    if (slab < 0) return;
     const int ti = tile / g.n2, tj = tile % g.n2;
     int64_t r0, c0;
     int32_t R, W;
@@ -66,7 +67,7 @@ __global__ void __launch_bounds__(kRegionThreads) k_region_skew(const Tin* __res
 #pragma unroll
     for (int u = 0; u < kPer; ++u) S[threadIdx.x + u * kRegionThreads] = v[u];
     __syncthreads();
-    write_skewed(S, Csk + (int64_t)tile * stride, sc.span, k, ts);
+    write_skewed(S, Csk + (int64_t)slab * stride, sc.span, k, ts);
 }
 
 // ---------------------------------------------------------------------------
@@ -89,12 +90,13 @@ template <int DMAX>
 __global__ void __launch_bounds__(kCostThreads, 2)
     k_cost_skew(const double* __restrict__ An, const double* __restrict__ Bn, const int d,
                 const Geo g, double* __restrict__ Csk, const int64_t stride,
-                const uint8_t* __restrict__ mask) {
+                const int32_t* __restrict__ slot) {
     extern __shared__ __align__(16) double sB[];  // [d][2][kCH]
     const int nchunk = ceil_div32(make_sched2(g.L, g.L, 1).span, kCT);
     const int tile = (int)(blockIdx.x / nchunk), k = blockIdx.y;
     const int ts = (int)(blockIdx.x % nchunk) * kCT;
-    if (mask && !mask[tile]) return;
+    const int slab = slot ? slot[tile] : tile;  // slab index; < 0: tile skipped
+    if (slab < 0) return;
     int64_t r0, c0;
     int32_t R, W;
     tile_rect(g, tile / g.n2, tile % g.n2, &r0, &c0, &R, &W);
@@ -116,7 +118,7 @@ __global__ void __launch_bounds__(kCostThreads, 2)
         aB[f] = (f < d && rB < R) ? __ldg(An + (int64_t)f * g.N + r0 + rB) : 0.0;
     }
     __syncthreads();
-    double2* out = reinterpret_cast<double2*>(Csk + (int64_t)tile * stride) + (int64_t)k * span * 32 + lane;
+    double2* out = reinterpret_cast<double2*>(Csk + (int64_t)slab * stride) + (int64_t)k * span * 32 + lane;
 #pragma unroll 1
     for (int blk = 0; blk < 32 / kCV; ++blk) {
         const int t0 = ts + 32 * warp + kCV * blk;  // warp-uniform
@@ -168,12 +170,13 @@ constexpr int kCH2 = kCX2 / 2;
 __global__ void __launch_bounds__(kCostThreads, 2)
     k_cost_skew_chunked(const double* __restrict__ An, const double* __restrict__ Bn, const int d,
                         const Geo g, double* __restrict__ Csk, const int64_t stride,
-                        const uint8_t* __restrict__ mask) {
+                        const int32_t* __restrict__ slot) {
     __shared__ __align__(16) double sB[kMaxFeat * kCX2];  // [16][2][kCH2]
     const int nchunk = ceil_div32(make_sched2(g.L, g.L, 1).span, kCT2);
     const int tile = (int)(blockIdx.x / nchunk), k = blockIdx.y;
     const int ts = (int)(blockIdx.x % nchunk) * kCT2;
-    if (mask && !mask[tile]) return;
+    const int slab = slot ? slot[tile] : tile;  // slab index; < 0: tile skipped
+    if (slab < 0) return;
     int64_t r0, c0;
     int32_t R, W;
     tile_rect(g, tile / g.n2, tile % g.n2, &r0, &c0, &R, &W);
@@ -218,7 +221,7 @@ __global__ void __launch_bounds__(kCostThreads, 2)
         }
     }
     if (t0 >= span) return;
-    double2* out = reinterpret_cast<double2*>(Csk + (int64_t)tile * stride) + (int64_t)k * span * 32 + lane;
+    double2* out = reinterpret_cast<double2*>(Csk + (int64_t)slab * stride) + (int64_t)k * span * 32 + lane;
 #pragma unroll
     for (int v = 0; v < kCV; ++v) {
         const int tau = t0 + v;
@@ -238,45 +241,45 @@ static dim3 region_grid(const Geo& g, int per_cta) {
 
 template <typename Tin, typename Tout>
 static cudaError_t relayout_t(const Tin* C, int64_t ldc, const Geo& g, Tout* Csk, int64_t stride,
-                              cudaStream_t st, const uint8_t* mask) {
+                              cudaStream_t st, const int32_t* slot) {
     const size_t smem = (size_t)64 * kWinStride * sizeof(Tout);
     auto kern = k_region_skew<Tin, Tout>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<region_grid(g, kTC), kRegionThreads, smem, st>>>(C, ldc, g, Csk, stride, mask);
+    kern<<<region_grid(g, kTC), kRegionThreads, smem, st>>>(C, ldc, g, Csk, stride, slot);
     count_launches(1);
     return cudaGetLastError();
 }
 
 cudaError_t launch_relayout_skew(const double* C, int64_t ldc, const Geo& g, double* Csk,
-                                 int64_t stride, cudaStream_t st, const uint8_t* mask) {
-    return relayout_t(C, ldc, g, Csk, stride, st, mask);
+                                 int64_t stride, cudaStream_t st, const int32_t* slot) {
+    return relayout_t(C, ldc, g, Csk, stride, st, slot);
 }
 
 cudaError_t launch_relayout_skew_f32(const double* C64, const float* C32, int64_t ldc,
                                      const Geo& g, float* Csk, int64_t stride, cudaStream_t st,
-                                     const uint8_t* mask) {
-    return C32 ? relayout_t(C32, ldc, g, Csk, stride, st, mask)
-               : relayout_t(C64, ldc, g, Csk, stride, st, mask);
+                                     const int32_t* slot) {
+    return C32 ? relayout_t(C32, ldc, g, Csk, stride, st, slot)
+               : relayout_t(C64, ldc, g, Csk, stride, st, slot);
 }
 
 cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Geo& g, double* Csk,
-                             int64_t stride, cudaStream_t st, const uint8_t* mask) {
+                             int64_t stride, cudaStream_t st, const int32_t* slot) {
     if (d < 1) return cudaErrorInvalidValue;
     if (d > kMaxFeat) {
         k_cost_skew_chunked<<<region_grid(g, kCT2), kCostThreads, 0, st>>>(An, Bn, d, g, Csk,
-                                                                          stride, mask);
+                                                                          stride, slot);
         count_launches(1);
         return cudaGetLastError();
     }
     const size_t smem = (size_t)d * kCX * sizeof(double);
     if (d == 12) {
         k_cost_skew<12><<<region_grid(g, kCT), kCostThreads, smem, st>>>(An, Bn, d, g, Csk, stride,
-                                                                         mask);
+                                                                         slot);
     } else {
         k_cost_skew<kMaxFeat><<<region_grid(g, kCT), kCostThreads, smem, st>>>(An, Bn, d, g, Csk,
-                                                                             stride, mask);
+                                                                             stride, slot);
     }
     count_launches(1);
     return cudaGetLastError();

@@ -29,8 +29,10 @@ struct pfx_plan {
     // stage-1 tile queue of this plan (descriptors in queue order) and its head
     pfx::TileDesc* descs;
     int* head;
-    // tile mask (pfx_plan_set_tile_mask): the masked queue and its device length
+    // tile mask (pfx_plan_set_tile_mask or a masked batch): the mask, each
+    // tile's cost slab (-1: skipped), the masked queue and its device length
     uint8_t* tile_mask;
+    int32_t* tile_slot;
     pfx::TileDesc* descs_sub;
     int* nsub;
     int mask_active;
@@ -44,7 +46,10 @@ struct pfx_plan {
 namespace pfx {
 int plan_init(pfx_plan* p, int64_t N, int64_t M, int32_t L, const int64_t* steps,
               const double* weights, int32_t n_steps, int nw, int fp32);
-void plan_tile_descs(const pfx_plan* p, const void* Csk, TileDesc* out);
+// Descriptors of every tile, largest first; with a host slot map, tile t's
+// slab is slab slot[t] of Csk (nullptr where slot[t] < 0).
+void plan_tile_descs(const pfx_plan* p, const void* Csk, TileDesc* out,
+                     const int32_t* slot = nullptr);
 inline int64_t plan_slab_bytes(const pfx_plan* p) {
     return (int64_t)p->g.n1 * p->g.n2 * p->skew_stride * (p->fp32 ? 4 : 8);
 }

@@ -589,6 +589,17 @@ __global__ void __launch_bounds__(1024) k_compact_descs(const TileDesc* __restri
     if (threadIdx.x == 0) *count = base;
 }
 
+__global__ void k_mask_slots(const uint8_t* __restrict__ mask, int n, int32_t* __restrict__ slot) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) slot[t] = mask[t] ? t : -1;
+}
+
+cudaError_t launch_mask_slots(const uint8_t* mask, int n, int32_t* slot, cudaStream_t st) {
+    k_mask_slots<<<(n + 255) / 256, 256, 0, st>>>(mask, n, slot);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_compact_descs(const TileDesc* in, int n, const uint8_t* mask, TileDesc* out,
                                  int* count, cudaStream_t st) {
     k_compact_descs<<<1, 1024, 0, st>>>(in, n, mask, out, count);

@@ -55,13 +55,13 @@ __global__ void k_edges(const double* __restrict__ C, const void* __restrict__ C
         const int32_t s = b.edge_P[q];
         int32_t sr, sc;
         decode_start(s, &sr, &sc);
-        const int64_t si = t * skew_stride + skew_index(W, sr, sc);
+        const int64_t slab = b.tile_slot ? b.tile_slot[t] : t;
+        const int64_t si = slab * skew_stride + skew_index(W, sr, sc);
         // a tile stage 1 skipped has no cost slab: its edges are +inf anyway
-        b.edge_Cf[q] = (b.tile_mask && !b.tile_mask[t])
-                           ? 0.0
-                           : (C ? C[(r0 + sr) * g.ldc + c0 + sc]
-                                : (f32 ? (double)static_cast<const float*>(Csk)[si]
-                                       : static_cast<const double*>(Csk)[si]));
+        b.edge_Cf[q] = slab < 0 ? 0.0
+                                : (C ? C[(r0 + sr) * g.ldc + c0 + sc]
+                                     : (f32 ? (double)static_cast<const float*>(Csk)[si]
+                                            : static_cast<const double*>(Csk)[si]));
         // mandatory slots: whole top edge of the last tile row, whole right
         // edge of the last tile column, and both ends of every edge
         const bool last = e == 0 ? (i == g.n1 - 1) : (j == g.n2 - 1);

@@ -287,3 +287,74 @@ def parflex_pruned(F1, F2, steps, weights, beta, L, proposer=None, threshold=Non
         plan.set_tile_mask(None)
         plan.set_warps(full_warps)
     return best, np.ascontiguousarray(wp.T), info
+
+
+class PrunedBatch:
+    """Learned pruning over a batch of pairs: one proposer pass per pair,
+    then the kept tiles of all pairs in one stage-1 launch per wave
+    (``pfx_batch_set_masks``), stage 2 per pair, and the full-tile method
+    (one plan per pair) for the pairs that need the fallback."""
+
+    def __init__(self, shapes, L, steps, weights, d, proposer=None, threshold=None,
+                 dilation=1, precision="fp64", wave_bytes=0, warps=0):
+        from .batch import Batch
+        self.batch = Batch(shapes, L, steps, weights, d, wave_bytes=wave_bytes, warps=warps,
+                           precision=precision)
+        self.proposer = proposer or TileProposer.load()
+        self.threshold = threshold
+        self.dilation = dilation
+        self.L = int(L)
+        self.steps, self.weights, self.precision = steps, weights, precision
+        self.shapes = [(int(n), int(m)) for n, m in shapes]
+        hop = self.L - 1
+        self.grids = [(-(-(n - 1) // hop), -(-(m - 1) // hop)) for n, m in self.shapes]
+        self.offs = np.concatenate([[0], np.cumsum([a * b for a, b in self.grids])])
+
+    def load(self, pairs, non_blocking=True):
+        self.batch.load(pairs, non_blocking=non_blocking)
+
+    def run(self, beta):
+        """[(best_cost, wp[2, K]) per pair], info."""
+        b = self.batch
+        masks = torch.empty(int(self.offs[-1]), dtype=torch.uint8, device=self.proposer.device)
+        for i, (N, M) in enumerate(self.shapes):
+            f1, f2 = b.feature_views(i)
+            pooled = self.proposer.pooled_cost(f1, f2)
+            m, _ = self.proposer.propose(pooled, N, M, self.L, self.threshold, self.dilation)
+            masks[self.offs[i]:self.offs[i + 1]] = m.reshape(-1)
+        b.set_masks(masks)
+        b.run(beta, use_graph=False)
+        best, end, lens = b.results()
+        paths = b.paths(lens)
+        m_host = masks.cpu().numpy()
+        out, fallbacks, reasons = [], 0, {}
+        kept = int(m_host.sum())
+        run_tiles = kept
+        for i, (N, M) in enumerate(self.shapes):
+            mk = m_host[self.offs[i]:self.offs[i + 1]].reshape(self.grids[i])
+            reason = None
+            if not end[i, 6]:
+                reason = "no endpoint among proposed tiles"
+            elif _needs_fallback(paths[i], mk, N, M, self.L):
+                reason = "path near a pruned tile"
+            if reason is None:
+                out.append((float(best[i]), np.ascontiguousarray(paths[i].T)))
+                continue
+            fallbacks += 1
+            reasons[reason] = reasons.get(reason, 0) + 1
+            f1, f2 = b.feature_views(i)
+            plan = Plan(N, M, self.L, self.steps, self.weights, precision=self.precision)
+            plan.load_features(f1, f2)
+            plan.run(None, beta)
+            bc, _, _, n = plan.result()
+            out.append((bc, np.ascontiguousarray(plan.path(n).T)))
+            run_tiles += plan.n1 * plan.n2
+            plan.close()
+        total = int(self.offs[-1])
+        info = {"tiles_total": total, "tiles_run": run_tiles, "tiles_proposed": kept,
+                "skipped_fraction": 1 - kept / total, "fallbacks": fallbacks,
+                "fallback_reasons": reasons, "waves": b.waves}
+        return out, info
+
+    def close(self):
+        self.batch.close()

@@ -198,3 +198,55 @@ def test_parflex_pruned_equals_full_and_falls_back():
     b2, wp2, info2 = pf.parflex_pruned(F1, F2, STD, WTS, 0.1, 500, proposer=net, threshold=-1e30)
     assert not info2["fallback"] and info2["tiles_run"] == info2["tiles_total"]
     assert b2 == best and np.array_equal(wp2, wp)
+
+
+def test_batch_masks_and_pruned_batch_exact(oracle_mod):
+    """Masked batches: all-ones masks and path-dilated masks reproduce the
+    unmasked results bit for bit; PrunedBatch (any proposer) returns the
+    full-tile results, through its fallback when needed."""
+    from parflexdtw_b200.batch import Batch
+    rng = np.random.default_rng(12)
+    sizes = [(2600, 2900), (1800, 1500), (3100, 3300)]
+    pairs = [W.warped_pair(rng, n, m, pad_frac=0.1) for n, m in sizes]
+    shapes = [(p[0].shape[1], p[1].shape[1]) for p in pairs]
+    L = 300
+    refs = [oracle_mod.parflex_full(W.cost_matrix_det(F1, F2), STD, WTS, 0.1, L)
+            for F1, F2 in pairs]
+    b = Batch(shapes, L, STD, WTS, 12, warps=4)
+    b.load(pairs)
+    grids = [(-(-(n - 1) // (L - 1)), -(-(m - 1) // (L - 1))) for n, m in shapes]
+    ones = torch.ones(sum(a * c for a, c in grids), dtype=torch.uint8, device="cuda")
+    b.set_masks(ones)
+    b.run(0.1, use_graph=False)
+    best, end, lens = b.results()
+    paths = b.paths(lens)
+    for i, r in enumerate(refs):
+        assert best[i] == r["best_cost"] and np.array_equal(paths[i].T, r["wp"])
+    dil = []
+    for (n, m), r in zip(shapes, refs):
+        lab = tiles_on_path(r["wp"], n, m, L).astype(bool)
+        p = np.pad(lab, 1)
+        d = np.zeros_like(lab)
+        for di in range(3):
+            for dj in range(3):
+                d |= p[di:di + lab.shape[0], dj:dj + lab.shape[1]]
+        dil.append(d.reshape(-1))
+    masks = torch.from_numpy(np.concatenate(dil).astype(np.uint8)).cuda()
+    assert int(masks.sum()) < masks.numel()
+    b.set_masks(masks)
+    for use_graph in (False, True):
+        b.run(0.1, use_graph=use_graph)
+        best, end, lens = b.results()
+        paths = b.paths(lens)
+        for i, r in enumerate(refs):
+            assert best[i] == r["best_cost"] and np.array_equal(paths[i].T, r["wp"])
+    b.close()
+    net = TileProposer(seed=6)
+    for thr in (-1e30, 1e30):  # everything kept / nothing kept (all fall back)
+        pb = pf.PrunedBatch(shapes, L, STD, WTS, 12, proposer=net, threshold=thr)
+        pb.load(pairs)
+        out, info = pb.run(0.1)
+        for (bc, wp), r in zip(out, refs):
+            assert bc == r["best_cost"] and np.array_equal(wp, r["wp"])
+        assert (info["fallbacks"] == 3) == (thr > 0)
+        pb.close()
