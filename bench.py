@@ -836,6 +836,7 @@ def prune_arm(args, spec):
 
     import parflexdtw_b200 as pf
     from parflexdtw_b200 import _lib
+    from parflexdtw_b200.batch import Batch
     from parflexdtw_b200.prune import TileProposer
 
     ws, rank, local = dist_env()
@@ -854,98 +855,108 @@ def prune_arm(args, spec):
                          seed=spec.seed + 1000 * rank)
     pairs = W.make_batch(spec_r)
     gen_s = time.perf_counter() - t0
+    shapes = [(F1.shape[1], F2.shape[1]) for F1, F2 in pairs]
+    cells = sum(tile_cells(n, m, Lb)[0] for n, m in shapes)
     net = TileProposer.load()
 
     def ev():
         return torch.cuda.Event(enable_timing=True)
 
-    def run_pair(F1, F2, reps):
-        """(plain ms, pruned ms, cells, results) of one pair; features resident."""
-        N, M = F1.shape[1], F2.shape[1]
-        f1, f2 = torch.from_numpy(F1).to(dev), torch.from_numpy(F2).to(dev)
-        plan = pf.Plan(N, M, Lb, spec.steps, spec.weights)
-        cells = tile_cells(N, M, Lb)[0]
-        out = []
-        for _ in range(reps):
-            a, b = ev(), ev()
-            torch.cuda.synchronize()
-            a.record()
-            plan.load_features(f1, f2)
-            plan.run(None, spec.beta)
-            b.record()
-            best, end, _, n = plan.result()
-            wp = plan.path(n)
-            c, d_ = ev(), ev()
-            torch.cuda.synchronize()
-            c.record()
-            bp, wpp, info = pf.parflex_pruned(f1, f2, spec.steps, spec.weights, spec.beta, Lb,
-                                              proposer=net, plan=plan)
-            d_.record()
-            torch.cuda.synchronize()
-            out.append((a.elapsed_time(b), c.elapsed_time(d_), best, wp, bp, wpp, info))
-        plan.close()
-        del f1, f2
-        return cells, out
+    def timed(fn, steps):
+        torch.cuda.synchronize()
+        a, b = ev(), ev()
+        a.record()
+        for _ in range(steps):
+            out = fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b), out
 
-    # warm-up on the first pair
-    run_pair(*pairs[0], max(1, args.warmup))
+    def max_ranks(x):
+        if ws == 1:
+            return x
+        t = torch.tensor([x], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # --- plain form: every tile, FP64, one batch (waves), graph replay --------
+    bp = Batch(shapes, Lb, spec.steps, spec.weights, 12)
+    bp.load(pairs)
+    bp.run(spec.beta, use_graph=False)
+    ph_plain = bp.timing()
+    best0, end0, lens0 = bp.results()
+    paths0 = bp.paths(lens0)
+    plain_info = {"waves": bp.waves, "warps_per_tile": bp.warps, "tiles": bp.tiles}
+    for _ in range(max(1, args.warmup - 1)):
+        bp.run(spec.beta)
     if ws > 1:
         dist.barrier()
-    torch.cuda.synchronize()
-    plain_ms = pruned_ms = 0.0
-    cells_tot = 0
-    agree = fallbacks = 0
-    reasons = {}
-    skipped, run_tiles, all_tiles = [], 0, 0
+    ms_plain, _ = timed(lambda: bp.run(spec.beta), args.plain_steps)
+    ms_plain = max_ranks(ms_plain)
+    bp.close()
+    del bp
+    torch.cuda.empty_cache()
+
+    # --- chosen form: proposer + kept tiles only, FP64 ----------------------
+    pb = pf.PrunedBatch(shapes, Lb, spec.steps, spec.weights, 12, proposer=net)
+    pb.load(pairs)
+    for _ in range(args.warmup):
+        out, info = pb.run(spec.beta)
+    if ws > 1:
+        dist.barrier()
     launches0 = lib.pfx_kernel_launches()
     with ClockSampler(uuid) as clk:
-        for step in range(args.steps):
-            for F1, F2 in pairs:
-                cells, res = run_pair(F1, F2, 1)
-                pms, qms, best, wp, bp, wpp, info = res[0]
-                plain_ms += pms
-                pruned_ms += qms
-                cells_tot += cells
-                if step == 0:
-                    agree += int(bp == best and np.array_equal(wpp, wp.T))
-                    fallbacks += int(info["fallback"])
-                    if info["fallback"]:
-                        reasons[info["reason"]] = reasons.get(info["reason"], 0) + 1
-                    skipped.append(info["skipped_fraction"])
-                    run_tiles += info["tiles_run"]
-                    all_tiles += info["tiles_total"]
+        ms_pruned, (out, info) = timed(lambda: pb.run(spec.beta), args.steps)
     launches = lib.pfx_kernel_launches() - launches0
-    if ws > 1:
-        t = torch.tensor([plain_ms, pruned_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        plain_ms, pruned_ms = (float(x) for x in t.tolist())
-    v_pruned = cells_tot * ws / (pruned_ms / 1e3)
-    v_plain = cells_tot * ws / (plain_ms / 1e3)
+    ms_pruned = max_ranks(ms_pruned)
+    agree = sum(int(bc == best0[i] and np.array_equal(wp, paths0[i].T))
+                for i, (bc, wp) in enumerate(out))
+    # e2e: pinned host features in, results out
+    pinned = [(torch.from_numpy(F1).pin_memory(), torch.from_numpy(F2).pin_memory())
+              for F1, F2 in pairs]
+    h2d = sum(a.numel() * 8 + c.numel() * 8 for a, c in pinned)
+
+    def e2e_step():
+        pb.load(pinned)
+        return pb.run(spec.beta)
+
+    e2e_step()
+    ms_e2e, (out2, _) = timed(e2e_step, args.e2e_steps)
+    ms_e2e = max_ranks(ms_e2e)
+    d2h = sum(wp.nbytes for _, wp in out2) + 8 * 9 * n_pairs
+    pb.close()
+
+    v_pruned = cells * ws * args.steps / (ms_pruned / 1e3)
+    v_plain = cells * ws * args.plain_steps / (ms_plain / 1e3)
     if rank == 0:
         line = {
             "metric": PRUNE_METRIC, "value": v_pruned, "unit": UNIT, "n_gpus": ws,
-            "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": pruned_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(spec.describe(), pairs_run=n_pairs, cells_per_step=cells_tot // args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_pruned / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": dict(spec.describe(), pairs_run=n_pairs, cells_per_step=cells,
                            generation_seconds=gen_s, parallelism="replicas",
-                           input="features resident in HBM; each timed pair builds its cost",
-                           timing="CUDA events around each pair's full call (host checks of "
-                                  "the proposer mask and the fallback included); plan "
-                                  "allocation outside", l2="cost slabs larger than L2"),
-            "pairs_per_s": ws * n_pairs * args.steps / (pruned_ms / 1e3),
-            "plain_fp64_full_tiles": {"value": v_plain, "unit": UNIT,
-                                      "ms_per_step": plain_ms / args.steps,
-                                      "pairs_per_s": ws * n_pairs * args.steps / (plain_ms / 1e3)},
+                           input="features resident in HBM; every step builds the cost",
+                           timing="CUDA events around whole steps (host-side proposer mask "
+                                  "read-back and fallback checks included)",
+                           l2="cost slabs larger than L2 (no flush needed)"),
+            "pairs_per_s": ws * n_pairs * args.steps / (ms_pruned / 1e3),
+            "plain_fp64_full_tiles": {
+                "value": v_plain, "unit": UNIT, "steps": args.plain_steps,
+                "ms_per_step": ms_plain / args.plain_steps,
+                "pairs_per_s": ws * n_pairs * args.plain_steps / (ms_plain / 1e3),
+                "form": "batched, all tiles, one graph replay", "batch": plain_info,
+                "phases_ms": {"cost": ph_plain[0], "stage1": ph_plain[1], "stage2": ph_plain[2]}},
             "speedup_over_plain": v_pruned / v_plain,
-            "pruning": {"tiles_skipped_fraction_mean": float(np.mean(skipped)),
-                        "tiles_run_fraction_incl_fallbacks": run_tiles / all_tiles,
-                        "fallback_rate": fallbacks / n_pairs,
-                        "fallback_reasons": reasons,
-                        "exact_path_agreement_rate": agree / n_pairs,
-                        "proposer": "3 conv layers, 32 channels, bf16 activations, "
-                                    "parflexdtw_b200/data/proposer_L2000.npz",
-                        "threshold": net.threshold, "dilation_tiles": 1},
+            "pruning": dict(info, exact_path_agreement_rate=agree / n_pairs,
+                            fallback_rate=info["fallbacks"] / n_pairs,
+                            proposer="3 conv layers, 32 channels, bf16 activations, "
+                                     "parflexdtw_b200/data/proposer_L2000.npz",
+                            threshold=net.threshold, dilation_tiles=1),
+            "e2e": {"value": cells * ws * args.e2e_steps / (ms_e2e / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "steps": args.e2e_steps, "ms_per_step": ms_e2e / args.e2e_steps,
+                    "api": "PrunedBatch.load (pinned host features) + run"},
             "gpu_launches": int(launches), "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)

@@ -330,7 +330,7 @@ int pfx_pooled_cost(const float *A, const float *B, int32_t d, int64_t P1, int64
 /* In place: x <- (x - row mean - column mean + mean) / std over the
  * P1 x P2 map (the proposer's input).  scratch: P1 + P2 + 2 floats. */
 int pfx_pooled_center(float *x, int64_t P1, int64_t P2, float *scratch, void *stream);
-/* y (Cout x Ho x Wo) = act(conv3x3(x) + b), zero padding 1, stride 1 or 2,
+/* y (Cout x Ho x Wo) = act(conv3x3(x) + b), zero padding 1, stride 1, 2 or 4,
  * Ho = (H - 1) / stride + 1; w is [Cout][Cin][3][3]; act = ReLU if relu. */
 int pfx_conv3x3_forward(const void *x, int32_t x_bf16, int32_t Cin, int32_t H, int32_t W,
                         const float *w, const float *b, int32_t Cout, int32_t stride,
@@ -357,10 +357,11 @@ int pfx_tile_max_backward(const float *dscore, const int32_t *argmax, int32_t n,
 /* One Adam update (bias-corrected, step >= 1) of n parameters. */
 int pfx_adam_step(float *param, const float *grad, float *m, float *v, int64_t n, float lr,
                   float beta1, float beta2, float eps, int32_t step, void *stream);
-/* mask[t] = 1 if some tile within Chebyshev distance `dilation` of t has
- * score > threshold. */
+/* mask[t] = 1 if some tile within distance `dilation` of t (Chebyshev, or
+ * Manhattan when `manhattan`) has score > threshold. */
 int pfx_tile_mask_from_scores(const float *score, int32_t n1, int32_t n2, float threshold,
-                              int32_t dilation, uint8_t *mask, void *stream);
+                              int32_t dilation, int32_t manhattan, uint8_t *mask,
+                              void *stream);
 
 #ifdef __cplusplus
 }

@@ -94,7 +94,8 @@ SIGNATURES = [
     ("pfx_tile_max_backward", ct.c_int, [_vp, _vp, _i32, _vp, _vp]),
     ("pfx_adam_step", ct.c_int, [_vp, _vp, _vp, _vp, _i64, ct.c_float, ct.c_float, ct.c_float,
                                  ct.c_float, _i32, _vp]),
-    ("pfx_tile_mask_from_scores", ct.c_int, [_vp, _i32, _i32, ct.c_float, _i32, _vp, _vp]),
+    ("pfx_tile_mask_from_scores", ct.c_int, [_vp, _i32, _i32, ct.c_float, _i32, _i32, _vp,
+                                             _vp]),
 ]
 
 _lib = None

@@ -80,9 +80,16 @@ __global__ void k_col_mean(const float* __restrict__ x, int64_t P1, int64_t P2,
                            float* __restrict__ cm) {
     const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (j >= P2) return;
-    float s = 0.f;
-    for (int64_t i = 0; i < P1; ++i) s += x[i * P2 + j];
-    cm[j] = s / (float)P1;
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+    int64_t i = 0;
+    for (; i + 3 < P1; i += 4) {
+        s0 += x[i * P2 + j];
+        s1 += x[(i + 1) * P2 + j];
+        s2 += x[(i + 2) * P2 + j];
+        s3 += x[(i + 3) * P2 + j];
+    }
+    for (; i < P1; ++i) s0 += x[i * P2 + j];
+    cm[j] = ((s0 + s1) + (s2 + s3)) / (float)P1;
 }
 
 // sc[P1 + P2] = grand mean (mean of the row means), sc[P1 + P2 + 1] = 0
@@ -101,17 +108,27 @@ __global__ void k_grand_mean(float* __restrict__ sc, int64_t P1, int64_t P2) {
     }
 }
 
-__global__ void k_center(float* __restrict__ x, int64_t P1, int64_t P2, float* __restrict__ sc) {
-    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    float v = 0.f;
-    if (q < P1 * P2) {
-        const int64_t i = q / P2, j = q % P2;
-        v = x[q] - sc[i] - sc[P1 + j] + sc[P1 + P2];
+// grid-stride; one atomic per CTA for the sum of squares
+__global__ void __launch_bounds__(256)
+    k_center(float* __restrict__ x, int64_t P1, int64_t P2, float* __restrict__ sc) {
+    const int64_t n = P1 * P2;
+    float s = 0.f;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n;
+         q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = q / P2, j = q - i * P2;
+        const float v = x[q] - sc[i] - sc[P1 + j] + sc[P1 + P2];
         x[q] = v;
+        s = fmaf(v, v, s);
     }
-    float s = v * v;
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(sc + P1 + P2 + 1, s);
+    __shared__ float ws[8];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int w = 0; w < 8; ++w) t += ws[w];
+        atomicAdd(sc + P1 + P2 + 1, t);
+    }
 }
 
 __global__ void k_scale(float* __restrict__ x, int64_t n, const float* __restrict__ ss) {
@@ -357,16 +374,17 @@ __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float
     p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
 
-// mask = dilate(score > threshold) by `dil` tiles (Chebyshev distance).
+// mask = dilate(score > threshold) by `dil` tiles (Chebyshev distance, or
+// Manhattan distance when `manhattan`).
 __global__ void k_tile_mask(const float* __restrict__ score, int n1, int n2, float thr, int dil,
-                            uint8_t* __restrict__ mask) {
+                            int manhattan, uint8_t* __restrict__ mask) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n1 * n2) return;
     const int i = t / n2, j = t % n2;
     uint8_t on = 0;
     for (int a = max(0, i - dil); a <= min(n1 - 1, i + dil) && !on; ++a)
         for (int b = max(0, j - dil); b <= min(n2 - 1, j + dil); ++b)
-            if (score[a * n2 + b] > thr) {
+            if ((!manhattan || abs(a - i) + abs(b - j) <= dil) && score[a * n2 + b] > thr) {
                 on = 1;
                 break;
             }
@@ -417,43 +435,42 @@ cudaError_t cnn_conv_forward(const void* x, int in_bf16, int Cin, int H, int W, 
     if (stride == 1) {
         PFX_CONV(1)
     }
+    if (stride == 4) {
+        PFX_CONV(4)
+    }
     PFX_CONV(2)
 #undef PFX_CONV
+}
+
+template <int S>
+static cudaError_t conv_bwd_t(const float* x, int Cin, int H, int W, const float* w, int Cout,
+                              const float* y, int relu, const float* dy, float* dx, float* dw,
+                              float* db, cudaStream_t st) {
+    const int Ho = (H - 1) / S + 1, Wo = (W - 1) / S + 1;
+    if (dx) {
+        const int64_t n = (int64_t)Cin * H * W;
+        k_conv3x3_bwd_data<S><<<blocks_for(n, 256), 256, 0, st>>>(w, Cin, H, W, Cout, Ho, Wo, y,
+                                                                 dy, relu, dx);
+        count_launches(1);
+    }
+    const dim3 grid(blocks_for(Wo, kCvT), blocks_for(Ho, kCvT), blocks_for(Cin, kWgCi));
+    constexpr int PT = (kCvT - 1) * S + 3;
+    const size_t smem = ((size_t)Cout * kCvT * kCvT + (size_t)kWgCi * PT * PT) * sizeof(float);
+    cudaError_t e = cudaFuncSetAttribute(k_conv3x3_bwd_weight<S>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_conv3x3_bwd_weight<S><<<grid, 256, smem, st>>>(x, Cin, H, W, Cout, Ho, Wo, y, dy, relu, dw,
+                                                     db);
+    count_launches(1);
+    return cudaGetLastError();
 }
 
 cudaError_t cnn_conv_backward(const float* x, int Cin, int H, int W, const float* w, int Cout,
                               int stride, const float* y, int relu, const float* dy, float* dx,
                               float* dw, float* db, cudaStream_t st) {
-    const int Ho = (H - 1) / stride + 1, Wo = (W - 1) / stride + 1;
-    if (dx) {
-        const int64_t n = (int64_t)Cin * H * W;
-        if (stride == 1)
-            k_conv3x3_bwd_data<1><<<blocks_for(n, 256), 256, 0, st>>>(w, Cin, H, W, Cout, Ho, Wo,
-                                                                     y, dy, relu, dx);
-        else
-            k_conv3x3_bwd_data<2><<<blocks_for(n, 256), 256, 0, st>>>(w, Cin, H, W, Cout, Ho, Wo,
-                                                                     y, dy, relu, dx);
-        count_launches(1);
-    }
-    const dim3 grid(blocks_for(Wo, kCvT), blocks_for(Ho, kCvT), blocks_for(Cin, kWgCi));
-    const int PT = (kCvT - 1) * stride + 3;
-    const size_t smem = ((size_t)Cout * kCvT * kCvT + (size_t)kWgCi * PT * PT) * sizeof(float);
-    cudaError_t e;
-    if (stride == 1) {
-        e = cudaFuncSetAttribute(k_conv3x3_bwd_weight<1>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        k_conv3x3_bwd_weight<1><<<grid, 256, smem, st>>>(x, Cin, H, W, Cout, Ho, Wo, y, dy, relu,
-                                                         dw, db);
-    } else {
-        e = cudaFuncSetAttribute(k_conv3x3_bwd_weight<2>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        k_conv3x3_bwd_weight<2><<<grid, 256, smem, st>>>(x, Cin, H, W, Cout, Ho, Wo, y, dy, relu,
-                                                         dw, db);
-    }
-    count_launches(1);
-    return cudaGetLastError();
+    if (stride == 1) return conv_bwd_t<1>(x, Cin, H, W, w, Cout, y, relu, dy, dx, dw, db, st);
+    if (stride == 4) return conv_bwd_t<4>(x, Cin, H, W, w, Cout, y, relu, dy, dx, dw, db, st);
+    return conv_bwd_t<2>(x, Cin, H, W, w, Cout, y, relu, dy, dx, dw, db, st);
 }
 
 }  // namespace pfx
@@ -495,9 +512,10 @@ extern "C" int pfx_pooled_center(float* x, int64_t P1, int64_t P2, float* scratc
     cudaStream_t st = (cudaStream_t)stream;
     const int64_t n = P1 * P2;
     k_row_mean<<<(unsigned)P1, 256, 0, st>>>(x, P1, P2, scratch);
-    k_col_mean<<<blocks_for(P2, 256), 256, 0, st>>>(x, P1, P2, scratch + P1);
+    k_col_mean<<<blocks_for(P2, 64), 64, 0, st>>>(x, P1, P2, scratch + P1);
     k_grand_mean<<<1, 1024, 0, st>>>(scratch, P1, P2);
-    k_center<<<blocks_for(n, 256), 256, 0, st>>>(x, P1, P2, scratch);
+    const int64_t cb = blocks_for(n, 256) < 1184 ? blocks_for(n, 256) : 1184;
+    k_center<<<(unsigned)cb, 256, 0, st>>>(x, P1, P2, scratch);
     k_scale<<<blocks_for(n, 256), 256, 0, st>>>(x, n, scratch + P1 + P2 + 1);
     count_launches(5);
     PFX_CNN_RET(cudaGetLastError());
@@ -508,7 +526,7 @@ extern "C" int pfx_conv3x3_forward(const void* x, int32_t x_bf16, int32_t Cin, i
                                    int32_t stride, int32_t relu, void* y, int32_t y_bf16,
                                    void* stream) {
     if (!x || !w || !b || !y || Cin < 1 || Cout < 1 || H < 1 || W < 1 ||
-        (stride != 1 && stride != 2) || (int64_t)H * W > (1LL << 31) / 64)
+        (stride != 1 && stride != 2 && stride != 4) || (int64_t)H * W > (1LL << 31) / 64)
         return report_status(PFX_ERR_ARG, "pfx_conv3x3_forward: bad argument");
     PFX_CNN_RET(cnn_conv_forward(x, x_bf16, Cin, H, W, w, b, Cout, stride, relu, y, y_bf16,
                                  (cudaStream_t)stream));
@@ -519,7 +537,7 @@ extern "C" int pfx_conv3x3_backward(const float* x, int32_t Cin, int32_t H, int3
                                     int32_t relu, const float* dy, float* dx, float* dw, float* db,
                                     void* stream) {
     if (!x || !w || !y || !dy || !dw || !db || Cin < 1 || Cout < 1 || Cout > 64 || H < 1 ||
-        W < 1 || (stride != 1 && stride != 2))
+        W < 1 || (stride != 1 && stride != 2 && stride != 4))
         return report_status(PFX_ERR_ARG, "pfx_conv3x3_backward: bad argument");
     PFX_CNN_RET(cnn_conv_backward(x, Cin, H, W, w, Cout, stride, y, relu, dy, dx, dw, db,
                                   (cudaStream_t)stream));
@@ -566,11 +584,11 @@ extern "C" int pfx_adam_step(float* param, const float* grad, float* m, float* v
 }
 
 extern "C" int pfx_tile_mask_from_scores(const float* score, int32_t n1, int32_t n2,
-                                         float threshold, int32_t dilation, uint8_t* mask,
-                                         void* stream) {
+                                         float threshold, int32_t dilation, int32_t manhattan,
+                                         uint8_t* mask, void* stream) {
     if (!score || !mask || n1 < 1 || n2 < 1 || dilation < 0)
         return report_status(PFX_ERR_ARG, "pfx_tile_mask_from_scores: bad argument");
     k_tile_mask<<<blocks_for((int64_t)n1 * n2, 256), 256, 0, (cudaStream_t)stream>>>(
-        score, n1, n2, threshold, dilation, mask);
+        score, n1, n2, threshold, dilation, manhattan, mask);
     PFX_CNN_LAUNCHED();
 }

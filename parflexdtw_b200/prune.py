@@ -6,15 +6,16 @@ The network reads the cost matrix average-pooled 16x16 (from 16-frame means
 of the normalised features: the pooled map of a bilinear cost, no full C),
 double centred (row and column means removed) and standardised:
 
-    conv3x3(1 -> 32, stride 2) + ReLU
+    conv3x3(1 -> 32, stride 4) + ReLU
     conv3x3(32 -> 32, stride 2) + ReLU
-    conv3x3(32 -> 1, stride 1)           -> logits, 64 frames per pixel
+    conv3x3(32 -> 1, stride 1)           -> logits, 128 frames per pixel
 
 A tile's score is the max logit over its region.  Training (hand-written
 forward / backward / Adam kernels of csrc/cnn.cu, driven from here) uses
 labels that the full method itself produces: a tile is positive when the
 stitched path of the full-tile FP64 run has a point in it.  Inference keeps
-the tiles scoring above a threshold, dilated by one tile; when the pruned
+the tiles scoring above a threshold, dilated by one tile (4- or
+8-neighbourhood, the one the threshold was calibrated for); when the pruned
 run's path comes within 64 to 128 cells of a pruned tile (or no endpoint
 qualifies) the full-tile method runs instead.  No counterpart in the reference.
 
@@ -33,7 +34,7 @@ from .plan import Plan, current_stream_ptr
 
 POOL = 16
 CH = 32
-STRIDES = (2, 2, 1)
+STRIDES = (4, 2, 1)
 FPP = POOL * STRIDES[0] * STRIDES[1]  # frames per logit pixel
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data",
                                "proposer_L2000.npz")
@@ -67,10 +68,11 @@ class TileProposer:
 
     NAMES = ("w1", "b1", "w2", "b2", "w3", "b3")
 
-    def __init__(self, params=None, threshold=0.0, seed=0, device=None):
+    def __init__(self, params=None, threshold=0.0, seed=0, device=None, manhattan=False):
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None
                                    else device)
         self.threshold = float(threshold)
+        self.manhattan = bool(manhattan)  # dilation the threshold was calibrated for
         if params is None:
             g = torch.Generator().manual_seed(seed)
             shapes = {"w1": (CH, 1, 3, 3), "w2": (CH, CH, 3, 3), "w3": (1, CH, 3, 3)}
@@ -86,13 +88,17 @@ class TileProposer:
 
     # -- persistence -------------------------------------------------------
     def save(self, path, **meta):
-        np.savez(path, threshold=self.threshold,
+        np.savez(path, threshold=self.threshold, manhattan=self.manhattan,
+                 strides=np.asarray(STRIDES),
                  **{k: v.cpu().numpy() for k, v in self.params.items()}, **meta)
 
     @classmethod
     def load(cls, path=DEFAULT_WEIGHTS):
         z = np.load(path)
-        return cls({k: z[k] for k in cls.NAMES}, threshold=float(z["threshold"]))
+        if "strides" not in z or tuple(int(x) for x in z["strides"]) != STRIDES:
+            raise ValueError(f"{path}: weights for another network layout")
+        return cls({k: z[k] for k in cls.NAMES}, threshold=float(z["threshold"]),
+                   manhattan=bool(z["manhattan"]))
 
     # -- building blocks ---------------------------------------------------
     @staticmethod
@@ -154,14 +160,18 @@ class TileProposer:
                                     _p(arg), current_stream_ptr()))
         return score, arg, (n1, n2)
 
-    def propose(self, pooled, N, M, L, threshold=None, dilation=1):
-        """Device uint8 mask (n1 x n2) of the tiles to run, and the scores."""
+    def propose(self, pooled, N, M, L, threshold=None, dilation=1, manhattan=None):
+        """Device uint8 mask (n1 x n2) of the tiles to run, and the scores:
+        tiles above the threshold, dilated by `dilation` tiles (Chebyshev
+        distance, or Manhattan with `manhattan`)."""
         logits = self.forward(pooled, bf16=True)
         score, _, (n1, n2) = self.tile_scores(logits, N, M, L)
         mask = torch.empty(n1 * n2, dtype=torch.uint8, device=pooled.device)
         thr = self.threshold if threshold is None else float(threshold)
+        manhattan = self.manhattan if manhattan is None else manhattan
         _lib.check(_lib.load().pfx_tile_mask_from_scores(_p(score), n1, n2, thr, int(dilation),
-                                                         _p(mask), current_stream_ptr()))
+                                                         int(bool(manhattan)), _p(mask),
+                                                         current_stream_ptr()))
         return mask.reshape(n1, n2), score.reshape(n1, n2)
 
     # -- training ------------------------------------------------------------
@@ -213,26 +223,39 @@ FALLBACK_MARGIN = 64  # cells
 def _needs_fallback(wp, mask, N, M, L, margin=FALLBACK_MARGIN):
     """True when the path comes within about `margin` cells of a pruned
     tile's cells: there it may have been cut off, and the full-tile method
-    decides.  Works on a grid of margin x margin cell blocks; a block counts
-    as pruned when any of its cells lies in a pruned tile, and that map is
-    dilated by one block (so the distance tested is margin to 2 margin)."""
+    decides.  The test works on margin x margin cell blocks: for every block
+    the path touches, the tiles covering a cell of it or of its 8
+    neighbouring blocks must all have run (so the distance tested is margin
+    to 2 margin cells).  The path is monotone, so per row of blocks it
+    touches one interval of blocks, and a summed-area table of the pruned
+    tiles answers each interval's rectangle at once."""
     wp = np.asarray(wp)
     if wp.shape[0] == 2 and wp.shape[1] != 2:
         wp = wp.T
     m = np.asarray(mask, bool)
-    if m.all():
+    if m.all() or wp.shape[0] == 0:
         return False
+    n1, n2 = m.shape
     hop, B = L - 1, int(margin)
-    nb1, nb2 = -(-N // B), -(-M // B)
-    pm = np.zeros((nb1 + 2, nb2 + 2), bool)  # one block of border for the dilation
-    for i, j in np.argwhere(~m):
-        pm[1 + i * hop // B:2 + min(N - 1, i * hop + L - 1) // B,
-           1 + j * hop // B:2 + min(M - 1, j * hop + L - 1) // B] = True
-    near = np.zeros((nb1, nb2), bool)
-    for di in range(3):
-        for dj in range(3):
-            near |= pm[di:di + nb1, dj:dj + nb2]
-    return bool(near[wp[:, 0] // B, wp[:, 1] // B].any())
+    r, c = wp[:, 0], wp[:, 1]
+    a = np.arange(r[0] // B, r[-1] // B + 1)
+    st = np.searchsorted(r, a * B, "left")
+    en = np.searchsorted(r, (a + 1) * B, "left")
+    ok = en > st
+    a, st, en = a[ok], st[ok], en[ok]
+    r0 = np.maximum(a - 1, 0) * B
+    r1 = np.minimum((a + 2) * B, N) - 1
+    c0 = np.maximum(c[st] // B - 1, 0) * B
+    c1 = np.minimum((c[en - 1] // B + 2) * B, M) - 1
+    # tiles i with i*hop <= r1 and i*hop + L - 1 >= r0
+    ilo = np.clip(-(-(r0 - (L - 1)) // hop), 0, n1 - 1)
+    ihi = np.clip(r1 // hop, 0, n1 - 1)
+    jlo = np.clip(-(-(c0 - (L - 1)) // hop), 0, n2 - 1)
+    jhi = np.clip(c1 // hop, 0, n2 - 1)
+    sat = np.zeros((n1 + 1, n2 + 1), np.int64)
+    sat[1:, 1:] = np.cumsum(np.cumsum(~m, axis=0), axis=1)
+    cnt = sat[ihi + 1, jhi + 1] - sat[ilo, jhi + 1] - sat[ihi + 1, jlo] + sat[ilo, jlo]
+    return bool((cnt > 0).any())
 
 
 def parflex_pruned(F1, F2, steps, weights, beta, L, proposer=None, threshold=None,
@@ -296,13 +319,14 @@ class PrunedBatch:
     (one plan per pair) for the pairs that need the fallback."""
 
     def __init__(self, shapes, L, steps, weights, d, proposer=None, threshold=None,
-                 dilation=1, precision="fp64", wave_bytes=0, warps=0):
+                 dilation=1, manhattan=None, precision="fp64", wave_bytes=0, warps=0):
         from .batch import Batch
         self.batch = Batch(shapes, L, steps, weights, d, wave_bytes=wave_bytes, warps=warps,
                            precision=precision)
         self.proposer = proposer or TileProposer.load()
         self.threshold = threshold
         self.dilation = dilation
+        self.manhattan = manhattan
         self.L = int(L)
         self.steps, self.weights, self.precision = steps, weights, precision
         self.shapes = [(int(n), int(m)) for n, m in shapes]
@@ -313,20 +337,35 @@ class PrunedBatch:
     def load(self, pairs, non_blocking=True):
         self.batch.load(pairs, non_blocking=non_blocking)
 
-    def run(self, beta):
-        """[(best_cost, wp[2, K]) per pair], info."""
+    def run(self, beta, profile=False):
+        """[(best_cost, wp[2, K]) per pair], info.  profile: synchronise
+        between phases and report their wall times (ms) in info."""
+        import time as _time
         b = self.batch
+        marks = []
+
+        def mark(name):
+            if profile:
+                torch.cuda.synchronize()
+                marks.append((name, _time.perf_counter()))
+
+        mark("start")
         masks = torch.empty(int(self.offs[-1]), dtype=torch.uint8, device=self.proposer.device)
         for i, (N, M) in enumerate(self.shapes):
             f1, f2 = b.feature_views(i)
             pooled = self.proposer.pooled_cost(f1, f2)
-            m, _ = self.proposer.propose(pooled, N, M, self.L, self.threshold, self.dilation)
+            m, _ = self.proposer.propose(pooled, N, M, self.L, self.threshold, self.dilation,
+                                         self.manhattan)
             masks[self.offs[i]:self.offs[i + 1]] = m.reshape(-1)
+        mark("proposer")
         b.set_masks(masks)
+        mark("set_masks")
         b.run(beta, use_graph=False)
+        mark("align")
         best, end, lens = b.results()
         paths = b.paths(lens)
         m_host = masks.cpu().numpy()
+        mark("results")
         out, fallbacks, reasons = [], 0, {}
         kept = int(m_host.sum())
         run_tiles = kept
@@ -350,10 +389,14 @@ class PrunedBatch:
             out.append((bc, np.ascontiguousarray(plan.path(n).T)))
             run_tiles += plan.n1 * plan.n2
             plan.close()
+        mark("checks")
         total = int(self.offs[-1])
         info = {"tiles_total": total, "tiles_run": run_tiles, "tiles_proposed": kept,
                 "skipped_fraction": 1 - kept / total, "fallbacks": fallbacks,
                 "fallback_reasons": reasons, "waves": b.waves}
+        if profile:
+            info["phases_ms"] = {marks[k][0]: 1e3 * (marks[k][1] - marks[k - 1][1])
+                                 for k in range(1, len(marks))}
         return out, info
 
     def close(self):

@@ -10,7 +10,8 @@ path of the full-tile FP64 method, run in device batches.  The network then
 trains with the library's own forward / backward / Adam kernels (batch of
 one map, weighted BCE over tiles).  The threshold saved with the weights is
 the highest at which, with the one-tile dilation, every labelled tile of a
-held-out split is run, minus a margin.
+held-out split is run, minus a margin (one tile of dilation: the
+4-neighbourhood by default).
 """
 from __future__ import annotations
 
@@ -91,10 +92,10 @@ def train(net, data, L, epochs, lr, log=print, seed=0):
     return hist, pos_weight
 
 
-def calibrate(net, data, L, margin=0.5):
-    """The highest threshold at which, with one tile of dilation, every
-    labelled tile of every pair in `data` is run (minus a margin); and the
-    fraction of tiles kept at that threshold."""
+def calibrate(net, data, L, margin=0.5, manhattan=True):
+    """The highest threshold at which, with one tile of dilation (4- or
+    8-neighbourhood), every labelled tile of every pair in `data` is run
+    (minus a margin); and the fraction of tiles kept at that threshold."""
     thr = np.inf
     for pooled, lab, N, M in data:
         s = net.tile_scores(net.forward(pooled, bf16=True), N, M, L)[0].cpu().numpy()
@@ -103,12 +104,14 @@ def calibrate(net, data, L, margin=0.5):
         nb = np.full_like(s, -np.inf)
         for di in range(3):
             for dj in range(3):
+                if manhattan and abs(di - 1) + abs(dj - 1) > 1:
+                    continue
                 nb = np.maximum(nb, p[di:di + s.shape[0], dj:dj + s.shape[1]])
         thr = min(thr, float(nb[lab.astype(bool)].min()))
     thr -= margin
     kept = total = 0
     for pooled, lab, N, M in data:
-        mask, _ = net.propose(pooled, N, M, L, thr, 1)
+        mask, _ = net.propose(pooled, N, M, L, thr, 1, manhattan)
         kept += int(mask.sum().item())
         total += lab.size
     return thr, kept / total
@@ -125,6 +128,7 @@ def main():
     ap.add_argument("--seed", type=int, default=12345)
     ap.add_argument("--out", required=True)
     ap.add_argument("--log", default=None)
+    ap.add_argument("--dilation", choices=("manhattan", "chebyshev"), default="manhattan")
     args = ap.parse_args()
     logf = open(args.log, "w") if args.log else None
 
@@ -140,11 +144,13 @@ def main():
     nval = max(1, int(len(data) * args.val))
     val, tr = data[:nval], data[nval:]
     hist, pw = train(net, tr, args.L, args.epochs, args.lr, log=log)
-    thr, kept = calibrate(net, val, args.L)
+    thr, kept = calibrate(net, val, args.L, manhattan=args.dilation == "manhattan")
     net.threshold = thr
+    net.manhattan = args.dilation == "manhattan"
     info = {"train_pairs": len(tr), "val_pairs": len(val), "epochs": args.epochs,
             "loss_history": hist, "pos_weight": pw, "threshold": thr,
-            "val_kept_fraction": kept, "L": args.L, "seconds": time.perf_counter() - t0}
+            "val_kept_fraction": kept, "dilation": args.dilation, "L": args.L,
+            "seconds": time.perf_counter() - t0}
     log(json.dumps(info))
     net.save(args.out, info=json.dumps(info))
 

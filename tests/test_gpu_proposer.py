@@ -18,8 +18,8 @@ if not torch.cuda.is_available():  # pragma: no cover - CPU container
 
 import parflexdtw_b200 as pf  # noqa: E402
 from parflexdtw_b200 import _lib, workloads as W  # noqa: E402
-from parflexdtw_b200.prune import (FPP, TileProposer, _needs_fallback, _p,  # noqa: E402
-                                   tiles_on_path)
+from parflexdtw_b200.prune import (FPP, STRIDES, TileProposer, _needs_fallback,  # noqa: E402
+                                   _p, tiles_on_path)
 from oracle import cnn_oracle as CO  # noqa: E402
 
 STD = [(1, 1), (1, 2), (2, 1)]
@@ -49,7 +49,8 @@ def test_pooled_cost_vs_oracle():
 
 
 @pytest.mark.parametrize("cin,cout,stride,relu,H,W", [(1, 32, 2, 1, 37, 51), (32, 32, 2, 1, 19, 23),
-                                                      (32, 1, 1, 0, 17, 30), (3, 5, 1, 1, 16, 16)])
+                                                      (32, 1, 1, 0, 17, 30), (3, 5, 1, 1, 16, 16),
+                                                      (1, 32, 4, 1, 70, 61), (2, 3, 4, 0, 9, 13)])
 def test_conv_forward_backward_vs_oracle(cin, cout, stride, relu, H, W):
     rng = np.random.default_rng(cin * 100 + cout)
     x = rng.standard_normal((cin, H, W)).astype(np.float32)
@@ -96,9 +97,9 @@ def test_network_gradients_vs_oracle():
     loss, grads = net.gradients(pooled, label, N, M, L, pos_weight=3.0)
     P = {k: v.cpu().numpy().astype(np.float64) for k, v in net.params.items()}
     x0 = pooled.cpu().numpy()[None].astype(np.float64)
-    a1 = CO.conv3x3(x0, P["w1"], P["b1"], 2, 1)
-    a2 = CO.conv3x3(a1, P["w2"], P["b2"], 2, 1)
-    a3 = CO.conv3x3(a2, P["w3"], P["b3"], 1, 0)
+    a1 = CO.conv3x3(x0, P["w1"], P["b1"], STRIDES[0], 1)
+    a2 = CO.conv3x3(a1, P["w2"], P["b2"], STRIDES[1], 1)
+    a3 = CO.conv3x3(a2, P["w3"], P["b3"], STRIDES[2], 0)
     logits = net.forward(pooled).cpu().numpy()
     assert close(logits, a3[0])
     score, arg = CO.tile_max(logits, n1, n2, hop, L, N, M, FPP)
@@ -110,9 +111,9 @@ def test_network_gradients_vs_oracle():
     d3 = np.zeros_like(a3[0]).reshape(-1)
     np.add.at(d3, arg, ds)
     d3 = d3.reshape(1, *a3.shape[1:])
-    dx2, dw3, db3 = CO.conv3x3_backward(a2, P["w3"], 1, a3, 0, d3)
-    dx1, dw2, db2 = CO.conv3x3_backward(a1, P["w2"], 2, a2, 1, dx2)
-    _, dw1, db1 = CO.conv3x3_backward(x0, P["w1"], 2, a1, 1, dx1)
+    dx2, dw3, db3 = CO.conv3x3_backward(a2, P["w3"], STRIDES[2], a3, 0, d3)
+    dx1, dw2, db2 = CO.conv3x3_backward(a1, P["w2"], STRIDES[1], a2, 1, dx2)
+    _, dw1, db1 = CO.conv3x3_backward(x0, P["w1"], STRIDES[0], a1, 1, dx1)
     for k, ref in (("w3", dw3), ("b3", db3), ("w2", dw2), ("b2", db2), ("w1", dw1), ("b1", db1)):
         assert close(grads[k].cpu().numpy(), ref, 1e-3), k
 
