@@ -909,6 +909,7 @@ def prune_arm(args, spec):
         ms_pruned, (out, info) = timed(lambda: pb.run(spec.beta), args.steps)
     launches = lib.pfx_kernel_launches() - launches0
     ms_pruned = max_ranks(ms_pruned)
+    _, prof = pb.run(spec.beta, profile=True)
     agree = sum(int(bc == best0[i] and np.array_equal(wp, paths0[i].T))
                 for i, (bc, wp) in enumerate(out))
     # e2e: pinned host features in, results out
@@ -949,6 +950,7 @@ def prune_arm(args, spec):
                 "phases_ms": {"cost": ph_plain[0], "stage1": ph_plain[1], "stage2": ph_plain[2]}},
             "speedup_over_plain": v_pruned / v_plain,
             "pruning": dict(info, exact_path_agreement_rate=agree / n_pairs,
+                            profiled_phases_ms=prof.get("phases_ms"),
                             fallback_rate=info["fallbacks"] / n_pairs,
                             proposer="3 conv layers, 32 channels, bf16 activations, "
                                      "parflexdtw_b200/data/proposer_L2000.npz",

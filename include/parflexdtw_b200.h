@@ -253,7 +253,8 @@ int pfx_flexdtw_tile_noalloc(const double *C, int64_t ldc, int32_t R, int32_t W,
  * of the free device memory); per wave, the cost of every pair is built
  * from its features, ONE persistent stage-1 launch runs all tiles of all
  * pairs of the wave (largest first) from a device work queue, and stage 2
- * of the pairs runs on forked streams.  pfx_batch_run records this whole
+ * of the pairs runs on forked streams, overlapping the next waves.
+ * pfx_batch_run records this whole
  * sequence once into a CUDA graph and replays it.
  *
  * The reference has no batch entry point: its notebooks loop over pairs
@@ -289,13 +290,21 @@ int pfx_batch_plan(pfx_batch *batch, int32_t i, pfx_plan **plan);
  * graph.  No reference counterpart. */
 int pfx_batch_set_masks(pfx_batch *batch, const uint8_t *masks, int32_t on_device,
                         void *stream);
+/* After a masked run: completes pair i with the full-tile method, reusing
+ * the stage-1 results of its masked-in tiles (cost of every tile rebuilt in
+ * the pool, stage 1 on the tiles the mask left out, stage 2 on all).  Its
+ * result is then read through pfx_batch_plan + pfx_result / pfx_copy_path
+ * (until the next pfx_batch_run).  The batch keeps its masks, queues and
+ * graph.  Synchronises `stream`.  No reference counterpart. */
+int pfx_batch_complete(pfx_batch *batch, int32_t i, double beta, void *stream);
 /* Aligns every pair (asynchronous on `stream`).  use_graph = 1 records the
  * launch sequence into a CUDA graph on the first call (and again when beta
  * changes) and replays it; 0 launches directly. */
 int pfx_batch_run(pfx_batch *batch, double beta, int32_t use_graph, void *stream);
 /* Device time (ms) of the phases of the last direct (use_graph = 0) run,
  * summed over waves: ms3[0] cost building from features, ms3[1] the stage-1
- * launches, ms3[2] stage 2 (end of stage 1 to the join of its streams).
+ * launches, ms3[2] stage 2 as far as it does not overlap later waves (the
+ * edge gathers, plus the tail after the last wave's gather).
  * Waits for that run.  No reference counterpart (benchmark hook). */
 int pfx_batch_timing(pfx_batch *batch, double *ms3);
 /* Synchronises `stream` and copies every pair's result to host arrays:

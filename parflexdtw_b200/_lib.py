@@ -77,6 +77,7 @@ SIGNATURES = [
     ("pfx_batch_features", ct.c_int, [_vp, _i32, ct.POINTER(_vp), ct.POINTER(_vp)]),
     ("pfx_batch_plan", ct.c_int, [_vp, _i32, ct.POINTER(_vp)]),
     ("pfx_batch_set_masks", ct.c_int, [_vp, _vp, _i32, _vp]),
+    ("pfx_batch_complete", ct.c_int, [_vp, _i32, _f64, _vp]),
     ("pfx_batch_run", ct.c_int, [_vp, _f64, _i32, _vp]),
     ("pfx_batch_timing", ct.c_int, [_vp, _f64p]),
     ("pfx_batch_results", ct.c_int, [_vp, _vp, _f64p, _i64p, _i64p]),

@@ -119,6 +119,15 @@ class Batch:
         self.waves = int(info[1])
         self.masked = True
 
+    def complete(self, i, beta, stream=None):
+        """Pair i with the full-tile method after a masked run (its
+        masked-in tiles' stage 1 is reused); returns (best_cost, (K, 2) path)."""
+        _lib.check(_lib.load().pfx_batch_complete(self._h, int(i), float(beta),
+                                                  stream or current_stream_ptr()))
+        p = self.plan(i)
+        best, end, found, n = p.result()
+        return best, p.path(n)
+
     def run(self, beta, use_graph=True, stream=None):
         """Aligns every pair (asynchronous on the current stream)."""
         _lib.check(_lib.load().pfx_batch_run(self._h, float(beta), 1 if use_graph else 0,
@@ -147,12 +156,16 @@ class Batch:
         offs = np.zeros(self.n, dtype=np.int64)
         if self.n > 1:
             offs[1:] = np.cumsum(lens)[:-1]
-        total = int(lens.sum())
-        out = np.empty((max(total, 1), 2), dtype=np.int64)
+        total = max(int(lens.sum()), 1)
+        # page-locked staging (kept between calls), then one copy per path
+        if getattr(self, "_pinned", None) is None or self._pinned.shape[0] < total:
+            self._pinned = torch.empty((int(total * 1.25) + 1024, 2), dtype=torch.int64,
+                                       pin_memory=True)
+        stage = self._pinned.numpy()
         _lib.check(_lib.load().pfx_batch_copy_paths(
-            self._h, stream or current_stream_ptr(), out.ctypes.data_as(_I64P),
-            offs.ctypes.data_as(_I64P), out.shape[0]))
-        return [out[o:o + k] for o, k in zip(offs, lens)]
+            self._h, stream or current_stream_ptr(), stage.ctypes.data_as(_I64P),
+            offs.ctypes.data_as(_I64P), stage.shape[0]))
+        return [stage[o:o + k].copy() for o, k in zip(offs, lens)]
 
     def plan(self, i) -> Plan:
         """Pair i's plan (borrowed from the batch: stage-2 buffers, results)."""

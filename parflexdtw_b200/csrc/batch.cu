@@ -426,6 +426,66 @@ extern "C" int pfx_batch_set_masks(pfx_batch* b, const uint8_t* masks, int32_t o
     return PFX_OK;
 }
 
+extern "C" int pfx_batch_complete(pfx_batch* b, int32_t i, double beta, void* stream) {
+    if (!b) return errf(PFX_ERR_ARG, "null batch");
+    if (i < 0 || i >= b->n) return errf(PFX_ERR_ARG, "pair %d of %d", i, b->n);
+    if (!b->masked) return errf(PFX_ERR_ARG, "pfx_batch_complete needs a masked batch");
+    pfx_plan& p = b->plans[i];
+    const int nt = p.g.n1 * p.g.n2;
+    if (plan_slab_bytes(&p) > (int64_t)b->slab_bytes)
+        return errf(PFX_ERR_TOO_LARGE, "pair %d: full cost slabs exceed the pool", i);
+    cudaStream_t s = (cudaStream_t)stream;
+    BCK(cudaStreamSynchronize(s));  // the pool and the queue buffers are free again
+    std::vector<uint8_t> m((size_t)nt);
+    BCK(cudaMemcpy(m.data(), p.tile_mask, (size_t)nt, cudaMemcpyDeviceToHost));
+    // every tile's slab, in place, at the start of the pool
+    const double* F1 = b->fin + b->fin_off[i];
+    const double* F2 = F1 + (int64_t)b->d * p.g.N;
+    if (b->fp32) {
+        char* A = static_cast<char*>(p.fbf);
+        char* B = A + (size_t)p.g.N * b->kp * 2;
+        BCK(launch_features_bf16(F1, b->d, p.g.N, b->kp, A, s));
+        BCK(launch_features_bf16(F2, b->d, p.g.M, b->kp, B, s));
+        BCK(launch_gemm_cost_skew(A, B, b->kp, p.g, reinterpret_cast<float*>(b->slabs),
+                                  p.skew_stride, b->status, s, nullptr));
+    } else {
+        double* An = p.feat;
+        double* Bn = p.feat + (int64_t)b->d * p.g.N;
+        BCK(launch_l2norm(F1, b->d, p.g.N, An, s));
+        BCK(launch_l2norm(F2, b->d, p.g.M, Bn, s));
+        BCK(launch_cost_skew(An, Bn, b->d, p.g, b->slabs, p.skew_stride, s, nullptr));
+    }
+    // stage 1 on the tiles the mask left out (the others' outputs stand)
+    std::vector<TileDesc> pd((size_t)nt), missing;
+    plan_tile_descs(&p, b->slabs, pd.data());
+    for (const TileDesc& d : pd)
+        if (!m[d.tile]) missing.push_back(d);
+    // queue space past the masked waves' queues: the masked-out tiles of
+    // one pair never outnumber the masked-out tiles of the batch
+    const int waves = (int)b->wave_first.size() - 1;
+    TileDesc* qd = b->descs + b->wave_desc_off[waves - 1] + b->wave_tiles[waves - 1];
+    int* head = b->heads + (waves < b->n ? waves : 0);
+    if (!missing.empty()) {
+        BCK(cudaMemcpyAsync(qd, missing.data(), missing.size() * sizeof(TileDesc),
+                            cudaMemcpyHostToDevice, s));
+        BCK(cudaMemsetAsync(head, 0, sizeof(int), s));
+        BCK(launch_stage1_queue(qd, (int)missing.size(), nullptr, head, b->gq, b->status, b->nw,
+                                b->fp32 != 0, s));
+    }
+    void* masked_Csk = p.Csk;
+    p.Csk = b->slabs;
+    p.s2.tile_slot = nullptr;
+    int st = pfx_stage2_propagate(&p, nullptr, 0, stream);
+    if (!st) st = pfx_stage2_scan(&p, beta, stream);
+    if (!st) st = pfx_stage2_stitch(&p, 1, 0, 0, 0, 0, stream);
+    // back to the masked state (the batch's queues and graph stay valid)
+    p.Csk = masked_Csk;
+    p.s2.tile_slot = p.tile_slot;
+    if (st) return st;
+    BCK(cudaStreamSynchronize(s));  // `missing` (host) fed an asynchronous copy
+    return PFX_OK;
+}
+
 extern "C" int pfx_batch_info(const pfx_batch* b, int64_t* info) {
     if (!b || !info) return errf(PFX_ERR_ARG, "null argument");
     info[0] = b->n;
@@ -460,7 +520,7 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
     const int waves = (int)b->wave_first.size() - 1;
     BCK(cudaMemsetAsync(b->heads, 0, (size_t)waves * sizeof(int), s));
     if (timed && b->phase_ev.empty()) {
-        b->phase_ev.resize((size_t)waves * 4);
+        b->phase_ev.resize((size_t)waves * 4 + 1);
         for (auto& e : b->phase_ev) BCK(cudaEventCreate(&e));
     }
     b->phase_valid = false;
@@ -468,6 +528,7 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
         return timed ? cudaEventRecord(b->phase_ev[(size_t)w * 4 + k], s) : cudaSuccess;
     };
     int st;
+    int used_side = 0;  // side streams forked so far (joined at the end)
     for (int w = 0; w < waves; ++w) {
         const int q0 = b->wave_first[w], q1 = b->wave_first[w + 1];
         BCK(mark(w, 0));
@@ -503,22 +564,31 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
                                 b->heads + w,
                                 b->gq, b->status, b->nw, b->fp32 != 0, s));
         BCK(mark(w, 2));
+        // stage 2 reads the cost slabs only in its edge gather: that part
+        // stays on the main stream, so the next wave may overwrite the pool
+        // while the rest of this wave's stage 2 runs on the side streams
+        for (int q = q0; q < q1; ++q) {
+            const pfx_plan& p = b->plans[b->wave_pairs[q]];
+            BCK(launch_stage2_edges(nullptr, p.Csk, p.skew_stride, p.fp32 != 0, p.g, p.s2, s));
+        }
+        BCK(mark(w, 3));
         BCK(cudaEventRecord(b->fork_ev, s));
         const int nside = std::min(kSide, q1 - q0);
+        used_side = std::max(used_side, nside);
         for (int k = 0; k < nside; ++k) BCK(cudaStreamWaitEvent(b->side[k], b->fork_ev, 0));
         for (int q = q0; q < q1; ++q) {
             pfx_plan* p = &b->plans[b->wave_pairs[q]];
             cudaStream_t ss = b->side[(q - q0) % nside];
-            if ((st = pfx_stage2_propagate(p, nullptr, 0, ss))) return st;
+            BCK(launch_stage2_prop(p->g, p->s2, ss));
             if ((st = pfx_stage2_scan(p, beta, ss))) return st;
             if ((st = pfx_stage2_stitch(p, 1, 0, 0, 0, 0, ss))) return st;
         }
-        for (int k = 0; k < nside; ++k) {
-            BCK(cudaEventRecord(b->join_ev[k], b->side[k]));
-            BCK(cudaStreamWaitEvent(s, b->join_ev[k], 0));
-        }
-        BCK(mark(w, 3));
     }
+    for (int k = 0; k < used_side; ++k) {
+        BCK(cudaEventRecord(b->join_ev[k], b->side[k]));
+        BCK(cudaStreamWaitEvent(s, b->join_ev[k], 0));
+    }
+    if (timed) BCK(cudaEventRecord(b->phase_ev[(size_t)waves * 4], s));
     b->phase_valid = timed;
     return PFX_OK;
 }
@@ -565,7 +635,7 @@ extern "C" int pfx_batch_timing(pfx_batch* b, double* ms3) {
     if (!b || !ms3) return errf(PFX_ERR_ARG, "null argument");
     if (!b->phase_valid) return errf(PFX_ERR_ARG, "no direct (use_graph = 0) run to time");
     const int waves = (int)b->wave_first.size() - 1;
-    BCK(cudaEventSynchronize(b->phase_ev[(size_t)waves * 4 - 1]));
+    BCK(cudaEventSynchronize(b->phase_ev[(size_t)waves * 4]));
     ms3[0] = ms3[1] = ms3[2] = 0.0;
     for (int w = 0; w < waves; ++w) {
         for (int k = 0; k < 3; ++k) {
@@ -575,6 +645,11 @@ extern "C" int pfx_batch_timing(pfx_batch* b, double* ms3) {
             ms3[k] += t;
         }
     }
+    // the rest of stage 2 overlaps the later waves: add only its tail
+    float tail = 0.f;
+    BCK(cudaEventElapsedTime(&tail, b->phase_ev[(size_t)waves * 4 - 1],
+                             b->phase_ev[(size_t)waves * 4]));
+    ms3[2] += tail;
     return PFX_OK;
 }
 

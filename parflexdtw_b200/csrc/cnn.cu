@@ -25,11 +25,34 @@ __device__ __forceinline__ void st_act(__nv_bfloat16* p, float v) { *p = __float
 // F (d x n, FP64, row-major by feature) -> out (d x P, FP32): per block of
 // `pool` frames the mean of the L2-normalised frames (last block: the frames
 // it has).
+constexpr int kPoolMaxD = 32;
+
 __global__ void k_pool_features(const double* __restrict__ F, int d, int64_t n, int pool,
                                 float* __restrict__ out, int64_t P) {
     const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (p >= P) return;
     const int64_t i0 = p * pool, i1 = min(n, i0 + pool);
+    if (d <= kPoolMaxD) {
+        // one pass over the block's frames: norm, then the normalised sums
+        double acc[kPoolMaxD];
+#pragma unroll
+        for (int f = 0; f < kPoolMaxD; ++f) acc[f] = 0.0;
+        for (int64_t i = i0; i < i1; ++i) {
+            double x[kPoolMaxD];
+            double ss = 0.0;
+#pragma unroll
+            for (int f = 0; f < kPoolMaxD; ++f) {
+                x[f] = f < d ? F[(int64_t)f * n + i] : 0.0;
+                ss += x[f] * x[f];
+            }
+            const double nr = sqrt(ss);
+            const double inv = nr > 0.0 ? 1.0 / nr : 0.0;
+#pragma unroll
+            for (int f = 0; f < kPoolMaxD; ++f) acc[f] += x[f] * inv;
+        }
+        for (int f = 0; f < d; ++f) out[(int64_t)f * P + p] = (float)(acc[f] / (double)(i1 - i0));
+        return;
+    }
     for (int f = 0; f < d; ++f) {
         double s = 0.0;
         for (int64_t i = i0; i < i1; ++i) {

@@ -214,6 +214,11 @@ int stage1_pick_warps(const Geo& g, int num_sms);
 cudaError_t launch_fill(double* p, int64_t n, double v, cudaStream_t st);
 cudaError_t launch_stage2(const double* C, const void* Csk, int64_t skew_stride, bool f32,
                           const Geo& g, const S2Buf& b, cudaStream_t st);
+// launch_stage2 in two parts: the edge tensors (the only part that reads the
+// cost slabs) and the cross-tile propagation.
+cudaError_t launch_stage2_edges(const double* C, const void* Csk, int64_t skew_stride, bool f32,
+                                const Geo& g, const S2Buf& b, cudaStream_t st);
+cudaError_t launch_stage2_prop(const Geo& g, const S2Buf& b, cudaStream_t st);
 cudaError_t launch_sync_scan(const Geo& g, const S2Buf& b, int64_t buf, cudaStream_t st);
 cudaError_t launch_stitch(const Geo& g, const S2Buf& b, cudaStream_t st, int from_best,
                           int64_t si, int64_t sj, int64_t se, int64_t sx);

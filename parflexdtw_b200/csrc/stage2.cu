@@ -497,6 +497,12 @@ cudaError_t launch_fill(double* p, int64_t n, double v, cudaStream_t st) {
 
 cudaError_t launch_stage2(const double* C, const void* Csk, int64_t skew_stride, bool f32,
                           const Geo& g, const S2Buf& b, cudaStream_t st) {
+    cudaError_t e = launch_stage2_edges(C, Csk, skew_stride, f32, g, b, st);
+    return e != cudaSuccess ? e : launch_stage2_prop(g, b, st);
+}
+
+cudaError_t launch_stage2_edges(const double* C, const void* Csk, int64_t skew_stride, bool f32,
+                                const Geo& g, const S2Buf& b, cudaStream_t st) {
     const int64_t nslots = (int64_t)g.n1 * g.n2 * 2 * g.L;
     cudaError_t e;
     if ((e = cudaMemsetAsync(b.valid, 0, (size_t)nslots, st)) != cudaSuccess) return e;
@@ -509,6 +515,11 @@ cudaError_t launch_stage2(const double* C, const void* Csk, int64_t skew_stride,
         count_launches(1);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
+    return cudaSuccess;
+}
+
+cudaError_t launch_stage2_prop(const Geo& g, const S2Buf& b, cudaStream_t st) {
+    cudaError_t e;
     for (int a = 0; a <= g.n1 + g.n2 - 2; ++a) {
         const int ilo = a - (g.n2 - 1) > 0 ? a - (g.n2 - 1) : 0;
         const int ihi = a < g.n1 - 1 ? a : g.n1 - 1;

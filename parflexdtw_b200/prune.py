@@ -316,7 +316,8 @@ class PrunedBatch:
     """Learned pruning over a batch of pairs: one proposer pass per pair,
     then the kept tiles of all pairs in one stage-1 launch per wave
     (``pfx_batch_set_masks``), stage 2 per pair, and the full-tile method
-    (one plan per pair) for the pairs that need the fallback."""
+    for the pairs that need the fallback (``pfx_batch_complete``: only the
+    tiles the mask left out run stage 1)."""
 
     def __init__(self, shapes, L, steps, weights, d, proposer=None, threshold=None,
                  dilation=1, manhattan=None, precision="fp64", wave_bytes=0, warps=0):
@@ -381,14 +382,10 @@ class PrunedBatch:
                 continue
             fallbacks += 1
             reasons[reason] = reasons.get(reason, 0) + 1
-            f1, f2 = b.feature_views(i)
-            plan = Plan(N, M, self.L, self.steps, self.weights, precision=self.precision)
-            plan.load_features(f1, f2)
-            plan.run(None, beta)
-            bc, _, _, n = plan.result()
-            out.append((bc, np.ascontiguousarray(plan.path(n).T)))
-            run_tiles += plan.n1 * plan.n2
-            plan.close()
+            bc, wp = self._full(i, N, M, beta)
+            out.append((bc, np.ascontiguousarray(wp.T)))
+            n_t = self.grids[i][0] * self.grids[i][1]
+            run_tiles += n_t - int(mk.sum())
         mark("checks")
         total = int(self.offs[-1])
         info = {"tiles_total": total, "tiles_run": run_tiles, "tiles_proposed": kept,
@@ -398,6 +395,24 @@ class PrunedBatch:
             info["phases_ms"] = {marks[k][0]: 1e3 * (marks[k][1] - marks[k - 1][1])
                                  for k in range(1, len(marks))}
         return out, info
+
+    def _full(self, i, N, M, beta):
+        """The full-tile method for pair i: completed inside the batch when
+        the pool holds its slabs (the masked-in tiles' stage 1 is reused),
+        else on a plan of its own."""
+        try:
+            return self.batch.complete(i, beta)
+        except ValueError as e:
+            if str(e) == _lib.NO_ENDPOINT_MSG:
+                raise
+            f1, f2 = self.batch.feature_views(i)
+            plan = Plan(N, M, self.L, self.steps, self.weights, precision=self.precision)
+            plan.load_features(f1, f2)
+            plan.run(None, beta)
+            bc, _, _, n = plan.result()
+            wp = plan.path(n)
+            plan.close()
+            return bc, wp
 
     def close(self):
         self.batch.close()

@@ -241,6 +241,21 @@ def test_batch_masks_and_pruned_batch_exact(oracle_mod):
         paths = b.paths(lens)
         for i, r in enumerate(refs):
             assert best[i] == r["best_cost"] and np.array_equal(paths[i].T, r["wp"])
+    # completion after a masked run reuses the kept tiles and leaves the
+    # batch's masked state (queues, graph) intact
+    rng = np.random.default_rng(3)
+    sparse = torch.from_numpy((rng.random(masks.numel()) < 0.4).astype(np.uint8)).cuda()
+    for m in (sparse, masks):
+        b.set_masks(m)
+        b.run(0.1, use_graph=True)
+        for i, r in enumerate(refs):
+            bc, wp = b.complete(i, 0.1)
+            assert bc == r["best_cost"] and np.array_equal(wp.T, r["wp"])
+    b.run(0.1, use_graph=True)
+    best, end, lens = b.results()
+    paths = b.paths(lens)
+    for i, r in enumerate(refs):
+        assert best[i] == r["best_cost"] and np.array_equal(paths[i].T, r["wp"])
     b.close()
     net = TileProposer(seed=6)
     for thr in (-1e30, 1e30):  # everything kept / nothing kept (all fall back)
