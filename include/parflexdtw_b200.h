@@ -290,13 +290,17 @@ int pfx_batch_plan(pfx_batch *batch, int32_t i, pfx_plan **plan);
  * graph.  No reference counterpart. */
 int pfx_batch_set_masks(pfx_batch *batch, const uint8_t *masks, int32_t on_device,
                         void *stream);
-/* After a masked run: completes pair i with the full-tile method, reusing
- * the stage-1 results of its masked-in tiles (cost of every tile rebuilt in
- * the pool, stage 1 on the tiles the mask left out, stage 2 on all).  Its
- * result is then read through pfx_batch_plan + pfx_result / pfx_copy_path
- * (until the next pfx_batch_run).  The batch keeps its masks, queues and
- * graph.  Synchronises `stream`.  No reference counterpart. */
-int pfx_batch_complete(pfx_batch *batch, int32_t i, double beta, void *stream);
+/* After a masked run: adds tiles to pair i's run and aligns it again.
+ * `tiles` (host, n1*n2; nonzero = run) names the tiles to add, NULL every
+ * tile (the full-tile method).  Stage 1 runs only on the added tiles that
+ * have not run since the last pfx_batch_run (the others' outputs are
+ * reused), the cost slabs of every run tile are rebuilt in the pool, and
+ * stage 2 runs on the pair.  Its result is then read through
+ * pfx_batch_plan + pfx_result / pfx_copy_path (until the next
+ * pfx_batch_run).  The batch keeps its masks, queues and graph.
+ * Synchronises `stream`.  No reference counterpart. */
+int pfx_batch_complete(pfx_batch *batch, int32_t i, double beta, const uint8_t *tiles,
+                       void *stream);
 /* Aligns every pair (asynchronous on `stream`).  use_graph = 1 records the
  * launch sequence into a CUDA graph on the first call (and again when beta
  * changes) and replays it; 0 launches directly. */
@@ -318,6 +322,21 @@ int pfx_batch_results(pfx_batch *batch, void *stream, double *best_cost,
  * pfx_batch_results; capacity `cap` points in total).  Synchronises. */
 int pfx_batch_copy_paths(pfx_batch *batch, void *stream, int64_t *wp_host,
                          const int64_t *offsets, int64_t cap);
+/* As pfx_batch_copy_paths, with each path as two rows: pair i's K_i row
+ * indices at host + 2*offsets[i], then its K_i column indices (lens[i] =
+ * K_i from pfx_batch_results).  One device-side gather, one copy.
+ * Synchronises. */
+int pfx_batch_copy_paths_rows(pfx_batch *batch, void *stream, int64_t *host,
+                              const int64_t *offsets, const int64_t *lens, int64_t cap);
+/* Masked batch, after a run: the test that decides whether a pair's path
+ * may have been cut off by its mask, on the device.  For every block of
+ * margin x margin cells the path touches, the tiles that cover a cell of
+ * it or of its 8 neighbouring blocks and were not run get near[t] = 1
+ * (device, the pairs' (n1 x n2) tile arrays concatenated in pair order),
+ * and the pair gets flags[i] = 1 (device, int32[n]).  Asynchronous on
+ * `stream`.  No reference counterpart. */
+int pfx_batch_check_paths(pfx_batch *batch, int32_t margin, uint8_t *near, int32_t *flags,
+                          void *stream);
 
 /* ---------------------------------------------------------------------------
  * Learned tile proposer (no reference counterpart).  A 3-layer CNN reads

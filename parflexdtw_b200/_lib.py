@@ -77,11 +77,13 @@ SIGNATURES = [
     ("pfx_batch_features", ct.c_int, [_vp, _i32, ct.POINTER(_vp), ct.POINTER(_vp)]),
     ("pfx_batch_plan", ct.c_int, [_vp, _i32, ct.POINTER(_vp)]),
     ("pfx_batch_set_masks", ct.c_int, [_vp, _vp, _i32, _vp]),
-    ("pfx_batch_complete", ct.c_int, [_vp, _i32, _f64, _vp]),
+    ("pfx_batch_complete", ct.c_int, [_vp, _i32, _f64, _vp, _vp]),
     ("pfx_batch_run", ct.c_int, [_vp, _f64, _i32, _vp]),
     ("pfx_batch_timing", ct.c_int, [_vp, _f64p]),
     ("pfx_batch_results", ct.c_int, [_vp, _vp, _f64p, _i64p, _i64p]),
     ("pfx_batch_copy_paths", ct.c_int, [_vp, _vp, _i64p, _i64p, _i64]),
+    ("pfx_batch_copy_paths_rows", ct.c_int, [_vp, _vp, _i64p, _i64p, _i64p, _i64]),
+    ("pfx_batch_check_paths", ct.c_int, [_vp, _i32, _vp, _vp, _vp]),
     ("pfx_pool_features", ct.c_int, [_vp, _i32, _i64, _i32, _vp, _vp]),
     ("pfx_pooled_cost", ct.c_int, [_vp, _vp, _i32, _i64, _i64, _vp, _vp]),
     ("pfx_pooled_center", ct.c_int, [_vp, _i64, _i64, _vp, _vp]),

@@ -119,10 +119,16 @@ class Batch:
         self.waves = int(info[1])
         self.masked = True
 
-    def complete(self, i, beta, stream=None):
-        """Pair i with the full-tile method after a masked run (its
-        masked-in tiles' stage 1 is reused); returns (best_cost, (K, 2) path)."""
-        _lib.check(_lib.load().pfx_batch_complete(self._h, int(i), float(beta),
+    def complete(self, i, beta, tiles=None, stream=None):
+        """After a masked run: pair i again with `tiles` ((n1, n2) bool,
+        host) added to its run, or every tile (None: the full-tile method);
+        stage 1 runs only on tiles that have not run.  Returns
+        (best_cost, (K, 2) path)."""
+        ptr = None
+        if tiles is not None:
+            tiles = np.ascontiguousarray(tiles, dtype=np.uint8).reshape(-1)
+            ptr = tiles.ctypes.data
+        _lib.check(_lib.load().pfx_batch_complete(self._h, int(i), float(beta), ptr,
                                                   stream or current_stream_ptr()))
         p = self.plan(i)
         best, end, found, n = p.result()
@@ -166,6 +172,37 @@ class Batch:
             self._h, stream or current_stream_ptr(), stage.ctypes.data_as(_I64P),
             offs.ctypes.data_as(_I64P), stage.shape[0]))
         return [stage[o:o + k].copy() for o, k in zip(offs, lens)]
+
+    def paths_rows(self, lens, stream=None):
+        """Every pair's stitched path as a (2, K_i) int64 array (rows, then
+        columns; the reference's ``wp`` layout), from one device gather and
+        one copy.  The arrays are views of one host buffer."""
+        lens = np.asarray(lens, dtype=np.int64)
+        offs = np.zeros(self.n, dtype=np.int64)
+        if self.n > 1:
+            offs[1:] = np.cumsum(lens)[:-1]
+        total = max(int(lens.sum()), 1)
+        if getattr(self, "_pinned", None) is None or self._pinned.shape[0] < total:
+            self._pinned = torch.empty((int(total * 1.25) + 1024, 2), dtype=torch.int64,
+                                       pin_memory=True)
+        stage = self._pinned.numpy()
+        _lib.check(_lib.load().pfx_batch_copy_paths_rows(
+            self._h, stream or current_stream_ptr(), stage.ctypes.data_as(_I64P),
+            offs.ctypes.data_as(_I64P), lens.ctypes.data_as(_I64P), stage.shape[0]))
+        flat = stage.reshape(-1)[:2 * int(lens.sum())].copy()
+        return [flat[2 * o:2 * o + 2 * k].reshape(2, k) for o, k in zip(offs, lens)]
+
+    def check_paths(self, margin, stream=None):
+        """Masked batch, after a run: (near, flags) on the device -- per tile
+        (pairs' (n1, n2) arrays concatenated) 1 where a tile not run lies
+        within about `margin` cells of the pair's path, per pair 1 where any
+        does (``pfx_batch_check_paths``)."""
+        near = torch.empty(self.tiles, dtype=torch.uint8, device=f"cuda:{self.device}")
+        flags = torch.empty(self.n, dtype=torch.int32, device=f"cuda:{self.device}")
+        _lib.check(_lib.load().pfx_batch_check_paths(
+            self._h, int(margin), ct.c_void_p(near.data_ptr()), ct.c_void_p(flags.data_ptr()),
+            stream or current_stream_ptr()))
+        return near, flags
 
     def plan(self, i) -> Plan:
         """Pair i's plan (borrowed from the batch: stage-2 buffers, results)."""

@@ -38,6 +38,91 @@ __global__ void k_gather_results(const PairOut* __restrict__ po, int n, int64_t*
     o[8] = *p.wp_len;
 }
 
+// Per pair: its stitched path, tile mask and geometry (path checks and copies).
+struct PathRef {
+    const int64_t* wp;    // [K][2]
+    const int64_t* len;   // K
+    const uint8_t* mask;  // [n1 * n2] tiles run by the mask
+    int64_t N, M;
+    int32_t n1, n2, L, pad;
+    int64_t tile_off;  // offset of the pair's tiles in concatenated per-tile arrays
+    int64_t row_off;   // offset of the pair's block rows in the row scratch
+};
+
+// Block rows of `B` path rows: the column of the first and of the last path
+// point in each (the path is monotone, so they bound its interval).
+__global__ void k_path_rows(const PathRef* __restrict__ pr, int B, int32_t* __restrict__ lo,
+                            int32_t* __restrict__ hi) {
+    const PathRef q = pr[blockIdx.y];
+    const int64_t K = *q.len;
+    const int64_t* wp = q.wp;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < K;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t a = wp[2 * k] / B;
+        if (k == 0 || wp[2 * (k - 1)] / B != a) lo[q.row_off + a] = (int32_t)wp[2 * k + 1];
+        if (k == K - 1 || wp[2 * (k + 1)] / B != a) hi[q.row_off + a] = (int32_t)wp[2 * k + 1];
+    }
+}
+
+// Tiles not run by the mask that cover a cell of the 3 x 3 block
+// neighbourhood of a block the path touches: near[tile] = 1, flag[pair] = 1.
+__global__ void k_path_near(const PathRef* __restrict__ pr, int B, const int32_t* __restrict__ lo,
+                            const int32_t* __restrict__ hi, uint8_t* __restrict__ near,
+                            int32_t* __restrict__ flag) {
+    const PathRef q = pr[blockIdx.y];
+    const int64_t K = *q.len;
+    if (K <= 0) return;
+    const int64_t a0 = q.wp[0] / B, a1 = q.wp[2 * (K - 1)] / B;
+    const int64_t hop = q.L - 1;
+    auto lo_tile = [&](int64_t x0, int n) {  // first tile whose cells reach x0
+        const int64_t x = x0 - (q.L - 1);
+        const int64_t t = x <= 0 ? 0 : (x + hop - 1) / hop;
+        return (int)(t < n - 1 ? t : n - 1);
+    };
+    auto hi_tile = [&](int64_t x1, int n) {  // last tile starting at or before x1
+        const int64_t t = x1 / hop;
+        return (int)(t < n - 1 ? t : n - 1);
+    };
+    for (int64_t a = a0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; a <= a1;
+         a += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t cl = lo[q.row_off + a], ch = hi[q.row_off + a];
+        if (cl < 0 || ch < 0) continue;  // no path point in this block row
+        const int64_t r0 = (a - 1 > 0 ? a - 1 : 0) * B;
+        const int64_t r1 = ((a + 2) * B < q.N ? (a + 2) * B : q.N) - 1;
+        const int64_t bl = cl / B - 1;
+        const int64_t c0 = (bl > 0 ? bl : 0) * B;
+        const int64_t c1 = ((ch / B + 2) * B < q.M ? (ch / B + 2) * B : q.M) - 1;
+        const int ilo = lo_tile(r0, q.n1), ihi = hi_tile(r1, q.n1);
+        const int jlo = lo_tile(c0, q.n2), jhi = hi_tile(c1, q.n2);
+        bool any = false;
+        for (int i = ilo; i <= ihi; ++i)
+            for (int j = jlo; j <= jhi; ++j) {
+                const int t = i * q.n2 + j;
+                if (!q.mask[t]) {
+                    near[q.tile_off + t] = 1;
+                    any = true;
+                }
+            }
+        if (any) flag[blockIdx.y] = 1;
+    }
+}
+
+// Paths as rows: pair p's K points go to out[2 o_p .. 2 o_p + 2K) as K row
+// indices then K column indices.
+__global__ void k_path_to_rows(const PathRef* __restrict__ pr, const int64_t* __restrict__ offs,
+                               const int64_t* __restrict__ lens, int64_t* __restrict__ out) {
+    const PathRef q = pr[blockIdx.y];
+    const int64_t Kd = *q.len, Kh = lens[blockIdx.y];
+    const int64_t K = Kd < Kh ? Kd : Kh;
+    int64_t* o = out + 2 * offs[blockIdx.y];
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < K;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const longlong2 v = reinterpret_cast<const longlong2*>(q.wp)[k];
+        o[k] = v.x;
+        o[Kh + k] = v.y;
+    }
+}
+
 int errf(int status, const char* fmt, ...) {
     char buf[512];
     va_list ap;
@@ -83,6 +168,19 @@ struct pfx_batch {
     // before stage 1, after stage 1, after the stage-2 join
     std::vector<cudaEvent_t> phase_ev;
     bool phase_valid = false;
+    char* stage = nullptr;  // pinned staging of pfx_batch_set_masks' uploads
+    size_t stage_bytes = 0;
+    // masked batches, per pair: the slot map and kept-tile list of the mask
+    // (host copies), and the tiles whose stage 1 ran since the last run
+    std::vector<std::vector<int32_t>> mask_slots, mask_lists;
+    std::vector<std::vector<uint8_t>> mask_host, done;
+    bool ran = false;  // a run since pfx_batch_set_masks
+    // path checks and row-layout copies (allocated on first use)
+    PathRef* pref = nullptr;
+    int32_t* rows = nullptr;  // lo | hi block-row scratch
+    size_t rows_cap = 0;
+    int64_t* prow = nullptr;  // device staging of row-layout paths, + offsets and lengths
+    size_t prow_cap = 0;
 };
 
 static void batch_free(pfx_batch* b) {
@@ -100,6 +198,10 @@ static void batch_free(pfx_batch* b) {
     if (b->cap) cudaStreamDestroy(b->cap);
     if (b->arena) cudaFree(b->arena);
     if (b->slabs) cudaFree(b->slabs);
+    if (b->stage) cudaFreeHost(b->stage);
+    if (b->pref) cudaFree(b->pref);
+    if (b->rows) cudaFree(b->rows);
+    if (b->prow) cudaFree(b->prow);
     cudaSetDevice(cur);
     delete b;
 }
@@ -374,6 +476,35 @@ extern "C" int pfx_batch_set_masks(pfx_batch* b, const uint8_t* masks, int32_t o
         wave_pairs.push_back(i);
     }
     wave_first.push_back(n);
+    // pinned staging for the uploads (per pair: slot map, mask, its queue of
+    // every tile; then the waves' queues of kept tiles), copied asynchronously
+    size_t need = (size_t)b->total_tiles * sizeof(TileDesc) + 16;
+    for (int i = 0; i < n; ++i) {
+        const int64_t nt = moff[i + 1] - moff[i];
+        need += (size_t)nt * (4 + 4 + 1 + sizeof(TileDesc)) + 4 * 16;
+    }
+    BCK(cudaStreamSynchronize(s));  // the staging buffer may still feed earlier copies
+    if (need > b->stage_bytes) {
+        if (b->stage) cudaFreeHost(b->stage);
+    if (b->pref) cudaFree(b->pref);
+    if (b->rows) cudaFree(b->rows);
+    if (b->prow) cudaFree(b->prow);
+        b->stage = nullptr;
+        b->stage_bytes = 0;
+        BCK(cudaMallocHost(&b->stage, need));
+        b->stage_bytes = need;
+    }
+    size_t so = 0;
+    auto stage = [&](const void* src, size_t bytes) {
+        char* dst = b->stage + so;
+        memcpy(dst, src, bytes);
+        so += (bytes + 15) & ~(size_t)15;
+        return dst;
+    };
+    b->mask_slots.assign(n, {});
+    b->mask_lists.assign(n, {});
+    b->mask_host.assign(n, {});
+    b->ran = false;
     // plans: slab base, slot map, mask; queues of the kept tiles
     std::vector<TileDesc> all;
     std::vector<int64_t> wdo, wt;
@@ -386,14 +517,26 @@ extern "C" int pfx_batch_set_masks(pfx_batch* b, const uint8_t* masks, int32_t o
             pfx_plan& p = b->plans[i];
             p.Csk = reinterpret_cast<char*>(b->slabs) + off[i];
             const int nt = p.g.n1 * p.g.n2;
-            BCK(cudaMemcpy(p.tile_slot, slots[i].data(), (size_t)nt * 4, cudaMemcpyHostToDevice));
-            BCK(cudaMemcpy(p.tile_mask, m.data() + moff[i], (size_t)nt, cudaMemcpyHostToDevice));
+            BCK(cudaMemcpyAsync(p.tile_slot, stage(slots[i].data(), (size_t)nt * 4),
+                                (size_t)nt * 4, cudaMemcpyHostToDevice, s));
+            BCK(cudaMemcpyAsync(p.tile_mask, stage(m.data() + moff[i], (size_t)nt), (size_t)nt,
+                                cudaMemcpyHostToDevice, s));
+            std::vector<int32_t> kl;
+            for (int t = 0; t < nt; ++t)
+                if (slots[i][t] >= 0) kl.push_back(t);
+            p.n_kept = (int32_t)kl.size();
+            b->mask_lists[i] = kl;
+            b->mask_slots[i] = slots[i];
+            b->mask_host[i].assign(m.begin() + moff[i], m.begin() + moff[i + 1]);
+            if (!kl.empty())
+                BCK(cudaMemcpyAsync(p.tile_list, stage(kl.data(), kl.size() * 4), kl.size() * 4,
+                                    cudaMemcpyHostToDevice, s));
             std::vector<TileDesc> pd((size_t)nt);
             plan_tile_descs(&p, p.Csk, pd.data(), slots[i].data());
             // the pair's own queue keeps every tile (pfx_stage1 compacts it by the mask)
-            BCK(cudaMemcpy(p.descs, pd.data(), pd.size() * sizeof(TileDesc),
-                           cudaMemcpyHostToDevice));
-            BCK(launch_compact_descs(p.descs, nt, p.tile_mask, p.descs_sub, p.nsub, 0));
+            BCK(cudaMemcpyAsync(p.descs, stage(pd.data(), pd.size() * sizeof(TileDesc)),
+                                pd.size() * sizeof(TileDesc), cudaMemcpyHostToDevice, s));
+            BCK(launch_compact_descs(p.descs, nt, p.tile_mask, p.descs_sub, p.nsub, s));
             for (const TileDesc& d : pd)
                 if (slots[i][d.tile] >= 0) wv.push_back(d);
             p.mask_active = 1;
@@ -406,9 +549,9 @@ extern "C" int pfx_batch_set_masks(pfx_batch* b, const uint8_t* masks, int32_t o
         all.insert(all.end(), wv.begin(), wv.end());
     }
     if (!all.empty())
-        BCK(cudaMemcpy(b->descs, all.data(), all.size() * sizeof(TileDesc),
-                       cudaMemcpyHostToDevice));
-    BCK(cudaDeviceSynchronize());
+        BCK(cudaMemcpyAsync(b->descs, stage(all.data(), all.size() * sizeof(TileDesc)),
+                            all.size() * sizeof(TileDesc), cudaMemcpyHostToDevice, s));
+    BCK(cudaStreamSynchronize(s));
     b->wave_pairs = wave_pairs;
     b->wave_first = wave_first;
     b->wave_desc_off = wdo;
@@ -426,19 +569,32 @@ extern "C" int pfx_batch_set_masks(pfx_batch* b, const uint8_t* masks, int32_t o
     return PFX_OK;
 }
 
-extern "C" int pfx_batch_complete(pfx_batch* b, int32_t i, double beta, void* stream) {
+extern "C" int pfx_batch_complete(pfx_batch* b, int32_t i, double beta, const uint8_t* tiles,
+                                  void* stream) {
     if (!b) return errf(PFX_ERR_ARG, "null batch");
     if (i < 0 || i >= b->n) return errf(PFX_ERR_ARG, "pair %d of %d", i, b->n);
     if (!b->masked) return errf(PFX_ERR_ARG, "pfx_batch_complete needs a masked batch");
+    if (!b->ran) return errf(PFX_ERR_ARG, "pfx_batch_complete needs a run since pfx_batch_set_masks");
     pfx_plan& p = b->plans[i];
     const int nt = p.g.n1 * p.g.n2;
     if (plan_slab_bytes(&p) > (int64_t)b->slab_bytes)
-        return errf(PFX_ERR_TOO_LARGE, "pair %d: full cost slabs exceed the pool", i);
+        return errf(PFX_ERR_TOO_LARGE, "pair %d: its cost slabs exceed the pool", i);
     cudaStream_t s = (cudaStream_t)stream;
     BCK(cudaStreamSynchronize(s));  // the pool and the queue buffers are free again
-    std::vector<uint8_t> m((size_t)nt);
-    BCK(cudaMemcpy(m.data(), p.tile_mask, (size_t)nt, cudaMemcpyDeviceToHost));
-    // every tile's slab, in place, at the start of the pool
+    // tiles whose stage 1 has run: the mask, then every completion since the run
+    std::vector<uint8_t>& done = b->done[i];
+    std::vector<int32_t> slot((size_t)nt), list;
+    std::vector<uint8_t> run((size_t)nt, 0);
+    for (int t = 0; t < nt; ++t) {
+        const bool want = !tiles || tiles[t];
+        run[t] = want && !done[t];
+        if (want) done[t] = 1;
+        slot[t] = done[t] ? t : -1;  // slab t of the pool (pool offset 0)
+        if (done[t]) list.push_back(t);
+    }
+    // the pair's slot map and tile list point at the pool's start meanwhile
+    BCK(cudaMemcpyAsync(p.tile_slot, slot.data(), (size_t)nt * 4, cudaMemcpyHostToDevice, s));
+    BCK(cudaMemcpyAsync(p.tile_list, list.data(), list.size() * 4, cudaMemcpyHostToDevice, s));
     const double* F1 = b->fin + b->fin_off[i];
     const double* F2 = F1 + (int64_t)b->d * p.g.N;
     if (b->fp32) {
@@ -447,43 +603,49 @@ extern "C" int pfx_batch_complete(pfx_batch* b, int32_t i, double beta, void* st
         BCK(launch_features_bf16(F1, b->d, p.g.N, b->kp, A, s));
         BCK(launch_features_bf16(F2, b->d, p.g.M, b->kp, B, s));
         BCK(launch_gemm_cost_skew(A, B, b->kp, p.g, reinterpret_cast<float*>(b->slabs),
-                                  p.skew_stride, b->status, s, nullptr));
+                                  p.skew_stride, b->status, s, p.tile_slot, p.tile_list,
+                                  (int)list.size()));
     } else {
         double* An = p.feat;
         double* Bn = p.feat + (int64_t)b->d * p.g.N;
         BCK(launch_l2norm(F1, b->d, p.g.N, An, s));
         BCK(launch_l2norm(F2, b->d, p.g.M, Bn, s));
-        BCK(launch_cost_skew(An, Bn, b->d, p.g, b->slabs, p.skew_stride, s, nullptr));
+        BCK(launch_cost_skew(An, Bn, b->d, p.g, b->slabs, p.skew_stride, s, p.tile_slot,
+                             p.tile_list, (int)list.size()));
     }
-    // stage 1 on the tiles the mask left out (the others' outputs stand)
-    std::vector<TileDesc> pd((size_t)nt), missing;
+    // stage 1 on the tiles added now (the others' outputs stand; tiles never
+    // run keep the +inf edges of the masked run)
+    std::vector<TileDesc> pd((size_t)nt), todo;
     plan_tile_descs(&p, b->slabs, pd.data());
     for (const TileDesc& d : pd)
-        if (!m[d.tile]) missing.push_back(d);
+        if (run[d.tile]) todo.push_back(d);
     // queue space past the masked waves' queues: the masked-out tiles of
     // one pair never outnumber the masked-out tiles of the batch
     const int waves = (int)b->wave_first.size() - 1;
     TileDesc* qd = b->descs + b->wave_desc_off[waves - 1] + b->wave_tiles[waves - 1];
     int* head = b->heads + (waves < b->n ? waves : 0);
-    if (!missing.empty()) {
-        BCK(cudaMemcpyAsync(qd, missing.data(), missing.size() * sizeof(TileDesc),
+    if (!todo.empty()) {
+        BCK(cudaMemcpyAsync(qd, todo.data(), todo.size() * sizeof(TileDesc),
                             cudaMemcpyHostToDevice, s));
         BCK(cudaMemsetAsync(head, 0, sizeof(int), s));
-        BCK(launch_stage1_queue(qd, (int)missing.size(), nullptr, head, b->gq, b->status, b->nw,
-                                b->fp32 != 0, s));
+        const int nw = stage1_queue_warps((int)todo.size(), b->gq.L, num_sms_cur());
+        BCK(launch_stage1_queue(qd, (int)todo.size(), nullptr, head, b->gq, b->status,
+                                nw ? nw : b->nw, b->fp32 != 0, s));
     }
     void* masked_Csk = p.Csk;
     p.Csk = b->slabs;
-    p.s2.tile_slot = nullptr;
     int st = pfx_stage2_propagate(&p, nullptr, 0, stream);
     if (!st) st = pfx_stage2_scan(&p, beta, stream);
     if (!st) st = pfx_stage2_stitch(&p, 1, 0, 0, 0, 0, stream);
     // back to the masked state (the batch's queues and graph stay valid)
     p.Csk = masked_Csk;
-    p.s2.tile_slot = p.tile_slot;
-    if (st) return st;
-    BCK(cudaStreamSynchronize(s));  // `missing` (host) fed an asynchronous copy
-    return PFX_OK;
+    const std::vector<int32_t>& ms = b->mask_slots[i];
+    const std::vector<int32_t>& ml = b->mask_lists[i];
+    BCK(cudaMemcpyAsync(p.tile_slot, ms.data(), ms.size() * 4, cudaMemcpyHostToDevice, s));
+    if (!ml.empty())
+        BCK(cudaMemcpyAsync(p.tile_list, ml.data(), ml.size() * 4, cudaMemcpyHostToDevice, s));
+    BCK(cudaStreamSynchronize(s));  // host vectors fed asynchronous copies
+    return st;
 }
 
 extern "C" int pfx_batch_info(const pfx_batch* b, int64_t* info) {
@@ -538,20 +700,21 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
             const double* F1 = b->fin + b->fin_off[i];
             const double* F2 = F1 + (int64_t)b->d * p.g.N;
             const int32_t* slot = b->masked ? p.tile_slot : nullptr;
+            const int32_t* list = b->masked ? p.tile_list : nullptr;
             if (b->fp32) {
                 char* A = static_cast<char*>(p.fbf);
                 char* B = A + (size_t)p.g.N * b->kp * 2;
                 BCK(launch_features_bf16(F1, b->d, p.g.N, b->kp, A, s));
                 BCK(launch_features_bf16(F2, b->d, p.g.M, b->kp, B, s));
                 BCK(launch_gemm_cost_skew(A, B, b->kp, p.g, static_cast<float*>(p.Csk),
-                                          p.skew_stride, b->status, s, slot));
+                                          p.skew_stride, b->status, s, slot, list, p.n_kept));
             } else {
                 double* An = p.feat;
                 double* Bn = p.feat + (int64_t)b->d * p.g.N;
                 BCK(launch_l2norm(F1, b->d, p.g.N, An, s));
                 BCK(launch_l2norm(F2, b->d, p.g.M, Bn, s));
                 BCK(launch_cost_skew(An, Bn, b->d, p.g, static_cast<double*>(p.Csk),
-                                     p.skew_stride, s, slot));
+                                     p.skew_stride, s, slot, list, p.n_kept));
             }
             if (b->masked) {
                 // skipped tiles keep +inf edges and start 0 for stage 2
@@ -596,6 +759,10 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
 extern "C" int pfx_batch_run(pfx_batch* b, double beta, int32_t use_graph, void* stream) {
     if (!b) return errf(PFX_ERR_ARG, "null batch");
     cudaStream_t s = (cudaStream_t)stream;
+    if (b->masked) {  // completions start again from the mask
+        b->done = b->mask_host;
+        b->ran = true;
+    }
     if (!use_graph) return batch_enqueue(b, beta, s, true);
     if (!b->exec || b->graph_beta != beta) {
         if (b->exec) {
@@ -675,6 +842,90 @@ extern "C" int pfx_batch_results(pfx_batch* b, void* stream, double* best_cost, 
         if (best_end7) memcpy(&best_end7[(size_t)i * 7], &r[1], 56);
         if (wp_len) wp_len[i] = r[8];
     }
+    return PFX_OK;
+}
+
+static int ensure_pref(pfx_batch* b) {
+    if (b->pref) return PFX_OK;
+    std::vector<PathRef> h((size_t)b->n);
+    int64_t to = 0, ro = 0;
+    for (int i = 0; i < b->n; ++i) {
+        const pfx_plan& p = b->plans[i];
+        h[i] = PathRef{p.s2.wp, p.s2.wp_len, p.tile_mask, p.g.N, p.g.M, p.g.n1, p.g.n2, p.g.L,
+                       0, to, ro};
+        to += (int64_t)p.g.n1 * p.g.n2;
+        ro += p.g.N + 2;  // block rows for any block size >= 1
+    }
+    BCK(cudaMalloc(&b->pref, h.size() * sizeof(PathRef)));
+    BCK(cudaMemcpy(b->pref, h.data(), h.size() * sizeof(PathRef), cudaMemcpyHostToDevice));
+    return PFX_OK;
+}
+
+extern "C" int pfx_batch_check_paths(pfx_batch* b, int32_t margin, uint8_t* near, int32_t* flags,
+                                     void* stream) {
+    if (!b || !near || !flags) return errf(PFX_ERR_ARG, "null argument");
+    if (margin < 1) return errf(PFX_ERR_ARG, "margin %d", margin);
+    if (!b->masked) return errf(PFX_ERR_ARG, "pfx_batch_check_paths needs a masked batch");
+    cudaStream_t s = (cudaStream_t)stream;
+    int st = ensure_pref(b);
+    if (st) return st;
+    size_t rows = 0;
+    for (int i = 0; i < b->n; ++i) rows += (size_t)b->plans[i].g.N + 2;
+    if (rows * 2 > b->rows_cap) {
+        BCK(cudaStreamSynchronize(s));
+        if (b->rows) cudaFree(b->rows);
+        b->rows = nullptr;
+        b->rows_cap = 0;
+        BCK(cudaMalloc(&b->rows, rows * 2 * sizeof(int32_t)));
+        b->rows_cap = rows * 2;
+    }
+    BCK(cudaMemsetAsync(b->rows, 0xff, rows * 2 * sizeof(int32_t), s));
+    BCK(cudaMemsetAsync(near, 0, (size_t)b->total_tiles, s));
+    BCK(cudaMemsetAsync(flags, 0, (size_t)b->n * sizeof(int32_t), s));
+    k_path_rows<<<dim3(32, b->n), 256, 0, s>>>(b->pref, margin, b->rows, b->rows + rows);
+    k_path_near<<<dim3(4, b->n), 256, 0, s>>>(b->pref, margin, b->rows, b->rows + rows, near,
+                                              flags);
+    count_launches(2);
+    BCK(cudaGetLastError());
+    return PFX_OK;
+}
+
+extern "C" int pfx_batch_copy_paths_rows(pfx_batch* b, void* stream, int64_t* host,
+                                         const int64_t* offsets, const int64_t* lens,
+                                         int64_t cap) {
+    if (!b || !host || !offsets || !lens) return errf(PFX_ERR_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    int64_t total = 0;
+    for (int i = 0; i < b->n; ++i) {
+        if (lens[i] < 0 || offsets[i] < 0 || offsets[i] + lens[i] > cap)
+            return errf(PFX_ERR_ARG, "pair %d: path of %lld points at offset %lld exceeds %lld", i,
+                        (long long)lens[i], (long long)offsets[i], (long long)cap);
+        total = std::max(total, offsets[i] + lens[i]);
+    }
+    int st = ensure_pref(b);
+    if (st) return st;
+    const size_t need = (size_t)2 * total + 2 * (size_t)b->n;
+    if (need > b->prow_cap) {
+        BCK(cudaStreamSynchronize(s));
+        if (b->prow) cudaFree(b->prow);
+        b->prow = nullptr;
+        b->prow_cap = 0;
+        const size_t cap2 = need + need / 4 + 1024;
+        BCK(cudaMalloc(&b->prow, cap2 * sizeof(int64_t)));
+        b->prow_cap = cap2;
+    }
+    int64_t* d_off = b->prow + b->prow_cap - 2 * (size_t)b->n;
+    int64_t* d_len = d_off + b->n;
+    std::vector<int64_t> ol((size_t)2 * b->n);
+    std::copy(offsets, offsets + b->n, ol.begin());
+    std::copy(lens, lens + b->n, ol.begin() + b->n);
+    BCK(cudaMemcpyAsync(d_off, ol.data(), ol.size() * 8, cudaMemcpyHostToDevice, s));
+    k_path_to_rows<<<dim3(16, b->n), 256, 0, s>>>(b->pref, d_off, d_len, b->prow);
+    count_launches(1);
+    BCK(cudaGetLastError());
+    if (total > 0)
+        BCK(cudaMemcpyAsync(host, b->prow, (size_t)2 * total * 8, cudaMemcpyDeviceToHost, s));
+    BCK(cudaStreamSynchronize(s));
     return PFX_OK;
 }
 

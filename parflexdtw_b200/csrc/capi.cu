@@ -211,6 +211,7 @@ int pfx::plan_init(pfx_plan* p, int64_t N, int64_t M, int32_t L, const int64_t* 
     PA(&p->head, 1);
     PA(&p->tile_mask, nt);
     PA(&p->tile_slot, nt);
+    PA(&p->tile_list, nt);
     PA(&p->descs_sub, nt);
     PA(&p->nsub, 1);
 #undef PA

@@ -69,14 +69,23 @@ __global__ void k_pool_features(const double* __restrict__ F, int d, int64_t n, 
 }
 
 // out[i][j] = 1 - sum_f A[f][i] B[f][j]   (A: d x P1, B: d x P2)
+// Four rows per thread: each B value read once serves four outputs.
 __global__ void k_pooled_cost(const float* __restrict__ A, const float* __restrict__ B, int d,
                               int64_t P1, int64_t P2, float* __restrict__ out) {
     const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t i = blockIdx.y;
+    const int64_t i0 = blockIdx.y * 4LL;
     if (j >= P2) return;
-    float acc = 0.f;
-    for (int f = 0; f < d; ++f) acc = fmaf(A[(int64_t)f * P1 + i], B[(int64_t)f * P2 + j], acc);
-    out[i * P2 + j] = 1.f - acc;
+    const int nr = P1 - i0 < 4 ? (int)(P1 - i0) : 4;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int f = 0; f < d; ++f) {
+        const float bv = B[(int64_t)f * P2 + j];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            if (r < nr) acc[r] = fmaf(A[(int64_t)f * P1 + i0 + r], bv, acc[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+        if (r < nr) out[(i0 + r) * P2 + j] = 1.f - acc[r];
 }
 
 // Double centring and standardisation of a P1 x P2 map, in place:
@@ -99,20 +108,30 @@ __global__ void k_row_mean(const float* __restrict__ x, int64_t P1, int64_t P2,
     }
 }
 
-__global__ void k_col_mean(const float* __restrict__ x, int64_t P1, int64_t P2,
-                           float* __restrict__ cm) {
-    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (j >= P2) return;
+// 32 columns per CTA; the 32 warps take every 32nd row, partial sums are
+// added in a fixed order (deterministic)
+__global__ void __launch_bounds__(1024)
+    k_col_mean(const float* __restrict__ x, int64_t P1, int64_t P2, float* __restrict__ cm) {
+    __shared__ float part[32][33];
+    const int64_t j = blockIdx.x * 32LL + threadIdx.x;
     float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-    int64_t i = 0;
-    for (; i + 3 < P1; i += 4) {
-        s0 += x[i * P2 + j];
-        s1 += x[(i + 1) * P2 + j];
-        s2 += x[(i + 2) * P2 + j];
-        s3 += x[(i + 3) * P2 + j];
+    if (j < P2) {
+        int64_t i = threadIdx.y;
+        for (; i + 96 < P1; i += 128) {
+            s0 += x[i * P2 + j];
+            s1 += x[(i + 32) * P2 + j];
+            s2 += x[(i + 64) * P2 + j];
+            s3 += x[(i + 96) * P2 + j];
+        }
+        for (; i < P1; i += 32) s0 += x[i * P2 + j];
     }
-    for (; i < P1; ++i) s0 += x[i * P2 + j];
-    cm[j] = ((s0 + s1) + (s2 + s3)) / (float)P1;
+    part[threadIdx.y][threadIdx.x] = (s0 + s1) + (s2 + s3);
+    __syncthreads();
+    if (threadIdx.y == 0 && j < P2) {
+        float t = 0.f;
+        for (int r = 0; r < 32; ++r) t += part[r][threadIdx.x];
+        cm[j] = t / (float)P1;
+    }
 }
 
 // sc[P1 + P2] = grand mean (mean of the row means), sc[P1 + P2 + 1] = 0
@@ -166,56 +185,70 @@ __global__ void k_scale(float* __restrict__ x, int64_t n, const float* __restric
 // for up to 32 output channels; per input channel the input patch and that
 // channel's weights ([tap][co], read 4 at a time) are staged in shared
 // memory.  y = act(conv(x) + b), act = ReLU or identity.
-constexpr int kCvT = 16;   // output tile edge
-constexpr int kCvCo = 32;  // output channels per CTA
+constexpr int kCvT = 16;  // output tile edge
 
-template <int S, typename Tin, typename Tout>
+// One thread per output pixel of a 16 x 16 tile, CO output channels per CTA;
+// CIB input channels are staged in shared memory per barrier.  The sum over
+// (ci, tap) runs in the same order for every CO / CIB.
+template <int S, int CO, int CIB, typename Tin, typename Tout>
 __global__ void __launch_bounds__(kCvT * kCvT)
     k_conv3x3_fwd(const Tin* __restrict__ x, int Cin, int H, int W, const float* __restrict__ w,
                   const float* __restrict__ b, int Cout, int Ho, int Wo, int relu,
                   Tout* __restrict__ y) {
     constexpr int PT = (kCvT - 1) * S + 3;  // input patch edge
-    __shared__ float patch[PT * PT];
-    __shared__ __align__(16) float ws[9 * kCvCo];
-    const int ox0 = blockIdx.x * kCvT, oy0 = blockIdx.y * kCvT, co0 = blockIdx.z * kCvCo;
+    __shared__ float patch[CIB][PT * PT];
+    __shared__ __align__(16) float ws[CIB][9 * CO];
+    const int ox0 = blockIdx.x * kCvT, oy0 = blockIdx.y * kCvT, co0 = blockIdx.z * CO;
     const int tx = threadIdx.x % kCvT, ty = threadIdx.x / kCvT;
     const int ox = ox0 + tx, oy = oy0 + ty;
-    const int nco = min(kCvCo, Cout - co0);
-    float acc[kCvCo];
+    const int nco = min(CO, Cout - co0);
+    float acc[CO];
 #pragma unroll
-    for (int c = 0; c < kCvCo; ++c) acc[c] = 0.f;
+    for (int c = 0; c < CO; ++c) acc[c] = 0.f;
     const int ix0 = ox0 * S - 1, iy0 = oy0 * S - 1;
-    for (int ci = 0; ci < Cin; ++ci) {
+    for (int ci0 = 0; ci0 < Cin; ci0 += CIB) {
+        const int ncb = min(CIB, Cin - ci0);
         __syncthreads();
-        for (int q = threadIdx.x; q < PT * PT; q += kCvT * kCvT) {
-            const int py = q / PT, px = q % PT;
+        for (int q = threadIdx.x; q < CIB * PT * PT; q += kCvT * kCvT) {
+            const int cb = q / (PT * PT), r = q % (PT * PT);
+            const int py = r / PT, px = r % PT;
             const int iy = iy0 + py, ix = ix0 + px;
-            patch[q] = (iy >= 0 && iy < H && ix >= 0 && ix < W)
-                           ? ld_act(x + ((int64_t)ci * H + iy) * W + ix)
-                           : 0.f;
+            patch[cb][r] = (cb < ncb && iy >= 0 && iy < H && ix >= 0 && ix < W)
+                               ? ld_act(x + ((int64_t)(ci0 + cb) * H + iy) * W + ix)
+                               : 0.f;
         }
-        for (int q = threadIdx.x; q < 9 * kCvCo; q += kCvT * kCvT) {
-            const int tap = q / kCvCo, c = q % kCvCo;
-            ws[q] = c < nco ? w[((int64_t)(co0 + c) * Cin + ci) * 9 + tap] : 0.f;
+        for (int q = threadIdx.x; q < CIB * 9 * CO; q += kCvT * kCvT) {
+            const int cb = q / (9 * CO), r = q % (9 * CO);
+            const int tap = r / CO, c = r % CO;
+            ws[cb][r] = (c < nco && cb < ncb)
+                            ? w[((int64_t)(co0 + c) * Cin + ci0 + cb) * 9 + tap]
+                            : 0.f;
         }
         __syncthreads();
+        for (int cb = 0; cb < ncb; ++cb) {
 #pragma unroll
-        for (int tap = 0; tap < 9; ++tap) {
-            const float xv = patch[(ty * S + tap / 3) * PT + tx * S + tap % 3];
-            const float4* w4 = reinterpret_cast<const float4*>(ws + tap * kCvCo);
+            for (int tap = 0; tap < 9; ++tap) {
+                const float xv = patch[cb][(ty * S + tap / 3) * PT + tx * S + tap % 3];
+                if constexpr (CO % 4 == 0) {
+                    const float4* w4 = reinterpret_cast<const float4*>(&ws[cb][tap * CO]);
 #pragma unroll
-            for (int c4 = 0; c4 < kCvCo / 4; ++c4) {
-                const float4 wv = w4[c4];
-                acc[4 * c4 + 0] = fmaf(wv.x, xv, acc[4 * c4 + 0]);
-                acc[4 * c4 + 1] = fmaf(wv.y, xv, acc[4 * c4 + 1]);
-                acc[4 * c4 + 2] = fmaf(wv.z, xv, acc[4 * c4 + 2]);
-                acc[4 * c4 + 3] = fmaf(wv.w, xv, acc[4 * c4 + 3]);
+                    for (int c4 = 0; c4 < CO / 4; ++c4) {
+                        const float4 wv = w4[c4];
+                        acc[4 * c4 + 0] = fmaf(wv.x, xv, acc[4 * c4 + 0]);
+                        acc[4 * c4 + 1] = fmaf(wv.y, xv, acc[4 * c4 + 1]);
+                        acc[4 * c4 + 2] = fmaf(wv.z, xv, acc[4 * c4 + 2]);
+                        acc[4 * c4 + 3] = fmaf(wv.w, xv, acc[4 * c4 + 3]);
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < CO; ++c) acc[c] = fmaf(ws[cb][tap * CO + c], xv, acc[c]);
+                }
             }
         }
     }
     if (ox >= Wo || oy >= Ho) return;
 #pragma unroll
-    for (int c = 0; c < kCvCo; ++c) {
+    for (int c = 0; c < CO; ++c) {
         if (c < nco) {
             float v = acc[c] + b[co0 + c];
             if (relu) v = fmaxf(v, 0.f);
@@ -429,20 +462,32 @@ cudaError_t cnn_pool_features(const double* F, int d, int64_t n, int pool, float
 cudaError_t cnn_pooled_cost(const float* A, const float* B, int d, int64_t P1, int64_t P2,
                             float* out, cudaStream_t st) {
     if (P1 <= 0 || P2 <= 0) return cudaSuccess;
-    k_pooled_cost<<<dim3(blocks_for(P2, 256), (unsigned)P1), 256, 0, st>>>(A, B, d, P1, P2, out);
+    k_pooled_cost<<<dim3(blocks_for(P2, 256), (unsigned)blocks_for(P1, 4)), 256, 0, st>>>(
+        A, B, d, P1, P2, out);
     count_launches(1);
     return cudaGetLastError();
 }
 
-template <int S, typename Tin, typename Tout>
-static cudaError_t conv_fwd_t(const void* x, int Cin, int H, int W, const float* w, const float* b,
-                              int Cout, int relu, void* y, cudaStream_t st) {
+template <int S, int CO, int CIB, typename Tin, typename Tout>
+static cudaError_t conv_fwd_launch(const void* x, int Cin, int H, int W, const float* w,
+                                   const float* b, int Cout, int relu, void* y, cudaStream_t st) {
     const int Ho = (H - 1) / S + 1, Wo = (W - 1) / S + 1;
-    const dim3 grid(blocks_for(Wo, kCvT), blocks_for(Ho, kCvT), blocks_for(Cout, kCvCo));
-    k_conv3x3_fwd<S, Tin, Tout><<<grid, kCvT * kCvT, 0, st>>>(
+    const dim3 grid(blocks_for(Wo, kCvT), blocks_for(Ho, kCvT), blocks_for(Cout, CO));
+    k_conv3x3_fwd<S, CO, CIB, Tin, Tout><<<grid, kCvT * kCvT, 0, st>>>(
         static_cast<const Tin*>(x), Cin, H, W, w, b, Cout, Ho, Wo, relu, static_cast<Tout*>(y));
     count_launches(1);
     return cudaGetLastError();
+}
+
+// 32 output channels per CTA, or one when the layer has fewer than 8; the
+// patch of 4 input channels (stride 1, 2) or one (stride 4) per barrier
+template <int S, typename Tin, typename Tout>
+static cudaError_t conv_fwd_t(const void* x, int Cin, int H, int W, const float* w, const float* b,
+                              int Cout, int relu, void* y, cudaStream_t st) {
+    constexpr int CIB = S == 4 ? 1 : 4;
+    if (Cout < 8)
+        return conv_fwd_launch<S, 1, 2 * CIB, Tin, Tout>(x, Cin, H, W, w, b, Cout, relu, y, st);
+    return conv_fwd_launch<S, 32, CIB, Tin, Tout>(x, Cin, H, W, w, b, Cout, relu, y, st);
 }
 
 // in_bf16 / out_bf16: activation storage types (FP32 otherwise).
@@ -535,7 +580,7 @@ extern "C" int pfx_pooled_center(float* x, int64_t P1, int64_t P2, float* scratc
     cudaStream_t st = (cudaStream_t)stream;
     const int64_t n = P1 * P2;
     k_row_mean<<<(unsigned)P1, 256, 0, st>>>(x, P1, P2, scratch);
-    k_col_mean<<<blocks_for(P2, 64), 64, 0, st>>>(x, P1, P2, scratch + P1);
+    k_col_mean<<<blocks_for(P2, 32), dim3(32, 32), 0, st>>>(x, P1, P2, scratch + P1);
     k_grand_mean<<<1, 1024, 0, st>>>(scratch, P1, P2);
     const int64_t cb = blocks_for(n, 256) < 1184 ? blocks_for(n, 256) : 1184;
     k_center<<<(unsigned)cb, 256, 0, st>>>(x, P1, P2, scratch);

@@ -190,6 +190,8 @@ cudaError_t launch_compact_descs(const TileDesc* in, int n, const uint8_t* mask,
 int stage1_queue_warps(int ntiles, int32_t L, int num_sms);
 // Cost-building launchers take an optional slot map: tile t's slab is slab
 // slot[t] of Csk, and tiles with slot[t] < 0 are skipped (null: slab = t).
+// The feature launchers also take an optional list of the nlist tiles to
+// build (no CTAs are launched for the others).
 cudaError_t launch_relayout_skew(const double* C, int64_t ldc, const Geo& g, double* Csk,
                                  int64_t skew_stride, cudaStream_t st,
                                  const int32_t* slot = nullptr);
@@ -199,13 +201,15 @@ cudaError_t launch_features_bf16(const double* F, int d, int64_t n, int Kp, void
                                  cudaStream_t st);
 cudaError_t launch_gemm_cost_skew(const void* Abf, const void* Bbf, int Kp, const Geo& g,
                                   float* Csk, int64_t stride, int32_t* status, cudaStream_t st,
-                                  const int32_t* slot = nullptr);
+                                  const int32_t* slot = nullptr, const int32_t* list = nullptr,
+                                  int nlist = 0);
 // FP32 slabs from a row-major FP64 (rounded) or FP32 C (exactly one non-null).
 cudaError_t launch_relayout_skew_f32(const double* C64, const float* C32, int64_t ldc,
                                      const Geo& g, float* Csk, int64_t stride, cudaStream_t st,
                                      const int32_t* slot = nullptr);
 cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Geo& g, double* Csk,
-                             int64_t skew_stride, cudaStream_t st, const int32_t* slot = nullptr);
+                             int64_t skew_stride, cudaStream_t st, const int32_t* slot = nullptr,
+                             const int32_t* list = nullptr, int nlist = 0);
 cudaError_t launch_l2norm(const double* F, int d, int64_t n, double* out, cudaStream_t st);
 cudaError_t launch_stage1(const double* C, const Geo& g, const S1Out& o, int tile0, int ntiles,
                           int nw, bool full, cudaStream_t st);

@@ -106,7 +106,8 @@ __global__ void __launch_bounds__(kGThreads, 1)
     k_gemm_cost_skew(const __grid_constant__ CUtensorMap mapA,
                      const __grid_constant__ CUtensorMap mapB, const Geo g,
                      float* __restrict__ Csk, const int64_t stride,
-                     int32_t* __restrict__ status, const int32_t* __restrict__ slot) {
+                     int32_t* __restrict__ status, const int32_t* __restrict__ slot,
+                     const int32_t* __restrict__ list) {
     extern __shared__ __align__(1024) unsigned char gsm_raw[];
     // operands (1024-byte aligned atoms), later reused as the skew stage
     unsigned char* base = reinterpret_cast<unsigned char*>(
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
     const int cb = q % ncb;
     q /= ncb;
     const int kk = q % nkk;
-    const int tile = q / nkk;
+    const int tile = list ? list[q / nkk] : q / nkk;
     const int slab = slot ? slot[tile] : tile;  // slab index; < 0: tile skipped
     if (slab < 0) return;  // uniform over the CTA
     int64_t r0, c0;
@@ -325,7 +326,8 @@ size_t gemm_cost_smem_bytes(int Kp) {
 
 template <int KB>
 static cudaError_t gemm_t(const CUtensorMap& ma, const CUtensorMap& mb, const Geo& g, float* Csk,
-                          int64_t stride, int32_t* status, cudaStream_t st, const int32_t* slot) {
+                          int64_t stride, int32_t* status, cudaStream_t st, const int32_t* slot,
+                          const int32_t* list, int nlist) {
     const size_t smem = gemm_cost_smem_bytes(64 * KB);
     auto kern = k_gemm_cost_skew<KB>;
     cudaError_t e =
@@ -333,25 +335,27 @@ static cudaError_t gemm_t(const CUtensorMap& ma, const CUtensorMap& mb, const Ge
     if (e != cudaSuccess) return e;
     const Sched2 s = make_sched2(g.L, g.L, 1);
     const int64_t nblk =
-        (int64_t)g.n1 * g.n2 * ((s.nS + 1) / 2) * ceil_div32(s.span, kGSteps);
+        (list ? (int64_t)nlist : (int64_t)g.n1 * g.n2) * ((s.nS + 1) / 2) *
+        ceil_div32(s.span, kGSteps);
     if (nblk > 0x7fffffffLL) return cudaErrorInvalidValue;
-    kern<<<(unsigned)nblk, kGThreads, smem, st>>>(ma, mb, g, Csk, stride, status, slot);
+    if (nblk == 0) return cudaSuccess;
+    kern<<<(unsigned)nblk, kGThreads, smem, st>>>(ma, mb, g, Csk, stride, status, slot, list);
     count_launches(1);
     return cudaGetLastError();
 }
 
 cudaError_t launch_gemm_cost_skew(const void* Abf, const void* Bbf, int Kp, const Geo& g,
                                   float* Csk, int64_t stride, int32_t* status, cudaStream_t st,
-                                  const int32_t* slot) {
+                                  const int32_t* slot, const int32_t* list, int nlist) {
     if (Kp % 64 || Kp < 64 || Kp > 256) return cudaErrorInvalidValue;
     CUtensorMap ma, mb;
     if (!make_map(&ma, Abf, g.N, Kp, kGRows) || !make_map(&mb, Bbf, g.M, Kp, kGCols))
         return cudaErrorInvalidValue;
     switch (Kp / 64) {
-        case 1: return gemm_t<1>(ma, mb, g, Csk, stride, status, st, slot);
-        case 2: return gemm_t<2>(ma, mb, g, Csk, stride, status, st, slot);
-        case 3: return gemm_t<3>(ma, mb, g, Csk, stride, status, st, slot);
-        default: return gemm_t<4>(ma, mb, g, Csk, stride, status, st, slot);
+        case 1: return gemm_t<1>(ma, mb, g, Csk, stride, status, st, slot, list, nlist);
+        case 2: return gemm_t<2>(ma, mb, g, Csk, stride, status, st, slot, list, nlist);
+        case 3: return gemm_t<3>(ma, mb, g, Csk, stride, status, st, slot, list, nlist);
+        default: return gemm_t<4>(ma, mb, g, Csk, stride, status, st, slot, list, nlist);
     }
 }
 

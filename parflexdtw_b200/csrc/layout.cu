@@ -90,10 +90,11 @@ template <int DMAX>
 __global__ void __launch_bounds__(kCostThreads, 2)
     k_cost_skew(const double* __restrict__ An, const double* __restrict__ Bn, const int d,
                 const Geo g, double* __restrict__ Csk, const int64_t stride,
-                const int32_t* __restrict__ slot) {
+                const int32_t* __restrict__ slot, const int32_t* __restrict__ list) {
     extern __shared__ __align__(16) double sB[];  // [d][2][kCH]
     const int nchunk = ceil_div32(make_sched2(g.L, g.L, 1).span, kCT);
-    const int tile = (int)(blockIdx.x / nchunk), k = blockIdx.y;
+    const int tile = list ? list[blockIdx.x / nchunk] : (int)(blockIdx.x / nchunk);
+    const int k = blockIdx.y;
     const int ts = (int)(blockIdx.x % nchunk) * kCT;
     const int slab = slot ? slot[tile] : tile;  // slab index; < 0: tile skipped
     if (slab < 0) return;
@@ -170,10 +171,11 @@ constexpr int kCH2 = kCX2 / 2;
 __global__ void __launch_bounds__(kCostThreads, 2)
     k_cost_skew_chunked(const double* __restrict__ An, const double* __restrict__ Bn, const int d,
                         const Geo g, double* __restrict__ Csk, const int64_t stride,
-                        const int32_t* __restrict__ slot) {
+                        const int32_t* __restrict__ slot, const int32_t* __restrict__ list) {
     __shared__ __align__(16) double sB[kMaxFeat * kCX2];  // [16][2][kCH2]
     const int nchunk = ceil_div32(make_sched2(g.L, g.L, 1).span, kCT2);
-    const int tile = (int)(blockIdx.x / nchunk), k = blockIdx.y;
+    const int tile = list ? list[blockIdx.x / nchunk] : (int)(blockIdx.x / nchunk);
+    const int k = blockIdx.y;
     const int ts = (int)(blockIdx.x % nchunk) * kCT2;
     const int slab = slot ? slot[tile] : tile;  // slab index; < 0: tile skipped
     if (slab < 0) return;
@@ -234,9 +236,11 @@ __global__ void __launch_bounds__(kCostThreads, 2)
     }
 }
 
-static dim3 region_grid(const Geo& g, int per_cta) {
+// ntiles: the tiles enumerated (all n1 * n2, or the length of a tile list)
+static dim3 region_grid(const Geo& g, int per_cta, int64_t ntiles = -1) {
     const Sched2 s = make_sched2(g.L, g.L, 1);
-    return dim3((unsigned)(ceil_div32(s.span, per_cta) * (int64_t)g.n1 * g.n2), (unsigned)s.nS, 1);
+    if (ntiles < 0) ntiles = (int64_t)g.n1 * g.n2;
+    return dim3((unsigned)(ceil_div32(s.span, per_cta) * ntiles), (unsigned)s.nS, 1);
 }
 
 template <typename Tin, typename Tout>
@@ -265,21 +269,24 @@ cudaError_t launch_relayout_skew_f32(const double* C64, const float* C32, int64_
 }
 
 cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Geo& g, double* Csk,
-                             int64_t stride, cudaStream_t st, const int32_t* slot) {
+                             int64_t stride, cudaStream_t st, const int32_t* slot,
+                             const int32_t* list, int nlist) {
     if (d < 1) return cudaErrorInvalidValue;
+    const int64_t nt = list ? nlist : -1;
+    if (list && nlist == 0) return cudaSuccess;
     if (d > kMaxFeat) {
-        k_cost_skew_chunked<<<region_grid(g, kCT2), kCostThreads, 0, st>>>(An, Bn, d, g, Csk,
-                                                                          stride, slot);
+        k_cost_skew_chunked<<<region_grid(g, kCT2, nt), kCostThreads, 0, st>>>(An, Bn, d, g, Csk,
+                                                                              stride, slot, list);
         count_launches(1);
         return cudaGetLastError();
     }
     const size_t smem = (size_t)d * kCX * sizeof(double);
     if (d == 12) {
-        k_cost_skew<12><<<region_grid(g, kCT), kCostThreads, smem, st>>>(An, Bn, d, g, Csk, stride,
-                                                                         slot);
+        k_cost_skew<12><<<region_grid(g, kCT, nt), kCostThreads, smem, st>>>(An, Bn, d, g, Csk,
+                                                                             stride, slot, list);
     } else {
-        k_cost_skew<kMaxFeat><<<region_grid(g, kCT), kCostThreads, smem, st>>>(An, Bn, d, g, Csk,
-                                                                             stride, slot);
+        k_cost_skew<kMaxFeat><<<region_grid(g, kCT, nt), kCostThreads, smem, st>>>(
+            An, Bn, d, g, Csk, stride, slot, list);
     }
     count_launches(1);
     return cudaGetLastError();

@@ -33,6 +33,8 @@ struct pfx_plan {
     // tile's cost slab (-1: skipped), the masked queue and its device length
     uint8_t* tile_mask;
     int32_t* tile_slot;
+    int32_t* tile_list;  // masked batch: the kept tiles in tile order, n_kept of them
+    int32_t n_kept;
     pfx::TileDesc* descs_sub;
     int* nsub;
     int mask_active;

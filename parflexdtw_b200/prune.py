@@ -220,11 +220,10 @@ class TileProposer:
 FALLBACK_MARGIN = 64  # cells
 
 
-def _needs_fallback(wp, mask, N, M, L, margin=FALLBACK_MARGIN):
-    """True when the path comes within about `margin` cells of a pruned
-    tile's cells: there it may have been cut off, and the full-tile method
-    decides.  The test works on margin x margin cell blocks: for every block
-    the path touches, the tiles covering a cell of it or of its 8
+def _pruned_near_path(wp, mask, N, M, L, margin=FALLBACK_MARGIN):
+    """(n1, n2) bool: the pruned tiles that come within about `margin` cells
+    of the path wp.  The test works on margin x margin cell blocks: for every
+    block the path touches, the tiles covering a cell of it or of its 8
     neighbouring blocks must all have run (so the distance tested is margin
     to 2 margin cells).  The path is monotone, so per row of blocks it
     touches one interval of blocks, and a summed-area table of the pruned
@@ -233,8 +232,9 @@ def _needs_fallback(wp, mask, N, M, L, margin=FALLBACK_MARGIN):
     if wp.shape[0] == 2 and wp.shape[1] != 2:
         wp = wp.T
     m = np.asarray(mask, bool)
+    near = np.zeros(m.shape, bool)
     if m.all() or wp.shape[0] == 0:
-        return False
+        return near
     n1, n2 = m.shape
     hop, B = L - 1, int(margin)
     r, c = wp[:, 0], wp[:, 1]
@@ -255,7 +255,15 @@ def _needs_fallback(wp, mask, N, M, L, margin=FALLBACK_MARGIN):
     sat = np.zeros((n1 + 1, n2 + 1), np.int64)
     sat[1:, 1:] = np.cumsum(np.cumsum(~m, axis=0), axis=1)
     cnt = sat[ihi + 1, jhi + 1] - sat[ilo, jhi + 1] - sat[ihi + 1, jlo] + sat[ilo, jlo]
-    return bool((cnt > 0).any())
+    for k in np.flatnonzero(cnt > 0):
+        near[ilo[k]:ihi[k] + 1, jlo[k]:jhi[k] + 1] = True
+    return near & ~m
+
+
+def _needs_fallback(wp, mask, N, M, L, margin=FALLBACK_MARGIN):
+    """True when the path comes within about `margin` cells of a pruned
+    tile's cells: there it may have been cut off (_pruned_near_path)."""
+    return bool(_pruned_near_path(wp, mask, N, M, L, margin).any())
 
 
 def parflex_pruned(F1, F2, steps, weights, beta, L, proposer=None, threshold=None,
@@ -315,12 +323,15 @@ def parflex_pruned(F1, F2, steps, weights, beta, L, proposer=None, threshold=Non
 class PrunedBatch:
     """Learned pruning over a batch of pairs: one proposer pass per pair,
     then the kept tiles of all pairs in one stage-1 launch per wave
-    (``pfx_batch_set_masks``), stage 2 per pair, and the full-tile method
-    for the pairs that need the fallback (``pfx_batch_complete``: only the
-    tiles the mask left out run stage 1)."""
+    (``pfx_batch_set_masks``), stage 2 per pair.  A pair whose path comes
+    near a pruned tile gets those tiles added and runs again (up to `expand`
+    times; ``pfx_batch_complete``: stage 1 only on the added tiles); a pair
+    still near one, or without an endpoint, falls back to the full-tile
+    method (every tile not run yet)."""
 
     def __init__(self, shapes, L, steps, weights, d, proposer=None, threshold=None,
-                 dilation=1, manhattan=None, precision="fp64", wave_bytes=0, warps=0):
+                 dilation=1, manhattan=None, precision="fp64", wave_bytes=0, warps=0,
+                 expand=2):
         from .batch import Batch
         self.batch = Batch(shapes, L, steps, weights, d, wave_bytes=wave_bytes, warps=warps,
                            precision=precision)
@@ -328,6 +339,7 @@ class PrunedBatch:
         self.threshold = threshold
         self.dilation = dilation
         self.manhattan = manhattan
+        self.expand = int(expand)
         self.L = int(L)
         self.steps, self.weights, self.precision = steps, weights, precision
         self.shapes = [(int(n), int(m)) for n, m in shapes]
@@ -363,38 +375,71 @@ class PrunedBatch:
         mark("set_masks")
         b.run(beta, use_graph=False)
         mark("align")
+        align_ms = b.timing() if profile else None
+        near_d, flags_d = b.check_paths(FALLBACK_MARGIN)
         best, end, lens = b.results()
-        paths = b.paths(lens)
-        m_host = masks.cpu().numpy()
+        flags = flags_d.cpu().numpy()
+        paths = b.paths_rows(lens)
         mark("results")
-        out, fallbacks, reasons = [], 0, {}
-        kept = int(m_host.sum())
+        out, fallbacks, reasons, expanded = [], 0, {}, 0
+        kept = int(masks.sum())
         run_tiles = kept
-        for i, (N, M) in enumerate(self.shapes):
+        n = len(self.shapes)
+        todo = [i for i in range(n) if flags[i] or not end[i, 6]]
+        if todo:
+            m_host = masks.cpu().numpy()
+            near = near_d.cpu().numpy()
+        out = [(float(best[i]), paths[i]) for i in range(n)]
+        for i in todo:
+            N, M = self.shapes[i]
             mk = m_host[self.offs[i]:self.offs[i + 1]].reshape(self.grids[i])
-            reason = None
-            if not end[i, 6]:
-                reason = "no endpoint among proposed tiles"
-            elif _needs_fallback(paths[i], mk, N, M, self.L):
-                reason = "path near a pruned tile"
-            if reason is None:
-                out.append((float(best[i]), np.ascontiguousarray(paths[i].T)))
-                continue
+            reason = "no endpoint among proposed tiles" if not end[i, 6] \
+                else "path near a pruned tile"
+            if reason == "path near a pruned tile" and self.expand > 0:
+                add = near[self.offs[i]:self.offs[i + 1]].reshape(self.grids[i]).astype(bool)
+                res, ran = self._expand(i, N, M, beta, add, mk)
+                if res is not None:
+                    expanded += 1
+                    run_tiles += ran
+                    out[i] = res
+                    continue
+            # the full-tile method: every tile not run yet
             fallbacks += 1
             reasons[reason] = reasons.get(reason, 0) + 1
             bc, wp = self._full(i, N, M, beta)
-            out.append((bc, np.ascontiguousarray(wp.T)))
-            n_t = self.grids[i][0] * self.grids[i][1]
-            run_tiles += n_t - int(mk.sum())
+            out[i] = (bc, np.ascontiguousarray(wp.T))
+            run_tiles += self.grids[i][0] * self.grids[i][1] - int(mk.sum())
         mark("checks")
         total = int(self.offs[-1])
         info = {"tiles_total": total, "tiles_run": run_tiles, "tiles_proposed": kept,
                 "skipped_fraction": 1 - kept / total, "fallbacks": fallbacks,
-                "fallback_reasons": reasons, "waves": b.waves}
+                "fallback_reasons": reasons, "expanded": expanded, "waves": b.waves}
         if profile:
             info["phases_ms"] = {marks[k][0]: 1e3 * (marks[k][1] - marks[k - 1][1])
                                  for k in range(1, len(marks))}
+            info["align_ms"] = dict(zip(("cost", "stage1", "stage2"), align_ms))
         return out, info
+
+    def _expand(self, i, N, M, beta, add, mk):
+        """Adds `add` (the pruned tiles the path came near) to pair i's run
+        and aligns it again (stage 1 only on the added tiles), up to
+        `expand` times while the new path stays near pruned tiles.  Returns
+        ((best_cost, wp[2, K]) or None when still near, tiles added)."""
+        m = np.asarray(mk, bool).copy()
+        ran = 0
+        for _ in range(self.expand):
+            try:
+                bc, wp = self.batch.complete(i, beta, add)
+            except ValueError as e:
+                if str(e) == _lib.NO_ENDPOINT_MSG:
+                    return None, ran
+                raise
+            ran += int(add.sum())
+            m |= add
+            add = _pruned_near_path(wp, m, N, M, self.L)
+            if not add.any():
+                return (bc, np.ascontiguousarray(wp.T)), ran
+        return None, ran
 
     def _full(self, i, N, M, beta):
         """The full-tile method for pair i: completed inside the batch when

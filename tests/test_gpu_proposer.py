@@ -19,7 +19,7 @@ if not torch.cuda.is_available():  # pragma: no cover - CPU container
 import parflexdtw_b200 as pf  # noqa: E402
 from parflexdtw_b200 import _lib, workloads as W  # noqa: E402
 from parflexdtw_b200.prune import (FPP, STRIDES, TileProposer, _needs_fallback,  # noqa: E402
-                                   _p, tiles_on_path)
+                                   _p, _pruned_near_path, tiles_on_path)
 from oracle import cnn_oracle as CO  # noqa: E402
 
 STD = [(1, 1), (1, 2), (2, 1)]
@@ -223,9 +223,10 @@ def test_batch_masks_and_pruned_batch_exact(oracle_mod):
     paths = b.paths(lens)
     for i, r in enumerate(refs):
         assert best[i] == r["best_cost"] and np.array_equal(paths[i].T, r["wp"])
-    dil = []
+    dil, labs = [], []
     for (n, m), r in zip(shapes, refs):
         lab = tiles_on_path(r["wp"], n, m, L).astype(bool)
+        labs.append(lab.reshape(-1))
         p = np.pad(lab, 1)
         d = np.zeros_like(lab)
         for di in range(3):
@@ -245,6 +246,35 @@ def test_batch_masks_and_pruned_batch_exact(oracle_mod):
     # batch's masked state (queues, graph) intact
     rng = np.random.default_rng(3)
     sparse = torch.from_numpy((rng.random(masks.numel()) < 0.4).astype(np.uint8)).cuda()
+    # the device path check and row-layout paths against the host statement
+    # (masks of the path tiles alone: the paths pass near pruned tiles)
+    on_path = torch.from_numpy(np.concatenate(labs).astype(np.uint8)).cuda()
+    b.set_masks(on_path)
+    b.run(0.1, use_graph=False)
+    near, flags = b.check_paths(32)
+    _, end_s, lens_s = b.results()
+    rows = b.paths_rows(lens_s)
+    pts = b.paths(lens_s)
+    near, flags, sp = near.cpu().numpy(), flags.cpu().numpy(), on_path.cpu().numpy()
+    offs = np.concatenate([[0], np.cumsum([a * c for a, c in grids])])
+    n_near = 0
+    for i, (n, m) in enumerate(shapes):
+        assert np.array_equal(rows[i], pts[i].T)
+        mk = sp[offs[i]:offs[i + 1]].reshape(grids[i]).astype(bool)
+        want = _pruned_near_path(rows[i], mk, n, m, L, 32)
+        got = near[offs[i]:offs[i + 1]].reshape(grids[i]).astype(bool)
+        assert np.array_equal(got, want)
+        assert bool(flags[i]) == bool(want.any())
+        n_near += int(want.sum())
+    assert n_near > 0
+    # adding tiles in steps: the path tiles' neighbourhood, then the rest
+    b.set_masks(sparse)
+    b.run(0.1, use_graph=True)
+    for i, r in enumerate(refs):
+        bc, wp = b.complete(i, 0.1, dil[i].reshape(grids[i]))
+        assert bc == r["best_cost"] and np.array_equal(wp.T, r["wp"])
+        bc, wp = b.complete(i, 0.1)
+        assert bc == r["best_cost"] and np.array_equal(wp.T, r["wp"])
     for m in (sparse, masks):
         b.set_masks(m)
         b.run(0.1, use_graph=True)
