@@ -275,8 +275,14 @@ class PruneSpec(BatchSpec):
 PRUNE64 = PruneSpec("chroma12_pairs64_N40000-60000_L2000_pruned", 64, 40000, 60000,
                     L_choices=(2000,), pad_frac=0.10)
 
+# Profiling case of the same method: 4 pairs, N ~ U(8000, 10000) (about 3 GB
+# of cost slabs on the device), L = 2000.
+PRUNE_NCU = PruneSpec("chroma12_pairs4_N8000-10000_L2000_pruned", 4, 8000, 10000,
+                      L_choices=(2000,), pad_frac=0.10)
+
 WORKLOADS = {"config0": CONFIG0, "config1": CONFIG1, "ncu_small": NCU_SMALL,
-             "batch256": BATCH256, "precision2048": PRECISION2048, "prune64": PRUNE64}
+             "batch256": BATCH256, "precision2048": PRECISION2048, "prune64": PRUNE64,
+             "prune_ncu": PRUNE_NCU}
 
 
 def make_pair(spec: PairSpec):
