@@ -20,7 +20,7 @@ using namespace pfx;
 
 namespace {
 
-constexpr int kSide = 8;  // streams stage 2 of a wave is spread over
+constexpr int kSide = 32;  // streams stage 2 of a wave is spread over
 
 struct PairOut {
     const double* best;

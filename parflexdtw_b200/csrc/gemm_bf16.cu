@@ -32,8 +32,11 @@ namespace pfx {
 constexpr int kGRows = 128;              // C rows per CTA (two strips)
 constexpr int kGSteps = 128;             // skewed steps per CTA
 constexpr int kGCols = kGSteps + 64;     // C columns per CTA (MMA N)
-constexpr int kGThreads = 128;
-constexpr int kGTmemCols = 256;          // power of two >= kGCols
+constexpr int kGEpiWarps = 12;           // epilogue warps: 3 per TMEM lane quarter,
+                                         // 2 of the 6 column chunks each
+constexpr int kGThreads = 32 * (2 + kGEpiWarps);  // + producer warp, MMA warp
+constexpr int kGAccCols = 256;           // TMEM columns per accumulator (>= kGCols)
+constexpr int kGTmemCols = 2 * kGAccCols;  // two accumulators
 constexpr int kGAtomBytes = 128;         // SWIZZLE_128B: 64 bf16 of K per row
 constexpr int kGWaitLimit = 1 << 22;
 constexpr int32_t kStatusGemmWait = 2;
@@ -101,39 +104,75 @@ __host__ __device__ constexpr uint32_t mma_idesc_bf16(int M, int N) {
            | ((uint32_t)(M >> 4) << 24);  // M / 16
 }
 
-template <int KB>  // feature dimension padded to 64 * KB
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bounded wait that also gives up when another role of the CTA aborted.
+__device__ __forceinline__ bool mbar_wait_ab(uint64_t* bar, uint32_t parity,
+                                             const volatile int* abort) {
+    const uint32_t a = smem_u32(bar);
+    for (int it = 0; it < kGWaitLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (*abort) return false;
+        if (it > 32) __nanosleep(64);
+    }
+    return false;
+}
+
+// (tile, strip pair kk, step block cb) of block q; false for blocks past a
+// small tile's strips or steps (every role skips them alike).
+struct GBlock {
+    int slab, kk, cb, nS, span, R, W;
+    int64_t r0, c0;
+};
+
+__device__ __forceinline__ bool gemm_block(const Geo& g, const int32_t* slot, const int32_t* list,
+                                           int nkk, int ncb, int64_t q, GBlock& b) {
+    b.cb = (int)(q % ncb);
+    q /= ncb;
+    b.kk = (int)(q % nkk);
+    const int tile = list ? list[q / nkk] : (int)(q / nkk);
+    b.slab = slot ? slot[tile] : tile;
+    if (b.slab < 0) return false;
+    tile_rect(g, tile / g.n2, tile % g.n2, &b.r0, &b.c0, &b.R, &b.W);
+    b.span = ceil_div32(b.W + kStripRows - 1, kBlk) * kBlk;
+    b.nS = ceil_div32(b.R, kStripRows);
+    return 2 * b.kk < b.nS && b.cb * kGSteps < b.span;
+}
+
+// Persistent, warp-specialised: warp 0 loads operands (TMA, NST stages),
+// warp 1 issues the MMAs into one of two TMEM accumulators, warps 2-5 read
+// the other accumulator, skew it through shared memory and store it with
+// bulk copies -- so block i's epilogue overlaps block i+1's loads and MMAs.
+template <int KB, int NST, int NSK>  // features padded to 64 * KB; operand stages;
+                                     // skew staging buffers
 __global__ void __launch_bounds__(kGThreads, 1)
     k_gemm_cost_skew(const __grid_constant__ CUtensorMap mapA,
                      const __grid_constant__ CUtensorMap mapB, const Geo g,
                      float* __restrict__ Csk, const int64_t stride,
                      int32_t* __restrict__ status, const int32_t* __restrict__ slot,
-                     const int32_t* __restrict__ list) {
+                     const int32_t* __restrict__ list, const int64_t nblk) {
     extern __shared__ __align__(1024) unsigned char gsm_raw[];
-    // operands (1024-byte aligned atoms), later reused as the skew stage
     unsigned char* base = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(gsm_raw) + 1023) & ~(uintptr_t)1023);
-    unsigned char* sA = base;                                  // [KB][128 rows][128 B]
-    unsigned char* sB = base + KB * kGRows * kGAtomBytes;     // [KB][192 rows][128 B]
-    float* Ssk = reinterpret_cast<float*>(base);               // [2][128 steps][64 rows]
-    __shared__ __align__(8) uint64_t bar_tma, bar_mma;
+    constexpr uint32_t kABytes = KB * kGRows * kGAtomBytes;  // [KB][128 rows][128 B]
+    constexpr uint32_t kBBytes = KB * kGCols * kGAtomBytes;  // [KB][192 rows][128 B]
+    constexpr uint32_t kStage = kABytes + kBBytes;
+    // NSK buffers of [2 strips][128 steps][64 rows]
+    float* Ssk0 = reinterpret_cast<float*>(base + NST * kStage);
+    __shared__ __align__(8) uint64_t full[NST], empty[NST], tfull[2], tempty[2];
     __shared__ uint32_t tmem_base_slot;
-
-    // CTA -> (tile, strip pair, step block)
-    const Sched2 sL = make_sched2(g.L, g.L, 1);
-    const int nkk = (sL.nS + 1) / 2, ncb = ceil_div32(sL.span, kGSteps);
-    int q = (int)blockIdx.x;
-    const int cb = q % ncb;
-    q /= ncb;
-    const int kk = q % nkk;
-    const int tile = list ? list[q / nkk] : q / nkk;
-    const int slab = slot ? slot[tile] : tile;  // slab index; < 0: tile skipped
-    if (slab < 0) return;  // uniform over the CTA
-    int64_t r0, c0;
-    int32_t R, W;
-    tile_rect(g, tile / g.n2, tile % g.n2, &r0, &c0, &R, &W);
-    const int span = ceil_div32(W + kStripRows - 1, kBlk) * kBlk;
-    const int nS = ceil_div32(R, kStripRows);
-    if (2 * kk >= nS || cb * kGSteps >= span) return;  // uniform over the CTA
+    __shared__ volatile int s_abort;
+    __shared__ int s_issued, s_consumed, s_mma, s_epi, s_go;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp == 0) {
@@ -142,102 +181,215 @@ __global__ void __launch_bounds__(kGThreads, 1)
                      "r"(kGTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    if (threadIdx.x == 0) {
-        mbar_init(&bar_tma, 1);
-        mbar_init(&bar_mma, 1);
+    if (threadIdx.x == 32) {
+        for (int i = 0; i < NST; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        for (int j = 0; j < 2; ++j) {
+            mbar_init(&tfull[j], 1);
+            mbar_init(&tempty[j], kGEpiWarps);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+        s_issued = s_consumed = s_mma = s_epi = 0;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base_slot;
+    const Sched2 sL = make_sched2(g.L, g.L, 1);
+    const int nkk = (sL.nS + 1) / 2, ncb = ceil_div32(sL.span, kGSteps);
+    auto fail = [&]() {
+        atomicExch(status, kStatusGemmWait);
+        s_abort = 1;
+    };
 
-    __shared__ int s_fail;
-    if (threadIdx.x == 0) {
-        s_fail = 0;
-        const uint32_t bytes = KB * (kGRows + kGCols) * kGAtomBytes;
-        mbar_expect_tx(&bar_tma, bytes);
-        const int ya = (int)(r0 + (int64_t)kGRows * kk);
-        const int yb = (int)(c0 + (int64_t)kGSteps * cb - 64);
+    if (warp == 0) {  // producer: the whole warp walks the blocks, lane 0 issues
+        int i = 0;
+        for (int64_t q = blockIdx.x; q < nblk; q += gridDim.x) {
+            GBlock b;
+            if (!gemm_block(g, slot, list, nkk, ncb, q, b)) continue;
+            const int st = i % NST;
+            int ok = 1;
+            if (lane == 0) ok = mbar_wait_ab(&empty[st], ((i / NST) & 1) ^ 1, &s_abort);
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) {
+                if (lane == 0) fail();
+                break;
+            }
+            if (lane == 0) {
+                unsigned char* sA = base + st * kStage;
+                unsigned char* sB = sA + kABytes;
+                mbar_expect_tx(&full[st], kStage);
+                const int ya = (int)(b.r0 + (int64_t)kGRows * b.kk);
+                const int yb = (int)(b.c0 + (int64_t)kGSteps * b.cb - 64);
 #pragma unroll
-        for (int kb = 0; kb < KB; ++kb) {
-            tma_load_2d(sA + kb * kGRows * kGAtomBytes, &mapA, 64 * kb, ya, &bar_tma);
-            tma_load_2d(sB + kb * kGCols * kGAtomBytes, &mapB, 64 * kb, yb, &bar_tma);
+                for (int kb = 0; kb < KB; ++kb) {
+                    tma_load_2d(sA + kb * kGRows * kGAtomBytes, &mapA, 64 * kb, ya, &full[st]);
+                    tma_load_2d(sB + kb * kGCols * kGAtomBytes, &mapB, 64 * kb, yb, &full[st]);
+                }
+                s_issued = i + 1;
+            }
+            __syncwarp();
+            ++i;
         }
-        bool ok = mbar_wait(&bar_tma, 0);
-        if (!ok) {
-            atomicExch(status, kStatusGemmWait);
-            mbar_wait(&bar_tma, 0);  // the copies target this CTA's memory: let them land
-            s_fail = 1;
-        } else {
+    } else if (warp == 1) {  // MMA issuer: the whole warp walks the blocks, lane 0 issues
+        constexpr uint32_t idesc = mma_idesc_bf16(kGRows, kGCols);
+        int i = 0;
+        for (int64_t q = blockIdx.x; q < nblk; q += gridDim.x) {
+            GBlock b;
+            if (!gemm_block(g, slot, list, nkk, ncb, q, b)) continue;
+            const int st = i % NST, j = i & 1;
+            int ok = 1;
+            if (lane == 0) {
+                ok = mbar_wait_ab(&full[st], (i / NST) & 1, &s_abort);
+                if (ok) {
+                    s_consumed = i + 1;
+                    ok = mbar_wait_ab(&tempty[j], ((i >> 1) & 1) ^ 1, &s_abort);
+                }
+            }
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) {
+                if (lane == 0) fail();
+                break;
+            }
+            if (lane == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t sA = smem_u32(base + st * kStage), sB = sA + kABytes;
+                const uint32_t d = tmem + (uint32_t)(kGAccCols * j);
+#pragma unroll
+                for (int kb = 0; kb < KB; ++kb) {
+#pragma unroll
+                    for (int k16 = 0; k16 < 4; ++k16) {
+                        const uint64_t da = sw128_desc(sA + kb * kGRows * kGAtomBytes + 32 * k16);
+                        const uint64_t db = sw128_desc(sB + kb * kGCols * kGAtomBytes + 32 * k16);
+                        const uint32_t acc = (kb | k16) ? 1u : 0u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+                            "l"(da), "l"(db), "r"(idesc), "r"(acc)
+                            : "memory");
+                    }
+                }
+                asm volatile(
+                    "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 "
+                    "[%0];" ::"r"(smem_u32(&empty[st]))
+                    : "memory");
+                asm volatile(
+                    "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 "
+                    "[%0];" ::"r"(smem_u32(&tfull[j]))
+                    : "memory");
+                s_mma = i + 1;
+            }
+            __syncwarp();
+            ++i;
+        }
+    } else {  // epilogue: TMEM lanes 32 (warp % 4) + [0, 32), column chunks 2e, 2e + 1
+        const int ew = warp - 2;
+        const bool leader = ew == 0 && lane == 0;
+        const int quarter = warp & 3, e = ew >> 2;
+        const int row = 32 * quarter + lane;
+        const int sr = row >> 6, rho = row & 63;
+        int i = 0;
+        for (int64_t q = blockIdx.x; q < nblk; q += gridDim.x) {
+            GBlock b;
+            if (!gemm_block(g, slot, list, nkk, ncb, q, b)) continue;
+            const int j = i & 1;
+            float* Ssk = Ssk0 + (i % NSK) * (2 * kGSteps * 64);
+            // one thread waits (for the accumulator, and for the bulk store
+            // that last read this staging buffer); the decision reaches every
+            // epilogue warp through the named barrier, which none may leave
+            if (leader) {
+                const bool ok = mbar_wait_ab(&tfull[j], (i >> 1) & 1, &s_abort);
+                if (!ok) fail();
+                else s_epi = i + 1;
+                asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(NSK - 1) : "memory");
+                s_go = ok ? 1 : 0;
+            }
+            __syncwarp();
+            asm volatile("bar.sync 1, %0;" ::"r"(32 * kGEpiWarps) : "memory");
+            if (!s_go) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            constexpr uint32_t idesc = mma_idesc_bf16(kGRows, kGCols);
+            const bool row_in = kGRows * b.kk + row < b.R;  // tile-local row inside
 #pragma unroll
-            for (int kb = 0; kb < KB; ++kb) {
+            for (int cc = 0; cc < 2; ++cc) {
+                const int j0 = 32 * (2 * e + cc);         // first window column
+                uint32_t v[32];
+                const uint32_t taddr = tmem + ((uint32_t)(32 * quarter) << 16) +
+                                       (uint32_t)(kGAccCols * j + j0);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                    "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+                    "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, "
+                    "%31}, [%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                      "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                      "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
+                      "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                      "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]),
+                      "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                // cell (row, window column j0 + jj) is step t0 + jj of its strip
+                const int t0 = j0 - 64 + rho;
+                const int c0 = kGSteps * b.cb - 64 + j0;  // its tile-local column at jj = 0
+                float* dst = Ssk + (sr * kGSteps + t0) * 64 + rho;
+                if (row_in && c0 >= 0 && c0 + 31 < b.W) {
 #pragma unroll
-                for (int k16 = 0; k16 < 4; ++k16) {
-                    const uint64_t da = sw128_desc(smem_u32(sA + kb * kGRows * kGAtomBytes) + 32 * k16);
-                    const uint64_t db = sw128_desc(smem_u32(sB + kb * kGCols * kGAtomBytes) + 32 * k16);
-                    const uint32_t acc = (kb | k16) ? 1u : 0u;
+                    for (int jj = 0; jj < 32; ++jj)
+                        if ((unsigned)(t0 + jj) < (unsigned)kGSteps)
+                            dst[jj * 64] = __fsub_rn(1.0f, __uint_as_float(v[jj]));
+                } else {
+#pragma unroll
+                    for (int jj = 0; jj < 32; ++jj)
+                        if ((unsigned)(t0 + jj) < (unsigned)kGSteps)
+                            dst[jj * 64] = (row_in && c0 + jj >= 0 && c0 + jj < b.W)
+                                               ? __fsub_rn(1.0f, __uint_as_float(v[jj]))
+                                               : 0.0f;
+                }
+            }
+            // the accumulator is free for block i + 2
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[j]);
+            // skewed rows out: (strip, step) rows of 256 B are contiguous per strip
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            asm volatile("bar.sync 1, %0;" ::"r"(32 * kGEpiWarps) : "memory");
+            if (leader) {
+                float* out = Csk + (int64_t)b.slab * stride;
+                const int tau0 = kGSteps * b.cb;
+                const int nt = b.span - tau0 < kGSteps ? b.span - tau0 : kGSteps;
+                for (int s2 = 0; s2 < 2; ++s2) {
+                    const int k = 2 * b.kk + s2;
+                    if (k >= b.nS) break;
+                    float* gdst = out + ((int64_t)k * b.span + tau0) * 64;
                     asm volatile(
-                        "{\n\t.reg .pred p;\n\t"
-                        "setp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-                        "l"(da), "l"(db), "r"(idesc), "r"(acc)
+                        "cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst),
+                        "r"(smem_u32(Ssk + s2 * kGSteps * 64)), "r"(nt * 256)
                         : "memory");
                 }
+                asm volatile("cp.async.bulk.commit_group;" ::: "memory");
             }
-            asm volatile(
-                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                    smem_u32(&bar_mma))
-                : "memory");
-            if (!mbar_wait(&bar_mma, 0)) {
-                atomicExch(status, kStatusGemmWait);
-                mbar_wait(&bar_mma, 0);
-                s_fail = 1;
-            }
+            ++i;
         }
+        if (leader) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     }
+    __syncwarp();
     __syncthreads();
-    if (!s_fail) {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        // accumulator lanes 32 warp + lane = CTA-local row, columns = window columns
-        const int row = 32 * warp + lane;
-        const int s = row >> 6, rho = row & 63;
-        const int r = kGRows * kk + row;  // tile-local row
-        const int cbase = kGSteps * cb - 64;
-        const bool row_in = r < R;
-#pragma unroll 1
-        for (int j0 = 0; j0 < kGCols; j0 += 32) {
-            uint32_t v[32];
-            const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)j0;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-                "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
-                "[%32];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
-                  "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
-                  "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]),
-                  "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
-                  "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
-                  "=r"(v[30]), "=r"(v[31])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                const int cw = j0 + j;             // window column
-                const int tl = cw - 64 + rho;      // CTA-local step of cell (row, cw)
-                if (tl >= 0 && tl < kGSteps) {
-                    const int c = cbase + cw;      // tile-local column
-                    const float val = (row_in && c >= 0 && c < W)
-                                          ? __fsub_rn(1.0f, __uint_as_float(v[j]))
-                                          : 0.0f;
-                    Ssk[(s * kGSteps + tl) * 64 + rho] = val;
-                }
-            }
-        }
+    // let this CTA's copies and MMAs in flight land before it exits (bounded;
+    // on the normal path only the last MMA commits are still to be observed)
+    if (threadIdx.x == 0) {
+        for (int i = s_consumed; i < s_issued; ++i) mbar_wait(&full[i % NST], (i / NST) & 1);
     }
+    if (threadIdx.x == 32) {
+        for (int i = s_mma - NST > 0 ? s_mma - NST : 0; i < s_mma; ++i)
+            mbar_wait(&empty[i % NST], (i / NST) & 1);
+        for (int i = s_epi; i < s_mma; ++i) mbar_wait(&tfull[i & 1], (i >> 1) & 1);
+    }
+    __syncwarp();
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
@@ -245,45 +397,52 @@ __global__ void __launch_bounds__(kGThreads, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                      "r"(kGTmemCols));
     }
-    if (s_fail) return;
-    // skewed rows out: 32 lanes x float2 = 256 contiguous bytes per (strip, step)
-    float2* out = reinterpret_cast<float2*>(Csk + (int64_t)slab * stride);
-#pragma unroll 4
-    for (int i = threadIdx.x; i < 2 * kGSteps * 32; i += kGThreads) {
-        const int s = i / (kGSteps * 32);
-        const int tl = (i / 32) % kGSteps;
-        const int l = i & 31;
-        const int k = 2 * kk + s, tau = kGSteps * cb + tl;
-        if (k < nS && tau < span) {
-            const float2 v2 = *reinterpret_cast<const float2*>(&Ssk[(s * kGSteps + tl) * 64 + 2 * l]);
-            __stcs(out + ((int64_t)k * span + tau) * 32 + l, v2);
-        }
-    }
 }
 
 // bf16 copy of L2-normalised features: F (d x n, FP64, row-major by feature)
 // -> out[n][Kp] (row per frame, zero past d), normalised in FP64 with the
-// same summation as the FP64 form, then rounded to nearest bf16.
-__global__ void k_features_bf16(const double* __restrict__ F, int d, int64_t n, int Kp,
-                                __nv_bfloat16* __restrict__ out) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double ss = 0.0;
-    for (int f = 0; f < d; ++f) {
-        const double x = F[(int64_t)f * n + i];
-        ss = __dadd_rn(ss, __dmul_rn(x, x));
+// same summation as the FP64 form, then rounded to nearest bf16.  A block
+// takes 32 frames: one thread per frame sums its squares (fixed order), then
+// all threads produce the block's rows -- contiguous in `out` -- one word
+// (two bf16) per thread and step, coalesced.
+constexpr int kFbFrames = 32;
+constexpr int kFbThreads = 256;
+
+__global__ void __launch_bounds__(kFbThreads)
+    k_features_bf16(const double* __restrict__ F, int d, int64_t n, int Kp,
+                    __nv_bfloat16* __restrict__ out) {
+    __shared__ double nrm[kFbFrames];
+    const int64_t i0 = blockIdx.x * (int64_t)kFbFrames;
+    const int rows = n - i0 < kFbFrames ? (int)(n - i0) : kFbFrames;
+    const int t = threadIdx.x;
+    if (t < rows) {
+        double ss = 0.0;
+        for (int f = 0; f < d; ++f) {
+            const double x = F[(int64_t)f * n + i0 + t];
+            ss = __dadd_rn(ss, __dmul_rn(x, x));
+        }
+        nrm[t] = sqrt(ss);
     }
-    const double nr = sqrt(ss);
-    for (int f = 0; f < Kp; ++f) {
-        const double x = f < d ? (nr > 0.0 ? __ddiv_rn(F[(int64_t)f * n + i], nr) : 0.0) : 0.0;
-        out[i * Kp + f] = __double2bfloat16(x);
+    __syncthreads();
+    const int W2 = Kp / 2;
+    uint32_t* o = reinterpret_cast<uint32_t*>(out + i0 * Kp);
+    for (int w = t; w < rows * W2; w += kFbThreads) {
+        const int fr = w / W2, f = 2 * (w % W2);
+        const double nr = nrm[fr];
+        const int64_t i = i0 + fr;
+        const double x0 = f < d ? (nr > 0.0 ? __ddiv_rn(F[(int64_t)f * n + i], nr) : 0.0) : 0.0;
+        const double x1 =
+            f + 1 < d ? (nr > 0.0 ? __ddiv_rn(F[(int64_t)(f + 1) * n + i], nr) : 0.0) : 0.0;
+        const __nv_bfloat162 pr = __halves2bfloat162(__double2bfloat16(x0), __double2bfloat16(x1));
+        o[w] = *reinterpret_cast<const uint32_t*>(&pr);
     }
 }
 
 cudaError_t launch_features_bf16(const double* F, int d, int64_t n, int Kp, void* out,
                                  cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
-    k_features_bf16<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(
+    if (Kp % 2) return cudaErrorInvalidValue;
+    k_features_bf16<<<(unsigned)((n + kFbFrames - 1) / kFbFrames), kFbThreads, 0, st>>>(
         F, d, n, Kp, static_cast<__nv_bfloat16*>(out));
     count_launches(1);
     return cudaGetLastError();
@@ -316,12 +475,17 @@ static bool make_map(CUtensorMap* m, const void* base, int64_t rows, int Kp, int
            CUDA_SUCCESS;
 }
 
+// Operand stages and skew staging buffers within the 227 KB of shared memory:
+// KB 1: 2 + 2, KB 2: 1 + 2 (the second accumulator already overlaps the next
+// block's loads with this block's epilogue), KB 3-4: 1 + 1.
+constexpr int gemm_stages(int KB) { return KB == 1 ? 2 : 1; }
+constexpr int gemm_skew_bufs(int KB) { return KB <= 2 ? 2 : 1; }
+
 size_t gemm_cost_smem_bytes(int Kp) {
-    const size_t ops = (size_t)(Kp / 64) * (kGRows + kGCols) * kGAtomBytes;
-    const size_t stage = (size_t)2 * kGSteps * 64 * sizeof(float);
-    // at least ~100 KB: at most two CTAs (2 x 256 TMEM columns) per SM
-    size_t b = (ops > stage ? ops : stage) + 1024;
-    return b < 100 * 1024 ? 100 * 1024 : b;
+    const int KB = Kp / 64;
+    const size_t stage = (size_t)KB * (kGRows + kGCols) * kGAtomBytes;
+    const size_t skew = (size_t)2 * kGSteps * 64 * sizeof(float);
+    return gemm_stages(KB) * stage + gemm_skew_bufs(KB) * skew + 1024;  // + 1024 B alignment
 }
 
 template <int KB>
@@ -329,7 +493,7 @@ static cudaError_t gemm_t(const CUtensorMap& ma, const CUtensorMap& mb, const Ge
                           int64_t stride, int32_t* status, cudaStream_t st, const int32_t* slot,
                           const int32_t* list, int nlist) {
     const size_t smem = gemm_cost_smem_bytes(64 * KB);
-    auto kern = k_gemm_cost_skew<KB>;
+    auto kern = k_gemm_cost_skew<KB, gemm_stages(KB), gemm_skew_bufs(KB)>;
     cudaError_t e =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -337,9 +501,13 @@ static cudaError_t gemm_t(const CUtensorMap& ma, const CUtensorMap& mb, const Ge
     const int64_t nblk =
         (list ? (int64_t)nlist : (int64_t)g.n1 * g.n2) * ((s.nS + 1) / 2) *
         ceil_div32(s.span, kGSteps);
-    if (nblk > 0x7fffffffLL) return cudaErrorInvalidValue;
     if (nblk == 0) return cudaSuccess;
-    kern<<<(unsigned)nblk, kGThreads, smem, st>>>(ma, mb, g, Csk, stride, status, slot, list);
+    // persistent: one CTA per SM (its two accumulators hold all 512 TMEM columns)
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = (int)(nblk < sms ? nblk : (int64_t)sms);
+    kern<<<grid, kGThreads, smem, st>>>(ma, mb, g, Csk, stride, status, slot, list, nblk);
     count_launches(1);
     return cudaGetLastError();
 }

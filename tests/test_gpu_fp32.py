@@ -101,6 +101,7 @@ def _normalised(F):
 
 @pytest.mark.parametrize("d,shape,Lb", [(128, (1000, 1300), 1000), (128, (2500, 1900), 1000),
                                          (64, (700, 500), 300), (200, (600, 900), 256),
+                                         (150, (500, 700), 256),
                                          (12, (400, 450), 128)])
 def test_tensor_core_cost_vs_torch(d, shape, Lb):
     rng = np.random.default_rng(d + shape[0])
