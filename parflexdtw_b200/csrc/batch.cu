@@ -168,6 +168,9 @@ struct pfx_batch {
     // before stage 1, after stage 1, after the stage-2 join
     std::vector<cudaEvent_t> phase_ev;
     bool phase_valid = false;
+    FbSeg* fbsegs = nullptr;  // FP32 form: every feature matrix's bf16 conversion
+    int fb_nseg = 0;
+    int64_t fb_blocks = 0;
     char* stage = nullptr;  // pinned staging of pfx_batch_set_masks' uploads
     size_t stage_bytes = 0;
     // masked batches, per pair: the slot map and kept-tile list of the mask
@@ -199,6 +202,7 @@ static void batch_free(pfx_batch* b) {
     if (b->arena) cudaFree(b->arena);
     if (b->slabs) cudaFree(b->slabs);
     if (b->stage) cudaFreeHost(b->stage);
+    if (b->fbsegs) cudaFree(b->fbsegs);
     if (b->pref) cudaFree(b->pref);
     if (b->rows) cudaFree(b->rows);
     if (b->prow) cudaFree(b->prow);
@@ -413,6 +417,26 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
         e = cudaMemcpy(b->descs, all.data(), all.size() * sizeof(TileDesc), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = cudaMemcpy(b->pout, po.data(), n * sizeof(PairOut), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && fp32) {
+        // the bf16 conversion of every pair's two feature matrices: one launch
+        std::vector<FbSeg> segs;
+        int64_t blk = 0;
+        for (int i = 0; i < n; ++i) {
+            const pfx_plan& p = b->plans[i];
+            const double* F1 = b->fin + b->fin_off[i];
+            char* A = static_cast<char*>(p.fbf);
+            segs.push_back(FbSeg{F1, p.g.N, A, blk});
+            blk += features_bf16_blocks(p.g.N);
+            segs.push_back(FbSeg{F1 + (int64_t)d * p.g.N, p.g.M, A + (size_t)p.g.N * kp * 2, blk});
+            blk += features_bf16_blocks(p.g.M);
+        }
+        b->fb_blocks = blk;
+        b->fb_nseg = (int)segs.size();
+        e = cudaMalloc(&b->fbsegs, segs.size() * sizeof(FbSeg));
+        if (e == cudaSuccess)
+            e = cudaMemcpy(b->fbsegs, segs.data(), segs.size() * sizeof(FbSeg),
+                           cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess) e = cudaMemset(b->status, 0, 4);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
     for (int k = 0; k < kSide && e == cudaSuccess; ++k) {
@@ -486,6 +510,7 @@ extern "C" int pfx_batch_set_masks(pfx_batch* b, const uint8_t* masks, int32_t o
     BCK(cudaStreamSynchronize(s));  // the staging buffer may still feed earlier copies
     if (need > b->stage_bytes) {
         if (b->stage) cudaFreeHost(b->stage);
+    if (b->fbsegs) cudaFree(b->fbsegs);
     if (b->pref) cudaFree(b->pref);
     if (b->rows) cudaFree(b->rows);
     if (b->prow) cudaFree(b->prow);
@@ -598,10 +623,9 @@ extern "C" int pfx_batch_complete(pfx_batch* b, int32_t i, double beta, const ui
     const double* F1 = b->fin + b->fin_off[i];
     const double* F2 = F1 + (int64_t)b->d * p.g.N;
     if (b->fp32) {
-        char* A = static_cast<char*>(p.fbf);
-        char* B = A + (size_t)p.g.N * b->kp * 2;
-        BCK(launch_features_bf16(F1, b->d, p.g.N, b->kp, A, s));
-        BCK(launch_features_bf16(F2, b->d, p.g.M, b->kp, B, s));
+        // the bf16 features of the run
+        const char* A = static_cast<const char*>(p.fbf);
+        const char* B = A + (size_t)p.g.N * b->kp * 2;
         BCK(launch_gemm_cost_skew(A, B, b->kp, p.g, reinterpret_cast<float*>(b->slabs),
                                   p.skew_stride, b->status, s, p.tile_slot, p.tile_list,
                                   (int)list.size()));
@@ -694,6 +718,8 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
     for (int w = 0; w < waves; ++w) {
         const int q0 = b->wave_first[w], q1 = b->wave_first[w + 1];
         BCK(mark(w, 0));
+        if (w == 0 && b->fp32)  // every pair's bf16 features, one launch
+            BCK(launch_features_bf16_segs(b->fbsegs, b->fb_nseg, b->fb_blocks, b->d, b->kp, s));
         for (int q = q0; q < q1; ++q) {
             const int i = b->wave_pairs[q];
             pfx_plan& p = b->plans[i];
@@ -702,10 +728,8 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
             const int32_t* slot = b->masked ? p.tile_slot : nullptr;
             const int32_t* list = b->masked ? p.tile_list : nullptr;
             if (b->fp32) {
-                char* A = static_cast<char*>(p.fbf);
-                char* B = A + (size_t)p.g.N * b->kp * 2;
-                BCK(launch_features_bf16(F1, b->d, p.g.N, b->kp, A, s));
-                BCK(launch_features_bf16(F2, b->d, p.g.M, b->kp, B, s));
+                const char* A = static_cast<const char*>(p.fbf);
+                const char* B = A + (size_t)p.g.N * b->kp * 2;
                 BCK(launch_gemm_cost_skew(A, B, b->kp, p.g, static_cast<float*>(p.Csk),
                                           p.skew_stride, b->status, s, slot, list, p.n_kept));
             } else {

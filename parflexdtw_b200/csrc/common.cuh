@@ -199,6 +199,18 @@ cudaError_t launch_relayout_skew(const double* C, int64_t ldc, const Geo& g, dou
 // features, then 1 - A B^T on the tensor cores into FP32 skewed slabs.
 cudaError_t launch_features_bf16(const double* F, int d, int64_t n, int Kp, void* out,
                                  cudaStream_t st);
+// Several feature matrices in one launch: segment s converts F (d x n) into
+// out, its blocks numbered from blk0 (features_bf16_blocks(n) per segment,
+// segments in order of blk0).
+struct FbSeg {
+    const double* F;
+    int64_t n;
+    void* out;
+    int64_t blk0;
+};
+int64_t features_bf16_blocks(int64_t n);
+cudaError_t launch_features_bf16_segs(const FbSeg* segs, int nseg, int64_t blocks, int d, int Kp,
+                                      cudaStream_t st);
 cudaError_t launch_gemm_cost_skew(const void* Abf, const void* Bbf, int Kp, const Geo& g,
                                   float* Csk, int64_t stride, int32_t* status, cudaStream_t st,
                                   const int32_t* slot = nullptr, const int32_t* list = nullptr,

@@ -313,9 +313,14 @@ __global__ void __launch_bounds__(kGThreads, 1)
             if (!s_go) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const bool row_in = kGRows * b.kk + row < b.R;  // tile-local row inside
+            // rows of this warp: rho0 .. rho0 + 31
+            const int rho0 = (32 * quarter) & 63;
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc) {
                 const int j0 = 32 * (2 * e + cc);         // first window column
+                // steps of the chunk's cells: t0 + jj, t0 = j0 - 64 + rho
+                const int tlo = j0 - 64 + rho0, thi = tlo + 31 + 31;
+                if (thi < 0 || tlo >= kGSteps) continue;  // no cell of the chunk is kept
                 uint32_t v[32];
                 const uint32_t taddr = tmem + ((uint32_t)(32 * quarter) << 16) +
                                        (uint32_t)(kGAccCols * j + j0);
@@ -332,23 +337,15 @@ __global__ void __launch_bounds__(kGThreads, 1)
                       "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                     : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                // cell (row, window column j0 + jj) is step t0 + jj of its strip
                 const int t0 = j0 - 64 + rho;
-                const int c0 = kGSteps * b.cb - 64 + j0;  // its tile-local column at jj = 0
+                const int c0 = kGSteps * b.cb - 64 + j0;  // tile-local column at jj = 0
                 float* dst = Ssk + (sr * kGSteps + t0) * 64 + rho;
-                if (row_in && c0 >= 0 && c0 + 31 < b.W) {
 #pragma unroll
-                    for (int jj = 0; jj < 32; ++jj)
-                        if ((unsigned)(t0 + jj) < (unsigned)kGSteps)
-                            dst[jj * 64] = __fsub_rn(1.0f, __uint_as_float(v[jj]));
-                } else {
-#pragma unroll
-                    for (int jj = 0; jj < 32; ++jj)
-                        if ((unsigned)(t0 + jj) < (unsigned)kGSteps)
-                            dst[jj * 64] = (row_in && c0 + jj >= 0 && c0 + jj < b.W)
-                                               ? __fsub_rn(1.0f, __uint_as_float(v[jj]))
-                                               : 0.0f;
-                }
+                for (int jj = 0; jj < 32; ++jj)
+                    if ((unsigned)(t0 + jj) < (unsigned)kGSteps)
+                        dst[jj * 64] = (row_in && c0 + jj >= 0 && c0 + jj < b.W)
+                                           ? __fsub_rn(1.0f, __uint_as_float(v[jj]))
+                                           : 0.0f;
             }
             // the accumulator is free for block i + 2
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -408,11 +405,25 @@ __global__ void __launch_bounds__(kGThreads, 1)
 constexpr int kFbFrames = 32;
 constexpr int kFbThreads = 256;
 
+// Block b of a segment list: the segment holding it (segs ordered by blk0).
+__device__ __forceinline__ int fb_segment(const FbSeg* segs, int nseg, int64_t b) {
+    int lo = 0, hi = nseg - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (segs[mid].blk0 <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// segs == nullptr: the single segment `one`.
 __global__ void __launch_bounds__(kFbThreads)
-    k_features_bf16(const double* __restrict__ F, int d, int64_t n, int Kp,
-                    __nv_bfloat16* __restrict__ out) {
+    k_features_bf16(const FbSeg* __restrict__ segs, int nseg, FbSeg one, int d, int Kp) {
     __shared__ double nrm[kFbFrames];
-    const int64_t i0 = blockIdx.x * (int64_t)kFbFrames;
+    const FbSeg sg = segs ? segs[fb_segment(segs, nseg, blockIdx.x)] : one;
+    const double* __restrict__ F = sg.F;
+    const int64_t n = sg.n;
+    const int64_t i0 = (blockIdx.x - sg.blk0) * (int64_t)kFbFrames;
     const int rows = n - i0 < kFbFrames ? (int)(n - i0) : kFbFrames;
     const int t = threadIdx.x;
     if (t < rows) {
@@ -425,7 +436,7 @@ __global__ void __launch_bounds__(kFbThreads)
     }
     __syncthreads();
     const int W2 = Kp / 2;
-    uint32_t* o = reinterpret_cast<uint32_t*>(out + i0 * Kp);
+    uint32_t* o = reinterpret_cast<uint32_t*>(static_cast<__nv_bfloat16*>(sg.out) + i0 * Kp);
     for (int w = t; w < rows * W2; w += kFbThreads) {
         const int fr = w / W2, f = 2 * (w % W2);
         const double nr = nrm[fr];
@@ -438,12 +449,24 @@ __global__ void __launch_bounds__(kFbThreads)
     }
 }
 
+int64_t features_bf16_blocks(int64_t n) { return (n + kFbFrames - 1) / kFbFrames; }
+
 cudaError_t launch_features_bf16(const double* F, int d, int64_t n, int Kp, void* out,
                                  cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     if (Kp % 2) return cudaErrorInvalidValue;
-    k_features_bf16<<<(unsigned)((n + kFbFrames - 1) / kFbFrames), kFbThreads, 0, st>>>(
-        F, d, n, Kp, static_cast<__nv_bfloat16*>(out));
+    const FbSeg one{F, n, out, 0};
+    k_features_bf16<<<(unsigned)features_bf16_blocks(n), kFbThreads, 0, st>>>(nullptr, 1, one, d,
+                                                                               Kp);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_features_bf16_segs(const FbSeg* segs, int nseg, int64_t blocks, int d, int Kp,
+                                      cudaStream_t st) {
+    if (blocks <= 0) return cudaSuccess;
+    if (Kp % 2 || blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+    k_features_bf16<<<(unsigned)blocks, kFbThreads, 0, st>>>(segs, nseg, FbSeg{}, d, Kp);
     count_launches(1);
     return cudaGetLastError();
 }
