@@ -96,10 +96,99 @@ __device__ __forceinline__ bool prev_slot(const Geo& g, int pi, int pj, int64_t 
     return *pp >= 0 && *pp < elen;
 }
 
-// One tile anti-diagonal a = i + j of the stage-2 DP
-// (_nb_initialize_chunks_sparse / _nb_dp_fill_chunks_sparse,
-// Parflex.py:632-855).  Every slot reads only slots of tiles (i-1, j) and
-// (i, j-1), so a diagonal's tiles are independent.
+// Stage-2 DP (_nb_initialize_chunks_sparse / _nb_dp_fill_chunks_sparse,
+// Parflex.py:632-855), tile anti-diagonal by anti-diagonal: every slot reads
+// only slots of tiles (i-1, j) and (i, j-1), so a diagonal's tiles are
+// independent.
+
+// Unconditional inheritance of position 0 on the first tile row / column.
+__device__ __forceinline__ void prop_inherit(const Geo& g, S2Buf& b, int i, int j) {
+    double* D = b.D_arr;
+    double* Lr = b.L_arr;
+    if (i == 0 && j >= 1) {
+        int64_t pr0, pc0;
+        int32_t pR, pW;
+        tile_rect(g, 0, j - 1, &pr0, &pc0, &pR, &pW);
+        D[slot(g, 0, j, 0, 0)] = D[slot(g, 0, j - 1, 0, pW - 1)];
+        Lr[slot(g, 0, j, 0, 0)] = Lr[slot(g, 0, j - 1, 0, pW - 1)];
+    } else if (j == 0 && i >= 1) {
+        int64_t pr0, pc0;
+        int32_t pR, pW;
+        tile_rect(g, i - 1, 0, &pr0, &pc0, &pR, &pW);
+        D[slot(g, i, 0, 1, 0)] = D[slot(g, i - 1, 0, 1, pR - 1)];
+        Lr[slot(g, i, 0, 1, 0)] = Lr[slot(g, i - 1, 0, 1, pR - 1)];
+    }
+}
+
+// Slot q (edge q / L, position q % L) of tile (i, j).
+__device__ __forceinline__ void prop_slot(const Geo& g, S2Buf& b, int i, int j, int64_t r0,
+                                          int64_t c0, int32_t R, int32_t W, int q) {
+    double* D = b.D_arr;
+    double* Lr = b.L_arr;
+    const int e = q / g.L;
+    const int pos = q % g.L;
+    const int32_t elen = e == 0 ? W : R;
+    if (pos >= elen) return;
+    const int64_t k = slot(g, i, j, e, pos);
+    if (i == 0 && j == 0) {
+        if (!b.valid[k]) return;
+    } else if (i == 0 || j == 0) {
+        if (pos == 0 || !b.valid[k]) return;
+    } else {
+        if (!b.valid[k]) return;
+        if (pos == 0) {
+            int64_t src;
+            if (e == 0) {
+                int64_t pr0, pc0;
+                int32_t pR, pW;
+                tile_rect(g, i, j - 1, &pr0, &pc0, &pR, &pW);
+                src = slot(g, i, j - 1, 0, pW - 1);
+            } else {
+                int64_t pr0, pc0;
+                int32_t pR, pW;
+                tile_rect(g, i - 1, j, &pr0, &pc0, &pR, &pW);
+                src = slot(g, i - 1, j, 1, pR - 1);
+            }
+            const double v = D[src];
+            if (isfinite(v)) {
+                D[k] = v;
+                Lr[k] = Lr[src];
+            }
+            return;
+        }
+    }
+    int32_t sr, sc;
+    decode_start(b.edge_P[k], &sr, &sc);
+    const int32_t lr = e == 0 ? R - 1 : pos, lc = e == 0 ? pos : W - 1;
+    const double own_len = (double)(abs(lr - sr) + abs(lc - sc));
+    int pi, pj;
+    if (i == 0 && j == 0) {
+        if (sr == 0 || sc == 0) { D[k] = b.edge_D[k]; Lr[k] = own_len; }
+        return;
+    } else if (i == 0) {
+        if (sr == 0) { D[k] = b.edge_D[k]; Lr[k] = own_len; return; }
+        if (sc != 0) return;
+        pi = 0; pj = j - 1;
+    } else if (j == 0) {
+        if (sc == 0) { D[k] = b.edge_D[k]; Lr[k] = own_len; return; }
+        if (sr != 0) return;
+        pi = i - 1; pj = 0;
+    } else {
+        if (sr == 0) { pi = i - 1; pj = j; }
+        else if (sc == 0) { pi = i; pj = j - 1; }
+        else { D[k] = b.edge_D[k]; Lr[k] = own_len; return; }
+    }
+    int pe;
+    int64_t pp;
+    if (!prev_slot(g, pi, pj, r0 + sr, c0 + sc, &pe, &pp)) return;
+    const int64_t src = slot(g, pi, pj, pe, pp);
+    const double prev = D[src];
+    if (!isfinite(prev)) return;
+    D[k] = __dsub_rn(__dadd_rn(prev, b.edge_D[k]), b.edge_Cf[k]);
+    Lr[k] = __dadd_rn(__dadd_rn(Lr[src], (double)abs(lr - sr)), (double)abs(lc - sc));
+}
+
+// One anti-diagonal a per launch (large grids).
 __global__ void k_propagate(const Geo g, S2Buf b, int a) {
     const int ilo = a - (g.n2 - 1) > 0 ? a - (g.n2 - 1) : 0;
     const int i = ilo + (int)blockIdx.y;
@@ -108,86 +197,30 @@ __global__ void k_propagate(const Geo g, S2Buf b, int a) {
     int64_t r0, c0;
     int32_t R, W;
     tile_rect(g, i, j, &r0, &c0, &R, &W);
-    double* D = b.D_arr;
-    double* Lr = b.L_arr;
-    // unconditional inheritance of position 0 on the first tile row / column
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        if (i == 0 && j >= 1) {
-            int64_t pr0, pc0;
-            int32_t pR, pW;
-            tile_rect(g, 0, j - 1, &pr0, &pc0, &pR, &pW);
-            D[slot(g, 0, j, 0, 0)] = D[slot(g, 0, j - 1, 0, pW - 1)];
-            Lr[slot(g, 0, j, 0, 0)] = Lr[slot(g, 0, j - 1, 0, pW - 1)];
-        } else if (j == 0 && i >= 1) {
-            int64_t pr0, pc0;
-            int32_t pR, pW;
-            tile_rect(g, i - 1, 0, &pr0, &pc0, &pR, &pW);
-            D[slot(g, i, 0, 1, 0)] = D[slot(g, i - 1, 0, 1, pR - 1)];
-            Lr[slot(g, i, 0, 1, 0)] = Lr[slot(g, i - 1, 0, 1, pR - 1)];
+    if (blockIdx.x == 0 && threadIdx.x == 0) prop_inherit(g, b, i, j);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 2 * g.L; q += gridDim.x * blockDim.x)
+        prop_slot(g, b, i, j, r0, c0, R, W, q);
+}
+
+// Every anti-diagonal in one CTA (small grids: one launch instead of
+// n1 + n2 - 1); a CTA barrier orders the diagonals.
+constexpr int kPropAllThreads = 1024;
+
+__global__ void __launch_bounds__(kPropAllThreads) k_propagate_all(const Geo g, S2Buf b) {
+    const int per = 2 * g.L;
+    for (int a = 0; a <= g.n1 + g.n2 - 2; ++a) {
+        const int ilo = a - (g.n2 - 1) > 0 ? a - (g.n2 - 1) : 0;
+        const int ihi = a < g.n1 - 1 ? a : g.n1 - 1;
+        const int nt = ihi - ilo + 1;
+        if ((int)threadIdx.x < nt) prop_inherit(g, b, ilo + (int)threadIdx.x, a - ilo - (int)threadIdx.x);
+        for (int x = threadIdx.x; x < nt * per; x += kPropAllThreads) {
+            const int i = ilo + x / per, j = a - i;
+            int64_t r0, c0;
+            int32_t R, W;
+            tile_rect(g, i, j, &r0, &c0, &R, &W);
+            prop_slot(g, b, i, j, r0, c0, R, W, x % per);
         }
-    }
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 2 * g.L; q += gridDim.x * blockDim.x) {
-        const int e = q / g.L;
-        const int pos = q % g.L;
-        const int32_t elen = e == 0 ? W : R;
-        if (pos >= elen) continue;
-        const int64_t k = slot(g, i, j, e, pos);
-        if (i == 0 && j == 0) {
-            if (!b.valid[k]) continue;
-        } else if (i == 0 || j == 0) {
-            if (pos == 0 || !b.valid[k]) continue;
-        } else {
-            if (!b.valid[k]) continue;
-            if (pos == 0) {
-                int64_t src;
-                if (e == 0) {
-                    int64_t pr0, pc0;
-                    int32_t pR, pW;
-                    tile_rect(g, i, j - 1, &pr0, &pc0, &pR, &pW);
-                    src = slot(g, i, j - 1, 0, pW - 1);
-                } else {
-                    int64_t pr0, pc0;
-                    int32_t pR, pW;
-                    tile_rect(g, i - 1, j, &pr0, &pc0, &pR, &pW);
-                    src = slot(g, i - 1, j, 1, pR - 1);
-                }
-                const double v = D[src];
-                if (isfinite(v)) {
-                    D[k] = v;
-                    Lr[k] = Lr[src];
-                }
-                continue;
-            }
-        }
-        int32_t sr, sc;
-        decode_start(b.edge_P[k], &sr, &sc);
-        const int32_t lr = e == 0 ? R - 1 : pos, lc = e == 0 ? pos : W - 1;
-        const double own_len = (double)(abs(lr - sr) + abs(lc - sc));
-        int pi, pj;
-        if (i == 0 && j == 0) {
-            if (sr == 0 || sc == 0) { D[k] = b.edge_D[k]; Lr[k] = own_len; }
-            continue;
-        } else if (i == 0) {
-            if (sr == 0) { D[k] = b.edge_D[k]; Lr[k] = own_len; continue; }
-            if (sc != 0) continue;
-            pi = 0; pj = j - 1;
-        } else if (j == 0) {
-            if (sc == 0) { D[k] = b.edge_D[k]; Lr[k] = own_len; continue; }
-            if (sr != 0) continue;
-            pi = i - 1; pj = 0;
-        } else {
-            if (sr == 0) { pi = i - 1; pj = j; }
-            else if (sc == 0) { pi = i; pj = j - 1; }
-            else { D[k] = b.edge_D[k]; Lr[k] = own_len; continue; }
-        }
-        int pe;
-        int64_t pp;
-        if (!prev_slot(g, pi, pj, r0 + sr, c0 + sc, &pe, &pp)) continue;
-        const int64_t src = slot(g, pi, pj, pe, pp);
-        const double prev = D[src];
-        if (!isfinite(prev)) continue;
-        D[k] = __dsub_rn(__dadd_rn(prev, b.edge_D[k]), b.edge_Cf[k]);
-        Lr[k] = __dadd_rn(__dadd_rn(Lr[src], (double)abs(lr - sr)), (double)abs(lc - sc));
+        __syncthreads();
     }
 }
 
@@ -520,6 +553,11 @@ cudaError_t launch_stage2_edges(const double* C, const void* Csk, int64_t skew_s
 
 cudaError_t launch_stage2_prop(const Geo& g, const S2Buf& b, cudaStream_t st) {
     cudaError_t e;
+    if ((int64_t)g.n1 * g.n2 * 2 * g.L <= (1 << 18)) {
+        k_propagate_all<<<1, kPropAllThreads, 0, st>>>(g, b);
+        count_launches(1);
+        return cudaGetLastError();
+    }
     for (int a = 0; a <= g.n1 + g.n2 - 2; ++a) {
         const int ilo = a - (g.n2 - 1) > 0 ? a - (g.n2 - 1) : 0;
         const int ihi = a < g.n1 - 1 ? a : g.n1 - 1;
