@@ -287,7 +287,8 @@ int pfx_batch_plan(pfx_batch *batch, int32_t i, pfx_plan **plan);
  * slabs are built and stage 1 runs only there (the pool now holds only
  * those slabs, so waves are repacked), other tiles keep +inf edges.  For the
  * learned tile proposer; synchronises `stream`; invalidates the recorded
- * graph.  No reference counterpart. */
+ * graph.  FP64 batches only (PFX_ERR_ARG for a batch of the FP32 form).  No
+ * reference counterpart. */
 int pfx_batch_set_masks(pfx_batch *batch, const uint8_t *masks, int32_t on_device,
                         void *stream);
 /* After a masked run: adds tiles to pair i's run and aligns it again.

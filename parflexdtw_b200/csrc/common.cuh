@@ -196,7 +196,9 @@ cudaError_t launch_relayout_skew(const double* C, int64_t ldc, const Geo& g, dou
                                  int64_t skew_stride, cudaStream_t st,
                                  const int32_t* slot = nullptr);
 // FP32 form cost from features (gemm_bf16.cu): bf16 rows of L2-normalised
-// features, then 1 - A B^T on the tensor cores into FP32 skewed slabs.
+// features, then 1 - A B^T on the tensor cores into FP32 skewed slabs.  cap:
+// FP32 elements available from Csk (< 0: n1 * n2 slabs); stores beyond it are
+// skipped and flagged in *status.
 cudaError_t launch_features_bf16(const double* F, int d, int64_t n, int Kp, void* out,
                                  cudaStream_t st);
 // Several feature matrices in one launch: segment s converts F (d x n) into
@@ -214,7 +216,7 @@ cudaError_t launch_features_bf16_segs(const FbSeg* segs, int nseg, int64_t block
 cudaError_t launch_gemm_cost_skew(const void* Abf, const void* Bbf, int Kp, const Geo& g,
                                   float* Csk, int64_t stride, int32_t* status, cudaStream_t st,
                                   const int32_t* slot = nullptr, const int32_t* list = nullptr,
-                                  int nlist = 0);
+                                  int nlist = 0, int64_t cap = -1);
 // FP32 slabs from a row-major FP64 (rounded) or FP32 C (exactly one non-null).
 cudaError_t launch_relayout_skew_f32(const double* C64, const float* C32, int64_t ldc,
                                      const Geo& g, float* Csk, int64_t stride, cudaStream_t st,

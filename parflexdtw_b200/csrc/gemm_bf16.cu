@@ -40,6 +40,7 @@ constexpr int kGTmemCols = 2 * kGAccCols;  // two accumulators
 constexpr int kGAtomBytes = 128;         // SWIZZLE_128B: 64 bf16 of K per row
 constexpr int kGWaitLimit = 1 << 22;
 constexpr int32_t kStatusGemmWait = 2;
+constexpr int32_t kStatusGemmBounds = 3;  // a block's tile or slab range out of bounds (skipped)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -136,11 +137,16 @@ struct GBlock {
 };
 
 __device__ __forceinline__ bool gemm_block(const Geo& g, const int32_t* slot, const int32_t* list,
-                                           int nkk, int ncb, int64_t q, GBlock& b) {
+                                           int nkk, int ncb, int64_t q, GBlock& b,
+                                           int32_t* status) {
     b.cb = (int)(q % ncb);
     q /= ncb;
     b.kk = (int)(q % nkk);
     const int tile = list ? list[q / nkk] : (int)(q / nkk);
+    if (tile < 0 || tile >= g.n1 * g.n2) {
+        atomicExch(status, kStatusGemmBounds);
+        return false;
+    }
     b.slab = slot ? slot[tile] : tile;
     if (b.slab < 0) return false;
     tile_rect(g, tile / g.n2, tile % g.n2, &b.r0, &b.c0, &b.R, &b.W);
@@ -160,7 +166,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
                      const __grid_constant__ CUtensorMap mapB, const Geo g,
                      float* __restrict__ Csk, const int64_t stride,
                      int32_t* __restrict__ status, const int32_t* __restrict__ slot,
-                     const int32_t* __restrict__ list, const int64_t nblk) {
+                     const int32_t* __restrict__ list, const int64_t nblk, const int64_t cap) {
     extern __shared__ __align__(1024) unsigned char gsm_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(gsm_raw) + 1023) & ~(uintptr_t)1023);
@@ -209,7 +215,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
         int i = 0;
         for (int64_t q = blockIdx.x; q < nblk; q += gridDim.x) {
             GBlock b;
-            if (!gemm_block(g, slot, list, nkk, ncb, q, b)) continue;
+            if (!gemm_block(g, slot, list, nkk, ncb, q, b, status)) continue;
             const int st = i % NST;
             int ok = 1;
             if (lane == 0) ok = mbar_wait_ab(&empty[st], ((i / NST) & 1) ^ 1, &s_abort);
@@ -239,7 +245,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
         int i = 0;
         for (int64_t q = blockIdx.x; q < nblk; q += gridDim.x) {
             GBlock b;
-            if (!gemm_block(g, slot, list, nkk, ncb, q, b)) continue;
+            if (!gemm_block(g, slot, list, nkk, ncb, q, b, status)) continue;
             const int st = i % NST, j = i & 1;
             int ok = 1;
             if (lane == 0) {
@@ -295,7 +301,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
         int i = 0;
         for (int64_t q = blockIdx.x; q < nblk; q += gridDim.x) {
             GBlock b;
-            if (!gemm_block(g, slot, list, nkk, ncb, q, b)) continue;
+            if (!gemm_block(g, slot, list, nkk, ncb, q, b, status)) continue;
             const int j = i & 1;
             float* Ssk = Ssk0 + (i % NSK) * (2 * kGSteps * 64);
             // one thread waits (for the accumulator, and for the bulk store
@@ -362,7 +368,14 @@ __global__ void __launch_bounds__(kGThreads, 1)
                 for (int s2 = 0; s2 < 2; ++s2) {
                     const int k = 2 * b.kk + s2;
                     if (k >= b.nS) break;
-                    float* gdst = out + ((int64_t)k * b.span + tau0) * 64;
+                    // the rows stay inside the slab, the slab inside the buffer
+                    const int64_t r_lo = ((int64_t)k * b.span + tau0) * 64;
+                    const int64_t r_hi = r_lo + (int64_t)nt * 64;
+                    if (nt <= 0 || r_hi > stride || (int64_t)b.slab * stride + r_hi > cap) {
+                        atomicExch(status, kStatusGemmBounds);
+                        continue;
+                    }
+                    float* gdst = out + r_lo;
                     asm volatile(
                         "cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst),
                         "r"(smem_u32(Ssk + s2 * kGSteps * 64)), "r"(nt * 256)
@@ -514,7 +527,7 @@ size_t gemm_cost_smem_bytes(int Kp) {
 template <int KB>
 static cudaError_t gemm_t(const CUtensorMap& ma, const CUtensorMap& mb, const Geo& g, float* Csk,
                           int64_t stride, int32_t* status, cudaStream_t st, const int32_t* slot,
-                          const int32_t* list, int nlist) {
+                          const int32_t* list, int nlist, int64_t cap) {
     const size_t smem = gemm_cost_smem_bytes(64 * KB);
     auto kern = k_gemm_cost_skew<KB, gemm_stages(KB), gemm_skew_bufs(KB)>;
     cudaError_t e =
@@ -530,23 +543,25 @@ static cudaError_t gemm_t(const CUtensorMap& ma, const CUtensorMap& mb, const Ge
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grid = (int)(nblk < sms ? nblk : (int64_t)sms);
-    kern<<<grid, kGThreads, smem, st>>>(ma, mb, g, Csk, stride, status, slot, list, nblk);
+    if (cap < 0) cap = (int64_t)g.n1 * g.n2 * stride;
+    kern<<<grid, kGThreads, smem, st>>>(ma, mb, g, Csk, stride, status, slot, list, nblk, cap);
     count_launches(1);
     return cudaGetLastError();
 }
 
 cudaError_t launch_gemm_cost_skew(const void* Abf, const void* Bbf, int Kp, const Geo& g,
                                   float* Csk, int64_t stride, int32_t* status, cudaStream_t st,
-                                  const int32_t* slot, const int32_t* list, int nlist) {
+                                  const int32_t* slot, const int32_t* list, int nlist,
+                                  int64_t cap) {
     if (Kp % 64 || Kp < 64 || Kp > 256) return cudaErrorInvalidValue;
     CUtensorMap ma, mb;
     if (!make_map(&ma, Abf, g.N, Kp, kGRows) || !make_map(&mb, Bbf, g.M, Kp, kGCols))
         return cudaErrorInvalidValue;
     switch (Kp / 64) {
-        case 1: return gemm_t<1>(ma, mb, g, Csk, stride, status, st, slot, list, nlist);
-        case 2: return gemm_t<2>(ma, mb, g, Csk, stride, status, st, slot, list, nlist);
-        case 3: return gemm_t<3>(ma, mb, g, Csk, stride, status, st, slot, list, nlist);
-        default: return gemm_t<4>(ma, mb, g, Csk, stride, status, st, slot, list, nlist);
+        case 1: return gemm_t<1>(ma, mb, g, Csk, stride, status, st, slot, list, nlist, cap);
+        case 2: return gemm_t<2>(ma, mb, g, Csk, stride, status, st, slot, list, nlist, cap);
+        case 3: return gemm_t<3>(ma, mb, g, Csk, stride, status, st, slot, list, nlist, cap);
+        default: return gemm_t<4>(ma, mb, g, Csk, stride, status, st, slot, list, nlist, cap);
     }
 }
 

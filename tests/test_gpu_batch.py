@@ -188,5 +188,12 @@ def test_batch_errors():
     with pytest.raises(ValueError):
         b.load([(np.zeros((12, 99)), np.zeros((12, 120)))])
     b.close()
+    # tile masks run the FP64 form only
+    b = Batch([(100, 120)], 50, STD, WTS, 12, precision="fp32")
+    with pytest.raises(ValueError):
+        b.set_masks(torch.ones(b.tiles, dtype=torch.uint8, device="cuda"))
+    b.close()
+    with pytest.raises(ValueError):
+        pf.PrunedBatch([(100, 120)], 50, STD, WTS, 12, precision="fp32")
     with pytest.raises(ValueError):
         pf.parflex_batch([np.zeros((10, 10))], STD, WTS, 0.1, L=8)
