@@ -86,21 +86,15 @@ constexpr int kCostThreads = 256;       // 8 warps x 32 steps
 constexpr int kCX = kCT + 66;           // window columns (x = c - ts + 64), even
 constexpr int kCH = kCX / 2;            // per parity
 
-// Two strips per CTA (blockIdx.y = strip pair): row rho of strips 2kk and
-// 2kk + 1 sits at the same column for a given step, so each column vector
-// read from shared memory serves four cells of a lane (A and B of both
-// strips); 4 steps per register pass.
-constexpr int kCV2 = 4;
-
 template <int DMAX>
-__global__ void __launch_bounds__(kCostThreads, 1)
+__global__ void __launch_bounds__(kCostThreads, 2)
     k_cost_skew(const double* __restrict__ An, const double* __restrict__ Bn, const int d,
                 const Geo g, double* __restrict__ Csk, const int64_t stride,
                 const int32_t* __restrict__ slot, const int32_t* __restrict__ list) {
     extern __shared__ __align__(16) double sB[];  // [d][2][kCH]
     const int nchunk = ceil_div32(make_sched2(g.L, g.L, 1).span, kCT);
     const int tile = list ? list[blockIdx.x / nchunk] : (int)(blockIdx.x / nchunk);
-    const int kk = blockIdx.y;
+    const int k = blockIdx.y;
     const int ts = (int)(blockIdx.x % nchunk) * kCT;
     const int slab = slot ? slot[tile] : tile;  // slab index; < 0: tile skipped
     if (slab < 0) return;
@@ -109,8 +103,7 @@ __global__ void __launch_bounds__(kCostThreads, 1)
     tile_rect(g, tile / g.n2, tile % g.n2, &r0, &c0, &R, &W);
     const int span = ceil_div32(W + kStripRows - 1, kBlk) * kBlk;
     const int nS = ceil_div32(R, kStripRows);
-    if (2 * kk >= nS || ts >= span) return;
-    const bool two = 2 * kk + 1 < nS;
+    if (k >= nS || ts >= span) return;
     for (int q = threadIdx.x; q < d * kCX; q += kCostThreads) {
         const int f = q / kCX, x = q - f * kCX;
         const int c = ts - 64 + x;
@@ -118,64 +111,50 @@ __global__ void __launch_bounds__(kCostThreads, 1)
             (c >= 0 && c < W) ? __ldg(Bn + (int64_t)f * g.M + c0 + c) : 0.0;
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int rA0 = 128 * kk + 2 * lane, rB0 = rA0 + 1, rA1 = rA0 + 64, rB1 = rA1 + 1;
-    double aA0[DMAX], aB0[DMAX], aA1[DMAX], aB1[DMAX];
+    const int rA = 64 * k + 2 * lane, rB = rA + 1;
+    double aA[DMAX], aB[DMAX];
 #pragma unroll
     for (int f = 0; f < DMAX; ++f) {
-        const double* Af = An + (int64_t)f * g.N + r0;
-        aA0[f] = (f < d && rA0 < R) ? __ldg(Af + rA0) : 0.0;
-        aB0[f] = (f < d && rB0 < R) ? __ldg(Af + rB0) : 0.0;
-        aA1[f] = (f < d && rA1 < R) ? __ldg(Af + rA1) : 0.0;
-        aB1[f] = (f < d && rB1 < R) ? __ldg(Af + rB1) : 0.0;
+        aA[f] = (f < d && rA < R) ? __ldg(An + (int64_t)f * g.N + r0 + rA) : 0.0;
+        aB[f] = (f < d && rB < R) ? __ldg(An + (int64_t)f * g.N + r0 + rB) : 0.0;
     }
     __syncthreads();
-    double2* out0 = reinterpret_cast<double2*>(Csk + (int64_t)slab * stride) +
-                    (int64_t)(2 * kk) * span * 32 + lane;
-    double2* out1 = out0 + (int64_t)span * 32;
+    double2* out = reinterpret_cast<double2*>(Csk + (int64_t)slab * stride) + (int64_t)k * span * 32 + lane;
 #pragma unroll 1
-    for (int blk = 0; blk < 32 / kCV2; ++blk) {
-        const int t0 = ts + 32 * warp + kCV2 * blk;  // warp-uniform
+    for (int blk = 0; blk < 32 / kCV; ++blk) {
+        const int t0 = ts + 32 * warp + kCV * blk;  // warp-uniform
         if (t0 >= span) break;
         // A's column at t0 + v is window x = t0 - ts + 64 - 2*lane + v (even at v = 0);
-        // b[j] holds x = xA0 - 1 + j, j = 0..kCV2 (B at v uses b[v], A uses b[v + 1])
+        // b[j] holds x = xA0 - 1 + j, j = 0..8 (B at v uses b[v], A uses b[v + 1])
         const int h0 = ((t0 - ts + 64) >> 1) - lane;  // half-index of xA0
-        double accA0[kCV2], accB0[kCV2], accA1[kCV2], accB1[kCV2];
+        double accA[kCV], accB[kCV];
 #pragma unroll
         for (int f = 0; f < DMAX; ++f) {
             if (f >= d) break;
             const double* se = sB + (f * 2) * kCH;  // even x
             const double* so = se + kCH;             // odd x
-            double b[kCV2 + 1];
+            double b[kCV + 1];
 #pragma unroll
-            for (int j = 0; j <= kCV2; ++j) {
+            for (int j = 0; j <= kCV; ++j) {
                 // x = 2*h0 - 1 + j: odd for even j (half-index h0 - 1 + j/2), even for odd j
                 b[j] = (j & 1) ? se[h0 + (j >> 1)] : so[h0 - 1 + (j >> 1)];
             }
 #pragma unroll
-            for (int v = 0; v < kCV2; ++v) {
-                const double pA0 = __dmul_rn(aA0[f], b[v + 1]);
-                const double pB0 = __dmul_rn(aB0[f], b[v]);
-                const double pA1 = __dmul_rn(aA1[f], b[v + 1]);
-                const double pB1 = __dmul_rn(aB1[f], b[v]);
-                accA0[v] = f == 0 ? pA0 : __dadd_rn(accA0[v], pA0);
-                accB0[v] = f == 0 ? pB0 : __dadd_rn(accB0[v], pB0);
-                accA1[v] = f == 0 ? pA1 : __dadd_rn(accA1[v], pA1);
-                accB1[v] = f == 0 ? pB1 : __dadd_rn(accB1[v], pB1);
+            for (int v = 0; v < kCV; ++v) {
+                const double pA = __dmul_rn(aA[f], b[v + 1]);
+                const double pB = __dmul_rn(aB[f], b[v]);
+                accA[v] = f == 0 ? pA : __dadd_rn(accA[v], pA);
+                accB[v] = f == 0 ? pB : __dadd_rn(accB[v], pB);
             }
         }
 #pragma unroll
-        for (int v = 0; v < kCV2; ++v) {
+        for (int v = 0; v < kCV; ++v) {
             const int tau = t0 + v;
             if (tau < span) {
                 const int cA = tau - 2 * lane, cB = cA - 1;
-                const bool inA = cA >= 0 && cA < W, inB = cB >= 0 && cB < W;
-                __stcs(out0 + (int64_t)tau * 32,
-                       make_double2((rA0 < R && inA) ? __dsub_rn(1.0, accA0[v]) : 0.0,
-                                    (rB0 < R && inB) ? __dsub_rn(1.0, accB0[v]) : 0.0));
-                if (two)
-                    __stcs(out1 + (int64_t)tau * 32,
-                           make_double2((rA1 < R && inA) ? __dsub_rn(1.0, accA1[v]) : 0.0,
-                                        (rB1 < R && inB) ? __dsub_rn(1.0, accB1[v]) : 0.0));
+                const double vA = (rA < R && cA >= 0 && cA < W) ? __dsub_rn(1.0, accA[v]) : 0.0;
+                const double vB = (rB < R && cB >= 0 && cB < W) ? __dsub_rn(1.0, accB[v]) : 0.0;
+                __stcs(out + (int64_t)tau * 32, make_double2(vA, vB));
             }
         }
     }
@@ -302,13 +281,12 @@ cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Ge
         return cudaGetLastError();
     }
     const size_t smem = (size_t)d * kCX * sizeof(double);
-    dim3 grid = region_grid(g, kCT, nt);
-    grid.y = (grid.y + 1) / 2;  // strip pairs
     if (d == 12) {
-        k_cost_skew<12><<<grid, kCostThreads, smem, st>>>(An, Bn, d, g, Csk, stride, slot, list);
+        k_cost_skew<12><<<region_grid(g, kCT, nt), kCostThreads, smem, st>>>(An, Bn, d, g, Csk,
+                                                                             stride, slot, list);
     } else {
-        k_cost_skew<kMaxFeat><<<grid, kCostThreads, smem, st>>>(An, Bn, d, g, Csk, stride, slot,
-                                                                 list);
+        k_cost_skew<kMaxFeat><<<region_grid(g, kCT, nt), kCostThreads, smem, st>>>(
+            An, Bn, d, g, Csk, stride, slot, list);
     }
     count_launches(1);
     return cudaGetLastError();
