@@ -147,6 +147,9 @@ extern "C" void pfx_plan_destroy(pfx_plan* p) {
     cudaGetDevice(&cur);
     cudaSetDevice(p->device);
     for (int i = 0; i < p->nblocks; ++i) cudaFree(p->blocks[i]);
+    if (p->aux) cudaStreamDestroy(p->aux);
+    if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+    if (p->ev_join) cudaEventDestroy(p->ev_join);
     cudaSetDevice(cur);
     free(p);
 }
@@ -209,6 +212,7 @@ int pfx::plan_init(pfx_plan* p, int64_t N, int64_t M, int32_t L, const int64_t* 
     PA(&p->s1.status, 1);
     PA(&p->descs, nt);
     PA(&p->head, 1);
+    PA(&p->head2, 1);
     PA(&p->tile_mask, nt);
     PA(&p->tile_slot, nt);
     PA(&p->tile_list, nt);
@@ -478,8 +482,39 @@ extern "C" int pfx_stage1(pfx_plan* p, const double* C, int64_t ldc, void* strea
         CK(launch_stage1_queue(p->descs_sub, p->g.n1 * p->g.n2, p->nsub, p->head, p->g,
                                p->s1.status, p->nw, p->fp32 != 0, s));
     } else {
-        CK(launch_stage1_queue(p->descs, p->g.n1 * p->g.n2, nullptr, p->head, p->g,
-                               p->s1.status, p->nw, p->fp32 != 0, s));
+        const int nt = p->g.n1 * p->g.n2;
+        const int sms = num_sms_cur();
+        const int maxc = (p->nw == 16 && p->arena_mode == 0 && nt < sms)
+                             ? stage1_cluster_max(p->g, p->fp32 != 0)
+                             : 0;
+        if (maxc > 0) {
+            // fewer tiles than SMs: the largest tiles (the queue is ordered
+            // largest first) take two SMs each, as many as leave one SM for
+            // every other tile and as many clusters as can run at once; the
+            // other tiles run at the same time on a second stream
+            int nbig = nt < sms - nt ? nt : sms - nt;
+            if (nbig > maxc) nbig = maxc;
+            if (!p->aux) {
+                CK(cudaStreamCreateWithFlags(&p->aux, cudaStreamNonBlocking));
+                CK(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
+                CK(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
+            }
+            CK(cudaMemsetAsync(p->head2, 0, sizeof(int), s));
+            CK(cudaEventRecord(p->ev_fork, s));
+            // the clusters first, so that they find pairs of free SMs
+            CK(launch_stage1_cluster(p->descs, nbig, p->head, p->g, p->s1.status,
+                                     p->fp32 != 0, s));
+            if (nt > nbig) {
+                CK(cudaStreamWaitEvent(p->aux, p->ev_fork, 0));
+                CK(launch_stage1_queue(p->descs + nbig, nt - nbig, nullptr, p->head2, p->g,
+                                       p->s1.status, 16, p->fp32 != 0, p->aux));
+                CK(cudaEventRecord(p->ev_join, p->aux));
+                CK(cudaStreamWaitEvent(s, p->ev_join, 0));
+            }
+        } else {
+            CK(launch_stage1_queue(p->descs, nt, nullptr, p->head, p->g, p->s1.status, p->nw,
+                                   p->fp32 != 0, s));
+        }
     }
     return PFX_OK;
 }

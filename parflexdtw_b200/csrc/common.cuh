@@ -186,6 +186,12 @@ cudaError_t launch_mask_slots(const uint8_t* mask, int n, int32_t* slot, cudaStr
 // Keeps the descriptors whose tile is set in `mask`, in order; *count = kept.
 cudaError_t launch_compact_descs(const TileDesc* in, int n, const uint8_t* mask, TileDesc* out,
                                  int* count, cudaStream_t st);
+// Stage 1 of descs[0, ntiles) on clusters of two 16-warp CTAs (32 warps per
+// tile), claimed through *head; for alignments with fewer tiles than SMs.
+cudaError_t launch_stage1_cluster(const TileDesc* descs, int ntiles, int* head, const Geo& g,
+                                  int32_t* status, bool fp32, cudaStream_t st);
+// Clusters of that kernel that can run at once on this device (0: none).
+int stage1_cluster_max(const Geo& g, bool fp32);
 // Smallest valid warps-per-tile choice heuristic for `ntiles` tiles of length L.
 int stage1_queue_warps(int ntiles, int32_t L, int num_sms);
 // Cost-building launchers take an optional slot map: tile t's slab is slab

@@ -29,6 +29,11 @@ struct pfx_plan {
     // stage-1 tile queue of this plan (descriptors in queue order) and its head
     pfx::TileDesc* descs;
     int* head;
+    // stage 1 of few tiles: the largest on 2-CTA clusters, the rest on single
+    // CTAs in a second stream (created on first use, plans outside a batch)
+    int* head2;
+    cudaStream_t aux;
+    cudaEvent_t ev_fork, ev_join;
     // tile mask (pfx_plan_set_tile_mask or a masked batch): the mask, each
     // tile's cost slab (-1: skipped), the masked queue and its device length
     uint8_t* tile_mask;

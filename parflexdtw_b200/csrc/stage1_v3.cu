@@ -40,6 +40,7 @@
 // for the bounds tests and the edge-row stores.  The cost queue runs two
 // steps ahead.
 #include <algorithm>
+#include <cooperative_groups.h>
 #include <cuda/atomic>
 
 #include "common.cuh"
@@ -225,12 +226,25 @@ struct Rings {
     int* BP;
 };
 
+// rg: the CTA's rings.  The producer warp's rings have the same layout and
+// start at rbase (rg.AD itself, or in a cluster the generic address of
+// another CTA's rings): a slot is read at rbase + its byte offset in rg, so
+// that the address derives from rbase alone.  bw (when non-null) receives
+// the block's backpointer word instead of the store to td.Bw.
+template <typename X, typename T>
+__device__ __forceinline__ X ring_at(const char* rbase, const Rings<T>& rg, const X* p) {
+    return *reinterpret_cast<const X*>(
+        rbase + (reinterpret_cast<const char*>(p) - reinterpret_cast<const char*>(rg.AD)));
+}
+
 template <bool EDGE, bool STD, typename T>
 __device__ __forceinline__ void run_block(const Geo& g, Wave<T>& st, const Rings<T>& rg,
+                                          const char* rbase,
                                           const typename Vec2<T>::type* __restrict__ Cs,
                                           int span, int tau0, int k, int R, int W, int lane,
                                           int prev_base, int mine_base, int rmask, int Tb,
-                                          int lag, const TileDesc& td, int nP) {
+                                          int lag, const TileDesc& td, int nP,
+                                          uint2* bw = nullptr) {
     using V2 = typename Vec2<T>::type;
     const unsigned F = 0xffffffffu;
     const T w_last = (T)(g.S == 1 ? g.w[0] : (g.S == 2 ? g.w[1] : g.w[2]));
@@ -253,8 +267,9 @@ __device__ __forceinline__ void run_block(const Geo& g, Wave<T>& st, const Rings
             {
                 // every lane reads the same slot (a broadcast); lane 0 keeps it
                 const int rs = prev_base + ((Tb + t - lag - 1) & rmask);
-                const T rBD = rg.BD[rs], rAD = rg.AD[rs];
-                const int rBP = rg.BP[rs], rAP = rg.AP[rs];
+                const T rBD = ring_at(rbase, rg, rg.BD + rs), rAD = ring_at(rbase, rg, rg.AD + rs);
+                const int rBP = ring_at(rbase, rg, rg.BP + rs);
+                const int rAP = ring_at(rbase, rg, rg.AP + rs);
                 if (lane == 0) {
                     x1D = rBD;
                     x1P = rBP;
@@ -337,7 +352,9 @@ __device__ __forceinline__ void run_block(const Geo& g, Wave<T>& st, const Rings
             st.xpD = x1D;    st.xpP = x1P;
         }
     }
-    if (rA < R) {
+    if (bw) {
+        *bw = make_uint2(bitsA, bitsB);
+    } else if (rA < R) {
         uint2* Bt = reinterpret_cast<uint2*>(td.Bw);
         Bt[((int64_t)k * nP + (tau0 >> 4)) * 32 + lane] = make_uint2(bitsA, bitsB);
     }
@@ -456,16 +473,185 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW)
                 }
                 const bool interior = k >= 1 && k <= sc.nS - 2 && tau0 >= 80 && tau0 + 17 <= W;
                 if (interior)
-                    run_block<false, STD>(g, st, rg, Cs, sc.span, tau0, k, R, W, lane, prevw * RB,
-                                          warp * RB, RB - 1, Tb, lag, td, sc.nP);
+                    run_block<false, STD>(g, st, rg, reinterpret_cast<const char*>(rg.AD), Cs,
+                                          sc.span, tau0, k, R, W, lane,
+                                          prevw * RB, warp * RB, RB - 1, Tb, lag, td, sc.nP);
                 else
-                    run_block<true, STD>(g, st, rg, Cs, sc.span, tau0, k, R, W, lane, prevw * RB,
-                                         warp * RB, RB - 1, Tb, lag, td, sc.nP);
+                    run_block<true, STD>(g, st, rg, reinterpret_cast<const char*>(rg.AD), Cs,
+                                         sc.span, tau0, k, R, W, lane,
+                                         prevw * RB, warp * RB, RB - 1, Tb, lag, td, sc.nP);
             }
             __syncwarp();
             if (lane == 31) my_prog.store(Tb + kBlk, cuda::memory_order_release);
         }
         __syncthreads();  // every warp is done with this tile's rings and descriptor
+    }
+}
+
+// ---------------------------------------------------------------------------
+// One tile on a cluster of two CTAs (16 warps each): 32 warps share the strip
+// pipeline of a tile, so a tile takes about (nS - 1 + 32) / 32 strip times
+// instead of (nS - 1 + 16) / 16.  For alignments with fewer tiles than SMs.
+// Virtual warp v = 16 * rank + warp takes strips v, v + 32, ...; strip k + 1
+// reads strip k's last rows from its producer's ring -- in the other CTA's
+// shared memory (distributed shared memory) where v = 15 -> 16 or 31 -> 0 --
+// and the pairwise progress words are read and written at cluster scope.
+// Rank 0 claims the tiles; three cluster barriers per tile (claim, set-up,
+// end), which every thread of both CTAs reaches on every path: waits are
+// bounded and a warp that gives up goes on to the tile's end barrier.
+constexpr int kClW = 16;   // warps per CTA
+constexpr int kClN = 2;    // CTAs per cluster
+
+__device__ __forceinline__ int ld_acquire_cluster(const int* p) {
+    int v;
+    asm volatile("ld.acquire.cluster.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_cluster(int* p, int v) {
+    asm volatile("st.release.cluster.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ bool wait_progress_cl(const int* p, int target,
+                                                 const volatile int* abort) {
+    for (int it = 0; it < kSpinLimit; ++it) {
+        if (ld_acquire_cluster(p) >= target) return true;
+        if (*abort) return false;
+        __nanosleep(32);
+    }
+    return false;
+}
+
+template <bool STD, typename T>
+__global__ void __launch_bounds__(kClW * 32, 1)
+    k_stage1_cl(const TileDesc* __restrict__ descs, const int ntiles, int* __restrict__ head,
+                const Geo g, int32_t* __restrict__ status, const int RB) {
+    using V2 = typename Vec2<T>::type;
+    constexpr int NWT = kClW * kClN;
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Rings<T> rg;  // this CTA's rings
+    rg.AD = reinterpret_cast<T*>(smem_raw);
+    rg.BD = rg.AD + kClW * RB;
+    rg.AP = reinterpret_cast<int*>(rg.BD + kClW * RB);
+    rg.BP = rg.AP + kClW * RB;
+    int* prog = rg.BP + kClW * RB;
+    __shared__ TileDesc td;
+    __shared__ Sched2 s_sc;
+    __shared__ int s_item, s_abort, s_ttot;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int vw = rank * kClW + warp;
+    const int pv = (vw + NWT - 1) % NWT, nv = (vw + 1) % NWT;
+    // the producer's rings (generic address, this CTA's or the peer's)
+    const char* rbase = reinterpret_cast<const char*>(cl.map_shared_rank(rg.AD, pv / kClW));
+    // cluster scope only where the neighbour is in the other CTA
+    const bool prev_remote = pv / kClW != rank, next_remote = nv / kClW != rank;
+    const bool read_remotely = warp == 0 || warp == kClW - 1;  // my progress word
+    if (threadIdx.x == 0) s_abort = 0;
+    cl.sync();  // both CTAs run before any access to the other's shared memory
+    for (;;) {
+        if (rank == 0 && threadIdx.x == 0) {
+            const int* peer_abort = cl.map_shared_rank(&s_abort, 1);
+            const int it = (s_abort || *peer_abort) ? ntiles : atomicAdd(head, 1);
+            s_item = it;
+            *cl.map_shared_rank(&s_item, 1) = it;
+        }
+        cl.sync();  // the claimed tile reaches both CTAs
+        if (s_item >= ntiles) return;  // both CTAs, nothing remote after the barrier
+        if (threadIdx.x == 0) {
+            td = descs[s_item];
+            s_sc = make_sched2(td.R, td.W, NWT);
+            s_ttot = (s_sc.nS - 1) * s_sc.lag + s_sc.span;
+        }
+        if (threadIdx.x < kClW) prog[threadIdx.x] = 0;
+        __syncthreads();
+        if (rank == 0) {
+            // edge rows past the tile's extent stay +inf / 0 (the DP writes the rest)
+            double* eD = td.eD;
+            int32_t* eP = td.eP;
+            for (int i = threadIdx.x; i < 2 * td.L; i += kClW * 32) {
+                eD[i] = CUDART_INF;
+                eP[i] = 0;
+            }
+        }
+        cl.sync();  // progress words reset and edges filled in both CTAs
+        const int32_t R = td.R, W = td.W;
+        const Sched2& sc = s_sc;
+        const int lag = sc.lag;
+        const int Ttot = s_ttot;
+        const V2* Ct = reinterpret_cast<const V2*>(td.Csk);
+
+        Wave<T> st;
+        st.aD1 = st.aD2 = st.aD3 = st.bD1 = st.bD2 = st.xpD = 0;
+        st.aP1 = st.aP2 = st.aP3 = st.bP1 = st.bP2 = st.xpP = 0;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) st.q[q].x = st.q[q].y = 0;
+
+        for (int Tb = 0; Tb < Ttot; Tb += kBlk) {
+            int k = -1;
+            uint2 bw = make_uint2(0u, 0u);
+            if (Tb >= vw * lag) {
+                const int j = (Tb - vw * lag) / (NWT * lag);
+                const int kk = vw + j * NWT;
+                if (kk < sc.nS && Tb < kk * lag + sc.span) k = kk;
+            }
+            if (k >= 0) {
+                int failed = 0;
+                if (lane == 0) {
+                    // producer (strip k-1) has written every ring slot this block reads
+                    if (k >= 1 &&
+                        !(prev_remote
+                              ? wait_progress_cl(cl.map_shared_rank(prog, pv / kClW) + pv % kClW,
+                                                 Tb - lag + 78, &s_abort)
+                              : wait_progress(prog + pv % kClW, Tb - lag + 78, &s_abort)))
+                        failed = 1;
+                    // consumer (strip k+1) has read every slot this block overwrites
+                    if (!failed && k + 1 < sc.nS &&
+                        !(next_remote
+                              ? wait_progress_cl(cl.map_shared_rank(prog, nv / kClW) + nv % kClW,
+                                                 Tb + lag - RB - 45, &s_abort)
+                              : wait_progress(prog + nv % kClW, Tb + lag - RB - 45, &s_abort)))
+                        failed = 1;
+                    if (failed) {
+                        if (status) atomicExch(status, kStatusWaitTimeout);
+                        s_abort = 1;
+                    }
+                }
+                if (__shfl_sync(0xffffffffu, failed, 0)) break;  // to the tile's end barrier
+                const int tau0 = Tb - k * lag;
+                const V2* Cs = Ct + (int64_t)k * sc.span * 32 + lane;
+                if (tau0 == 0) {
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) st.q[q] = __ldcs(Cs + q * 32);
+                }
+                const bool interior = k >= 1 && k <= sc.nS - 2 && tau0 >= 80 && tau0 + 17 <= W;
+                if (interior)
+                    run_block<false, STD>(g, st, rg, rbase, Cs, sc.span, tau0, k, R, W, lane,
+                                          (pv % kClW) * RB, warp * RB, RB - 1, Tb, lag, td,
+                                          sc.nP, &bw);
+                else
+                    run_block<true, STD>(g, st, rg, rbase, Cs, sc.span, tau0, k, R, W, lane,
+                                         (pv % kClW) * RB, warp * RB, RB - 1, Tb, lag, td,
+                                         sc.nP, &bw);
+            }
+            __syncwarp();
+            // publish first: the backpointer store below is nobody's dependency
+            if (lane == 31) {
+                if (read_remotely) {
+                    st_release_cluster(prog + warp, Tb + kBlk);
+                } else {
+                    cuda::atomic_ref<int, cuda::thread_scope_block> a(prog[warp]);
+                    a.store(Tb + kBlk, cuda::memory_order_release);
+                }
+            }
+            if (k >= 0 && 64 * k + 2 * lane < R) {
+                uint2* Bt = reinterpret_cast<uint2*>(td.Bw);
+                Bt[((int64_t)k * sc.nP + ((Tb - k * lag) >> 4)) * 32 + lane] = bw;
+            }
+        }
+        cl.sync();  // every warp of both CTAs is done with this tile's rings
     }
 }
 
@@ -531,6 +717,87 @@ static cudaError_t launch_q_t(const TileDesc* descs, int ntiles, const int* ntil
     kern<<<grid, NW * 32, smem, st>>>(descs, ntiles, ntiles_dev, head, g, status, rb);
     count_launches(1);
     return cudaGetLastError();
+}
+
+template <bool STD, typename T>
+static cudaError_t launch_cl_t(const TileDesc* descs, int ntiles, int* head, const Geo& g,
+                               int32_t* status, cudaStream_t st) {
+    const int limit = cta_budget(kClW);
+    const Sched2 s = make_sched2(g.L, g.L, kClW * kClN);
+    const int rb = ring_len(s.lag, kClW, limit, (int)sizeof(T));
+    if (rb == 0) return cudaErrorInvalidValue;
+    const size_t smem =
+        (size_t)kClW * rb * (2 * sizeof(T) + 2 * sizeof(int)) + kClW * sizeof(int);
+    auto kern = k_stage1_cl<STD, T>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kClN;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(kClW * 32);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(kClN * (unsigned)ntiles);
+    int maxc = 0;
+    e = cudaOccupancyMaxActiveClusters(&maxc, kern, &cfg);
+    if (e != cudaSuccess) return e;
+    if (maxc < 1) return cudaErrorInvalidConfiguration;
+    const int nc = ntiles < maxc ? ntiles : maxc;
+    if (nc <= 0) return cudaSuccess;
+    cfg.gridDim = dim3(kClN * (unsigned)nc);
+    e = cudaLaunchKernelEx(&cfg, kern, descs, ntiles, head, g, status, rb);
+    count_launches(1);
+    return e;
+}
+
+template <bool STD, typename T>
+static int cl_max_t(const Geo& g) {
+    const int limit = cta_budget(kClW);
+    const Sched2 s = make_sched2(g.L, g.L, kClW * kClN);
+    const int rb = ring_len(s.lag, kClW, limit, (int)sizeof(T));
+    if (rb == 0) return 0;
+    const size_t smem =
+        (size_t)kClW * rb * (2 * sizeof(T) + 2 * sizeof(int)) + kClW * sizeof(int);
+    auto kern = k_stage1_cl<STD, T>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return 0;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kClN;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(kClW * 32);
+    cfg.dynamicSmemBytes = smem;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cfg.gridDim = dim3(kClN);
+    int maxc = 0;
+    if (cudaOccupancyMaxActiveClusters(&maxc, kern, &cfg) != cudaSuccess) return 0;
+    return maxc;
+}
+
+int stage1_cluster_max(const Geo& g, bool fp32) {
+    const bool std_steps = g.S == 3 && g.kind[0] == 0 && g.kind[1] == 1 && g.kind[2] == 2;
+    if (fp32) return std_steps ? cl_max_t<true, float>(g) : cl_max_t<false, float>(g);
+    return std_steps ? cl_max_t<true, double>(g) : cl_max_t<false, double>(g);
+}
+
+cudaError_t launch_stage1_cluster(const TileDesc* descs, int ntiles, int* head, const Geo& g,
+                                  int32_t* status, bool fp32, cudaStream_t st) {
+    const bool std_steps = g.S == 3 && g.kind[0] == 0 && g.kind[1] == 1 && g.kind[2] == 2;
+    if (fp32)
+        return std_steps ? launch_cl_t<true, float>(descs, ntiles, head, g, status, st)
+                         : launch_cl_t<false, float>(descs, ntiles, head, g, status, st);
+    return std_steps ? launch_cl_t<true, double>(descs, ntiles, head, g, status, st)
+                     : launch_cl_t<false, double>(descs, ntiles, head, g, status, st);
 }
 
 template <typename T>
