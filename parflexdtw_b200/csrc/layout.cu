@@ -73,11 +73,11 @@ __global__ void __launch_bounds__(kRegionThreads) k_region_skew(const Tin* __res
 // ---------------------------------------------------------------------------
 // Cost from features straight into the skewed layout.  Lane l of a warp owns
 // rows 64k + 2l (A) and 64k + 2l + 1 (B) of strip k -- the stage-1 mapping --
-// with their d features in registers, and produces 8 consecutive steps
-// tau per pass: A = (64k+2l, tau-2l), B = (64k+2l+1, tau-2l-1), stored as one
-// 16-byte (A, B) pair per lane and step, so a warp writes 512 contiguous bytes
-// per step.  B's column at tau is A's column at tau-1: one pass reads 9
-// column vectors for 16 cells.  Column features of the CTA's window are
+// and produces 8 consecutive steps tau per pass: A = (64k+2l, tau-2l),
+// B = (64k+2l+1, tau-2l-1), stored as one 16-byte (A, B) pair per lane and
+// step, so a warp writes 512 contiguous bytes per step.  B's column at tau
+// is A's column at tau-1: one pass reads 9 column vectors for 16 cells of a
+// strip (k_cost_skew takes two strips at once: 32 cells).  Column features of the CTA's window are
 // staged in shared memory split by column parity; at one instruction every
 // lane reads the same parity at consecutive half-indices (conflict-free).
 constexpr int kCT = 256;                // steps per CTA
@@ -86,15 +86,21 @@ constexpr int kCostThreads = 256;       // 8 warps x 32 steps
 constexpr int kCX = kCT + 66;           // window columns (x = c - ts + 64), even
 constexpr int kCH = kCX / 2;            // per parity
 
+// Two strips per CTA (blockIdx.y = strip pair): rows 64k + rho of strips 2kk
+// and 2kk + 1 sit at the same column for a given step, so each column vector
+// read from shared memory serves four cells of a lane.  The rows' features
+// are staged in shared memory too ([f][strip][64 rows], one 16-byte (A, B)
+// pair per lane: conflict-free), which keeps the registers to 32 sums.
 template <int DMAX>
 __global__ void __launch_bounds__(kCostThreads, 2)
     k_cost_skew(const double* __restrict__ An, const double* __restrict__ Bn, const int d,
                 const Geo g, double* __restrict__ Csk, const int64_t stride,
                 const int32_t* __restrict__ slot, const int32_t* __restrict__ list) {
-    extern __shared__ __align__(16) double sB[];  // [d][2][kCH]
+    extern __shared__ __align__(16) double sB[];  // [d][2][kCH], then sA [d][2][64]
+    double* sA = sB + d * kCX;
     const int nchunk = ceil_div32(make_sched2(g.L, g.L, 1).span, kCT);
     const int tile = list ? list[blockIdx.x / nchunk] : (int)(blockIdx.x / nchunk);
-    const int k = blockIdx.y;
+    const int kk = blockIdx.y;
     const int ts = (int)(blockIdx.x % nchunk) * kCT;
     const int slab = slot ? slot[tile] : tile;  // slab index; < 0: tile skipped
     if (slab < 0) return;
@@ -103,23 +109,25 @@ __global__ void __launch_bounds__(kCostThreads, 2)
     tile_rect(g, tile / g.n2, tile % g.n2, &r0, &c0, &R, &W);
     const int span = ceil_div32(W + kStripRows - 1, kBlk) * kBlk;
     const int nS = ceil_div32(R, kStripRows);
-    if (k >= nS || ts >= span) return;
+    if (2 * kk >= nS || ts >= span) return;
+    const bool two = 2 * kk + 1 < nS;
     for (int q = threadIdx.x; q < d * kCX; q += kCostThreads) {
         const int f = q / kCX, x = q - f * kCX;
         const int c = ts - 64 + x;
         sB[(f * 2 + (x & 1)) * kCH + (x >> 1)] =
             (c >= 0 && c < W) ? __ldg(Bn + (int64_t)f * g.M + c0 + c) : 0.0;
     }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int rA = 64 * k + 2 * lane, rB = rA + 1;
-    double aA[DMAX], aB[DMAX];
-#pragma unroll
-    for (int f = 0; f < DMAX; ++f) {
-        aA[f] = (f < d && rA < R) ? __ldg(An + (int64_t)f * g.N + r0 + rA) : 0.0;
-        aB[f] = (f < d && rB < R) ? __ldg(An + (int64_t)f * g.N + r0 + rB) : 0.0;
+    for (int q = threadIdx.x; q < d * 128; q += kCostThreads) {
+        const int f = q >> 7, r = 128 * kk + (q & 127);
+        sA[q] = r < R ? __ldg(An + (int64_t)f * g.N + r0 + r) : 0.0;
     }
     __syncthreads();
-    double2* out = reinterpret_cast<double2*>(Csk + (int64_t)slab * stride) + (int64_t)k * span * 32 + lane;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int rA0 = 128 * kk + 2 * lane, rB0 = rA0 + 1, rA1 = rA0 + 64, rB1 = rA1 + 1;
+    const double2* sA2 = reinterpret_cast<const double2*>(sA);  // [f][strip][32 lanes]
+    double2* out0 = reinterpret_cast<double2*>(Csk + (int64_t)slab * stride) +
+                    (int64_t)(2 * kk) * span * 32 + lane;
+    double2* out1 = out0 + (int64_t)span * 32;
 #pragma unroll 1
     for (int blk = 0; blk < 32 / kCV; ++blk) {
         const int t0 = ts + 32 * warp + kCV * blk;  // warp-uniform
@@ -127,7 +135,7 @@ __global__ void __launch_bounds__(kCostThreads, 2)
         // A's column at t0 + v is window x = t0 - ts + 64 - 2*lane + v (even at v = 0);
         // b[j] holds x = xA0 - 1 + j, j = 0..8 (B at v uses b[v], A uses b[v + 1])
         const int h0 = ((t0 - ts + 64) >> 1) - lane;  // half-index of xA0
-        double accA[kCV], accB[kCV];
+        double accA0[kCV], accB0[kCV], accA1[kCV], accB1[kCV];
 #pragma unroll
         for (int f = 0; f < DMAX; ++f) {
             if (f >= d) break;
@@ -139,12 +147,17 @@ __global__ void __launch_bounds__(kCostThreads, 2)
                 // x = 2*h0 - 1 + j: odd for even j (half-index h0 - 1 + j/2), even for odd j
                 b[j] = (j & 1) ? se[h0 + (j >> 1)] : so[h0 - 1 + (j >> 1)];
             }
+            const double2 a0 = sA2[(f * 2) * 32 + lane], a1 = sA2[(f * 2 + 1) * 32 + lane];
 #pragma unroll
             for (int v = 0; v < kCV; ++v) {
-                const double pA = __dmul_rn(aA[f], b[v + 1]);
-                const double pB = __dmul_rn(aB[f], b[v]);
-                accA[v] = f == 0 ? pA : __dadd_rn(accA[v], pA);
-                accB[v] = f == 0 ? pB : __dadd_rn(accB[v], pB);
+                const double pA0 = __dmul_rn(a0.x, b[v + 1]);
+                const double pB0 = __dmul_rn(a0.y, b[v]);
+                const double pA1 = __dmul_rn(a1.x, b[v + 1]);
+                const double pB1 = __dmul_rn(a1.y, b[v]);
+                accA0[v] = f == 0 ? pA0 : __dadd_rn(accA0[v], pA0);
+                accB0[v] = f == 0 ? pB0 : __dadd_rn(accB0[v], pB0);
+                accA1[v] = f == 0 ? pA1 : __dadd_rn(accA1[v], pA1);
+                accB1[v] = f == 0 ? pB1 : __dadd_rn(accB1[v], pB1);
             }
         }
 #pragma unroll
@@ -152,9 +165,14 @@ __global__ void __launch_bounds__(kCostThreads, 2)
             const int tau = t0 + v;
             if (tau < span) {
                 const int cA = tau - 2 * lane, cB = cA - 1;
-                const double vA = (rA < R && cA >= 0 && cA < W) ? __dsub_rn(1.0, accA[v]) : 0.0;
-                const double vB = (rB < R && cB >= 0 && cB < W) ? __dsub_rn(1.0, accB[v]) : 0.0;
-                __stcs(out + (int64_t)tau * 32, make_double2(vA, vB));
+                const bool inA = cA >= 0 && cA < W, inB = cB >= 0 && cB < W;
+                __stcs(out0 + (int64_t)tau * 32,
+                       make_double2((rA0 < R && inA) ? __dsub_rn(1.0, accA0[v]) : 0.0,
+                                    (rB0 < R && inB) ? __dsub_rn(1.0, accB0[v]) : 0.0));
+                if (two)
+                    __stcs(out1 + (int64_t)tau * 32,
+                           make_double2((rA1 < R && inA) ? __dsub_rn(1.0, accA1[v]) : 0.0,
+                                        (rB1 < R && inB) ? __dsub_rn(1.0, accB1[v]) : 0.0));
             }
         }
     }
@@ -280,13 +298,21 @@ cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Ge
         count_launches(1);
         return cudaGetLastError();
     }
-    const size_t smem = (size_t)d * kCX * sizeof(double);
+    const size_t smem = (size_t)d * (kCX + 128) * sizeof(double);
+    dim3 grid = region_grid(g, kCT, nt);
+    grid.y = (grid.y + 1) / 2;  // strip pairs
+    cudaError_t e;
     if (d == 12) {
-        k_cost_skew<12><<<region_grid(g, kCT, nt), kCostThreads, smem, st>>>(An, Bn, d, g, Csk,
-                                                                             stride, slot, list);
+        e = cudaFuncSetAttribute(k_cost_skew<12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        if (e != cudaSuccess) return e;
+        k_cost_skew<12><<<grid, kCostThreads, smem, st>>>(An, Bn, d, g, Csk, stride, slot, list);
     } else {
-        k_cost_skew<kMaxFeat><<<region_grid(g, kCT, nt), kCostThreads, smem, st>>>(
-            An, Bn, d, g, Csk, stride, slot, list);
+        e = cudaFuncSetAttribute(k_cost_skew<kMaxFeat>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_cost_skew<kMaxFeat><<<grid, kCostThreads, smem, st>>>(An, Bn, d, g, Csk, stride, slot,
+                                                                 list);
     }
     count_launches(1);
     return cudaGetLastError();
