@@ -283,15 +283,19 @@ def b200_arm(args, spec):
                     kv[a.strip()] = b.strip()
         if kv.get("workload") == spec.name:
             traffic = float(kv["bytes_per_launch"])
-    roofline = {"bound": "hbm", "kernel": "k_stage1_v3", "achieved": achieved,
+    roofline = {"bound": "hbm",
+                "kernel": "stage 1: k_stage1_cl (largest tiles, 2-CTA clusters) + k_stage1_v3 "
+                          "(other tiles, second stream), timed together",
+                "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback",
                 "stage1_ms_per_launch": ms_s1,
                 "alg_bytes_per_cell": 8.25,
                 "fp64_dp_cells_per_s": cells / (ms_s1 / 1e3),
-                "traffic_source": "profiles/k_stage1_v3_ncu_small.md (dram read+write per "
-                                  "launch, scaled by cells)"}
+                "traffic_source": "profiles/k_stage1_cl_ncu_small.md and "
+                                  "k_stage1_v3_ncu_small.md (dram read+write per cell, both "
+                                  "8.41-8.42 B; scaled by cells)"}
 
     # --- row-major C input: the relayout into the tile-skewed layout --------
     C_dev = pf.cost_matrix_from_features_gpu(F1, F2)
