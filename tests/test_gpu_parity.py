@@ -340,3 +340,27 @@ def test_plan_reuse_across_pairs(oracle_mod):
         ref = oracle_mod.parflex_full(C, STD, [2, 3, 3], 0.1, 200)
         assert best == ref["best_cost"]
         assert same(plan.path(n).T, ref["wp"])
+
+
+# fewer tiles than SMs, more than half: the largest tiles run on 2-CTA
+# clusters and the rest on single CTAs in a second stream, at the same time
+@pytest.mark.parametrize("shape,Lb,fp32", [((600, 700), 64, False), ((900, 1000), 100, False),
+                                          ((600, 700), 64, True), ((300, 320), 300, False)])
+def test_cluster_and_single_tiles_vs_oracle(shape, Lb, fp32, oracle_mod):
+    rng = np.random.default_rng(shape[0] + Lb)
+    F1, F2 = W.warped_pair(rng, shape[0], shape[1], pad_frac=0.1)
+    C = W.cost_matrix_det(F1, F2)
+    if fp32:
+        C = C.astype(np.float32).astype(np.float64)
+    ref = oracle_mod.parflex_full(C, STD, [2, 3, 3], 0.1, Lb, fp32=fp32)
+    plan = pf.Plan(C.shape[0], C.shape[1], Lb, STD, [2, 3, 3],
+                   precision="fp32" if fp32 else "fp64")
+    Cd = torch.from_numpy(C).cuda()
+    for _ in range(2):  # the second run reuses the plan's streams and queues
+        plan.run(Cd, 0.1)
+        best, end, found, n = plan.result()
+        assert same(plan.host("EDGE_D"), ref["edge_Df"])
+        assert same(plan.host("EDGE_P"), ref["edge_S"])
+        assert best == ref["best_cost"] and end == ref["best_end"]
+        assert same(plan.path(n).T, ref["wp"])
+    plan.close()
