@@ -176,20 +176,16 @@ class Batch:
     def paths_rows(self, lens, stream=None):
         """Every pair's stitched path as a (2, K_i) int64 array (rows, then
         columns; the reference's ``wp`` layout), from one device gather and
-        one copy.  The arrays are views of one host buffer."""
+        one copy into a fresh host array (the arrays are views of it)."""
         lens = np.asarray(lens, dtype=np.int64)
         offs = np.zeros(self.n, dtype=np.int64)
         if self.n > 1:
             offs[1:] = np.cumsum(lens)[:-1]
-        total = max(int(lens.sum()), 1)
-        if getattr(self, "_pinned", None) is None or self._pinned.shape[0] < total:
-            self._pinned = torch.empty((int(total * 1.25) + 1024, 2), dtype=torch.int64,
-                                       pin_memory=True)
-        stage = self._pinned.numpy()
+        total = int(lens.sum())
+        flat = np.empty(max(2 * total, 2), dtype=np.int64)
         _lib.check(_lib.load().pfx_batch_copy_paths_rows(
-            self._h, stream or current_stream_ptr(), stage.ctypes.data_as(_I64P),
-            offs.ctypes.data_as(_I64P), lens.ctypes.data_as(_I64P), stage.shape[0]))
-        flat = stage.reshape(-1)[:2 * int(lens.sum())].copy()
+            self._h, stream or current_stream_ptr(), flat.ctypes.data_as(_I64P),
+            offs.ctypes.data_as(_I64P), lens.ctypes.data_as(_I64P), max(total, 1)))
         return [flat[2 * o:2 * o + 2 * k].reshape(2, k) for o, k in zip(offs, lens)]
 
     def check_paths(self, margin, stream=None):
