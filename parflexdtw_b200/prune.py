@@ -342,6 +342,7 @@ class PrunedBatch:
         self.dilation = dilation
         self.manhattan = manhattan
         self.expand = int(expand)
+        self._streams = None
         self.L = int(L)
         self.steps, self.weights, self.precision = steps, weights, precision
         self.shapes = [(int(n), int(m)) for n, m in shapes]
@@ -366,12 +367,22 @@ class PrunedBatch:
 
         mark("start")
         masks = torch.empty(int(self.offs[-1]), dtype=torch.uint8, device=self.proposer.device)
+        # the proposer's kernels are small: pairs run on several streams at once
+        main = torch.cuda.current_stream()
+        if self._streams is None:
+            self._streams = [torch.cuda.Stream(device=self.proposer.device)
+                             for _ in range(min(8, len(self.shapes)))]
+        for st in self._streams:
+            st.wait_stream(main)  # features loaded, masks allocated
         for i, (N, M) in enumerate(self.shapes):
-            f1, f2 = b.feature_views(i)
-            pooled = self.proposer.pooled_cost(f1, f2)
-            m, _ = self.proposer.propose(pooled, N, M, self.L, self.threshold, self.dilation,
-                                         self.manhattan)
-            masks[self.offs[i]:self.offs[i + 1]] = m.reshape(-1)
+            with torch.cuda.stream(self._streams[i % len(self._streams)]):
+                f1, f2 = b.feature_views(i)
+                pooled = self.proposer.pooled_cost(f1, f2)
+                m, _ = self.proposer.propose(pooled, N, M, self.L, self.threshold,
+                                             self.dilation, self.manhattan)
+                masks[self.offs[i]:self.offs[i + 1]] = m.reshape(-1)
+        for st in self._streams:
+            main.wait_stream(st)
         mark("proposer")
         b.set_masks(masks)
         mark("set_masks")
