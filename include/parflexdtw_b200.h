@@ -249,8 +249,8 @@ int pfx_flexdtw_tile_noalloc(const double *C, int64_t ldc, int32_t R, int32_t W,
  * own shape (N[i], M[i]) and tile length L[i].  It owns, in one device
  * arena, a plan per pair (pfx_batch_plan), the raw feature inputs, one
  * pool of tile-skewed cost slabs and the stage-1 tile queues.  Pairs are
- * packed into "waves" whose cost slabs fit the pool (wave_bytes; 0 = half
- * of the free device memory); per wave, the cost of every pair is built
+ * packed into "waves" whose cost slabs fit the pool (wave_bytes; 0 = 70 %
+ * of the device memory the batch's other buffers leave free); per wave, the cost of every pair is built
  * from its features, ONE persistent stage-1 launch runs all tiles of all
  * pairs of the wave (largest first) from a device work queue, and stage 2
  * of the pairs runs on forked streams, overlapping the next waves.

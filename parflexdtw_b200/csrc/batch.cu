@@ -295,7 +295,8 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
     }();
     const size_t fixed = arena + fin_total + round256(b->total_tiles * sizeof(TileDesc)) + (1 << 20);
     int64_t budget = wave_bytes;
-    if (budget <= 0) budget = (int64_t)((freeb > fixed ? freeb - fixed : 0) / 2);
+    // default: 70 % of the memory the batch's other buffers leave free
+    if (budget <= 0) budget = (int64_t)((freeb > fixed ? freeb - fixed : 0) / 10 * 7);
     std::vector<int> order(n);
     for (int i = 0; i < n; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return slab[a] > slab[c]; });
