@@ -168,6 +168,9 @@ struct pfx_batch {
     // before stage 1, after stage 1, after the stage-2 join
     std::vector<cudaEvent_t> phase_ev;
     bool phase_valid = false;
+    GPair* gpairs = nullptr;  // FP32 form: per wave, its pairs' cost GEMM table
+    std::vector<int> wave_gp_off;
+    std::vector<int64_t> wave_gp_blocks;
     FbSeg* fbsegs = nullptr;  // FP32 form: every feature matrix's bf16 conversion
     int fb_nseg = 0;
     int64_t fb_blocks = 0;
@@ -203,6 +206,7 @@ static void batch_free(pfx_batch* b) {
     if (b->slabs) cudaFree(b->slabs);
     if (b->stage) cudaFreeHost(b->stage);
     if (b->fbsegs) cudaFree(b->fbsegs);
+    if (b->gpairs) cudaFree(b->gpairs);
     if (b->pref) cudaFree(b->pref);
     if (b->rows) cudaFree(b->rows);
     if (b->prow) cudaFree(b->prow);
@@ -438,6 +442,30 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
             e = cudaMemcpy(b->fbsegs, segs.data(), segs.size() * sizeof(FbSeg),
                            cudaMemcpyHostToDevice);
     }
+    if (e == cudaSuccess && fp32) {
+        // the cost GEMM of a wave's pairs in one launch: per wave, its pairs'
+        // tensor maps, geometry and slabs (pairs in wave order, blocks
+        // numbered from 0 in each wave)
+        std::vector<GPair> gp((size_t)n);
+        for (int w = 0; w < waves && e == cudaSuccess; ++w) {
+            b->wave_gp_off.push_back(b->wave_first[w]);
+            int64_t blk = 0;
+            for (int q = b->wave_first[w]; q < b->wave_first[w + 1]; ++q) {
+                const pfx_plan& p = b->plans[b->wave_pairs[q]];
+                const char* A = static_cast<const char*>(p.fbf);
+                const char* B = A + (size_t)p.g.N * kp * 2;
+                const int64_t nb = gemm_pair_setup(A, B, kp, p.g, static_cast<float*>(p.Csk),
+                                                   p.skew_stride, blk, &gp[q]);
+                if (nb <= 0) e = cudaErrorInvalidValue;
+                blk += nb;
+            }
+            b->wave_gp_blocks.push_back(blk);
+        }
+        if (e == cudaSuccess) e = cudaMalloc(&b->gpairs, gp.size() * sizeof(GPair));
+        if (e == cudaSuccess)
+            e = cudaMemcpy(b->gpairs, gp.data(), gp.size() * sizeof(GPair),
+                           cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess) e = cudaMemset(b->status, 0, 4);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
     for (int k = 0; k < kSide && e == cudaSuccess; ++k) {
@@ -517,6 +545,7 @@ extern "C" int pfx_batch_set_masks(pfx_batch* b, const uint8_t* masks, int32_t o
     if (need > b->stage_bytes) {
         if (b->stage) cudaFreeHost(b->stage);
     if (b->fbsegs) cudaFree(b->fbsegs);
+    if (b->gpairs) cudaFree(b->gpairs);
     if (b->pref) cudaFree(b->pref);
     if (b->rows) cudaFree(b->rows);
     if (b->prow) cudaFree(b->prow);
@@ -726,6 +755,9 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
         BCK(mark(w, 0));
         if (w == 0 && b->fp32)  // every pair's bf16 features, one launch
             BCK(launch_features_bf16_segs(b->fbsegs, b->fb_nseg, b->fb_blocks, b->d, b->kp, s));
+        if (b->fp32 && !b->masked)  // the wave's cost GEMM, one launch
+            BCK(launch_gemm_cost_multi(b->gpairs + b->wave_gp_off[w], q1 - q0,
+                                       b->wave_gp_blocks[w], b->kp, b->status, s));
         for (int q = q0; q < q1; ++q) {
             const int i = b->wave_pairs[q];
             pfx_plan& p = b->plans[i];
@@ -733,7 +765,9 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
             const double* F2 = F1 + (int64_t)b->d * p.g.N;
             const int32_t* slot = b->masked ? p.tile_slot : nullptr;
             const int32_t* list = b->masked ? p.tile_list : nullptr;
-            if (b->fp32) {
+            if (b->fp32 && !b->masked) {
+                // built above
+            } else if (b->fp32) {
                 const char* A = static_cast<const char*>(p.fbf);
                 const char* B = A + (size_t)p.g.N * b->kp * 2;
                 BCK(launch_gemm_cost_skew(A, B, b->kp, p.g, static_cast<float*>(p.Csk),

@@ -1,5 +1,6 @@
 // Shared definitions for the ParFlex B200 kernels.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -201,6 +202,23 @@ int stage1_queue_warps(int ntiles, int32_t L, int num_sms);
 cudaError_t launch_relayout_skew(const double* C, int64_t ldc, const Geo& g, double* Csk,
                                  int64_t skew_stride, cudaStream_t st,
                                  const int32_t* slot = nullptr);
+// One pair of a multi-pair cost GEMM launch (gemm_bf16.cu): its operands'
+// tensor maps, geometry and output slabs, and its first block in the launch.
+struct GPair {
+    CUtensorMap ma, mb;
+    Geo g;
+    float* Csk;
+    int64_t stride, blk0;
+    int32_t nkk, ncb;
+};
+// Fills *out for pair (A: N x Kp bf16 rows, B: M x Kp) into Csk; returns its
+// number of blocks (0 on failure to encode the tensor maps).
+int64_t gemm_pair_setup(const void* Abf, const void* Bbf, int Kp, const Geo& g, float* Csk,
+                        int64_t stride, int64_t blk0, GPair* out);
+// The cost GEMM of npairs pairs (a device table, blocks numbered by blk0) in
+// one persistent launch.
+cudaError_t launch_gemm_cost_multi(const GPair* pairs, int npairs, int64_t nblk, int Kp,
+                                   int32_t* status, cudaStream_t st);
 // FP32 form cost from features (gemm_bf16.cu): bf16 rows of L2-normalised
 // features, then 1 - A B^T on the tensor cores into FP32 skewed slabs.  cap:
 // FP32 elements available from Csk (< 0: n1 * n2 slabs); stores beyond it are

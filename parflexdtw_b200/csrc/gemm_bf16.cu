@@ -22,6 +22,7 @@
 // (bounded) for the CTA's own copies or MMAs still in flight, frees its TMEM
 // and returns.
 #include <cuda.h>
+#include <string.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 
@@ -129,19 +130,33 @@ __device__ __forceinline__ bool mbar_wait_ab(uint64_t* bar, uint32_t parity,
     return false;
 }
 
-// (tile, strip pair kk, step block cb) of block q; false for blocks past a
-// small tile's strips or steps (every role skips them alike).
+// (tile, strip pair kk, step block cb) of block q, with the operands and the
+// output slabs of its pair; false for blocks past a small tile's strips or
+// steps (every role skips them alike).
 struct GBlock {
     int slab, kk, cb, nS, span, R, W;
     int64_t r0, c0;
+    const CUtensorMap* ma;
+    const CUtensorMap* mb;
+    float* Csk;
+    int64_t stride, cap;
 };
+
+__device__ __forceinline__ bool gemm_tile(const Geo& g, int tile, int kk, int cb, GBlock& b) {
+    b.kk = kk;
+    b.cb = cb;
+    tile_rect(g, tile / g.n2, tile % g.n2, &b.r0, &b.c0, &b.R, &b.W);
+    b.span = ceil_div32(b.W + kStripRows - 1, kBlk) * kBlk;
+    b.nS = ceil_div32(b.R, kStripRows);
+    return 2 * b.kk < b.nS && b.cb * kGSteps < b.span;
+}
 
 __device__ __forceinline__ bool gemm_block(const Geo& g, const int32_t* slot, const int32_t* list,
                                            int nkk, int ncb, int64_t q, GBlock& b,
                                            int32_t* status) {
-    b.cb = (int)(q % ncb);
+    const int cb = (int)(q % ncb);
     q /= ncb;
-    b.kk = (int)(q % nkk);
+    const int kk = (int)(q % nkk);
     const int tile = list ? list[q / nkk] : (int)(q / nkk);
     if (tile < 0 || tile >= g.n1 * g.n2) {
         atomicExch(status, kStatusGemmBounds);
@@ -149,10 +164,32 @@ __device__ __forceinline__ bool gemm_block(const Geo& g, const int32_t* slot, co
     }
     b.slab = slot ? slot[tile] : tile;
     if (b.slab < 0) return false;
-    tile_rect(g, tile / g.n2, tile % g.n2, &b.r0, &b.c0, &b.R, &b.W);
-    b.span = ceil_div32(b.W + kStripRows - 1, kBlk) * kBlk;
-    b.nS = ceil_div32(b.R, kStripRows);
-    return 2 * b.kk < b.nS && b.cb * kGSteps < b.span;
+    return gemm_tile(g, tile, kk, cb, b);
+}
+
+// Block q of a multi-pair launch: its pair by binary search on blk0.
+__device__ __forceinline__ bool gemm_block_multi(const GPair* pairs, int npairs, int64_t q,
+                                                 GBlock& b) {
+    int lo = 0, hi = npairs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pairs[mid].blk0 <= q) lo = mid;
+        else hi = mid - 1;
+    }
+    const GPair& P = pairs[lo];
+    int64_t ql = q - P.blk0;
+    const int cb = (int)(ql % P.ncb);
+    ql /= P.ncb;
+    const int kk = (int)(ql % P.nkk);
+    const int tile = (int)(ql / P.nkk);
+    if (tile >= P.g.n1 * P.g.n2) return false;
+    b.slab = tile;
+    b.ma = &P.ma;
+    b.mb = &P.mb;
+    b.Csk = P.Csk;
+    b.stride = P.stride;
+    b.cap = (int64_t)P.g.n1 * P.g.n2 * P.stride;
+    return gemm_tile(P.g, tile, kk, cb, b);
 }
 
 // Persistent, warp-specialised: warp 0 loads operands (TMA, NST stages),
@@ -166,7 +203,8 @@ __global__ void __launch_bounds__(kGThreads, 1)
                      const __grid_constant__ CUtensorMap mapB, const Geo g,
                      float* __restrict__ Csk, const int64_t stride,
                      int32_t* __restrict__ status, const int32_t* __restrict__ slot,
-                     const int32_t* __restrict__ list, const int64_t nblk, const int64_t cap) {
+                     const int32_t* __restrict__ list, const int64_t nblk, const int64_t cap,
+                     const GPair* __restrict__ pairs, const int npairs) {
     extern __shared__ __align__(1024) unsigned char gsm_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(gsm_raw) + 1023) & ~(uintptr_t)1023);
@@ -206,6 +244,16 @@ __global__ void __launch_bounds__(kGThreads, 1)
     const uint32_t tmem = tmem_base_slot;
     const Sched2 sL = make_sched2(g.L, g.L, 1);
     const int nkk = (sL.nS + 1) / 2, ncb = ceil_div32(sL.span, kGSteps);
+    // block q: of the one pair given by the parameters, or of the pair table
+    auto next_block = [&](int64_t q, GBlock& b) -> bool {
+        if (pairs) return gemm_block_multi(pairs, npairs, q, b);
+        b.ma = &mapA;
+        b.mb = &mapB;
+        b.Csk = Csk;
+        b.stride = stride;
+        b.cap = cap;
+        return gemm_block(g, slot, list, nkk, ncb, q, b, status);
+    };
     auto fail = [&]() {
         atomicExch(status, kStatusGemmWait);
         s_abort = 1;
@@ -215,7 +263,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
         int i = 0;
         for (int64_t q = blockIdx.x; q < nblk; q += gridDim.x) {
             GBlock b;
-            if (!gemm_block(g, slot, list, nkk, ncb, q, b, status)) continue;
+            if (!next_block(q, b)) continue;
             const int st = i % NST;
             int ok = 1;
             if (lane == 0) ok = mbar_wait_ab(&empty[st], ((i / NST) & 1) ^ 1, &s_abort);
@@ -232,8 +280,8 @@ __global__ void __launch_bounds__(kGThreads, 1)
                 const int yb = (int)(b.c0 + (int64_t)kGSteps * b.cb - 64);
 #pragma unroll
                 for (int kb = 0; kb < KB; ++kb) {
-                    tma_load_2d(sA + kb * kGRows * kGAtomBytes, &mapA, 64 * kb, ya, &full[st]);
-                    tma_load_2d(sB + kb * kGCols * kGAtomBytes, &mapB, 64 * kb, yb, &full[st]);
+                    tma_load_2d(sA + kb * kGRows * kGAtomBytes, b.ma, 64 * kb, ya, &full[st]);
+                    tma_load_2d(sB + kb * kGCols * kGAtomBytes, b.mb, 64 * kb, yb, &full[st]);
                 }
                 s_issued = i + 1;
             }
@@ -245,7 +293,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
         int i = 0;
         for (int64_t q = blockIdx.x; q < nblk; q += gridDim.x) {
             GBlock b;
-            if (!gemm_block(g, slot, list, nkk, ncb, q, b, status)) continue;
+            if (!next_block(q, b)) continue;
             const int st = i % NST, j = i & 1;
             int ok = 1;
             if (lane == 0) {
@@ -301,7 +349,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
         int i = 0;
         for (int64_t q = blockIdx.x; q < nblk; q += gridDim.x) {
             GBlock b;
-            if (!gemm_block(g, slot, list, nkk, ncb, q, b, status)) continue;
+            if (!next_block(q, b)) continue;
             const int j = i & 1;
             float* Ssk = Ssk0 + (i % NSK) * (2 * kGSteps * 64);
             // one thread waits (for the accumulator, and for the bulk store
@@ -362,7 +410,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
             __syncwarp();
             asm volatile("bar.sync 1, %0;" ::"r"(32 * kGEpiWarps) : "memory");
             if (leader) {
-                float* out = Csk + (int64_t)b.slab * stride;
+                float* out = b.Csk + (int64_t)b.slab * b.stride;
                 const int tau0 = kGSteps * b.cb;
                 const int nt = b.span - tau0 < kGSteps ? b.span - tau0 : kGSteps;
                 for (int s2 = 0; s2 < 2; ++s2) {
@@ -371,7 +419,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
                     // the rows stay inside the slab, the slab inside the buffer
                     const int64_t r_lo = ((int64_t)k * b.span + tau0) * 64;
                     const int64_t r_hi = r_lo + (int64_t)nt * 64;
-                    if (nt <= 0 || r_hi > stride || (int64_t)b.slab * stride + r_hi > cap) {
+                    if (nt <= 0 || r_hi > b.stride || (int64_t)b.slab * b.stride + r_hi > b.cap) {
                         atomicExch(status, kStatusGemmBounds);
                         continue;
                     }
@@ -544,7 +592,8 @@ static cudaError_t gemm_t(const CUtensorMap& ma, const CUtensorMap& mb, const Ge
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grid = (int)(nblk < sms ? nblk : (int64_t)sms);
     if (cap < 0) cap = (int64_t)g.n1 * g.n2 * stride;
-    kern<<<grid, kGThreads, smem, st>>>(ma, mb, g, Csk, stride, status, slot, list, nblk, cap);
+    kern<<<grid, kGThreads, smem, st>>>(ma, mb, g, Csk, stride, status, slot, list, nblk, cap,
+                                        nullptr, 0);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -562,6 +611,56 @@ cudaError_t launch_gemm_cost_skew(const void* Abf, const void* Bbf, int Kp, cons
         case 2: return gemm_t<2>(ma, mb, g, Csk, stride, status, st, slot, list, nlist, cap);
         case 3: return gemm_t<3>(ma, mb, g, Csk, stride, status, st, slot, list, nlist, cap);
         default: return gemm_t<4>(ma, mb, g, Csk, stride, status, st, slot, list, nlist, cap);
+    }
+}
+
+int64_t gemm_pair_setup(const void* Abf, const void* Bbf, int Kp, const Geo& g, float* Csk,
+                        int64_t stride, int64_t blk0, GPair* out) {
+    memset(out, 0, sizeof(GPair));
+    if (!make_map(&out->ma, Abf, g.N, Kp, kGRows) || !make_map(&out->mb, Bbf, g.M, Kp, kGCols))
+        return 0;
+    const Sched2 s = make_sched2(g.L, g.L, 1);
+    out->g = g;
+    out->Csk = Csk;
+    out->stride = stride;
+    out->blk0 = blk0;
+    out->nkk = (s.nS + 1) / 2;
+    out->ncb = ceil_div32(s.span, kGSteps);
+    return (int64_t)g.n1 * g.n2 * out->nkk * out->ncb;
+}
+
+template <int KB>
+static cudaError_t gemm_multi_t(const GPair* pairs, int npairs, int64_t nblk, int32_t* status,
+                                cudaStream_t st) {
+    const size_t smem = gemm_cost_smem_bytes(64 * KB);
+    auto kern = k_gemm_cost_skew<KB, gemm_stages(KB), gemm_skew_bufs(KB)>;
+    cudaError_t e =
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (nblk <= 0 || npairs <= 0) return cudaSuccess;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = (int)(nblk < sms ? nblk : (int64_t)sms);
+    CUtensorMap none;
+    memset(&none, 0, sizeof(none));
+    Geo g0;
+    memset(&g0, 0, sizeof(g0));
+    g0.L = 1;
+    kern<<<grid, kGThreads, smem, st>>>(none, none, g0, nullptr, 0, status, nullptr, nullptr,
+                                        nblk, 0, pairs, npairs);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_cost_multi(const GPair* pairs, int npairs, int64_t nblk, int Kp,
+                                   int32_t* status, cudaStream_t st) {
+    if (Kp % 64 || Kp < 64 || Kp > 256) return cudaErrorInvalidValue;
+    switch (Kp / 64) {
+        case 1: return gemm_multi_t<1>(pairs, npairs, nblk, status, st);
+        case 2: return gemm_multi_t<2>(pairs, npairs, nblk, status, st);
+        case 3: return gemm_multi_t<3>(pairs, npairs, nblk, status, st);
+        default: return gemm_multi_t<4>(pairs, npairs, nblk, status, st);
     }
 }
 
