@@ -20,6 +20,7 @@ from .parflex import (  # noqa: F401
     cost_matrix_from_features_gpu,
     cost_matrix_to_gpu,
     cost_matrix_to_gpu_f32,
+    flexdtw,
     flexdtw_chunk_from_global_C,
     is_gpu_available,
     parflex,

@@ -200,6 +200,18 @@ def flexdtw_chunk_from_global_C(C_dev, L2_global, r0, r1, c0, c1, steps, weights
     return best, wp, D, P, B, debug
 
 
+def flexdtw(C, steps, weights, buffer=1):
+    """``FlexDTW.flexdtw`` (FlexDTW.py:326-378) on the GPU: the untiled
+    FlexDTW of the whole cost matrix -- the accuracy baseline ParFlex
+    approximates (with ``buffer = buffer_global(L1, L2, beta)``).  Returns
+    ``(best_cost, wp[2, K], D, P, B, debug)`` as the reference does, bit-exact
+    in FP64.  The DP runs as one device tile; D, P and B (13 bytes per cell)
+    come back to the host for the endpoint search and the backtrace."""
+    C_dev = cost_matrix_to_gpu(C)
+    N, M = int(C_dev.shape[0]), int(C_dev.shape[1])
+    return flexdtw_chunk_from_global_C(C_dev, M, 0, N, 0, M, steps, weights, buffer)
+
+
 # ---------------------------------------------------------------------------
 # lazy chunks_dict (Parflex.py:446-454 keys)
 # ---------------------------------------------------------------------------
@@ -638,7 +650,7 @@ def buffer_global(L1, L2, beta):
 
 __all__ = [
     "DEFAULT_CHUNK_LENGTH", "parflex", "tiled_stage1_from_features",
-    "run_stage2_from_tiled", "run_flexdtw_on_tiles", "flexdtw_chunk_from_global_C",
+    "run_stage2_from_tiled", "run_flexdtw_on_tiles", "flexdtw", "flexdtw_chunk_from_global_C",
     "cost_matrix_from_features_gpu", "cost_matrix_to_gpu", "cost_matrix_to_gpu_f32",
     "is_gpu_available", "buffer_global", "ChunksDict", "Stage2Result", "Plan",
     "TiledResult", "clear_plan_cache",

@@ -364,3 +364,18 @@ def test_cluster_and_single_tiles_vs_oracle(shape, Lb, fp32, oracle_mod):
         assert best == ref["best_cost"] and end == ref["best_end"]
         assert same(plan.path(n).T, ref["wp"])
     plan.close()
+
+
+# the untiled FlexDTW (one device tile over the whole matrix), with the
+# global buffer ParFlex's stage 2 uses
+@pytest.mark.parametrize("n,m,beta", [(300, 360, 0.1), (900, 700, 0.3), (64, 2000, 0.1)])
+def test_global_flexdtw_vs_oracle(n, m, beta, oracle_mod):
+    rng = np.random.default_rng(n + m)
+    F1, F2 = W.warped_pair(rng, n, m, pad_frac=0.1)
+    C = W.cost_matrix_det(F1, F2)
+    buf = pf.buffer_global(C.shape[0], C.shape[1], beta)
+    best, wp, D, P, B, debug = pf.flexdtw(C, STD, [2, 3, 3], buf)
+    rbest, rwp, rD, rP, rB = oracle_mod.flexdtw(C, STD, [2, 3, 3], buf)
+    assert best == rbest
+    assert same(wp, rwp)
+    assert same(D, rD) and same(P, rP) and same(B, rB)
