@@ -166,6 +166,17 @@ int pfx_stage1(pfx_plan *plan, const double *C, int64_t ldc, void *stream);
  * Overlap costs are read from C if non-null, else from the loaded cost. */
 int pfx_stage2_propagate(pfx_plan *plan, const double *C, int64_t ldc, void *stream);
 
+/* Stage 2a in two parts, for a pair whose tiles are sharded across devices
+ * (each owner runs stage 1 and pfx_stage2_edges on its tiles under a tile
+ * mask; one rank gathers edge_D, edge_P, edge_Cf and the OR of the valid
+ * masks, then runs pfx_stage2_prop).  pfx_stage2_edges: edge tensors and
+ * valid mask (_build_edge_data, Parflex.py:509-564; _build_valid_mask,
+ * Parflex.py:582-624), the only part of stage 2 that reads the cost; it
+ * also resets D_arr / L_arr to +inf.  pfx_stage2_prop: the cross-tile
+ * propagation (Parflex.py:632-855).  pfx_stage2_propagate = both. */
+int pfx_stage2_edges(pfx_plan *plan, const double *C, int64_t ldc, void *stream);
+int pfx_stage2_prop(pfx_plan *plan, void *stream);
+
 /* Copies D_arr / L_arr into the D_PROP / L_PROP buffers (test hook: the
  * state between propagation and overlap sync). */
 int pfx_snapshot_prop(pfx_plan *plan, void *stream);
@@ -181,6 +192,17 @@ int pfx_stage2_scan(pfx_plan *plan, double beta, void *stream);
  * idx (from_best = 0). */
 int pfx_stage2_stitch(pfx_plan *plan, int from_best, int64_t i, int64_t j,
                       int64_t edge, int64_t idx, void *stream);
+
+/* The tile chain of the stitched backtrace alone (backtrace_and_stitch's
+ * tile-to-tile walk, Parflex.py:1032-1103): reads only the start encodings
+ * on the tile edges, not the backpointers, and copies the crossed tiles'
+ * (i, j) into tiles_host[2 * k], [2 * k + 1] (cap >= 101 entries), end tile
+ * first; *n_tiles = their number.  Synchronises `stream`.  A sharded pair
+ * uses it to fetch only the crossed tiles' backpointers before
+ * pfx_stage2_stitch. */
+int pfx_stage2_chain(pfx_plan *plan, int from_best, int64_t i, int64_t j,
+                     int64_t edge, int64_t idx, int32_t *tiles_host, int32_t cap,
+                     int32_t *n_tiles, void *stream);
 
 /* Stage 1 + 2a + 2b + 2c in one call on a device-resident C (or, with C
  * null, on the loaded cost). */

@@ -57,9 +57,13 @@ SIGNATURES = [
     ("pfx_plan_set_tile_mask", ct.c_int, [_vp, _vp, _i32, _vp]),
     ("pfx_stage1", ct.c_int, [_vp, _vp, _i64, _vp]),
     ("pfx_stage2_propagate", ct.c_int, [_vp, _vp, _i64, _vp]),
+    ("pfx_stage2_edges", ct.c_int, [_vp, _vp, _i64, _vp]),
+    ("pfx_stage2_prop", ct.c_int, [_vp, _vp]),
     ("pfx_snapshot_prop", ct.c_int, [_vp, _vp]),
     ("pfx_stage2_scan", ct.c_int, [_vp, _f64, _vp]),
     ("pfx_stage2_stitch", ct.c_int, [_vp, ct.c_int, _i64, _i64, _i64, _i64, _vp]),
+    ("pfx_stage2_chain", ct.c_int, [_vp, ct.c_int, _i64, _i64, _i64, _i64, _i32p, _i32,
+                                    _i32p, _vp]),
     ("pfx_parflex_device", ct.c_int, [_vp, _vp, _i64, _f64, _vp]),
     ("pfx_result", ct.c_int, [_vp, _vp, _f64p, _i64p, _i64p]),
     ("pfx_copy_path", ct.c_int, [_vp, _vp, _i64p, _i64]),

@@ -519,7 +519,7 @@ extern "C" int pfx_stage1(pfx_plan* p, const double* C, int64_t ldc, void* strea
     return PFX_OK;
 }
 
-extern "C" int pfx_stage2_propagate(pfx_plan* p, const double* C, int64_t ldc, void* stream) {
+extern "C" int pfx_stage2_edges(pfx_plan* p, const double* C, int64_t ldc, void* stream) {
     if (!p) return fail(PFX_ERR_ARG, "null plan");
     Geo g = p->g;
     if (C && !p->fp32) {
@@ -531,9 +531,21 @@ extern "C" int pfx_stage2_propagate(pfx_plan* p, const double* C, int64_t ldc, v
     }
     // the FP32 form reads overlap costs from its own FP32 slabs (the values
     // its DP used), never from an FP64 C
-    CK(launch_stage2(p->fp32 ? nullptr : C, p->Csk, p->skew_stride, p->fp32 != 0, g, p->s2,
-                     (cudaStream_t)stream));
+    CK(launch_stage2_edges(p->fp32 ? nullptr : C, p->Csk, p->skew_stride, p->fp32 != 0, g,
+                           p->s2, (cudaStream_t)stream));
     return PFX_OK;
+}
+
+extern "C" int pfx_stage2_prop(pfx_plan* p, void* stream) {
+    if (!p) return fail(PFX_ERR_ARG, "null plan");
+    CK(launch_stage2_prop(p->g, p->s2, (cudaStream_t)stream));
+    return PFX_OK;
+}
+
+extern "C" int pfx_stage2_propagate(pfx_plan* p, const double* C, int64_t ldc, void* stream) {
+    int st;
+    if ((st = pfx_stage2_edges(p, C, ldc, stream))) return st;
+    return pfx_stage2_prop(p, stream);
 }
 
 extern "C" int pfx_snapshot_prop(pfx_plan* p, void* stream) {
@@ -561,6 +573,30 @@ extern "C" int pfx_stage2_stitch(pfx_plan* p, int from_best, int64_t i, int64_t 
                                  int64_t idx, void* stream) {
     if (!p) return fail(PFX_ERR_ARG, "null plan");
     CK(launch_stitch(p->g, p->s2, (cudaStream_t)stream, from_best, i, j, edge, idx));
+    return PFX_OK;
+}
+
+extern "C" int pfx_stage2_chain(pfx_plan* p, int from_best, int64_t i, int64_t j, int64_t edge,
+                                int64_t idx, int32_t* tiles_host, int32_t cap, int32_t* n_tiles,
+                                void* stream) {
+    if (!p || !tiles_host || !n_tiles) return fail(PFX_ERR_ARG, "null argument");
+    if (cap < 101) return fail(PFX_ERR_ARG, "tiles_host holds %d entries; the chain has up to 101", cap);
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(launch_stitch_chain(p->g, p->s2, s, from_best, i, j, edge, idx));
+    int32_t n = 0;
+    int32_t E[12 * 101];
+    CK(cudaMemcpyAsync(&n, p->s2.chain_len, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (n < 0 || n > 101) return fail(PFX_ERR_CUDA, "tile chain length %d out of range", n);
+    if (n > 0) {
+        CK(cudaMemcpyAsync(E, p->s2.chain, sizeof(int32_t) * 12 * n, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    for (int k = 0; k < n; ++k) {
+        tiles_host[2 * k] = E[12 * k];
+        tiles_host[2 * k + 1] = E[12 * k + 1];
+    }
+    *n_tiles = n;
     return PFX_OK;
 }
 

@@ -264,6 +264,10 @@ cudaError_t launch_stage2_prop(const Geo& g, const S2Buf& b, cudaStream_t st);
 cudaError_t launch_sync_scan(const Geo& g, const S2Buf& b, int64_t buf, cudaStream_t st);
 cudaError_t launch_stitch(const Geo& g, const S2Buf& b, cudaStream_t st, int from_best,
                           int64_t si, int64_t sj, int64_t se, int64_t sx);
+// The tile chain of the stitched backtrace alone (b.chain, b.chain_len): it
+// reads only the start encodings on the tile edges, never the backpointers.
+cudaError_t launch_stitch_chain(const Geo& g, const S2Buf& b, cudaStream_t st, int from_best,
+                                int64_t si, int64_t sj, int64_t se, int64_t sx);
 cudaError_t launch_cost_f64(const double* F1, const double* F2, int d, int64_t N, int64_t M,
                             double* An, double* Bn, double* C, int64_t ldc, cudaStream_t st);
 

@@ -592,12 +592,17 @@ cudaError_t launch_sync_scan(const Geo& g, const S2Buf& b, int64_t buf, cudaStre
     return cudaGetLastError();
 }
 
+cudaError_t launch_stitch_chain(const Geo& g, const S2Buf& b, cudaStream_t st, int from_best,
+                                int64_t si, int64_t sj, int64_t se, int64_t sx) {
+    k_stitch_chain<<<1, 32, 0, st>>>(g, b, si, sj, se, sx, from_best);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_stitch(const Geo& g, const S2Buf& b, cudaStream_t st, int from_best,
                           int64_t si, int64_t sj, int64_t se, int64_t sx) {
     cudaError_t e;
-    k_stitch_chain<<<1, 32, 0, st>>>(g, b, si, sj, se, sx, from_best);
-    count_launches(1);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = launch_stitch_chain(g, b, st, from_best, si, sj, se, sx)) != cudaSuccess) return e;
     k_stitch_walk<<<26, 128, 0, st>>>(g, b);  // one warp per chain entry (<= 101)
     count_launches(1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -238,6 +238,28 @@ class Plan:
         if snapshot:
             L.check(lib.pfx_snapshot_prop(self._h, s))
 
+    def edges(self, C_dev: torch.Tensor = None, stream=None):
+        """First part of ``propagate``: edge tensors and valid mask (the only
+        stage-2 step that reads the cost)."""
+        p, ld = self._cptr(C_dev)
+        L.check(L.load().pfx_stage2_edges(self._h, p, ld, stream or current_stream_ptr()))
+
+    def prop(self, stream=None):
+        """Second part of ``propagate``: the cross-tile propagation."""
+        L.check(L.load().pfx_stage2_prop(self._h, stream or current_stream_ptr()))
+
+    def chain(self, start=None, stream=None) -> np.ndarray:
+        """Tiles the stitched backtrace crosses, end tile first, as an (n, 2)
+        int array of (i, j); reads no backpointers.  Synchronises."""
+        lib = L.load()
+        s = stream or current_stream_ptr()
+        buf = (ct.c_int32 * 202)()
+        n = ct.c_int32()
+        fb, (i, j, e, x) = (1, (0, 0, 0, 0)) if start is None else (0, start)
+        L.check(lib.pfx_stage2_chain(self._h, fb, int(i), int(j), int(e), int(x), buf, 101,
+                                     ct.byref(n), s))
+        return np.frombuffer(buf, dtype=np.int32)[:2 * n.value].reshape(-1, 2).copy()
+
     def scan(self, beta, stream=None):
         L.check(L.load().pfx_stage2_scan(self._h, float(beta),
                                          stream or current_stream_ptr()))

@@ -1,11 +1,23 @@
-"""Multi-GPU batches: pairs sharded across ranks, results gathered on rank 0.
+"""Multi-GPU alignment: pairs of a batch, or the tiles of one long pair,
+sharded across ranks (one process per GPU, launched by torchrun).
 
-Pairs are independent (one alignment never needs another's data), so a
-batch splits across processes — one per GPU, launched by torchrun — with no
-data-path collective: each rank aligns its share with ``parflex_batch`` on
-its own device, and one ``gather_object`` brings (best cost, path) to rank 0
-at the end.  Shares are balanced by DP cells (N x M), largest pair first,
-each to the least-loaded rank.
+Batches: pairs are independent (one alignment never needs another's data),
+so a batch splits with no data-path collective: each rank aligns its share
+with ``parflex_batch`` on its own device, and one ``gather_object`` brings
+(best cost, path) to rank 0 at the end.  Shares are balanced by DP cells
+(N x M), largest pair first, each to the least-loaded rank.
+
+One long pair: stage-1 tiles are independent (Parflex.py:421-454), so each
+rank runs the cost and stage 1 of a contiguous range of tile indices
+(``shard_tiles``, balanced by cells) under a tile mask, plus the edge-tensor
+step of stage 2 for those tiles.  One exchange step follows: rank 0 gathers
+every tile's edge costs, start encodings and overlap costs (contiguous
+slices of the tile-major edge arrays, a few MB) and reduces the valid masks
+with MAX.  Rank 0 runs the propagation, the scan and the tile chain of the
+stitched backtrace; it broadcasts the crossed tiles, and their owners send
+only those tiles' packed backpointers (``exchange_backptr``) before rank 0
+walks the path.  Over NCCL the tensors stay on the device; over gloo they
+are staged through host memory.
 """
 from __future__ import annotations
 
@@ -58,3 +70,191 @@ def parflex_batch_sharded(pairs, steps, weights, beta, L=None, aligner=None, gro
         for i, r in part:
             out[i] = r
     return out
+
+
+# -- one long pair, tiles sharded ---------------------------------------------
+
+def tile_cells(n1, n2, N, M, Lb, hop):
+    """DP cells of every tile in tile order (t = i * n2 + j)."""
+    rows = [min(Lb, N - i * hop) for i in range(n1)]
+    cols = [min(Lb, M - j * hop) for j in range(n2)]
+    return [r * c for r in rows for c in cols]
+
+
+def shard_tiles(cells, world_size):
+    """Contiguous tile-index ranges [lo, hi), one per rank, balanced by cells
+    (each boundary at the prefix sum closest to its share).  Rank 0, which
+    runs stage 2, always gets a tile; other ranges may be empty when there
+    are fewer tiles than ranks."""
+    if world_size < 1:
+        raise ValueError("world_size must be >= 1")
+    pre = np.concatenate([[0], np.cumsum(np.asarray(cells, dtype=np.int64))])
+    nt, total = len(cells), int(pre[-1])
+    bounds = [0]
+    for k in range(1, world_size):
+        target = total * k / world_size
+        t = int(np.searchsorted(pre, target))
+        if t > 0 and (t > nt or target - pre[t - 1] <= pre[t] - target):
+            t -= 1
+        bounds.append(min(max(t, bounds[-1], 1 if nt else 0), nt))
+    bounds.append(nt)
+    return [(bounds[r], bounds[r + 1]) for r in range(world_size)]
+
+
+def _comm_device(group):
+    import torch
+    import torch.distributed as dist
+    if dist.get_backend(group) == "nccl":
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device("cpu")
+
+
+def exchange_edges(edge_D, edge_P, edge_Cf, valid, ranges, group=None):
+    """Gather every rank's tile slices of the tile-major edge arrays into
+    rank 0's (in place) and reduce the valid masks with MAX there.
+
+    All four arrays hold n1 * n2 * 2 * L entries in tile order; rank r's
+    tiles are ``ranges[r]``.  Every rank calls this with its own arrays.
+    """
+    import torch
+    import torch.distributed as dist
+    rank, ws = dist.get_rank(group), dist.get_world_size(group)
+    dev = _comm_device(group)
+    nt = sum(hi - lo for lo, hi in ranges)
+    spt = edge_D.numel() // nt if nt else 0
+    lens = [(hi - lo) * spt for lo, hi in ranges]
+    width = max(max(lens), 1)
+    lo = ranges[rank][0] * spt
+    n = lens[rank]
+    flat = [x.reshape(-1) for x in (edge_D, edge_P, edge_Cf, valid)]
+    pk64 = torch.zeros(2, width, dtype=torch.float64, device=dev)
+    pk32 = torch.zeros(width, dtype=torch.int32, device=dev)
+    pk64[0, :n].copy_(flat[0][lo:lo + n])
+    pk64[1, :n].copy_(flat[2][lo:lo + n])
+    pk32[:n].copy_(flat[1][lo:lo + n])
+    g64 = [torch.empty_like(pk64) for _ in range(ws)] if rank == 0 else None
+    g32 = [torch.empty_like(pk32) for _ in range(ws)] if rank == 0 else None
+    dist.gather(pk64, g64, dst=0, group=group)
+    dist.gather(pk32, g32, dst=0, group=group)
+    # a rank without tiles ran nothing: its valid mask contributes no marks
+    vm = flat[3].to(dev) if n else torch.zeros(flat[3].numel(), dtype=flat[3].dtype, device=dev)
+    dist.reduce(vm, dst=0, op=dist.ReduceOp.MAX, group=group)
+    if rank != 0:
+        return
+    for r in range(1, ws):
+        a, m = ranges[r][0] * spt, lens[r]
+        if m == 0:
+            continue
+        flat[0][a:a + m].copy_(g64[r][0, :m])
+        flat[2][a:a + m].copy_(g64[r][1, :m])
+        flat[1][a:a + m].copy_(g32[r][:m])
+    flat[3].copy_(vm)
+
+
+def _owner(t, ranges):
+    for r, (lo, hi) in enumerate(ranges):
+        if lo <= t < hi:
+            return r
+    raise ValueError(f"tile {t} has no owner")
+
+
+def exchange_backptr(bw, crossed, ranges, group=None):
+    """Bring the packed backpointers of the crossed tiles to rank 0.
+
+    ``bw`` is this rank's (n1 * n2, b_words) backpointer array; ``crossed``
+    the crossed tile indices on rank 0 (ignored elsewhere: rank 0 broadcasts
+    them, at most 101).  Returns the crossed tile list on every rank.
+    """
+    import torch
+    import torch.distributed as dist
+    rank, ws = dist.get_rank(group), dist.get_world_size(group)
+    dev = _comm_device(group)
+    msg = torch.full((102,), -1, dtype=torch.int64, device=dev)
+    if rank == 0:
+        c = [int(t) for t in crossed]
+        if len(c) > 101:
+            raise ValueError("the stitched backtrace crosses at most 101 tiles")
+        msg[0] = len(c)
+        if c:
+            msg[1:1 + len(c)] = torch.tensor(c, dtype=torch.int64)
+    dist.broadcast(msg, src=0, group=group)
+    n = int(msg[0])
+    tiles = [int(t) for t in msg[1:1 + n].tolist()]
+    mine = [[t for t in tiles if _owner(t, ranges) == r] for r in range(ws)]
+    cnt = max(len(m) for m in mine[1:]) if ws > 1 else 0
+    if cnt == 0:
+        return tiles
+    bwords = bw.shape[1]
+    pk = torch.zeros(cnt, bwords, dtype=bw.dtype, device=dev)
+    for k, t in enumerate(mine[rank] if rank else []):
+        pk[k].copy_(bw[t])
+    got = [torch.empty_like(pk) for _ in range(ws)] if rank == 0 else None
+    dist.gather(pk, got, dst=0, group=group)
+    if rank == 0:
+        for r in range(1, ws):
+            for k, t in enumerate(mine[r]):
+                bw[t].copy_(got[r][k])
+    return tiles
+
+
+def parflex_sharded(F1, F2, steps, weights, beta, L=None, group=None):
+    """ParFlex of one long pair with its tiles sharded across the ranks of
+    ``group`` (default: the default process group).
+
+    Every rank passes the same features (d x N and d x M, FP64); rank 0
+    returns ``(best_cost, wp)`` exactly as ``parflex`` on the same cost
+    would, the other ranks None.  Each rank builds the cost and runs stage 1
+    only for its own tiles; see the module docstring for the exchange.
+    """
+    import torch
+    import torch.distributed as dist
+    from .parflex import DEFAULT_CHUNK_LENGTH, _features_to_device
+    from .plan import Plan
+    ws = dist.get_world_size(group) if dist.is_initialized() else 1
+    rank = dist.get_rank(group) if dist.is_initialized() else 0
+    Lb = int(DEFAULT_CHUNK_LENGTH if L is None else L)
+    F1d, F2d = _features_to_device(F1), _features_to_device(F2)
+    plan = Plan(F1d.shape[1], F2d.shape[1], Lb, steps, weights)
+    ranges = shard_tiles(tile_cells(plan.n1, plan.n2, plan.N, plan.M, Lb, plan.hop), ws)
+    lo, hi = ranges[rank]
+    status = 0
+    try:
+        if hi > lo:
+            mask = np.zeros(plan.n1 * plan.n2, dtype=np.uint8)
+            mask[lo:hi] = 1
+            plan.set_tile_mask(mask)
+            plan.load_features(F1d, F2d)
+            plan.stage1()
+            plan.edges()
+            plan.result(raise_no_endpoint=False)  # synchronises; raises if a wait ran out
+    except RuntimeError:
+        status = 1
+    if ws > 1:
+        st = torch.tensor([status], dtype=torch.int32, device=_comm_device(group))
+        dist.all_reduce(st, op=dist.ReduceOp.MAX, group=group)
+        status = int(st.item())
+    if status:
+        raise RuntimeError("stage 1 of a tile shard failed on some rank")
+    if ws > 1:
+        exchange_edges(plan.view("EDGE_D"), plan.view("EDGE_P"), plan.view("EDGE_CF"),
+                       plan.view("VALID"), ranges, group)
+    crossed = []
+    if rank == 0:
+        plan.set_tile_mask(None)
+        plan.prop()
+        plan.scan(beta)
+        crossed = [int(i) * plan.n2 + int(j) for i, j in plan.chain()]
+    if ws > 1:
+        bw = plan.view("BACKPTR").view(torch.int32).reshape(plan.n1 * plan.n2, -1)
+        exchange_backptr(bw, crossed, ranges, group)
+    if rank != 0:
+        torch.cuda.synchronize()
+        plan.close()
+        return None
+    plan.stitch()
+    best, end, found, n = plan.result()
+    wp = plan.path(n)
+    plan.close()
+    if wp.shape[0] == 0:
+        return best, np.array([[], []], dtype=np.int64)
+    return best, np.ascontiguousarray(wp.T)

@@ -13,7 +13,9 @@ import torch.distributed as dist  # noqa: E402
 import torch.multiprocessing as mp  # noqa: E402
 
 from parflexdtw_b200 import workloads as W  # noqa: E402
-from parflexdtw_b200.shard import parflex_batch_sharded, shard_pairs  # noqa: E402
+from parflexdtw_b200.shard import (exchange_backptr, exchange_edges,  # noqa: E402
+                                   parflex_batch_sharded, shard_pairs, shard_tiles,
+                                   tile_cells)
 
 STD = [(1, 1), (1, 2), (2, 1)]
 WTS = [2.0, 3.0, 3.0]
@@ -89,3 +91,92 @@ def test_two_gloo_ranks_gather_in_order(Ls):
     assert len(gathered) == len(single)
     for (b, wp), (b1, wp1) in zip(gathered, single):
         assert b == b1 and np.array_equal(np.asarray(wp), wp1)
+
+
+# -- one long pair, tiles sharded: the host-side exchange on gloo ranks ------
+
+NT, SPT, BW = 7, 10, 6  # tiles, edge slots per tile (2 * L), backpointer words per tile
+
+
+def _truth():
+    rng = np.random.default_rng(5)
+    D = rng.standard_normal(NT * SPT)
+    D[::7] = np.inf
+    P = rng.integers(-50, 50, NT * SPT).astype(np.int32)
+    Cf = rng.random(NT * SPT)
+    bw = rng.integers(-2**31, 2**31 - 1, (NT, BW)).astype(np.int32)
+    return D, P, Cf, bw
+
+
+def _exchange_main(rank, port, world, ranges, crossed, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        D, P, Cf, bw = _truth()
+        lo, hi = ranges[rank]
+        own = np.zeros(NT * SPT, bool)
+        own[lo * SPT:hi * SPT] = True
+        # what a masked stage 1 leaves outside the rank's tiles: +inf, 0 and
+        # garbage; valid marks differ per rank
+        tD = torch.from_numpy(np.where(own, D, np.inf))
+        tP = torch.from_numpy(np.where(own, P, 0).astype(np.int32))
+        tCf = torch.from_numpy(np.where(own, Cf, -7.0 - rank))
+        valid = np.random.default_rng(100 + rank).integers(0, 2, NT * SPT).astype(np.uint8)
+        tV = torch.from_numpy(valid.copy())
+        exchange_edges(tD, tP, tCf, tV, ranges)
+        tbw = torch.from_numpy(bw.copy())
+        for t in range(NT):
+            if not lo <= t < hi:
+                tbw[t] = 1000 + rank
+        tiles = exchange_backptr(tbw, crossed if rank == 0 else None, ranges)
+        q.put((rank, tD.numpy(), tP.numpy(), tCf.numpy(), tV.numpy(), tbw.numpy(), tiles))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_shard_tiles_partition():
+    cells = tile_cells(4, 5, 1700, 2100, 500, 400)
+    assert len(cells) == 20 and cells[0] == 500 * 500 and cells[-1] == (1700 - 1200) * (2100 - 1600)
+    for ws in (1, 2, 3, 8, 25):
+        rg = shard_tiles(cells, ws)
+        assert rg[0][0] == 0 and rg[-1][1] == 20 and rg[0][1] >= 1
+        assert all(a[1] == b[0] and a[0] <= a[1] for a, b in zip(rg, rg[1:]))
+        loads = [sum(cells[lo:hi]) for lo, hi in rg]
+        if ws <= 3:
+            assert max(loads) - sum(cells) / ws <= max(cells)
+    assert shard_tiles([9], 3) == [(0, 1), (1, 1), (1, 1)]
+    with pytest.raises(ValueError):
+        shard_tiles(cells, 0)
+
+
+@pytest.mark.parametrize("world,ranges", [(2, [(0, 3), (3, 7)]),
+                                          (3, [(0, 2), (2, 2), (2, 7)])])
+def test_exchange_edges_and_backptr_gloo(world, ranges):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    crossed = [6, 4, 3, 1, 0]
+    procs = [ctx.Process(target=_exchange_main, args=(r, port, world, ranges, crossed, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    got = {}
+    for _ in procs:
+        r, *rest = q.get(timeout=300)
+        got[r] = rest
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    D, P, Cf, bw = _truth()
+    tD, tP, tCf, tV, tbw, tiles = got[0]
+    assert np.array_equal(tD, D) and np.array_equal(tP, P) and np.array_equal(tCf, Cf)
+    want_v = np.zeros(NT * SPT, np.uint8)
+    for r in range(world):
+        if ranges[r][1] > ranges[r][0]:  # a rank without tiles contributes no marks
+            want_v |= np.random.default_rng(100 + r).integers(0, 2, NT * SPT).astype(np.uint8)
+    assert np.array_equal(tV, want_v)
+    for t in crossed:
+        assert np.array_equal(tbw[t], bw[t]), t
+    for r in range(world):
+        assert got[r][-1] == crossed
