@@ -155,6 +155,14 @@ int pfx_plan_load_features_bf16(pfx_plan *plan, const double *F1, const double *
 int pfx_plan_set_tile_mask(pfx_plan *plan, const uint8_t *mask, int32_t on_device,
                            void *stream);
 
+/* Restrict the plan for good to tiles [lo, hi) of the tile order
+ * (t = i * n2 + j): it allocates cost slabs for those tiles only, packed,
+ * and works as a tile mask of that range that cannot be changed or lifted
+ * (pfx_plan_set_tile_mask then fails).  Must come before any cost is
+ * loaded.  For a pair whose tiles are sharded across devices, so that each
+ * device holds the cost of its own tiles only; no reference counterpart. */
+int pfx_plan_set_tile_range(pfx_plan *plan, int32_t lo, int32_t hi, void *stream);
+
 /* Stage 1: FlexDTW on every tile (run_flexdtw_on_tiles, Parflex.py:376-469;
  * GPU variant flexdtw_chunk_from_global_C, gpu_flexdtw.py:288-402).  Writes D
  * and S on tile edges and the packed backpointers.  C non-null: loads it

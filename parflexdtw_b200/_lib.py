@@ -55,6 +55,7 @@ SIGNATURES = [
     ("pfx_plan_load_cost_f32", ct.c_int, [_vp, _vp, _i64, _vp]),
     ("pfx_plan_load_features_bf16", ct.c_int, [_vp, _vp, _vp, _i32, _vp]),
     ("pfx_plan_set_tile_mask", ct.c_int, [_vp, _vp, _i32, _vp]),
+    ("pfx_plan_set_tile_range", ct.c_int, [_vp, _i32, _i32, _vp]),
     ("pfx_stage1", ct.c_int, [_vp, _vp, _i64, _vp]),
     ("pfx_stage2_propagate", ct.c_int, [_vp, _vp, _i64, _vp]),
     ("pfx_stage2_edges", ct.c_int, [_vp, _vp, _i64, _vp]),

@@ -370,6 +370,7 @@ static const int32_t* active_mask(const pfx_plan* p) {
 extern "C" int pfx_plan_set_tile_mask(pfx_plan* p, const uint8_t* mask, int32_t on_device,
                                       void* stream) {
     if (!p) return fail(PFX_ERR_ARG, "null plan");
+    if (p->range_hi > 0) return fail(PFX_ERR_ARG, "the plan has a tile range: its mask stays");
     if (!mask) {
         p->mask_active = 0;
         p->s2.tile_slot = nullptr;
@@ -385,6 +386,40 @@ extern "C" int pfx_plan_set_tile_mask(pfx_plan* p, const uint8_t* mask, int32_t 
     CK(launch_compact_descs(p->descs, nt, p->tile_mask, p->descs_sub, p->nsub, s));
     // a plan keeps every tile's slab in place: slot = tile where set, -1 elsewhere
     CK(launch_mask_slots(p->tile_mask, nt, p->tile_slot, s));
+    p->mask_active = 1;
+    p->s2.tile_slot = p->tile_slot;
+    return PFX_OK;
+}
+
+extern "C" int pfx_plan_set_tile_range(pfx_plan* p, int32_t lo, int32_t hi, void* stream) {
+    if (!p) return fail(PFX_ERR_ARG, "null plan");
+    const int nt = p->g.n1 * p->g.n2;
+    if (lo < 0 || hi > nt || lo >= hi)
+        return fail(PFX_ERR_ARG, "tile range [%d, %d) of %d tiles", lo, hi, nt);
+    if (p->Csk) return fail(PFX_ERR_ARG, "the plan already holds cost slabs: set the range first");
+    p->range_lo = lo;
+    p->range_hi = hi;
+    char* slabs = nullptr;
+    int st = plan_alloc(p, &slabs, (size_t)plan_slab_bytes(p));
+    if (st) {
+        p->range_lo = p->range_hi = 0;
+        return st;
+    }
+    p->Csk = slabs;
+    std::vector<int32_t> slot((size_t)nt, -1);
+    std::vector<uint8_t> mask((size_t)nt, 0);
+    for (int t = lo; t < hi; ++t) {
+        slot[t] = t - lo;
+        mask[t] = 1;
+    }
+    std::vector<TileDesc> d((size_t)nt);
+    plan_tile_descs(p, p->Csk, d.data(), slot.data());
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(cudaMemcpyAsync(p->descs, d.data(), d.size() * sizeof(TileDesc), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(p->tile_mask, mask.data(), (size_t)nt, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(p->tile_slot, slot.data(), (size_t)nt * 4, cudaMemcpyHostToDevice, s));
+    CK(launch_compact_descs(p->descs, nt, p->tile_mask, p->descs_sub, p->nsub, s));
+    CK(cudaStreamSynchronize(s));  // the host vectors go away
     p->mask_active = 1;
     p->s2.tile_slot = p->tile_slot;
     return PFX_OK;

@@ -43,6 +43,9 @@ struct pfx_plan {
     pfx::TileDesc* descs_sub;
     int* nsub;
     int mask_active;
+    // tile range (pfx_plan_set_tile_range): cost slabs only for tiles
+    // [range_lo, range_hi), packed; range_hi == 0 means every tile has a slab
+    int32_t range_lo, range_hi;
     // arena allocation: 0 = cudaMalloc per buffer, 1 = count bytes only,
     // 2 = carve from `arena`
     int arena_mode;
@@ -58,7 +61,9 @@ int plan_init(pfx_plan* p, int64_t N, int64_t M, int32_t L, const int64_t* steps
 void plan_tile_descs(const pfx_plan* p, const void* Csk, TileDesc* out,
                      const int32_t* slot = nullptr);
 inline int64_t plan_slab_bytes(const pfx_plan* p) {
-    return (int64_t)p->g.n1 * p->g.n2 * p->skew_stride * (p->fp32 ? 4 : 8);
+    const int64_t slabs = p->range_hi > 0 ? (int64_t)p->range_hi - p->range_lo
+                                          : (int64_t)p->g.n1 * p->g.n2;
+    return slabs * p->skew_stride * (p->fp32 ? 4 : 8);
 }
 int num_sms_cur();
 }  // namespace pfx

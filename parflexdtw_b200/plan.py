@@ -140,6 +140,8 @@ class Plan:
     def cost_matrix(self) -> np.ndarray:
         """The loaded cost as an N x M host array, read back from the
         tile-skewed slabs (FP64, or FP32 in the FP32 form)."""
+        if getattr(self, "tile_range", None):
+            raise ValueError("a plan with a tile range holds part of the cost only")
         slab = self.host("COST")
         spanL = -(-(self.L + 63) // 16) * 16
         nSL = -(-self.L // 64)
@@ -217,6 +219,13 @@ class Plan:
             if m.size != self.n1 * self.n2:
                 raise ValueError("mask must have n1 * n2 entries")
             L.check(lib.pfx_plan_set_tile_mask(self._h, m.ctypes.data_as(ct.c_void_p), 0, s))
+
+    def set_tile_range(self, lo, hi, stream=None):
+        """Hold cost slabs for tiles [lo, hi) of the tile order only and run
+        stage 1 on them alone, for good (before any cost is loaded)."""
+        L.check(L.load().pfx_plan_set_tile_range(self._h, int(lo), int(hi),
+                                                 stream or current_stream_ptr()))
+        self.tile_range = (int(lo), int(hi))
 
     # -- stages ----------------------------------------------------------
     @staticmethod

@@ -220,9 +220,7 @@ def parflex_sharded(F1, F2, steps, weights, beta, L=None, group=None):
     status = 0
     try:
         if hi > lo:
-            mask = np.zeros(plan.n1 * plan.n2, dtype=np.uint8)
-            mask[lo:hi] = 1
-            plan.set_tile_mask(mask)
+            plan.set_tile_range(lo, hi)  # cost slabs of the own tiles only
             plan.load_features(F1d, F2d)
             plan.stage1()
             plan.edges()
@@ -240,7 +238,7 @@ def parflex_sharded(F1, F2, steps, weights, beta, L=None, group=None):
                        plan.view("VALID"), ranges, group)
     crossed = []
     if rank == 0:
-        plan.set_tile_mask(None)
+        # the rest of stage 2 reads no cost: the tile range may stay
         plan.prop()
         plan.scan(beta)
         crossed = [int(i) * plan.n2 + int(j) for i, j in plan.chain()]

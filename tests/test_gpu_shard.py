@@ -19,6 +19,7 @@ import torch.multiprocessing as mp  # noqa: E402
 
 import parflexdtw_b200 as pf  # noqa: E402
 from parflexdtw_b200 import workloads as W  # noqa: E402
+from parflexdtw_b200.plan import Plan  # noqa: E402
 from parflexdtw_b200.shard import parflex_sharded  # noqa: E402
 
 STD = [(1, 1), (1, 2), (2, 1)]
@@ -86,3 +87,36 @@ def test_tile_sharded_single_process_vs_oracle(oracle_mod):
     best, wp = parflex_sharded(F1, F2, STD, WTS, 0.1, L=300)
     ref = oracle_mod.parflex_full(W.cost_matrix_det(F1, F2), STD, WTS, 0.1, 300)
     assert best == ref["best_cost"] and np.array_equal(wp, ref["wp"])
+
+
+def test_tile_range_plan_holds_its_tiles_only():
+    """A ranged plan: packed slabs for its tiles, stage 1 on them alone with
+    the same edges and backpointers as the full plan, and a mask that stays."""
+    F1, F2 = _pair(15, 1300, 1500)
+    F1d, F2d = (torch.from_numpy(np.ascontiguousarray(F)).cuda() for F in (F1, F2))
+    full = Plan(F1.shape[1], F2.shape[1], 400, STD, WTS)
+    full.load_features(F1d, F2d)
+    full.stage1()
+    nt = full.n1 * full.n2
+    lo, hi = 3, nt - 2
+    part = Plan(F1.shape[1], F2.shape[1], 400, STD, WTS)
+    part.set_tile_range(lo, hi)
+    with pytest.raises(ValueError):
+        part.set_tile_range(0, 1)
+    with pytest.raises(ValueError):
+        part.set_tile_mask(None)
+    part.load_features(F1d, F2d)
+    part.stage1()
+    torch.cuda.synchronize()
+    assert part.view("COST").numel() == full.view("COST").numel() // nt * (hi - lo)
+    eD, fD = part.host("EDGE_D").reshape(nt, -1), full.host("EDGE_D").reshape(nt, -1)
+    eP, fP = part.host("EDGE_P").reshape(nt, -1), full.host("EDGE_P").reshape(nt, -1)
+    assert np.array_equal(eD[lo:hi], fD[lo:hi]) and np.array_equal(eP[lo:hi], fP[lo:hi])
+    assert np.all(np.isinf(eD[:lo])) and np.all(eP[hi:] == 0)
+    bw_p = part.host("BACKPTR").reshape(nt, -1)
+    bw_f = full.host("BACKPTR").reshape(nt, -1)
+    assert np.array_equal(bw_p[lo:hi], bw_f[lo:hi])
+    with pytest.raises(ValueError):
+        Plan(100, 100, 50, STD, WTS).set_tile_range(2, 2)
+    part.close()
+    full.close()
