@@ -933,6 +933,34 @@ def prune_arm(args, spec):
     del pb
     torch.cuda.empty_cache()
 
+    # --- the same proposer over the FP32 form (BF16 tcgen05 cost GEMM, FP32
+    # DP): its full-tile results, then the pruned run against them ----------
+    b32 = Batch(shapes, Lb, spec.steps, spec.weights, 12, precision="fp32")
+    b32.load(pairs)
+    b32.run(spec.beta, use_graph=False)
+    best32, _, lens32 = b32.results()
+    paths32 = b32.paths(lens32)
+    b32.close()
+    del b32
+    torch.cuda.empty_cache()
+    p32 = pf.PrunedBatch(shapes, Lb, spec.steps, spec.weights, 12, proposer=net,
+                         precision="fp32")
+    p32.load(pairs)
+    for _ in range(args.warmup):
+        p32.run(spec.beta)
+    if ws > 1:
+        dist.barrier()
+    ms_32, (out32, info32) = timed(lambda: p32.run(spec.beta), args.steps)
+    ms_32 = max_ranks(ms_32)
+    p32.close()
+    del p32
+    torch.cuda.empty_cache()
+    agree32 = sum(int(bc == best32[i] and np.array_equal(wp, paths32[i].T))
+                  for i, (bc, wp) in enumerate(out32))
+    agree32_64 = sum(int(np.array_equal(wp, paths0[i].T)) for i, (_, wp) in enumerate(out32))
+    rel32 = [abs(bc - best0[i]) / abs(best0[i]) for i, (bc, _) in enumerate(out32)]
+    v_32 = cells * ws * args.steps / (ms_32 / 1e3)
+
     v_pruned = cells * ws * args.steps / (ms_pruned / 1e3)
     v_plain = cells * ws * args.plain_steps / (ms_plain / 1e3)
     if rank == 0:
@@ -962,6 +990,15 @@ def prune_arm(args, spec):
                             proposer="3 conv layers, 32 channels, bf16 activations, "
                                      "parflexdtw_b200/data/proposer_L2000.npz",
                             threshold=net.threshold, dilation_tiles=1),
+            "fp32_pruned": {
+                "value": v_32, "unit": UNIT, "ms_per_step": ms_32 / args.steps,
+                "speedup_over_plain": v_32 / v_plain,
+                "exact_agreement_with_fp32_full_tiles": agree32 / n_pairs,
+                "path_agreement_with_fp64_full_tiles": agree32_64 / n_pairs,
+                "best_cost_rel_err_vs_fp64": {"max": max(rel32), "mean": float(np.mean(rel32))},
+                "skipped_fraction": info32["skipped_fraction"],
+                "fallbacks": info32["fallbacks"],
+                "form": "same proposer; BF16 tcgen05 cost GEMM, FP32 DP"},
             "e2e": {"value": cells * ws * args.e2e_steps / (ms_e2e / 1e3), "unit": UNIT,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "steps": args.e2e_steps, "ms_per_step": ms_e2e / args.e2e_steps,

@@ -317,8 +317,7 @@ int pfx_batch_plan(pfx_batch *batch, int32_t i, pfx_plan **plan);
  * slabs are built and stage 1 runs only there (the pool now holds only
  * those slabs, so waves are repacked), other tiles keep +inf edges.  For the
  * learned tile proposer; synchronises `stream`; invalidates the recorded
- * graph.  FP64 batches only (PFX_ERR_ARG for a batch of the FP32 form).  No
- * reference counterpart. */
+ * graph.  Either form (FP64 or FP32).  No reference counterpart. */
 int pfx_batch_set_masks(pfx_batch *batch, const uint8_t *masks, int32_t on_device,
                         void *stream);
 /* After a masked run: adds tiles to pair i's run and aligns it again.

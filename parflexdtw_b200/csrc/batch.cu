@@ -484,11 +484,6 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
 extern "C" int pfx_batch_set_masks(pfx_batch* b, const uint8_t* masks, int32_t on_device,
                                    void* stream) {
     if (!b || !masks) return errf(PFX_ERR_ARG, "null argument");
-    // Masked FP32 batches are disabled: on a B200, a masked FP32 batch of 64
-    // pairs of 40000-60000 frames (L = 2000, two waves) raised an illegal
-    // address whose cause has not been found (the same batch unmasked, the
-    // same masks over the FP64 form, and 8 such pairs masked all ran clean).
-    if (b->fp32) return errf(PFX_ERR_ARG, "tile masks need a batch of the FP64 form");
     cudaStream_t s = (cudaStream_t)stream;
     const int n = b->n;
     std::vector<int64_t> moff(n + 1, 0);
@@ -544,11 +539,6 @@ extern "C" int pfx_batch_set_masks(pfx_batch* b, const uint8_t* masks, int32_t o
     BCK(cudaStreamSynchronize(s));  // the staging buffer may still feed earlier copies
     if (need > b->stage_bytes) {
         if (b->stage) cudaFreeHost(b->stage);
-    if (b->fbsegs) cudaFree(b->fbsegs);
-    if (b->gpairs) cudaFree(b->gpairs);
-    if (b->pref) cudaFree(b->pref);
-    if (b->rows) cudaFree(b->rows);
-    if (b->prow) cudaFree(b->prow);
         b->stage = nullptr;
         b->stage_bytes = 0;
         BCK(cudaMallocHost(&b->stage, need));

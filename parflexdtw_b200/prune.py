@@ -333,8 +333,6 @@ class PrunedBatch:
                  dilation=1, manhattan=None, precision="fp64", wave_bytes=0, warps=0,
                  expand=2):
         from .batch import Batch
-        if precision != "fp64":
-            raise ValueError("PrunedBatch runs the FP64 form (masked FP32 batches are disabled)")
         self.batch = Batch(shapes, L, steps, weights, d, wave_bytes=wave_bytes, warps=warps,
                            precision=precision)
         self.proposer = proposer or TileProposer.load()

@@ -175,6 +175,57 @@ def test_batch_fp32_vs_oracle(oracle_mod):
     b.close()
 
 
+def test_batch_fp32_masked_vs_unmasked(oracle_mod):
+    """Masked FP32 batches: all-ones masks and path-dilated masks give the
+    unmasked FP32 results bit for bit, which equal the oracle's FP32 form on
+    the device's own cost; so does PrunedBatch in the FP32 form."""
+    from parflexdtw_b200.prune import tiles_on_path
+    sizes = [(1900, 2100), (2600, 2300), (900, 1000), (1500, 1700)]
+    rng = np.random.default_rng(21)
+    pairs = [W.warped_pair(rng, n, m, d=12, noise=0.1, latent="gaussian") for n, m in sizes]
+    shapes = [(p[0].shape[1], p[1].shape[1]) for p in pairs]
+    L = 300
+    b = Batch(shapes, L, STD, WTS, 12, precision="fp32", warps=4)
+    b.load(pairs)
+    b.run(0.1, use_graph=False)
+    torch.cuda.synchronize()
+    refs = [oracle_mod.parflex_full(b.plan(i).cost_matrix().astype(np.float64), STD, WTS, 0.1,
+                                    L, fp32=True) for i in range(b.n)]
+    _check(b, refs)
+    grids = [(-(-(n - 1) // (L - 1)), -(-(m - 1) // (L - 1))) for n, m in shapes]
+    b.set_masks(torch.ones(sum(a * c for a, c in grids), dtype=torch.uint8, device="cuda"))
+    for use_graph in (False, True):
+        b.run(0.1, use_graph=use_graph)
+        _check(b, refs)
+    dil = []
+    for (n, m), r in zip(shapes, refs):
+        lab = tiles_on_path(r["wp"], n, m, L).astype(bool)
+        p = np.pad(lab, 1)
+        d = np.zeros_like(lab)
+        for di in range(3):
+            for dj in range(3):
+                d |= p[di:di + lab.shape[0], dj:dj + lab.shape[1]]
+        dil.append(d.reshape(-1))
+    masks = torch.from_numpy(np.concatenate(dil).astype(np.uint8)).cuda()
+    assert int(masks.sum()) < masks.numel()
+    b.set_masks(masks)
+    for use_graph in (False, True):
+        b.run(0.1, use_graph=use_graph)
+        _check(b, refs)
+    for i, r in enumerate(refs):
+        bc, wp = b.complete(i, 0.1)
+        assert bc == r["best_cost"] and same(wp.T, r["wp"])
+    b.close()
+    from parflexdtw_b200.prune import TileProposer
+    pb = pf.PrunedBatch(shapes, L, STD, WTS, 12, proposer=TileProposer(seed=6),
+                        threshold=-1e30, precision="fp32")
+    pb.load(pairs)
+    out, info = pb.run(0.1)
+    for (bc, wp), r in zip(out, refs):
+        assert bc == r["best_cost"] and same(wp, r["wp"])
+    pb.close()
+
+
 def test_batch_errors():
     with pytest.raises(ValueError):
         Batch([(100, 100)], 100, STD, WTS, 0)  # no features
@@ -188,12 +239,5 @@ def test_batch_errors():
     with pytest.raises(ValueError):
         b.load([(np.zeros((12, 99)), np.zeros((12, 120)))])
     b.close()
-    # tile masks run the FP64 form only
-    b = Batch([(100, 120)], 50, STD, WTS, 12, precision="fp32")
-    with pytest.raises(ValueError):
-        b.set_masks(torch.ones(b.tiles, dtype=torch.uint8, device="cuda"))
-    b.close()
-    with pytest.raises(ValueError):
-        pf.PrunedBatch([(100, 120)], 50, STD, WTS, 12, precision="fp32")
     with pytest.raises(ValueError):
         pf.parflex_batch([np.zeros((10, 10))], STD, WTS, 0.1, L=8)
