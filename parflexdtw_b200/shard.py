@@ -137,7 +137,9 @@ def exchange_edges(edge_D, edge_P, edge_Cf, valid, ranges, group=None):
     dist.gather(pk64, g64, dst=0, group=group)
     dist.gather(pk32, g32, dst=0, group=group)
     # a rank without tiles ran nothing: its valid mask contributes no marks
-    vm = flat[3].to(dev) if n else torch.zeros(flat[3].numel(), dtype=flat[3].dtype, device=dev)
+    # (a copy: the collective gets a tensor of its own allocator, not the plan's)
+    vm = flat[3].to(dev, copy=True) if n else torch.zeros(flat[3].numel(), dtype=flat[3].dtype,
+                                                          device=dev)
     dist.reduce(vm, dst=0, op=dist.ReduceOp.MAX, group=group)
     if rank != 0:
         return

@@ -38,7 +38,7 @@ def _pair(seed, n, m):
     return W.warped_pair(np.random.default_rng(seed), n, m, pad_frac=0.1)
 
 
-def _rank_main(rank, port, world, seed, n, m, Lb, q):
+def _rank_main(rank, port, world, seed, n, m, Lb, q, wts=WTS):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     os.environ.setdefault("GLOO_SOCKET_IFNAME", "lo")
@@ -46,7 +46,7 @@ def _rank_main(rank, port, world, seed, n, m, Lb, q):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         F1, F2 = _pair(seed, n, m)
-        res = parflex_sharded(F1, F2, STD, WTS, 0.1, L=Lb)
+        res = parflex_sharded(F1, F2, STD, wts, 0.1, L=Lb)
         q.put((rank, None if res is None else (float(res[0]), res[1].tolist())))
     except Exception as e:  # report instead of hanging the parent
         q.put((rank, repr(e)))
@@ -55,14 +55,15 @@ def _rank_main(rank, port, world, seed, n, m, Lb, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world,seed,n,m,Lb", [(2, 11, 1500, 1800, 400),
-                                               (3, 12, 2300, 1900, 500),
-                                               (2, 13, 300, 350, 400)])
-def test_tile_sharded_pair_vs_oracle(oracle_mod, world, seed, n, m, Lb):
+@pytest.mark.parametrize("world,seed,n,m,Lb,wts", [(2, 11, 1500, 1800, 400, WTS),
+                                                   (3, 12, 2300, 1900, 500, WTS),
+                                                   (2, 13, 300, 350, 400, WTS),
+                                                   (2, 16, 1700, 1400, 300, [1.25, 3.0, 3.0])])
+def test_tile_sharded_pair_vs_oracle(oracle_mod, world, seed, n, m, Lb, wts):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank_main, args=(r, port, world, seed, n, m, Lb, q))
+    procs = [ctx.Process(target=_rank_main, args=(r, port, world, seed, n, m, Lb, q, wts))
              for r in range(world)]
     for p in procs:
         p.start()
@@ -74,10 +75,10 @@ def test_tile_sharded_pair_vs_oracle(oracle_mod, world, seed, n, m, Lb):
     best, wp = got[0][0], np.asarray(got[0][1], dtype=np.int64)
     F1, F2 = _pair(seed, n, m)
     C = W.cost_matrix_det(F1, F2)
-    ref = oracle_mod.parflex_full(C, STD, WTS, 0.1, Lb)
+    ref = oracle_mod.parflex_full(C, STD, wts, 0.1, Lb)
     assert best == ref["best_cost"]
     assert np.array_equal(wp, ref["wp"])
-    b1, wp1 = pf.parflex(C, STD, WTS, 0.1, L=Lb, profile_dir=None)
+    b1, wp1 = pf.parflex(C, STD, wts, 0.1, L=Lb, profile_dir=None)
     assert b1 == best and np.array_equal(wp1, wp)
 
 
