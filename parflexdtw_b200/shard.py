@@ -219,7 +219,9 @@ def parflex_sharded(F1, F2, steps, weights, beta, L=None, group=None):
     plan = Plan(F1d.shape[1], F2d.shape[1], Lb, steps, weights)
     ranges = shard_tiles(tile_cells(plan.n1, plan.n2, plan.N, plan.M, Lb, plan.hop), ws)
     lo, hi = ranges[rank]
-    status = 0
+    # every rank reaches the status reduction, so that a failure on one rank
+    # ends the call on all of them instead of leaving them in a collective
+    failure = None
     try:
         if hi > lo:
             plan.set_tile_range(lo, hi)  # cost slabs of the own tiles only
@@ -227,14 +229,19 @@ def parflex_sharded(F1, F2, steps, weights, beta, L=None, group=None):
             plan.stage1()
             plan.edges()
             plan.result(raise_no_endpoint=False)  # synchronises; raises if a wait ran out
-    except RuntimeError:
-        status = 1
+    except Exception as e:  # noqa: BLE001 - re-raised below, after the reduction
+        failure = e
+    status = 0 if failure is None else 1
     if ws > 1:
         st = torch.tensor([status], dtype=torch.int32, device=_comm_device(group))
         dist.all_reduce(st, op=dist.ReduceOp.MAX, group=group)
         status = int(st.item())
+    if failure is not None:
+        plan.close()
+        raise failure
     if status:
-        raise RuntimeError("stage 1 of a tile shard failed on some rank")
+        plan.close()
+        raise RuntimeError("stage 1 of a tile shard failed on another rank")
     if ws > 1:
         exchange_edges(plan.view("EDGE_D"), plan.view("EDGE_P"), plan.view("EDGE_CF"),
                        plan.view("VALID"), ranges, group)

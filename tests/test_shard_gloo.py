@@ -180,3 +180,75 @@ def test_exchange_edges_and_backptr_gloo(world, ranges):
         assert np.array_equal(tbw[t], bw[t]), t
     for r in range(world):
         assert got[r][-1] == crossed
+
+
+# -- failure on one rank: every rank leaves the call, none waits forever ------
+
+class _FakePlan:
+    """Host stand-in for Plan: stage 1 fails on the rank named by FAIL_RANK."""
+
+    def __init__(self, N, M, Lb, steps, weights, precision="fp64"):
+        self.N, self.M, self.L = N, M, Lb
+        self.hop = Lb - 1
+        self.n1 = max(1, -(-(N - 1) // (Lb - 1)))
+        self.n2 = max(1, -(-(M - 1) // (Lb - 1)))
+        self.closed = False
+
+    def set_tile_range(self, lo, hi):
+        pass
+
+    def load_features(self, F1, F2):
+        pass
+
+    def stage1(self):
+        if dist.get_rank() == int(os.environ["FAIL_RANK"]):
+            raise RuntimeError("a bounded device wait ran out (host fake)")
+
+    def edges(self):
+        pass
+
+    def result(self, raise_no_endpoint=True):
+        return 0.0, (0,) * 6, False, 0
+
+    def close(self):
+        self.closed = True
+
+
+def _fail_main(rank, port, world, fail_rank, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    os.environ["FAIL_RANK"] = str(fail_rank)
+    import sys
+
+    from parflexdtw_b200.shard import parflex_sharded
+    # the package exports a function named parflex: take the modules themselves
+    sys.modules["parflexdtw_b200.plan"].Plan = _FakePlan
+    sys.modules["parflexdtw_b200.parflex"]._features_to_device = \
+        lambda F: torch.as_tensor(np.asarray(F))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        F1 = np.ones((12, 900))
+        F2 = np.ones((12, 1000))
+        try:
+            parflex_sharded(F1, F2, STD, WTS, 0.1, L=300)
+            q.put((rank, "returned"))
+        except RuntimeError as e:
+            q.put((rank, str(e)))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("fail_rank", [0, 1])
+def test_tile_shard_failure_on_one_rank_ends_all(fail_rank):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_fail_main, args=(r, port, 2, fail_rank, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=300) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert "bounded device wait" in got[fail_rank]
+    assert "another rank" in got[1 - fail_rank]
