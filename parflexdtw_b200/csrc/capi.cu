@@ -224,6 +224,9 @@ int pfx::plan_init(pfx_plan* p, int64_t N, int64_t M, int32_t L, const int64_t* 
     CK(cudaMemset(p->s2.chain_len, 0, sizeof(int32_t)));
     CK(cudaMemset(p->s2.wp_len, 0, sizeof(int64_t)));
     CK(cudaMemset(p->s1.status, 0, sizeof(int32_t)));
+    // backpointer words stage 1 never writes (past a tile's rows or steps)
+    // read as 0, so that two plans' arrays compare equal
+    CK(cudaMemset(p->s1.Bw, 0, (size_t)nt * g.b_words * sizeof(uint32_t)));
     return PFX_OK;
 }
 

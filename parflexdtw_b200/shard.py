@@ -199,14 +199,15 @@ def exchange_backptr(bw, crossed, ranges, group=None):
     return tiles
 
 
-def parflex_sharded(F1, F2, steps, weights, beta, L=None, group=None):
+def parflex_sharded(F1, F2, steps, weights, beta, L=None, group=None, precision="fp64"):
     """ParFlex of one long pair with its tiles sharded across the ranks of
     ``group`` (default: the default process group).
 
     Every rank passes the same features (d x N and d x M, FP64); rank 0
     returns ``(best_cost, wp)`` exactly as ``parflex`` on the same cost
-    would, the other ranks None.  Each rank builds the cost and runs stage 1
-    only for its own tiles; see the module docstring for the exchange.
+    would (``precision="fp32"``: as a single FP32-form plan would), the
+    other ranks None.  Each rank builds the cost and runs stage 1 only for
+    its own tiles; see the module docstring for the exchange.
     """
     import torch
     import torch.distributed as dist
@@ -216,7 +217,7 @@ def parflex_sharded(F1, F2, steps, weights, beta, L=None, group=None):
     rank = dist.get_rank(group) if dist.is_initialized() else 0
     Lb = int(DEFAULT_CHUNK_LENGTH if L is None else L)
     F1d, F2d = _features_to_device(F1), _features_to_device(F2)
-    plan = Plan(F1d.shape[1], F2d.shape[1], Lb, steps, weights)
+    plan = Plan(F1d.shape[1], F2d.shape[1], Lb, steps, weights, precision=precision)
     ranges = shard_tiles(tile_cells(plan.n1, plan.n2, plan.N, plan.M, Lb, plan.hop), ws)
     lo, hi = ranges[rank]
     # every rank reaches the status reduction, so that a failure on one rank

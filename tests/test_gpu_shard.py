@@ -82,12 +82,71 @@ def test_tile_sharded_pair_vs_oracle(oracle_mod, world, seed, n, m, Lb, wts):
     assert b1 == best and np.array_equal(wp1, wp)
 
 
+def _rank_main_fp32(rank, port, world, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    os.environ.setdefault("GLOO_SOCKET_IFNAME", "lo")
+    torch.cuda.set_device(0)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        rng = np.random.default_rng(17)
+        F1, F2 = W.warped_pair(rng, 1600, 1500, d=64, noise=0.1, latent="gaussian")
+        res = parflex_sharded(F1, F2, STD, WTS, 0.1, L=400, precision="fp32")
+        q.put((rank, None if res is None else (float(res[0]), res[1].tolist())))
+    except Exception as e:  # report instead of hanging the parent
+        q.put((rank, repr(e)))
+        raise
+    finally:
+        dist.destroy_process_group()
+
+
+def test_tile_sharded_fp32_form_vs_single_plan():
+    """The FP32 form sharded over two ranks equals one FP32-form plan."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main_fp32, args=(r, port, 2, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=600) for _ in procs)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0, got
+    assert got[1] is None
+    rng = np.random.default_rng(17)
+    F1, F2 = W.warped_pair(rng, 1600, 1500, d=64, noise=0.1, latent="gaussian")
+    p = Plan(F1.shape[1], F2.shape[1], 400, STD, WTS, precision="fp32")
+    p.load_features(torch.from_numpy(np.ascontiguousarray(F1)).cuda(),
+                    torch.from_numpy(np.ascontiguousarray(F2)).cuda())
+    p.run(None, 0.1)
+    best, _, _, n = p.result()
+    wp = p.path(n).T
+    assert got[0][0] == best
+    assert np.array_equal(np.asarray(got[0][1], dtype=np.int64), wp)
+    p.close()
+
+
 def test_tile_sharded_single_process_vs_oracle(oracle_mod):
     """Without a process group the whole pair is rank 0's shard."""
     F1, F2 = _pair(14, 1200, 1000)
     best, wp = parflex_sharded(F1, F2, STD, WTS, 0.1, L=300)
     ref = oracle_mod.parflex_full(W.cost_matrix_det(F1, F2), STD, WTS, 0.1, 300)
     assert best == ref["best_cost"] and np.array_equal(wp, ref["wp"])
+
+
+def _written_bp_words(plan, t):
+    """Indices of tile t's packed backpointer words that stage 1 writes: per
+    strip k, 16-step block p and lane, the (A, B) word pair of rows
+    64k + 2 lane (+1), for lanes whose first row is inside the tile."""
+    i, j = divmod(t, plan.n2)
+    R = min(plan.L, plan.N - i * plan.hop)
+    W_ = min(plan.L, plan.M - j * plan.hop)
+    nS = -(-R // 64)
+    nP = -(-(W_ + 63) // 16)
+    k, p, lane = np.meshgrid(np.arange(nS), np.arange(nP), np.arange(32), indexing="ij")
+    keep = 64 * k + 2 * lane < R
+    base = 2 * ((k * nP + p) * 32 + lane)[keep]
+    return np.sort(np.concatenate([base, base + 1]))
 
 
 def test_tile_range_plan_holds_its_tiles_only():
@@ -116,7 +175,9 @@ def test_tile_range_plan_holds_its_tiles_only():
     assert np.all(np.isinf(eD[:lo])) and np.all(eP[hi:] == 0)
     bw_p = part.host("BACKPTR").reshape(nt, -1)
     bw_f = full.host("BACKPTR").reshape(nt, -1)
-    assert np.array_equal(bw_p[lo:hi], bw_f[lo:hi])
+    for t in range(lo, hi):  # the words stage 1 writes (the rest is never read)
+        w = _written_bp_words(part, t)
+        assert np.array_equal(bw_p[t][w], bw_f[t][w]), t
     with pytest.raises(ValueError):
         Plan(100, 100, 50, STD, WTS).set_tile_range(2, 2)
     part.close()
