@@ -150,6 +150,26 @@ def test_shard_tiles_partition():
         shard_tiles(cells, 0)
 
 
+def test_shard_tiles_random_properties():
+    """Random tile sizes and rank counts: contiguous cover in order, rank 0
+    never empty, every share within one tile of the even split."""
+    rng = np.random.default_rng(8)
+    for _ in range(300):
+        nt = int(rng.integers(1, 60))
+        ws = int(rng.integers(1, 12))
+        cells = rng.integers(1, 10_000, nt).tolist()
+        rg = shard_tiles(cells, ws)
+        assert len(rg) == ws and rg[0][0] == 0 and rg[-1][1] == nt and rg[0][1] >= 1
+        assert all(a[1] == b[0] and a[0] <= a[1] for a, b in zip(rg, rg[1:]))
+        pre = np.concatenate([[0], np.cumsum(cells)])
+        for r in range(1, ws):  # each boundary within one tile of its share
+            b = rg[r][0]
+            target = pre[-1] * r / ws
+            lo = pre[b - 1] if b > 0 else 0
+            hi = pre[b + 1] if b < nt else pre[-1]
+            assert lo <= target <= hi or b == rg[r - 1][0] or b == 1
+
+
 @pytest.mark.parametrize("world,ranges", [(2, [(0, 3), (3, 7)]),
                                           (3, [(0, 2), (2, 2), (2, 7)])])
 def test_exchange_edges_and_backptr_gloo(world, ranges):
