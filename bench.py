@@ -296,7 +296,7 @@ def b200_arm(args, spec):
                 "traffic_source": "profiles/k_stage1_cl_ncu_small.md and "
                                   "k_stage1_v3_ncu_small.md (dram read+write per cell, both "
                                   "8.41-8.42 B; scaled by cells)",
-                "limiter": "instruction issue of the strip pipeline, not HBM: about 163 "
+                "limiter": "instruction issue of the strip pipeline, not HBM: about 310 "
                            "warp instructions per 64-cell warp-step, issue active 38 %, "
                            "FP64 pipe 14 % (profiles/k_stage1_cl_ncu_small.md); keeping "
                            "more warps active lengthened each step by as much as it saved"}
