@@ -51,6 +51,18 @@ namespace pfx {
 
 constexpr int kSpinLimit = 1 << 22;
 
+// Pulls the cost of a strip's next block of steps (kBlk steps x 32 lanes,
+// contiguous in the skewed slab) into L2 with one bulk prefetch, so that the
+// DP's own loads, two steps ahead, hit L2 instead of HBM.  Issued by one lane;
+// the range must lie inside the strip (the caller checks).
+template <typename V2>
+__device__ __forceinline__ void prefetch_next_block(const V2* strip, int tau_next) {
+    const V2* p = strip + (int64_t)tau_next * 32;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p),
+                 "r"((uint32_t)(kBlk * 32 * sizeof(V2)))
+                 : "memory");
+}
+
 // IEEE arithmetic of the DP's value type (FP64 plain form, FP32 chosen form),
 // rounded to nearest, never contracted.
 __device__ __forceinline__ double addr(double a, double b) { return __dadd_rn(a, b); }
@@ -467,6 +479,8 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW)
                 if (__shfl_sync(0xffffffffu, failed, 0)) break;  // to the tile barrier
                 const int tau0 = Tb - k * lag;
                 const V2* Cs = Ct + (int64_t)k * sc.span * 32 + lane;
+                if (lane == 0 && tau0 + 2 * kBlk <= sc.span)
+                    prefetch_next_block(Ct + (int64_t)k * sc.span * 32, tau0 + kBlk);
                 if (tau0 == 0) {
 #pragma unroll
                     for (int q = 0; q < 2; ++q) st.q[q] = __ldcs(Cs + q * 32);
@@ -622,6 +636,8 @@ __global__ void __launch_bounds__(kClW * 32, 1)
                 if (__shfl_sync(0xffffffffu, failed, 0)) break;  // to the tile's end barrier
                 const int tau0 = Tb - k * lag;
                 const V2* Cs = Ct + (int64_t)k * sc.span * 32 + lane;
+                if (lane == 0 && tau0 + 2 * kBlk <= sc.span)
+                    prefetch_next_block(Ct + (int64_t)k * sc.span * 32, tau0 + kBlk);
                 if (tau0 == 0) {
 #pragma unroll
                     for (int q = 0; q < 2; ++q) st.q[q] = __ldcs(Cs + q * 32);
