@@ -293,13 +293,13 @@ def b200_arm(args, spec):
                 "stage1_ms_per_launch": ms_s1,
                 "alg_bytes_per_cell": 8.25,
                 "fp64_dp_cells_per_s": cells / (ms_s1 / 1e3),
-                "traffic_source": "profiles/k_stage1_cl_ncu_small.md and "
-                                  "k_stage1_v3_ncu_small.md (dram read+write per cell, both "
-                                  "8.41-8.42 B; scaled by cells)",
-                "limiter": "instruction issue of the strip pipeline, not HBM: about 310 "
-                           "warp instructions per 64-cell warp-step, issue active 38 %, "
-                           "FP64 pipe 14 % (profiles/k_stage1_cl_ncu_small.md); keeping "
-                           "more warps active lengthened each step by as much as it saved"}
+                "traffic_source": "profiles/stage1_traffic.txt: dram read+write per cell of "
+                                  "k_stage1_cl (8.52 B, profiles/k_stage1_cl_ncu_small.md), "
+                                  "scaled by cells",
+                "limiter": "the strip pipeline, not HBM: each strip follows the one above "
+                           "it (producer waits dominate), about 300 warp instructions per "
+                           "64-cell warp-step at 40 % issue, FP64 pipe 15 % "
+                           "(profiles/k_stage1_cl_ncu_small.md)"}
 
     # --- row-major C input: the relayout into the tile-skewed layout --------
     C_dev = pf.cost_matrix_from_features_gpu(F1, F2)
