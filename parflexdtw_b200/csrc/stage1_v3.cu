@@ -238,20 +238,28 @@ struct Rings {
     int* BP;
 };
 
-// rg: the CTA's rings.  The producer warp's rings have the same layout and
-// start at rbase (rg.AD itself, or in a cluster the generic address of
-// another CTA's rings): a slot is read at rbase + its byte offset in rg, so
-// that the address derives from rbase alone.  bw (when non-null) receives
-// the block's backpointer word instead of the store to td.Bw.
+// rg: the CTA's rings.  A warp reads its producer's ring at rbase and
+// writes its own at wbase, both with rg's layout: rg.AD itself, or in a
+// cluster the generic address of the other CTA's rings.  A slot is accessed
+// at base + its byte offset in rg, so that the address derives from the base
+// alone.  bw (when non-null) receives the block's backpointer word instead of
+// the store to td.Bw.
 template <typename X, typename T>
 __device__ __forceinline__ X ring_at(const char* rbase, const Rings<T>& rg, const X* p) {
     return *reinterpret_cast<const X*>(
         rbase + (reinterpret_cast<const char*>(p) - reinterpret_cast<const char*>(rg.AD)));
 }
+template <typename X, typename T>
+__device__ __forceinline__ void ring_put(char* wbase, const Rings<T>& rg, const X* p, X v) {
+    *reinterpret_cast<X*>(wbase + (reinterpret_cast<const char*>(p) -
+                                   reinterpret_cast<const char*>(rg.AD))) = v;
+}
 
-template <bool EDGE, bool STD, typename T>
+// PUSH: the ring is written at wbase (generic address, a cluster peer's
+// shared memory possibly); otherwise straight into this CTA's rings.
+template <bool EDGE, bool STD, bool PUSH, typename T>
 __device__ __forceinline__ void run_block(const Geo& g, Wave<T>& st, const Rings<T>& rg,
-                                          const char* rbase,
+                                          const char* rbase, char* wbase,
                                           const typename Vec2<T>::type* __restrict__ Cs,
                                           int span, int tau0, int k, int R, int W, int lane,
                                           int prev_base, int mine_base, int rmask, int Tb,
@@ -345,13 +353,23 @@ __device__ __forceinline__ void run_block(const Geo& g, Wave<T>& st, const Rings
             if (lane == 31) {
                 if (actA) {
                     const int ws = mine_base + ((Tb + t - 62) & rmask);
-                    rg.AD[ws] = oAD;
-                    rg.AP[ws] = oAP;
+                    if (PUSH) {
+                        ring_put(wbase, rg, rg.AD + ws, oAD);
+                        ring_put(wbase, rg, rg.AP + ws, oAP);
+                    } else {
+                        rg.AD[ws] = oAD;
+                        rg.AP[ws] = oAP;
+                    }
                 }
                 if (actB) {
                     const int ws = mine_base + ((Tb + t - 63) & rmask);
-                    rg.BD[ws] = oBD;
-                    rg.BP[ws] = oBP;
+                    if (PUSH) {
+                        ring_put(wbase, rg, rg.BD + ws, oBD);
+                        ring_put(wbase, rg, rg.BP + ws, oBP);
+                    } else {
+                        rg.BD[ws] = oBD;
+                        rg.BP[ws] = oBP;
+                    }
                 }
             }
             bitsA |= (uint32_t)codeA << (2 * t);
@@ -487,11 +505,13 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW)
                 }
                 const bool interior = k >= 1 && k <= sc.nS - 2 && tau0 >= 80 && tau0 + 17 <= W;
                 if (interior)
-                    run_block<false, STD>(g, st, rg, reinterpret_cast<const char*>(rg.AD), Cs,
+                    run_block<false, STD, false>(g, st, rg, reinterpret_cast<const char*>(rg.AD),
+                                          reinterpret_cast<char*>(rg.AD), Cs,
                                           sc.span, tau0, k, R, W, lane,
                                           prevw * RB, warp * RB, RB - 1, Tb, lag, td, sc.nP);
                 else
-                    run_block<true, STD>(g, st, rg, reinterpret_cast<const char*>(rg.AD), Cs,
+                    run_block<true, STD, false>(g, st, rg, reinterpret_cast<const char*>(rg.AD),
+                                         reinterpret_cast<char*>(rg.AD), Cs,
                                          sc.span, tau0, k, R, W, lane,
                                          prevw * RB, warp * RB, RB - 1, Tb, lag, td, sc.nP);
             }
@@ -559,7 +579,12 @@ __global__ void __launch_bounds__(kClW * 32, 1)
     const int vw = rank * kClW + warp;
     const int pv = (vw + NWT - 1) % NWT, nv = (vw + 1) % NWT;
     // the producer's rings (generic address, this CTA's or the peer's)
-    const char* rbase = reinterpret_cast<const char*>(cl.map_shared_rank(rg.AD, pv / kClW));
+    // a warp writes its ring into its consumer's CTA (posted stores, off the
+    // dependency chain) and reads its producer's ring from its own CTA: ring
+    // region w of a CTA is written by warp w of the CTA that feeds it (its own
+    // warp w, or for w = kClW - 1 the other CTA's last warp)
+    const char* rbase = reinterpret_cast<const char*>(rg.AD);
+    char* wbase = reinterpret_cast<char*>(cl.map_shared_rank(rg.AD, nv / kClW));
     // cluster scope only where the neighbour is in the other CTA
     const bool prev_remote = pv / kClW != rank, next_remote = nv / kClW != rank;
     const bool read_remotely = warp == 0 || warp == kClW - 1;  // my progress word
@@ -644,11 +669,13 @@ __global__ void __launch_bounds__(kClW * 32, 1)
                 }
                 const bool interior = k >= 1 && k <= sc.nS - 2 && tau0 >= 80 && tau0 + 17 <= W;
                 if (interior)
-                    run_block<false, STD>(g, st, rg, rbase, Cs, sc.span, tau0, k, R, W, lane,
+                    run_block<false, STD, true>(g, st, rg, rbase, wbase, Cs, sc.span, tau0, k, R, W,
+                                          lane,
                                           (pv % kClW) * RB, warp * RB, RB - 1, Tb, lag, td,
                                           sc.nP, &bw);
                 else
-                    run_block<true, STD>(g, st, rg, rbase, Cs, sc.span, tau0, k, R, W, lane,
+                    run_block<true, STD, true>(g, st, rg, rbase, wbase, Cs, sc.span, tau0, k, R, W,
+                                         lane,
                                          (pv % kClW) * RB, warp * RB, RB - 1, Tb, lag, td,
                                          sc.nP, &bw);
             }
