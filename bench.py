@@ -294,11 +294,11 @@ def b200_arm(args, spec):
                 "alg_bytes_per_cell": 8.25,
                 "fp64_dp_cells_per_s": cells / (ms_s1 / 1e3),
                 "traffic_source": "profiles/stage1_traffic.txt: dram read+write per cell of "
-                                  "k_stage1_cl (8.52 B, profiles/k_stage1_cl_ncu_small.md), "
+                                  "k_stage1_cl (8.49 B, profiles/k_stage1_cl_ncu_small.md), "
                                   "scaled by cells",
                 "limiter": "the strip pipeline, not HBM: each strip follows the one above "
                            "it (producer waits dominate), about 300 warp instructions per "
-                           "64-cell warp-step at 40 % issue, FP64 pipe 15 % "
+                           "64-cell warp-step at 43 % issue, FP64 pipe 16 % "
                            "(profiles/k_stage1_cl_ncu_small.md)"}
 
     # --- row-major C input: the relayout into the tile-skewed layout --------
