@@ -527,9 +527,11 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW)
 // pipeline of a tile, so a tile takes about (nS - 1 + 32) / 32 strip times
 // instead of (nS - 1 + 16) / 16.  For alignments with fewer tiles than SMs.
 // Virtual warp v = 16 * rank + warp takes strips v, v + 32, ...; strip k + 1
-// reads strip k's last rows from its producer's ring -- in the other CTA's
-// shared memory (distributed shared memory) where v = 15 -> 16 or 31 -> 0 --
-// and the pairwise progress words are read and written at cluster scope.
+// reads strip k's last rows from a ring in its own CTA's shared memory.
+// Where producer and consumer sit in different CTAs (v = 15 -> 16 or
+// 31 -> 0) the producer writes that ring into the consumer's CTA
+// (distributed shared memory, posted stores off the dependency chain), and
+// the pairwise progress words are read and written at cluster scope.
 // Rank 0 claims the tiles; three cluster barriers per tile (claim, set-up,
 // end), which every thread of both CTAs reaches on every path: waits are
 // bounded and a warp that gives up goes on to the tile's end barrier.
