@@ -573,6 +573,9 @@ __global__ void __launch_bounds__(kClW * 32, 1)
     rg.BD = rg.AD + kClW * RB;
     rg.AP = reinterpret_cast<int*>(rg.BD + kClW * RB);
     rg.BP = rg.AP + kClW * RB;
+    // progress words: [w] warp w's; [kClW] the other CTA's last warp's (this
+    // CTA's warp 0 waits on it); [kClW + 1] the other CTA's warp 0's (this
+    // CTA's last warp waits on it) -- written by the other CTA, polled here
     int* prog = rg.BP + kClW * RB;
     __shared__ TileDesc td;
     __shared__ Sched2 s_sc;
@@ -590,6 +593,7 @@ __global__ void __launch_bounds__(kClW * 32, 1)
     // cluster scope only where the neighbour is in the other CTA
     const bool prev_remote = pv / kClW != rank, next_remote = nv / kClW != rank;
     const bool read_remotely = warp == 0 || warp == kClW - 1;  // my progress word
+    int* rprog = cl.map_shared_rank(prog, 1 - rank);  // the other CTA's words
     if (threadIdx.x == 0) s_abort = 0;
     cl.sync();  // both CTAs run before any access to the other's shared memory
     for (;;) {
@@ -606,7 +610,7 @@ __global__ void __launch_bounds__(kClW * 32, 1)
             s_sc = make_sched2(td.R, td.W, NWT);
             s_ttot = (s_sc.nS - 1) * s_sc.lag + s_sc.span;
         }
-        if (threadIdx.x < kClW) prog[threadIdx.x] = 0;
+        if (threadIdx.x < kClW + 2) prog[threadIdx.x] = 0;
         __syncthreads();
         if (rank == 0) {
             // edge rows past the tile's extent stay +inf / 0 (the DP writes the rest)
@@ -644,15 +648,13 @@ __global__ void __launch_bounds__(kClW * 32, 1)
                     // producer (strip k-1) has written every ring slot this block reads
                     if (k >= 1 &&
                         !(prev_remote
-                              ? wait_progress_cl(cl.map_shared_rank(prog, pv / kClW) + pv % kClW,
-                                                 Tb - lag + 78, &s_abort)
+                              ? wait_progress_cl(prog + kClW, Tb - lag + 78, &s_abort)
                               : wait_progress(prog + pv % kClW, Tb - lag + 78, &s_abort)))
                         failed = 1;
                     // consumer (strip k+1) has read every slot this block overwrites
                     if (!failed && k + 1 < sc.nS &&
                         !(next_remote
-                              ? wait_progress_cl(cl.map_shared_rank(prog, nv / kClW) + nv % kClW,
-                                                 Tb + lag - RB - 45, &s_abort)
+                              ? wait_progress_cl(prog + kClW + 1, Tb + lag - RB - 45, &s_abort)
                               : wait_progress(prog + nv % kClW, Tb + lag - RB - 45, &s_abort)))
                         failed = 1;
                     if (failed) {
@@ -685,7 +687,9 @@ __global__ void __launch_bounds__(kClW * 32, 1)
             // publish first: the backpointer store below is nobody's dependency
             if (lane == 31) {
                 if (read_remotely) {
+                    // also into the other CTA's copy, so that its reader polls locally
                     st_release_cluster(prog + warp, Tb + kBlk);
+                    st_release_cluster(rprog + (warp == 0 ? kClW + 1 : kClW), Tb + kBlk);
                 } else {
                     cuda::atomic_ref<int, cuda::thread_scope_block> a(prog[warp]);
                     a.store(Tb + kBlk, cuda::memory_order_release);
@@ -772,7 +776,7 @@ static cudaError_t launch_cl_t(const TileDesc* descs, int ntiles, int* head, con
     const int rb = ring_len(s.lag, kClW, limit, (int)sizeof(T));
     if (rb == 0) return cudaErrorInvalidValue;
     const size_t smem =
-        (size_t)kClW * rb * (2 * sizeof(T) + 2 * sizeof(int)) + kClW * sizeof(int);
+        (size_t)kClW * rb * (2 * sizeof(T) + 2 * sizeof(int)) + (kClW + 2) * sizeof(int);
     auto kern = k_stage1_cl<STD, T>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
@@ -808,7 +812,7 @@ static int cl_max_t(const Geo& g) {
     const int rb = ring_len(s.lag, kClW, limit, (int)sizeof(T));
     if (rb == 0) return 0;
     const size_t smem =
-        (size_t)kClW * rb * (2 * sizeof(T) + 2 * sizeof(int)) + kClW * sizeof(int);
+        (size_t)kClW * rb * (2 * sizeof(T) + 2 * sizeof(int)) + (kClW + 2) * sizeof(int);
     auto kern = k_stage1_cl<STD, T>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
