@@ -414,20 +414,22 @@ __global__ void k_stitch_chain(const Geo g, S2Buf b, int64_t start_i, int64_t st
 // end cell to its start cell (_nb_backtrace_within_chunk,
 // Parflex.py:977-1012), writing global points end-first.  The walk only
 // moves up and left, so the warp stages a 64-row x 64-column window of
-// backpointer words in registers (lane l holds rows w0+l and w0+32+l, five
-// 16-cell words each), anchored with the current cell at its bottom-right
-// corner, and reads each step's code with one shuffle; it reloads the window
-// (one coalesced round trip) only when the path leaves it, about every 32-63
-// steps, instead of one dependent global load per step.
-__device__ __forceinline__ uint32_t pick5(const uint32_t (&w)[5], int q) {
-    return q == 0 ? w[0] : q == 1 ? w[1] : q == 2 ? w[2] : q == 3 ? w[3] : w[4];
-}
+// backpointer words (rows w0+l and w0+32+l loaded by lane l, five 16-cell
+// words each) in its own shared memory, anchored with the current cell at
+// its bottom-right corner.  Every lane then follows the same path, reading
+// each step's word with one broadcast shared-memory load (no shuffle in the
+// step's dependency chain).  The window is reloaded (one coalesced round
+// trip) only when the path leaves it, about every 32-63 steps, instead of
+// one dependent global load per step.
+constexpr int kWalkThreads = 128;
 
-__global__ void k_stitch_walk(const Geo g, S2Buf b) {
+__global__ void __launch_bounds__(kWalkThreads) k_stitch_walk(const Geo g, S2Buf b) {
+    __shared__ uint32_t s_win[kWalkThreads / 32][64][5];  // per warp: window row x word
     const int n = *b.chain_len;
     const int lane = threadIdx.x & 31;
     const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (e >= n) return;
+    uint32_t (*win)[5] = s_win[threadIdx.x >> 5];
     const int32_t* E = b.chain + e * 12;
     const int32_t ti = E[0], tj = E[1];
     int32_t r = E[4], c = E[5];
@@ -439,8 +441,6 @@ __global__ void k_stitch_walk(const Geo g, S2Buf b) {
     const int64_t max_iters = (int64_t)R + W;
     bool done = false;
     int32_t w0r = -1, w0c = 0;  // window origin (row, column); -1 = empty
-    uint32_t wa[5], wb[5];      // words of rows w0r+lane and w0r+32+lane
-    int32_t pa = 0, pbw = 0;    // first period held for each of the two rows
     for (int64_t it = 0; it < max_iters; ++it) {
         if (lane == 0) { out[2 * k] = r + gro; out[2 * k + 1] = c + gco; }
         ++k;
@@ -448,26 +448,25 @@ __global__ void k_stitch_walk(const Geo g, S2Buf b) {
         if (w0r < 0 || r < w0r || c < w0c) {
             w0r = r - 63 > 0 ? r - 63 : 0;
             w0c = c - 63 > 0 ? c - 63 : 0;
-            const int32_t ra = w0r + lane, rb = w0r + 32 + lane;
-            pa = (w0c + (ra & 63)) >> 4;
-            pbw = (w0c + (rb & 63)) >> 4;
+            __syncwarp();  // every lane is done with the previous window
 #pragma unroll
-            for (int q = 0; q < 5; ++q) {
-                wa[q] = (ra < R && pa + q < nP) ? __ldg(slab + bp_word_index2(W, ra, (pa + q) << 4))
+            for (int h = 0; h < 2; ++h) {
+                const int32_t ra = w0r + 32 * h + lane;
+                const int32_t pa = (w0c + (ra & 63)) >> 4;  // first period held for row ra
+#pragma unroll
+                for (int q = 0; q < 5; ++q)
+                    win[32 * h + lane][q] =
+                        (ra < R && pa + q < nP) ? __ldg(slab + bp_word_index2(W, ra, (pa + q) << 4))
                                                 : 0u;
-                wb[q] = (rb < R && pbw + q < nP) ? __ldg(slab + bp_word_index2(W, rb, (pbw + q) << 4))
-                                                 : 0u;
             }
+            __syncwarp();
         }
-        // lane holding row r, and the word / bit of column c within that row
-        const int32_t dr = r - w0r;
-        const int src = dr & 31;
-        const bool hi = dr >= 32;
-        const int32_t my_row = w0r + (hi ? 32 : 0) + lane;
-        const int32_t tau = c + (my_row & 63);
-        const uint32_t mine = hi ? pick5(wb, (tau >> 4) - pbw) : pick5(wa, (tau >> 4) - pa);
-        const uint32_t word = __shfl_sync(0xffffffffu, mine, src);
-        const int code = (int)((word >> (((c + (r & 63)) & 15) * 2)) & 3u);
+        // word of cell (r, c): row r - w0r (0..63) of the window, period
+        // (c + rho) / 16 counted from the row's first period (w0c + rho) / 16,
+        // rho = r mod 64 (0..4, since c - w0c is 0..63)
+        const int32_t rr = r & 63;
+        const uint32_t word = win[r - w0r][((c + rr) >> 4) - ((w0c + rr) >> 4)];
+        const int code = (int)((word >> (((c + rr) & 15) * 2)) & 3u);
         if (code >= g.S) { done = false; break; }
         const int kd = code == 0 ? g.kind[0] : (code == 1 ? g.kind[1] : g.kind[2]);
         const int32_t pr = r - (kd == 2 ? 2 : 1), pc = c - (kd == 1 ? 2 : 1);
@@ -603,7 +602,7 @@ cudaError_t launch_stitch(const Geo& g, const S2Buf& b, cudaStream_t st, int fro
                           int64_t si, int64_t sj, int64_t se, int64_t sx) {
     cudaError_t e;
     if ((e = launch_stitch_chain(g, b, st, from_best, si, sj, se, sx)) != cudaSuccess) return e;
-    k_stitch_walk<<<26, 128, 0, st>>>(g, b);  // one warp per chain entry (<= 101)
+    k_stitch_walk<<<26, kWalkThreads, 0, st>>>(g, b);  // one warp per chain entry (<= 101)
     count_launches(1);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     k_stitch_concat<<<1, 1024, 0, st>>>(b);
