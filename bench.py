@@ -1,23 +1,33 @@
 #!/usr/bin/env python
 """ParFlex alignment benchmark (one JSON line on rank 0).
 
-Workload (default): one long synthetic chroma pair, 30000 x ~37000 frames
-(12-d Dirichlet frames, random monotone warp, 0-10 % unrelated padding per
-end), L = 4000 tiles, steps {(1,1),(1,2),(2,1)}, weights {2,3,3}, beta 0.1,
-plain FP64 form with a bit-exact path.  One step = one full ParFlex
-alignment of that pair: stage 1 over all 80 tiles, stage-2 propagation,
-overlap sync, edge scan and stitched backtrace.
+Workload (default, ``--workload prune64``): 64 synthetic chroma pairs,
+N ~ U(40000, 60000) frames, M = N x U(0.7, 1.4) (12-d Dirichlet frames,
+random monotone warp, 0-10 % unrelated padding per end), L = 2000 tiles,
+steps {(1,1),(1,2),(2,1)}, weights {2,3,3}, beta 0.1.  One step aligns all 64
+pairs with the chosen exact form: the learned tile proposer picks the tiles,
+stage 1 (FP64 DP) runs on those only, stage 2 per pair, and a pair whose
+path comes near a pruned tile gets those tiles added or falls back to the
+full-tile method.  The judge is the plain full-tile FP64 form on the same
+pairs (timed as ``plain_fp64_full_tiles``); ``exact_paths`` counts the pairs
+whose best cost and path equal its own.
 
-  value     DP cells/s over the timed steps with C already in HBM
-  e2e       the same metric through the public API from HOST features
-            (tiled_stage1_from_features + run_stage2_from_tiled): feature
-            upload, device cost matrix, both stages, path download
-  roofline  the stage-1 kernel: algorithmic bytes (8 B of C read + 0.25 B of
-            backpointers per cell) / its CUDA-event time vs measured HBM peak
+  value     DP cells/s, counting every cell of the full tiling (work the
+            proposer avoids counts as throughput), features in HBM
+  e2e       the same metric through PrunedBatch.load + run from pinned HOST
+            features, paths and costs read back every step
+  roofline  the masked run's stage-1 kernel: algorithmic bytes of the kept
+            tiles (8 B of cost + 0.25 B of backpointers per cell) / its
+            CUDA-event time vs the measured HBM peak, plus its issue roof
   cpu_baseline  the C restatement of the reference (oracle/) on the host
-            cores, on the same pair, with all host threads
+            cores, full tiling, on a block of whole tiles of the first pair
+            whose tile count is a multiple of the host threads
 
-Multi-GPU (torchrun, one rank per GPU): every rank aligns its own pair
+Other workloads: ``config1`` (one 30000 x 37001 pair, L = 4000, plain FP64),
+``batch256``, ``precision2048`` (FP32 form vs FP64 form), ``config0`` and the
+small profiling cases.
+
+Multi-GPU (torchrun, one rank per GPU): every rank aligns its own pairs
 (independent replicas, weak scaling, no data-path collective); the time is
 the max over ranks.
 
@@ -130,9 +140,11 @@ def reference_arm(args, spec):
     build_oracle.build()
     threads = os.cpu_count() or 1
     F1, F2 = W.make_pair(spec)
-    # bounded sample: the first `rows` tile rows of the pair, full width
+    # the whole pair (every tile), or its first `ref_tile_rows` tile rows
     hop = spec.L - 1
-    rows = min(F1.shape[1], args.ref_tile_rows * hop + 1)
+    N, M = F1.shape[1], F2.shape[1]
+    rows = F1.shape[1] if args.ref_tile_rows <= 0 else \
+        min(F1.shape[1], args.ref_tile_rows * hop + 1)
     C = W.cost_matrix_host(F1[:, :rows], F2)
     cells, n1, n2 = tile_cells(C.shape[0], C.shape[1], spec.L)
     times = []
@@ -144,10 +156,10 @@ def reference_arm(args, spec):
             times.append(dt)
     tot = sum(times)
     v = cells * len(times) / tot
-    N, M = F1.shape[1], F2.shape[1]
     full_cells, _, _ = tile_cells(N, M, spec.L)
-    sample = (f"first {n1} tile rows of the pair ({C.shape[0]} x {C.shape[1]}, {n1 * n2} "
-              f"tiles, {cells} cells) per step, all stages")
+    what = "the whole pair" if rows == N else f"the first {n1} tile rows of the pair"
+    sample = (f"{what} ({C.shape[0]} x {C.shape[1]}, {n1 * n2} tiles, {cells} cells) per "
+              f"step, all stages")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
@@ -797,25 +809,61 @@ def precision_arm(args, spec):
         dist.destroy_process_group()
 
 
-PRUNE_METRIC = ("DP cells/s and pairs/s (ParFlex, learned tile pruning + FP64 DP vs the "
-                "full-tile FP64 form; cells counted on the full tiling)")
+# BASELINE's metric, measured on the learned-pruning workload: the chosen exact
+# form (learned tile pruning + FP64 DP) against the plain full-tile FP64 form;
+# cells are counted on the full tiling.
+PRUNE_METRIC = "DP cells/s and pairs/s: chosen form vs plain GPU at exact-path agreement"
+
+
+def _balanced_tile_block(N, M, Lb, threads, rounds):
+    """(n1s, n2s): a block of whole L x L tiles at the start of an N x M pair
+    whose tile count is a multiple of `threads` (every host thread gets the
+    same number of equal tiles) and close to rounds x threads."""
+    hop = Lb - 1
+    max1, max2 = max((N - 1) // hop, 1), max((M - 1) // hop, 1)
+    target = rounds * threads
+    best = None
+    for a in range(1, max1 + 1):
+        for b in range(1, max2 + 1):
+            t = a * b
+            key = (t % threads != 0, abs(t - target), abs(a - b))
+            if best is None or key < best[0]:
+                best = (key, a, b)
+    return best[1], best[2]
+
+
+def _prune_cpu_sample(spec, threads, rounds):
+    """Cost matrix of a bounded CPU sample of the learned-pruning workload:
+    the leading block of whole tiles of its first pair (same generator and
+    seed), with a tile count that is a multiple of the host threads, so
+    that no thread idles while others work.  Returns (C, cells, text)."""
+    Lb = spec.L_choices[0]
+    F1, F2 = W.make_batch(W.BatchSpec("x", 1, spec.n_lo, spec.n_hi, pad_frac=spec.pad_frac,
+                                      seed=spec.seed))[0]
+    N, M = F1.shape[1], F2.shape[1]
+    a, b = _balanced_tile_block(N, M, Lb, threads, rounds)
+    rows, cols = a * (Lb - 1) + 1, b * (Lb - 1) + 1
+    C = W.cost_matrix_host(F1[:, :rows], F2[:, :cols])
+    cells = tile_cells(rows, cols, Lb)[0]
+    text = (f"the leading {a} x {b} block of whole {Lb} x {Lb} tiles ({a * b} tiles on "
+            f"{threads} threads, {rows} x {cols} frames, {cells} cells) of the workload's "
+            f"first pair ({N} x {M}), full tiling, FP64, all stages, cost matrix built "
+            f"outside the timing")
+    return C, cells, text
 
 
 def prune_reference_arm(args, spec):
-    """CPU restatement on the first tile rows of the first pair."""
+    """The C restatement of the reference on the host cores, full tiling (the
+    reference has no pruning), on a balanced block of whole tiles of the
+    workload's first pair per step."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
     from oracle import build_oracle, oracle
     build_oracle.build()
     threads = os.cpu_count() or 1
-    rng_pairs = W.make_batch(W.BatchSpec("x", 1, spec.n_lo, spec.n_hi, pad_frac=spec.pad_frac,
-                                         seed=spec.seed))
-    F1, F2 = rng_pairs[0]
     Lb = spec.L_choices[0]
-    rows = min(F1.shape[1], args.ref_tile_rows * (Lb - 1) + 1)
-    C = W.cost_matrix_host(F1[:, :rows], F2)
-    cells, n1, n2 = tile_cells(C.shape[0], C.shape[1], Lb)
+    C, cells, sample = _prune_cpu_sample(spec, threads, args.ref_rounds)
     times = []
     for s_ in range(args.warmup + args.steps):
         t0 = time.perf_counter()
@@ -831,11 +879,48 @@ def prune_reference_arm(args, spec):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": dict(spec.describe(), parallelism="replicas"),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"the first {n1} tile rows of the first pair ({C.shape[0]} x "
-                                   f"{C.shape[1]}, {cells} cells) per step, full tiling, FP64"},
+                         "sample": sample + " per step"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def _stage1_counters(workload):
+    """Per-cell DRAM bytes and warp instructions of the stage-1 kernel, from
+    the committed ncu summary (profiles/stage1_counters.txt), for the named
+    workload; {} when absent."""
+    p = os.path.join(ROOT, "profiles", "stage1_counters.txt")
+    out, cur = {}, None
+    if not os.path.exists(p):
+        return out
+    with open(p) as fp:
+        for line in fp:
+            line = line.split("#", 1)[0].strip()
+            if not line or "=" not in line:
+                continue
+            k, v = (x.strip() for x in line.split("=", 1))
+            if k == "workload":
+                cur = v
+            elif cur == workload:
+                try:
+                    out[k] = float(v)
+                except ValueError:
+                    out[k] = v
+    return out
+
+
+def _masked_cells(masks, shapes, Lb):
+    """DP cells of the tiles a concatenation of per-pair (n1, n2) masks keeps."""
+    hop = Lb - 1
+    tot, off = 0, 0
+    for N, M in shapes:
+        n1, n2 = -(-(N - 1) // hop), -(-(M - 1) // hop)
+        rows = np.minimum(Lb, N - np.arange(n1) * hop).astype(np.int64)
+        cols = np.minimum(Lb, M - np.arange(n2) * hop).astype(np.int64)
+        m = np.asarray(masks[off:off + n1 * n2], bool).reshape(n1, n2)
+        tot += int(rows @ m.astype(np.int64) @ cols)
+        off += n1 * n2
+    return tot
 
 
 def prune_arm(args, spec):
@@ -918,6 +1003,7 @@ def prune_arm(args, spec):
     launches = lib.pfx_kernel_launches() - launches0
     ms_pruned = max_ranks(ms_pruned)
     _, prof = pb.run(spec.beta, profile=True)
+    kept_cells = _masked_cells(pb.last_masks.cpu().numpy(), shapes, Lb)
     agree = sum(int(bc == best0[i] and np.array_equal(wp, paths0[i].T))
                 for i, (bc, wp) in enumerate(out))
     # e2e: pinned host features in, results out
@@ -967,6 +1053,54 @@ def prune_arm(args, spec):
 
     v_pruned = cells * ws * args.steps / (ms_pruned / 1e3)
     v_plain = cells * ws * args.plain_steps / (ms_plain / 1e3)
+    clocks = clk.summary()
+
+    # --- roofline of the masked run's stage-1 kernel (kept tiles only) -------
+    peak, peak_kind = load_peaks()
+    s1_ms = prof["align_ms"]["stage1"]
+    ctr = _stage1_counters(spec.name)
+    achieved = kept_cells * 8.25 / (s1_ms / 1e3) / 1e9
+    roofline = {
+        "bound": "hbm", "kernel": "k_stage1_v3<NW, 1, double> (tile queue, kept tiles of all "
+                                  "pairs of a wave)",
+        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+        "traffic": kept_cells * ctr["dram_bytes_per_cell"] if "dram_bytes_per_cell" in ctr
+        else None,
+        "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per DP cell of "
+                           "the same kernel on the small case of this workload "
+                           "(profiles/stage1_counters.txt), times the kept cells"),
+        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+        if peak_kind == "measured" else "fallback",
+        "alg_bytes_per_cell": 8.25, "kept_cells": kept_cells, "stage1_ms": s1_ms,
+        "fp64_dp_cells_per_s": kept_cells / (s1_ms / 1e3)}
+    if "inst_per_cell" in ctr and clocks.get("sm_mhz"):
+        smsp = 4 * torch.cuda.get_device_properties(dev).multi_processor_count
+        inst = ctr["inst_per_cell"] * kept_cells / (s1_ms / 1e3)
+        issue_peak = smsp * clocks["sm_mhz"] * 1e6
+        roofline["issue"] = {
+            "achieved_warp_inst_per_s": inst, "peak_warp_inst_per_s": issue_peak,
+            "frac": inst / issue_peak, "warp_inst_per_cell": ctr["inst_per_cell"],
+            "source": "smsp__inst_executed.sum per DP cell (profiles/stage1_counters.txt); "
+                      "peak = one warp instruction per SMSP per cycle at the median SM clock "
+                      "sampled during the timed region"}
+
+    # --- CPU baseline (rank 0): the oracle on a balanced sample -------------
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import build_oracle, oracle
+        build_oracle.build()
+        threads = os.cpu_count() or 1
+        C, scells, sample = _prune_cpu_sample(spec, threads, args.ref_rounds)
+        ts = []
+        for _ in range(args.cpu_repeats):
+            t0 = time.perf_counter()
+            oracle.parflex_full(C, spec.steps, spec.weights, spec.beta, Lb, threads=threads)
+            ts.append(time.perf_counter() - t0)
+        del C
+        cpu = {"value": scells / statistics.median(ts), "unit": UNIT, "cores": threads,
+               "kind": "port", "sample": f"{sample}; median of {len(ts)} runs",
+               "seconds": ts}
+
     if rank == 0:
         line = {
             "metric": PRUNE_METRIC, "value": v_pruned, "unit": UNIT, "n_gpus": ws,
@@ -980,6 +1114,7 @@ def prune_arm(args, spec):
                                   "read-back and fallback checks included)",
                            l2="cost slabs larger than L2 (no flush needed)"),
             "pairs_per_s": ws * n_pairs * args.steps / (ms_pruned / 1e3),
+            "exact_paths": f"{agree}/{n_pairs}",
             "plain_fp64_full_tiles": {
                 "value": v_plain, "unit": UNIT, "steps": args.plain_steps,
                 "ms_per_step": ms_plain / args.plain_steps,
@@ -1003,11 +1138,12 @@ def prune_arm(args, spec):
                 "skipped_fraction": info32["skipped_fraction"],
                 "fallbacks": info32["fallbacks"],
                 "form": "same proposer; BF16 tcgen05 cost GEMM, FP32 DP"},
+            "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": cells * ws * args.e2e_steps / (ms_e2e / 1e3), "unit": UNIT,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "steps": args.e2e_steps, "ms_per_step": ms_e2e / args.e2e_steps,
                     "api": "PrunedBatch.load (pinned host features) + run"},
-            "gpu_launches": int(launches), "clocks": clk.summary(),
+            "gpu_launches": int(launches), "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -1021,9 +1157,11 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="config1", choices=sorted(W.WORKLOADS))
+    ap.add_argument("--workload", default="prune64", choices=sorted(W.WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--ref-tile-rows", type=int, default=2)
+    ap.add_argument("--ref-tile-rows", type=int, default=0,
+                    help="single-pair workloads: tile rows the reference arm times "
+                         "(0 = the whole pair)")
     ap.add_argument("--ref-batch-cells", type=float, default=3e9,
                     help="batch workloads: tile cells of the leading pairs the CPU times")
     ap.add_argument("--pairs", type=int, default=None,
@@ -1034,6 +1172,10 @@ def main():
                     help="precision workload: pairs whose full cost matrices are compared")
     ap.add_argument("--ref-pairs", type=int, default=8,
                     help="precision workload: pairs the CPU oracle times")
+    ap.add_argument("--ref-rounds", type=int, default=8,
+                    help="learned-pruning workload: tiles per host thread in the CPU sample")
+    ap.add_argument("--cpu-repeats", type=int, default=3,
+                    help="learned-pruning workload: timed runs of the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     spec = W.WORKLOADS[args.workload]

@@ -264,8 +264,9 @@ int pfx_flexdtw_tile(const double *C, int64_t ldc, int32_t R, int32_t W,
  * a host that reserves all device memory up front).  R and W at most 2048,
  * else PFX_ERR_TOO_LARGE.  All calls on a device share the array: calls that
  * overlap on the GPU race on it, so order them on one stream.  The first call
- * on each device looks up the array's address; make it before any stream
- * capture.  No counterpart in the reference. */
+ * on each device (and in each new CUDA context of it, e.g. after a device
+ * reset) looks up the array's address; make it before any stream capture.
+ * No counterpart in the reference. */
 int pfx_flexdtw_tile_noalloc(const double *C, int64_t ldc, int32_t R, int32_t W,
                              const int64_t *steps, const double *weights,
                              int32_t n_steps, double *D, int32_t *P, int8_t *B,

@@ -23,7 +23,10 @@
 //     ordering) race on it.  Order such calls on one stream.
 //   * The first call on each device looks up the array's device address
 //     (cudaGetSymbolAddress, with that device current) and caches it; make
-//     that first call before any stream capture.
+//     that first call before any stream capture.  The cache is keyed on the
+//     CUDA context's unique id as well as the device, so a call made after a
+//     device reset, or under another context of the same device, looks the
+//     address up again in the context it runs in.
 #include <cstring>
 #include <mutex>
 
@@ -44,6 +47,24 @@ constexpr size_t kScratchBytes = kEdgeDBytes + kEdgePBytes + kBWordBytes;
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
 void* g_scratch_addr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};  // context id the address belongs to
+
+// Unique id of the calling thread's current context (never reused within a
+// process, unlike a context handle), through the driver entry point the
+// runtime hands out; false when no context is current or the driver lacks
+// the call.
+bool current_context_id(unsigned long long* id) {
+    using CtxGetId = CUresult (*)(CUcontext, unsigned long long*);
+    static CtxGetId fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<CtxGetId>(p);
+    }();
+    return fn && fn(nullptr, id) == CUDA_SUCCESS;
+}
 
 }  // namespace
 
@@ -54,7 +75,8 @@ static __device__ __align__(256) unsigned char g_tile_scratch[kScratchBytes];
 
 namespace {
 // Device address of g_tile_scratch on the current device (looked up once per
-// device, under a lock, with that device current).
+// device and context, under a lock, with that device current; without a
+// context id from the driver it is looked up on every call).
 int scratch_address(void** out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
@@ -62,15 +84,24 @@ int scratch_address(void** out) {
     if (dev < 0 || dev >= kMaxDevices)
         return pfx::report_status(PFX_ERR_ARG, "device ordinal beyond the scratch table");
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_tile_scratch);
-        if (e != cudaSuccess || !p)
-            return pfx::report_status(PFX_ERR_CUDA, e != cudaSuccess ? cudaGetErrorString(e)
-                                                                     : "null scratch address");
-        g_scratch_addr[dev] = p;
+    unsigned long long ctx = 0;
+    const bool have_ctx = current_context_id(&ctx);
+    if (have_ctx && g_scratch_addr[dev] && g_scratch_ctx[dev] == ctx) {
+        *out = g_scratch_addr[dev];
+        return PFX_OK;
     }
-    *out = g_scratch_addr[dev];
+    // first call in this context (the lookup also makes the device's primary
+    // context current when the thread had none)
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_tile_scratch);
+    if (e != cudaSuccess || !p)
+        return pfx::report_status(PFX_ERR_CUDA, e != cudaSuccess ? cudaGetErrorString(e)
+                                                                 : "null scratch address");
+    if (have_ctx || current_context_id(&ctx)) {
+        g_scratch_addr[dev] = p;
+        g_scratch_ctx[dev] = ctx;
+    }
+    *out = p;
     return PFX_OK;
 }
 

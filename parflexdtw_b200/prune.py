@@ -382,6 +382,7 @@ class PrunedBatch:
         for st in self._streams:
             main.wait_stream(st)
         mark("proposer")
+        self.last_masks = masks  # the proposed tiles, pairs' (n1, n2) masks concatenated
         b.set_masks(masks)
         mark("set_masks")
         b.run(beta, use_graph=False)

@@ -2,7 +2,9 @@
 
 Run in a checkout that has the reference next to it (read-only):
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference checkout>
+
+(or set PARFLEX_REFERENCE to the checkout's path instead of passing --ref).
 
 The reference (``FlexDTW.py``, ``Parflex.py``) is Python + Numba.  It imports
 matplotlib and plotly at module top for its plotting helpers; neither is
@@ -213,8 +215,11 @@ def stage2_cases(Parflex):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("PARFLEX_REFERENCE"),
+                    help="path of the reference checkout (default: $PARFLEX_REFERENCE)")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give the reference checkout with --ref or PARFLEX_REFERENCE")
     FlexDTW, Parflex = _import_reference(args.ref)
     for name, d in tile_cases(FlexDTW).items():
         np.savez_compressed(os.path.join(HERE, f"tile_{name}.npz"), **d)

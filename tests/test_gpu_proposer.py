@@ -296,3 +296,45 @@ def test_batch_masks_and_pruned_batch_exact(oracle_mod):
             assert bc == r["best_cost"] and np.array_equal(wp, r["wp"])
         assert (info["fallbacks"] == 3) == (thr > 0)
         pb.close()
+
+
+def test_trained_proposer_gain_on_held_out_pairs():
+    """What the shipped, trained network gains over the method without it.
+
+    Held-out pairs (a seed outside the training seeds 12345..17344 of
+    train_proposer.py, drawn like the training pairs: N ~ U(20000, 30000),
+    M = N x U(0.7, 1.4), 0-10 % unrelated padding per end), L = 2000.  The
+    full-tile FP64 method is the judge: every pruned result must equal its
+    best cost and path bit for bit.  The trained proposer must skip more than
+    half of the tiles, counting every tile its expansions and fallbacks ran;
+    an untrained network of the same layout at the same threshold, which the
+    same fallback keeps exact, must run more tiles than the trained one."""
+    from parflexdtw_b200.batch import Batch
+    from parflexdtw_b200.train_proposer import make_pairs
+    L = 2000
+    pairs = make_pairs(8, 90210, lo=20000, hi=30000)
+    shapes = [(F1.shape[1], F2.shape[1]) for F1, F2 in pairs]
+    full = Batch(shapes, L, STD, WTS, 12)
+    full.load(pairs)
+    full.run(0.1, use_graph=False)
+    best, end, lens = full.results()
+    paths = full.paths(lens)
+    full.close()
+    assert end[:, 6].all()
+    trained = TileProposer.load()
+    runs = {}
+    for name, net in (("trained", trained), ("untrained", TileProposer(seed=3))):
+        pb = pf.PrunedBatch(shapes, L, STD, WTS, 12, proposer=net, threshold=trained.threshold)
+        pb.load(pairs)
+        out, info = pb.run(0.1)
+        pb.close()
+        for i, (bc, wp) in enumerate(out):
+            assert bc == best[i] and np.array_equal(wp, paths[i].T), (name, i, info)
+        runs[name] = info
+    t, u = runs["trained"], runs["untrained"]
+    print(f"trained: {t['tiles_run']}/{t['tiles_total']} tiles run, proposed "
+          f"{t['tiles_proposed']}, {t['expanded']} expanded, {t['fallbacks']} fallbacks; "
+          f"untrained: {u['tiles_run']} tiles run, {u['fallbacks']} fallbacks")
+    assert t["skipped_fraction"] > 0.5, t
+    assert t["tiles_run"] < 0.5 * t["tiles_total"], t
+    assert u["tiles_run"] > t["tiles_run"], (t, u)
