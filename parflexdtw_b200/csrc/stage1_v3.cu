@@ -230,16 +230,24 @@ struct Wave {
     typename Vec2<T>::type q[2];     // cost queue, step tau in slot tau & 1
 };
 
+// Per-warp rings of a strip's last two rows, [NW][RB] slots.  Slot s of a
+// ring holds row 64k+63 ("B") at the strip's local step s+63 and row 64k+62
+// ("A") at step s+62, the pair the next strip's lane 0 reads at once: D as
+// one {B, A} vector and the start encodings as one {B, A} int2, so a read is
+// two shared-memory loads and a write two stores (lane 31 writes A one step
+// late, together with B).
 template <typename T>
 struct Rings {
-    T* AD;  // [NW][RB] row 64k+62 of each warp's strips
-    T* BD;  // row 64k+63
-    int* AP;
-    int* BP;
+    typename Vec2<T>::type* D;  // {D of row 64k+63, D of row 64k+62}
+    int2* P;                    // {P of row 64k+63, P of row 64k+62}
 };
+template <typename T>
+__host__ __device__ constexpr int ring_slot_bytes() {
+    return (int)(sizeof(typename Vec2<T>::type) + sizeof(int2));
+}
 
 // rg: the CTA's rings.  A warp reads its producer's ring at rbase and
-// writes its own at wbase, both with rg's layout: rg.AD itself, or in a
+// writes its own at wbase, both with rg's layout: rg.D itself, or in a
 // cluster the generic address of the other CTA's rings.  A slot is accessed
 // at base + its byte offset in rg, so that the address derives from the base
 // alone.  bw (when non-null) receives the block's backpointer word instead of
@@ -247,12 +255,19 @@ struct Rings {
 template <typename X, typename T>
 __device__ __forceinline__ X ring_at(const char* rbase, const Rings<T>& rg, const X* p) {
     return *reinterpret_cast<const X*>(
-        rbase + (reinterpret_cast<const char*>(p) - reinterpret_cast<const char*>(rg.AD)));
+        rbase + (reinterpret_cast<const char*>(p) - reinterpret_cast<const char*>(rg.D)));
 }
 template <typename X, typename T>
 __device__ __forceinline__ void ring_put(char* wbase, const Rings<T>& rg, const X* p, X v) {
     *reinterpret_cast<X*>(wbase + (reinterpret_cast<const char*>(p) -
-                                   reinterpret_cast<const char*>(rg.AD))) = v;
+                                   reinterpret_cast<const char*>(rg.D))) = v;
+}
+template <typename T>
+__device__ __forceinline__ typename Vec2<T>::type make_v2(T x, T y) {
+    typename Vec2<T>::type v;
+    v.x = x;
+    v.y = y;
+    return v;
 }
 
 // PUSH: the ring is written at wbase (generic address, a cluster peer's
@@ -287,14 +302,13 @@ __device__ __forceinline__ void run_block(const Geo& g, Wave<T>& st, const Rings
             {
                 // every lane reads the same slot (a broadcast); lane 0 keeps it
                 const int rs = prev_base + ((Tb + t - lag - 1) & rmask);
-                const T rBD = ring_at(rbase, rg, rg.BD + rs), rAD = ring_at(rbase, rg, rg.AD + rs);
-                const int rBP = ring_at(rbase, rg, rg.BP + rs);
-                const int rAP = ring_at(rbase, rg, rg.AP + rs);
+                const V2 rD = ring_at(rbase, rg, rg.D + rs);
+                const int2 rP = ring_at(rbase, rg, rg.P + rs);
                 if (lane == 0) {
-                    x1D = rBD;
-                    x1P = rBP;
-                    x3D = rAD;
-                    x3P = rAP;
+                    x1D = rD.x;
+                    x1P = rP.x;
+                    x3D = rD.y;
+                    x3P = rP.y;
                 }
             }
             const T x2D = st.xpD;
@@ -350,26 +364,16 @@ __device__ __forceinline__ void run_block(const Geo& g, Wave<T>& st, const Rings
                 if (actA && cA == W - 1) { eD[td.L + rA] = (double)oAD; eP[td.L + rA] = oAP; }
                 if (actB && cB == W - 1) { eD[td.L + rB] = (double)oBD; eP[td.L + rB] = oBP; }
             }
-            if (lane == 31) {
-                if (actA) {
-                    const int ws = mine_base + ((Tb + t - 62) & rmask);
-                    if (PUSH) {
-                        ring_put(wbase, rg, rg.AD + ws, oAD);
-                        ring_put(wbase, rg, rg.AP + ws, oAP);
-                    } else {
-                        rg.AD[ws] = oAD;
-                        rg.AP[ws] = oAP;
-                    }
-                }
-                if (actB) {
-                    const int ws = mine_base + ((Tb + t - 63) & rmask);
-                    if (PUSH) {
-                        ring_put(wbase, rg, rg.BD + ws, oBD);
-                        ring_put(wbase, rg, rg.BP + ws, oBP);
-                    } else {
-                        rg.BD[ws] = oBD;
-                        rg.BP[ws] = oBP;
-                    }
+            if (lane == 31 && actB) {
+                // B of this step and A of the previous one (the same column,
+                // active whenever B is): slot (step - 63)
+                const int ws = mine_base + ((Tb + t - 63) & rmask);
+                if (PUSH) {
+                    ring_put(wbase, rg, rg.D + ws, make_v2<T>(oBD, st.aD1));
+                    ring_put(wbase, rg, rg.P + ws, make_int2(oBP, st.aP1));
+                } else {
+                    rg.D[ws] = make_v2<T>(oBD, st.aD1);
+                    rg.P[ws] = make_int2(oBP, st.aP1);
                 }
             }
             bitsA |= (uint32_t)codeA << (2 * t);
@@ -385,6 +389,186 @@ __device__ __forceinline__ void run_block(const Geo& g, Wave<T>& st, const Rings
     if (bw) {
         *bw = make_uint2(bitsA, bitsB);
     } else if (rA < R) {
+        uint2* Bt = reinterpret_cast<uint2*>(td.Bw);
+        Bt[((int64_t)k * nP + (tau0 >> 4)) * 32 + lane] = make_uint2(bitsA, bitsB);
+    }
+}
+
+// Division-free decision of "the new candidate's quotient is strictly below
+// the incumbent's", RN(a_new / m_new) < RN(a_inc / m_inc) with positive
+// integer-valued m, for the FP64 form.  Returns whether the cross products
+// decide it (else the caller divides); `win` is the answer when they do.
+//   U = RN(a_new * m_inc), V = RN(a_inc * m_new), d = RN(V - U) and the
+//   threshold t = RN(|U| * 2^-46 + 2^-900) (one FMA).  d's error is below
+//   2^-52 (|U| + |V|) (plus 2^-1073 where a product is subnormal).
+//   * |V| <= 3 |U|: t >= 2^-48 (|U| + |V|) + 2^-900 exceeds that error by a
+//     factor of 16, so |d| > t fixes the sign of the exact a_inc m_new -
+//     a_new m_inc and leaves a relative gap > 2^-49 between the exact
+//     quotients: their roundings cannot meet.
+//   * |V| > 3 |U|: the exact difference has V's sign and |V| / 2 or more of
+//     magnitude, the same conclusion.
+//   |d| > t needs max(|U|, |V|) > 2^-901: no quotient is subnormal.  A NaN
+//   or infinite product never decides (every comparison with it is false or
+//   t is infinite).
+__device__ __forceinline__ bool decide_quot(double a_new, double m_new, double a_inc,
+                                            double m_inc, bool& win) {
+    const double U = __dmul_rn(a_new, m_inc);
+    const double V = __dmul_rn(a_inc, m_new);
+    const double d = __dadd_rn(V, -U);
+    const double t = __fma_rn(fabs(U), 0x1p-46, 0x1p-900);
+    win = d > t;
+    return win || -d > t;
+}
+// FP32 form: the cross products of FP32 values and integers below 2^24 are
+// exact in FP64 (see the FP32 qless_exact): d <= 0 decides "not below", a
+// relative margin of 2^-21 decides "below".
+__device__ __forceinline__ bool decide_quot(float a_new, float m_new, float a_inc, float m_inc,
+                                            bool& win) {
+    const double U = __dmul_rn((double)a_new, (double)m_inc);
+    const double V = __dmul_rn((double)a_inc, (double)m_new);
+    const double d = __dadd_rn(V, -U);
+    win = d > __dmul_rn(__dadd_rn(fabs(U), fabs(V)), 0x1p-21);
+    return win || d <= 0.0;
+}
+__device__ __forceinline__ bool finite_first(double a0, double, double) { return a0 < CUDART_INF; }
+__device__ __forceinline__ bool finite_first(float a0, float a1, float a2) {
+    return a0 < CUDART_INF_F && a1 < CUDART_INF_F && a2 < CUDART_INF_F;
+}
+
+// Steps (1,1), (1,2), (2,1) at a cell with every predecessor inside the tile
+// and r, c >= 2, mdists given: the selection of select_fast_std<false>.
+template <typename T>
+__device__ __forceinline__ bool select_std_m(T cval, T w0, T w1, T w2, T x1D, int x1P, T m0,
+                                             T x2D, int x2P, T m1, T x3D, int x3P, T m2, T& oD,
+                                             int& oP, int& code) {
+    const T a0 = addr(x1D, mulr(cval, w0));
+    const T a1 = addr(x2D, mulr(cval, w1));
+    const T a2 = addr(x3D, mulr(cval, w2));
+    bool win1, win2;
+    const bool ok1 = decide_quot(a1, m1, a0, m0, win1);
+    const T bA = win1 ? a1 : a0, bM = win1 ? m1 : m0;
+    const bool ok2 = decide_quot(a2, m2, bA, bM, win2);
+    oD = win2 ? a2 : bA;
+    oP = win2 ? x3P : (win1 ? x2P : x1P);
+    code = win2 ? 2 : (win1 ? 1 : 0);
+    return finite_first(a0, a1, a2) && ok1 && ok2;
+}
+
+// Out-of-line exact selection for the fast block's undecided cells (rare):
+// keeping it out of the unrolled steps keeps the hot loop small.
+template <typename T>
+__device__ __noinline__ void select_exact_std_call(const Geo& g, int r, int c, T rc, T cval,
+                                                   T x1D, int x1P, T x2D, int x2P, T x3D,
+                                                   int x3P, T* oD, int* oP, int* code) {
+    T d;
+    int p, k;
+    select_exact<true, true>(g, (T)g.w[2], r, c, rc, cval, x1D, x1P, x2D, x2P, x3D, x3P, d, p,
+                             k);
+    *oD = d;
+    *oP = p;
+    *code = k;
+}
+
+// A block of 16 steps of the standard step set in which every cell of the
+// strip is inside the tile with r, c >= 2 and off the tile's last row and
+// column (the caller's "interior" test).  Same results as
+// run_block<false, true, PUSH, T>, with fewer instructions per step:
+//  * no bounds tests, no edge stores, and no guard on the cost loads (the
+//    block ends at least 17 steps before the strip's span);
+//  * mdist of a predecessor that the previous step also used is that step's
+//    mdist + 1 (r + c grows by one per step), and B's (2,1) predecessor is
+//    A's (1,2) one, so a step converts three start encodings, not six;
+//  * ring slots are read and written as {B, A} pairs (two shared-memory
+//    loads per step, two stores by lane 31);
+//  * the FP64 decision margin is one FMA (decide_quot);
+//  * the exact routine for undecided cells is called out of line.
+template <bool PUSH, typename T>
+__device__ __forceinline__ void run_block_std(const Geo& g, Wave<T>& st, const Rings<T>& rg,
+                                              char* wbase,
+                                              const typename Vec2<T>::type* __restrict__ Cs,
+                                              int tau0, int k, int lane, int prev_base,
+                                              int mine_base, int rmask, int Tb, int lag,
+                                              const TileDesc& td, int nP, uint2* bw) {
+    using V2 = typename Vec2<T>::type;
+    const unsigned F = 0xffffffffu;
+    const T w0 = (T)g.w[0], w1 = (T)g.w[1], w2 = (T)g.w[2];
+    const int rA = 64 * k + 2 * lane, rB = rA + 1;
+    const T rc0 = (T)(64 * k + tau0);
+    // mdist of A's and B's (1,2) predecessors at the next step
+    T m1A_next = addr(rc0, -fabs((T)st.xpP));
+    T m1B_next = addr(rc0, -fabs((T)st.aP3));
+    uint32_t bitsA = 0, bitsB = 0;
+    const V2* cp = Cs + (int64_t)(tau0 + 2) * 32;  // the cost two steps ahead
+    const V2* rD = rg.D + prev_base;
+    const int2* rP = rg.P + prev_base;
+    const int rs0 = Tb - lag - 1;
+#pragma unroll 1
+    for (int tq = 0; tq < kBlk; tq += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int t = tq + u;
+            const T rc = addr(rc0, (T)t);
+            const V2 cc = st.q[u & 1];
+            st.q[u & 1] = __ldcs(cp + (int64_t)t * 32);
+            const int rs = (rs0 + t) & rmask;
+            const V2 ringD = rD[rs];  // every lane reads the same slot; lane 0 keeps it
+            const int2 ringP = rP[rs];
+            T x1D = __shfl_up_sync(F, st.bD2, 1);
+            int x1P = __shfl_up_sync(F, st.bP2, 1);
+            T x3D = __shfl_up_sync(F, st.aD3, 1);
+            int x3P = __shfl_up_sync(F, st.aP3, 1);
+            x1D = lane == 0 ? ringD.x : x1D;
+            x1P = lane == 0 ? ringP.x : x1P;
+            x3D = lane == 0 ? ringD.y : x3D;
+            x3P = lane == 0 ? ringP.y : x3P;
+            const T x2D = st.xpD;
+            const int x2P = st.xpP;
+            const T m0A = addr(rc, -fabs((T)x1P));
+            const T m1A = m1A_next;
+            const T m2A = addr(rc, -fabs((T)x3P));
+            const T m0B = addr(rc, -fabs((T)st.aP2));
+            const T m1B = m1B_next;
+            m1A_next = addr(m0A, (T)1);
+            m1B_next = addr(m0B, (T)1);
+            T oAD, oBD;
+            int oAP, oBP, codeA, codeB;
+            const bool okA = select_std_m<T>(cc.x, w0, w1, w2, x1D, x1P, m0A, x2D, x2P, m1A,
+                                             x3D, x3P, m2A, oAD, oAP, codeA);
+            const bool okB = select_std_m<T>(cc.y, w0, w1, w2, st.aD2, st.aP2, m0B, st.aD3,
+                                             st.aP3, m1B, x2D, x2P, m1A, oBD, oBP, codeB);
+            if (__any_sync(F, !(okA && okB))) {
+                const int cA = tau0 + t - 2 * lane;
+                if (!okA)
+                    select_exact_std_call<T>(g, rA, cA, rc, cc.x, x1D, x1P, x2D, x2P, x3D, x3P,
+                                             &oAD, &oAP, &codeA);
+                if (!okB)
+                    select_exact_std_call<T>(g, rB, cA - 1, rc, cc.y, st.aD2, st.aP2, st.aD3,
+                                             st.aP3, x2D, x2P, &oBD, &oBP, &codeB);
+            }
+            if (lane == 31) {
+                // B of this step and A of the previous one: slot (step - 63)
+                const int ws = mine_base + ((Tb + t - 63) & rmask);
+                if (PUSH) {
+                    ring_put(wbase, rg, rg.D + ws, make_v2<T>(oBD, st.aD1));
+                    ring_put(wbase, rg, rg.P + ws, make_int2(oBP, st.aP1));
+                } else {
+                    rg.D[ws] = make_v2<T>(oBD, st.aD1);
+                    rg.P[ws] = make_int2(oBP, st.aP1);
+                }
+            }
+            bitsA |= (uint32_t)codeA << (2 * t);
+            bitsB |= (uint32_t)codeB << (2 * t);
+            st.aD3 = st.aD2; st.aP3 = st.aP2;
+            st.aD2 = st.aD1; st.aP2 = st.aP1;
+            st.aD1 = oAD;    st.aP1 = oAP;
+            st.bD2 = st.bD1; st.bP2 = st.bP1;
+            st.bD1 = oBD;    st.bP1 = oBP;
+            st.xpD = x1D;    st.xpP = x1P;
+        }
+    }
+    if (bw) {
+        *bw = make_uint2(bitsA, bitsB);
+    } else {
         uint2* Bt = reinterpret_cast<uint2*>(td.Bw);
         Bt[((int64_t)k * nP + (tau0 >> 4)) * 32 + lane] = make_uint2(bitsA, bitsB);
     }
@@ -411,7 +595,7 @@ __host__ __device__ inline int ring_len(int lag, int nw, int smem_limit, int vby
     while (cap * 2 <= lag + 64) cap *= 2;
     if (cap < lag + 64) cap *= 2;
     int fit = 16;
-    const int per = nw * (2 * vbytes + 2 * (int)sizeof(int));
+    const int per = nw * (2 * vbytes + (int)sizeof(int2));
     while ((fit * 2) * per + nw * (int)sizeof(int) <= smem_limit) fit *= 2;
     const int rb = cap < fit ? cap : fit;
     return rb >= lag - 29 ? rb : 0;
@@ -425,11 +609,9 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW)
     using V2 = typename Vec2<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Rings<T> rg;
-    rg.AD = reinterpret_cast<T*>(smem_raw);
-    rg.BD = rg.AD + NW * RB;
-    rg.AP = reinterpret_cast<int*>(rg.BD + NW * RB);
-    rg.BP = rg.AP + NW * RB;
-    int* prog = rg.BP + NW * RB;
+    rg.D = reinterpret_cast<V2*>(smem_raw);
+    rg.P = reinterpret_cast<int2*>(rg.D + NW * RB);
+    int* prog = reinterpret_cast<int*>(rg.P + NW * RB);
     __shared__ TileDesc td;
     __shared__ Sched2 s_sc;  // schedule of the current tile (read from smem, not held in registers)
     __shared__ int s_item, s_abort, s_ttot;
@@ -504,14 +686,20 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW)
                     for (int q = 0; q < 2; ++q) st.q[q] = __ldcs(Cs + q * 32);
                 }
                 const bool interior = k >= 1 && k <= sc.nS - 2 && tau0 >= 80 && tau0 + 17 <= W;
-                if (interior)
-                    run_block<false, STD, false>(g, st, rg, reinterpret_cast<const char*>(rg.AD),
-                                          reinterpret_cast<char*>(rg.AD), Cs,
-                                          sc.span, tau0, k, R, W, lane,
-                                          prevw * RB, warp * RB, RB - 1, Tb, lag, td, sc.nP);
-                else
-                    run_block<true, STD, false>(g, st, rg, reinterpret_cast<const char*>(rg.AD),
-                                         reinterpret_cast<char*>(rg.AD), Cs,
+                if (interior) {
+                    if constexpr (STD)
+                        run_block_std<false, T>(g, st, rg, reinterpret_cast<char*>(rg.D), Cs,
+                                                tau0, k, lane, prevw * RB, warp * RB, RB - 1, Tb,
+                                                lag, td, sc.nP, nullptr);
+                    else
+                        run_block<false, STD, false>(g, st, rg,
+                                                     reinterpret_cast<const char*>(rg.D),
+                                                     reinterpret_cast<char*>(rg.D), Cs, sc.span,
+                                                     tau0, k, R, W, lane, prevw * RB, warp * RB,
+                                                     RB - 1, Tb, lag, td, sc.nP);
+                } else
+                    run_block<true, STD, false>(g, st, rg, reinterpret_cast<const char*>(rg.D),
+                                         reinterpret_cast<char*>(rg.D), Cs,
                                          sc.span, tau0, k, R, W, lane,
                                          prevw * RB, warp * RB, RB - 1, Tb, lag, td, sc.nP);
             }
@@ -569,14 +757,12 @@ __global__ void __launch_bounds__(kClW * 32, 1)
     const int rank = (int)cl.block_rank();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Rings<T> rg;  // this CTA's rings
-    rg.AD = reinterpret_cast<T*>(smem_raw);
-    rg.BD = rg.AD + kClW * RB;
-    rg.AP = reinterpret_cast<int*>(rg.BD + kClW * RB);
-    rg.BP = rg.AP + kClW * RB;
+    rg.D = reinterpret_cast<V2*>(smem_raw);
+    rg.P = reinterpret_cast<int2*>(rg.D + kClW * RB);
     // progress words: [w] warp w's; [kClW] the other CTA's last warp's (this
     // CTA's warp 0 waits on it); [kClW + 1] the other CTA's warp 0's (this
     // CTA's last warp waits on it) -- written by the other CTA, polled here
-    int* prog = rg.BP + kClW * RB;
+    int* prog = reinterpret_cast<int*>(rg.P + kClW * RB);
     __shared__ TileDesc td;
     __shared__ Sched2 s_sc;
     __shared__ int s_item, s_abort, s_ttot;
@@ -588,8 +774,8 @@ __global__ void __launch_bounds__(kClW * 32, 1)
     // dependency chain) and reads its producer's ring from its own CTA: ring
     // region w of a CTA is written by warp w of the CTA that feeds it (its own
     // warp w, or for w = kClW - 1 the other CTA's last warp)
-    const char* rbase = reinterpret_cast<const char*>(rg.AD);
-    char* wbase = reinterpret_cast<char*>(cl.map_shared_rank(rg.AD, nv / kClW));
+    const char* rbase = reinterpret_cast<const char*>(rg.D);
+    char* wbase = reinterpret_cast<char*>(cl.map_shared_rank(rg.D, nv / kClW));
     // cluster scope only where the neighbour is in the other CTA
     const bool prev_remote = pv / kClW != rank, next_remote = nv / kClW != rank;
     const bool read_remotely = warp == 0 || warp == kClW - 1;  // my progress word
@@ -672,12 +858,16 @@ __global__ void __launch_bounds__(kClW * 32, 1)
                     for (int q = 0; q < 2; ++q) st.q[q] = __ldcs(Cs + q * 32);
                 }
                 const bool interior = k >= 1 && k <= sc.nS - 2 && tau0 >= 80 && tau0 + 17 <= W;
-                if (interior)
-                    run_block<false, STD, true>(g, st, rg, rbase, wbase, Cs, sc.span, tau0, k, R, W,
-                                          lane,
-                                          (pv % kClW) * RB, warp * RB, RB - 1, Tb, lag, td,
-                                          sc.nP, &bw);
-                else
+                if (interior) {
+                    if constexpr (STD)
+                        run_block_std<true, T>(g, st, rg, wbase, Cs, tau0, k, lane,
+                                               (pv % kClW) * RB, warp * RB, RB - 1, Tb, lag, td,
+                                               sc.nP, &bw);
+                    else
+                        run_block<false, STD, true>(g, st, rg, rbase, wbase, Cs, sc.span, tau0, k,
+                                                    R, W, lane, (pv % kClW) * RB, warp * RB,
+                                                    RB - 1, Tb, lag, td, sc.nP, &bw);
+                } else
                     run_block<true, STD, true>(g, st, rg, rbase, wbase, Cs, sc.span, tau0, k, R, W,
                                          lane,
                                          (pv % kClW) * RB, warp * RB, RB - 1, Tb, lag, td,
@@ -729,7 +919,7 @@ static size_t smem_bytes(int32_t L, int nw, int smem_limit, int vbytes) {
     const Sched2 s = make_sched2(L, L, nw);
     const int rb = ring_len(s.lag, nw, smem_limit, vbytes);
     if (rb == 0) return (size_t)1 << 30;  // does not fit
-    return (size_t)nw * rb * (2 * vbytes + 2 * sizeof(int)) + nw * sizeof(int);
+    return (size_t)nw * rb * (2 * vbytes + sizeof(int2)) + nw * sizeof(int);
 }
 
 int stage1_queue_warps(int ntiles, int32_t L, int num_sms) {
@@ -776,7 +966,7 @@ static cudaError_t launch_cl_t(const TileDesc* descs, int ntiles, int* head, con
     const int rb = ring_len(s.lag, kClW, limit, (int)sizeof(T));
     if (rb == 0) return cudaErrorInvalidValue;
     const size_t smem =
-        (size_t)kClW * rb * (2 * sizeof(T) + 2 * sizeof(int)) + (kClW + 2) * sizeof(int);
+        (size_t)kClW * rb * ring_slot_bytes<T>() + (kClW + 2) * sizeof(int);
     auto kern = k_stage1_cl<STD, T>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
@@ -812,7 +1002,7 @@ static int cl_max_t(const Geo& g) {
     const int rb = ring_len(s.lag, kClW, limit, (int)sizeof(T));
     if (rb == 0) return 0;
     const size_t smem =
-        (size_t)kClW * rb * (2 * sizeof(T) + 2 * sizeof(int)) + (kClW + 2) * sizeof(int);
+        (size_t)kClW * rb * ring_slot_bytes<T>() + (kClW + 2) * sizeof(int);
     auto kern = k_stage1_cl<STD, T>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)

@@ -280,9 +280,15 @@ PRUNE64 = PruneSpec("chroma12_pairs64_N40000-60000_L2000_pruned", 64, 40000, 600
 PRUNE_NCU = PruneSpec("chroma12_pairs4_N8000-10000_L2000_pruned", 4, 8000, 10000,
                       L_choices=(2000,), pad_frac=0.10)
 
+# Profiling case of the stage-1 kernel as the learned-pruning workload runs it
+# (4 warps per tile CTA, four CTAs per SM: 720 tiles of up to 1000 x 1000,
+# about 6 GB of cost slabs): 20 pairs, N ~ U(5000, 6000), L = 1000.
+PRUNE_NCU_W4 = PruneSpec("chroma12_pairs20_N5000-6000_L1000_pruned", 20, 5000, 6000,
+                         L_choices=(1000,), pad_frac=0.10)
+
 WORKLOADS = {"config0": CONFIG0, "config1": CONFIG1, "ncu_small": NCU_SMALL,
              "batch256": BATCH256, "precision2048": PRECISION2048, "prune64": PRUNE64,
-             "prune_ncu": PRUNE_NCU}
+             "prune_ncu": PRUNE_NCU, "prune_ncu_w4": PRUNE_NCU_W4}
 
 
 def make_pair(spec: PairSpec):
