@@ -1151,6 +1151,179 @@ def prune_arm(args, spec):
         dist.destroy_process_group()
 
 
+SHARD_METRIC = ("DP cells/s (ParFlex plain FP64 form, one long pair, tiles sharded across "
+                "GPUs with one edge exchange)")
+
+
+def _shard_cpu_sample(spec, threads, rounds):
+    """Cost matrix of a bounded CPU sample of the tile-sharded pair: a block
+    of whole tiles at its start with a tile count that is a multiple of the
+    host threads.  Returns (C, cells, text)."""
+    F1, F2 = W.make_pair(spec)
+    N, M = F1.shape[1], F2.shape[1]
+    a, b = _balanced_tile_block(N, M, spec.L, threads, rounds)
+    rows, cols = a * (spec.L - 1) + 1, b * (spec.L - 1) + 1
+    C = W.cost_matrix_host(F1[:, :rows], F2[:, :cols])
+    cells = tile_cells(rows, cols, spec.L)[0]
+    text = (f"the leading {a} x {b} block of whole {spec.L} x {spec.L} tiles ({a * b} tiles on "
+            f"{threads} threads, {rows} x {cols} frames, {cells} cells) of the pair "
+            f"({N} x {M}), FP64, all stages, cost matrix built outside the timing")
+    return C, cells, text
+
+
+def shard_reference_arm(args, spec):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import build_oracle, oracle
+    build_oracle.build()
+    threads = os.cpu_count() or 1
+    C, cells, sample = _shard_cpu_sample(spec, threads, 2)
+    times = []
+    for s_ in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        oracle.parflex_full(C, spec.steps, spec.weights, spec.beta, spec.L, threads=threads)
+        if s_ >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    v = cells * len(times) / tot
+    line = {
+        "impl": "reference", "metric": SHARD_METRIC, "value": v, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot / len(times), "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(spec.describe(), parallelism="tiles"),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample + " per step"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def shard_arm(args, spec):
+    """One long pair, its tiles sharded across the ranks (strong scaling):
+    every rank builds the cost and runs stage 1 for its own tile range,
+    rank 0 gathers the tile edges (NCCL) and runs stage 2, the crossed
+    tiles' backpointers travel to rank 0.  Step time = max over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    from parflexdtw_b200 import _lib
+    from parflexdtw_b200.shard import ShardedPair
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    lib = _lib.load()
+    F1, F2 = W.make_pair(spec)  # the same pair on every rank
+    N, M = F1.shape[1], F2.shape[1]
+    cells, n1, n2 = tile_cells(N, M, spec.L)
+    f1d, f2d = torch.from_numpy(F1).to(dev), torch.from_numpy(F2).to(dev)
+    sp = ShardedPair(N, M, spec.steps, spec.weights, L=spec.L)
+    ref = None
+    for _ in range(args.warmup):
+        ref = sp.run(spec.beta, f1d, f2d)
+
+    def max_ranks(x):
+        if ws == 1:
+            return x
+        t = torch.tensor([x], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    local_ms = []
+    launches0 = lib.pfx_kernel_launches()
+    with ClockSampler(uuid) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            out = sp.run(spec.beta, f1d, f2d, events=True)
+            local_ms.append(sp.local_ms())
+            if rank == 0:
+                assert out[0] == ref[0] and np.array_equal(out[1], ref[1]), "non-deterministic"
+        e1.record()
+        torch.cuda.synchronize()
+    launches = lib.pfx_kernel_launches() - launches0
+    ms_total = max_ranks(e0.elapsed_time(e1))
+    cost_ms = max_ranks(sum(a for a, _ in local_ms) / args.steps)
+    s1_ms = max_ranks(sum(b for _, b in local_ms) / args.steps)
+
+    # e2e: pinned host features in, result out, every step
+    f1p, f2p = torch.from_numpy(F1).pin_memory(), torch.from_numpy(F2).pin_memory()
+    h2d = f1p.numel() * 8 + f2p.numel() * 8
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    d2h = 0
+    for _ in range(args.e2e_steps):
+        f1d.copy_(f1p, non_blocking=True)
+        f2d.copy_(f2p, non_blocking=True)
+        out = sp.run(spec.beta, f1d, f2d)
+        if rank == 0:
+            d2h = out[1].nbytes + 8
+    b.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_ranks(a.elapsed_time(b))
+    own = sp.own_cells
+    ex_bytes = sp.edge_exchange_bytes()
+    sp.close()
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        from oracle import build_oracle, oracle
+        build_oracle.build()
+        threads = os.cpu_count() or 1
+        C, scells, sample = _shard_cpu_sample(spec, threads, 2)
+        t0 = time.perf_counter()
+        oracle.parflex_full(C, spec.steps, spec.weights, spec.beta, spec.L, threads=threads)
+        dt = time.perf_counter() - t0
+        cpu = {"value": scells / dt, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": sample, "seconds": dt}
+        del C
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        achieved = own * 8.25 / (s1_ms / 1e3) / 1e9
+        line = {
+            "metric": SHARD_METRIC, "value": cells * args.steps / (ms_total / 1e3), "unit": UNIT,
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(spec.describe(), N=N, M=M, tiles=n1 * n2, cells_per_step=cells,
+                           parallelism=f"tiles over {ws} rank(s)",
+                           input="features resident in HBM; every step builds the cost",
+                           l2="cost slabs larger than L2 (no flush needed)"),
+            "pairs_per_s": args.steps / (ms_total / 1e3),
+            "per_rank": {"cost_ms_max": cost_ms, "stage1_ms_max": s1_ms,
+                         "rank0_cells": own, "edge_exchange_bytes": ex_bytes},
+            "roofline": {"bound": "hbm", "kernel": "k_stage1_v3 (rank 0's tile range)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                         if peak_kind == "measured" else "fallback",
+                         "alg_bytes_per_cell": 8.25},
+            "cpu_baseline": cpu,
+            "e2e": {"value": cells * args.e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "steps": args.e2e_steps, "ms_per_step": e2e_ms / args.e2e_steps,
+                    "api": "ShardedPair.run from features copied from pinned host memory"},
+            "gpu_launches": int(launches), "clocks": clk.summary(),
+            "note": "N > 1 not measured on hardware here (one GPU per call)",
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1179,6 +1352,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     spec = W.WORKLOADS[args.workload]
+    if isinstance(spec, W.ShardSpec):
+        (shard_reference_arm if args.impl == "reference" else shard_arm)(args, spec)
+        return
     if isinstance(spec, W.PruneSpec):
         (prune_reference_arm if args.impl == "reference" else prune_arm)(args, spec)
         return

@@ -454,19 +454,28 @@ __device__ __forceinline__ bool select_std_m(T cval, T w0, T w1, T w2, T x1D, in
     return finite_first(a0, a1, a2) && ok1 && ok2;
 }
 
-// Out-of-line exact selection for the fast block's undecided cells (rare):
-// keeping it out of the unrolled steps keeps the hot loop small.
+// Exact selection of the fast block's undecided cells (rare), by value.
 template <typename T>
-__device__ __noinline__ void select_exact_std_call(const Geo& g, int r, int c, T rc, T cval,
-                                                   T x1D, int x1P, T x2D, int x2P, T x3D,
-                                                   int x3P, T* oD, int* oP, int* code) {
+struct SelOut {
     T d;
-    int p, k;
-    select_exact<true, true>(g, (T)g.w[2], r, c, rc, cval, x1D, x1P, x2D, x2P, x3D, x3P, d, p,
-                             k);
-    *oD = d;
-    *oP = p;
-    *code = k;
+    int p, code;
+};
+template <typename T>
+__device__ __forceinline__ SelOut<T> select_exact_std_call(T w0, T w1, T w2, int r, int c, T rc,
+                                                        T cval, T x1D, int x1P, T x2D, int x2P,
+                                                        T x3D, int x3P) {
+    Geo g;
+    g.S = 3;
+    g.kind[0] = 0;
+    g.kind[1] = 1;
+    g.kind[2] = 2;
+    g.w[0] = (double)w0;
+    g.w[1] = (double)w1;
+    g.w[2] = (double)w2;
+    SelOut<T> o;
+    select_exact<true, true>(g, w2, r, c, rc, cval, x1D, x1P, x2D, x2P, x3D, x3P, o.d, o.p,
+                             o.code);
+    return o;
 }
 
 // A block of 16 steps of the standard step set in which every cell of the
@@ -480,8 +489,11 @@ __device__ __noinline__ void select_exact_std_call(const Geo& g, int r, int c, T
 //    A's (1,2) one, so a step converts three start encodings, not six;
 //  * ring slots are read and written as {B, A} pairs (two shared-memory
 //    loads per step, two stores by lane 31);
-//  * the FP64 decision margin is one FMA (decide_quot);
-//  * the exact routine for undecided cells is called out of line.
+//  * the FP64 decision margin is one FMA (decide_quot).
+// The loop is unrolled two steps deep only: steps t and t+1 are independent
+// (each reads outputs of two steps back), and a small loop body stays in the
+// instruction cache (a 16-step unroll, or a second copy of the body, each
+// measured slower).
 template <bool PUSH, typename T>
 __device__ __forceinline__ void run_block_std(const Geo& g, Wave<T>& st, const Rings<T>& rg,
                                               char* wbase,
@@ -503,11 +515,12 @@ __device__ __forceinline__ void run_block_std(const Geo& g, Wave<T>& st, const R
     const int2* rP = rg.P + prev_base;
     const int rs0 = Tb - lag - 1;
 #pragma unroll 1
-    for (int tq = 0; tq < kBlk; tq += 4) {
+    for (int tq = 0; tq < kBlk; tq += 2) {
+        const T rcq = addr(rc0, (T)tq);
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < 2; ++u) {
             const int t = tq + u;
-            const T rc = addr(rc0, (T)t);
+            const T rc = addr(rcq, (T)u);
             const V2 cc = st.q[u & 1];
             st.q[u & 1] = __ldcs(cp + (int64_t)t * 32);
             const int rs = (rs0 + t) & rmask;
@@ -538,12 +551,21 @@ __device__ __forceinline__ void run_block_std(const Geo& g, Wave<T>& st, const R
                                              st.aP3, m1B, x2D, x2P, m1A, oBD, oBP, codeB);
             if (__any_sync(F, !(okA && okB))) {
                 const int cA = tau0 + t - 2 * lane;
-                if (!okA)
-                    select_exact_std_call<T>(g, rA, cA, rc, cc.x, x1D, x1P, x2D, x2P, x3D, x3P,
-                                             &oAD, &oAP, &codeA);
-                if (!okB)
-                    select_exact_std_call<T>(g, rB, cA - 1, rc, cc.y, st.aD2, st.aP2, st.aD3,
-                                             st.aP3, x2D, x2P, &oBD, &oBP, &codeB);
+                if (!okA) {
+                    const SelOut<T> o = select_exact_std_call<T>(w0, w1, w2, rA, cA, rc, cc.x,
+                                                                 x1D, x1P, x2D, x2P, x3D, x3P);
+                    oAD = o.d;
+                    oAP = o.p;
+                    codeA = o.code;
+                }
+                if (!okB) {
+                    const SelOut<T> o = select_exact_std_call<T>(w0, w1, w2, rB, cA - 1, rc,
+                                                                 cc.y, st.aD2, st.aP2, st.aD3,
+                                                                 st.aP3, x2D, x2P);
+                    oBD = o.d;
+                    oBP = o.p;
+                    codeB = o.code;
+                }
             }
             if (lane == 31) {
                 // B of this step and A of the previous one: slot (step - 63)

@@ -199,6 +199,120 @@ def exchange_backptr(bw, crossed, ranges, group=None):
     return tiles
 
 
+class ShardedPair:
+    """One long pair with its tiles sharded across the ranks of ``group``
+    (default: the default process group), set up once and aligned any
+    number of times: per rank a plan that holds the cost slabs of its own
+    contiguous tile range only (``shard_tiles``, balanced by cells).
+
+    ``run(beta, F1d, F2d)`` is one alignment: each rank builds the cost of
+    its tiles from the device features (when given; else the last loaded
+    cost is reused) and runs stage 1 and the edge step of stage 2 on them;
+    rank 0 gathers the edges, runs the rest of stage 2 and the tile chain,
+    the owners of the crossed tiles send their backpointers, and rank 0
+    walks the path.  Rank 0 returns ``(best_cost, wp)``, the others None.
+    Every rank takes the same collective steps in the same order, failures
+    included (a stage-1 failure anywhere ends the call on every rank).
+    """
+
+    def __init__(self, N, M, steps, weights, L=None, group=None, precision="fp64"):
+        import torch.distributed as dist
+        from .parflex import DEFAULT_CHUNK_LENGTH
+        from .plan import Plan
+        self.group = group
+        self.ws = dist.get_world_size(group) if dist.is_initialized() else 1
+        self.rank = dist.get_rank(group) if dist.is_initialized() else 0
+        self.L = int(DEFAULT_CHUNK_LENGTH if L is None else L)
+        self.plan = Plan(int(N), int(M), self.L, steps, weights, precision=precision)
+        p = self.plan
+        self.cells = tile_cells(p.n1, p.n2, p.N, p.M, self.L, p.hop)
+        self.ranges = shard_tiles(self.cells, self.ws)
+        self.lo, self.hi = self.ranges[self.rank]
+        if self.hi > self.lo:
+            p.set_tile_range(self.lo, self.hi)  # cost slabs of the own tiles only
+
+    @property
+    def own_cells(self):
+        return int(sum(self.cells[self.lo:self.hi]))
+
+    def edge_exchange_bytes(self):
+        """Bytes rank 0 receives in the edge exchange per alignment: 20 B
+        per edge slot (D f64, overlap cost f64, start i32) of the other
+        ranks' tiles, plus the valid mask reduction (1 B per slot per rank)."""
+        if self.ws == 1:
+            return 0
+        spt = 2 * self.L
+        other = sum(hi - lo for r, (lo, hi) in enumerate(self.ranges) if r)
+        return other * spt * 20 + (self.ws - 1) * len(self.cells) * spt
+
+    def run(self, beta, F1d=None, F2d=None, events=False):
+        """One alignment (see the class docstring).  ``events``: record CUDA
+        events around this rank's cost build and stage 1, read back with
+        ``local_ms()``."""
+        import torch
+        import torch.distributed as dist
+        plan, ws, rank, group = self.plan, self.ws, self.rank, self.group
+        failure = None
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)] if events else None
+        try:
+            if self.hi > self.lo:
+                if ev:
+                    ev[0].record()
+                if F1d is not None:
+                    plan.load_features(F1d, F2d)
+                if ev:
+                    ev[1].record()
+                plan.stage1()
+                if ev:
+                    ev[2].record()
+                plan.edges()
+                plan.result(raise_no_endpoint=False)  # synchronises; raises if a wait ran out
+            self._ev = ev if self.hi > self.lo else None
+        except Exception as e:  # noqa: BLE001 - re-raised below, after the reduction
+            failure = e
+        status = 0 if failure is None else 1
+        if ws > 1:
+            st = torch.tensor([status], dtype=torch.int32, device=_comm_device(group))
+            dist.all_reduce(st, op=dist.ReduceOp.MAX, group=group)
+            status = int(st.item())
+        if failure is not None:
+            raise failure
+        if status:
+            raise RuntimeError("stage 1 of a tile shard failed on another rank")
+        if ws > 1:
+            exchange_edges(plan.view("EDGE_D"), plan.view("EDGE_P"), plan.view("EDGE_CF"),
+                           plan.view("VALID"), self.ranges, group)
+        crossed = []
+        if rank == 0:
+            # the rest of stage 2 reads no cost: the tile range may stay
+            plan.prop()
+            plan.scan(beta)
+            crossed = [int(i) * plan.n2 + int(j) for i, j in plan.chain()]
+        if ws > 1:
+            bw = plan.view("BACKPTR").view(torch.int32).reshape(plan.n1 * plan.n2, -1)
+            exchange_backptr(bw, crossed, self.ranges, group)
+        if rank != 0:
+            torch.cuda.synchronize()
+            return None
+        plan.stitch()
+        best, end, found, n = plan.result()
+        wp = plan.path(n)
+        if wp.shape[0] == 0:
+            return best, np.array([[], []], dtype=np.int64)
+        return best, np.ascontiguousarray(wp.T)
+
+    def local_ms(self):
+        """(cost build ms, stage-1 ms) of this rank's last ``run(events=True)``
+        ((0, 0) for a rank without tiles)."""
+        ev = getattr(self, "_ev", None)
+        if not ev:
+            return 0.0, 0.0
+        return ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+
+    def close(self):
+        self.plan.close()
+
+
 def parflex_sharded(F1, F2, steps, weights, beta, L=None, group=None, precision="fp64"):
     """ParFlex of one long pair with its tiles sharded across the ranks of
     ``group`` (default: the default process group).
@@ -209,60 +323,11 @@ def parflex_sharded(F1, F2, steps, weights, beta, L=None, group=None, precision=
     other ranks None.  Each rank builds the cost and runs stage 1 only for
     its own tiles; see the module docstring for the exchange.
     """
-    import torch
-    import torch.distributed as dist
-    from .parflex import DEFAULT_CHUNK_LENGTH, _features_to_device
-    from .plan import Plan
-    ws = dist.get_world_size(group) if dist.is_initialized() else 1
-    rank = dist.get_rank(group) if dist.is_initialized() else 0
-    Lb = int(DEFAULT_CHUNK_LENGTH if L is None else L)
+    from .parflex import _features_to_device
     F1d, F2d = _features_to_device(F1), _features_to_device(F2)
-    plan = Plan(F1d.shape[1], F2d.shape[1], Lb, steps, weights, precision=precision)
-    ranges = shard_tiles(tile_cells(plan.n1, plan.n2, plan.N, plan.M, Lb, plan.hop), ws)
-    lo, hi = ranges[rank]
-    # every rank reaches the status reduction, so that a failure on one rank
-    # ends the call on all of them instead of leaving them in a collective
-    failure = None
+    sp = ShardedPair(F1d.shape[1], F2d.shape[1], steps, weights, L=L, group=group,
+                     precision=precision)
     try:
-        if hi > lo:
-            plan.set_tile_range(lo, hi)  # cost slabs of the own tiles only
-            plan.load_features(F1d, F2d)
-            plan.stage1()
-            plan.edges()
-            plan.result(raise_no_endpoint=False)  # synchronises; raises if a wait ran out
-    except Exception as e:  # noqa: BLE001 - re-raised below, after the reduction
-        failure = e
-    status = 0 if failure is None else 1
-    if ws > 1:
-        st = torch.tensor([status], dtype=torch.int32, device=_comm_device(group))
-        dist.all_reduce(st, op=dist.ReduceOp.MAX, group=group)
-        status = int(st.item())
-    if failure is not None:
-        plan.close()
-        raise failure
-    if status:
-        plan.close()
-        raise RuntimeError("stage 1 of a tile shard failed on another rank")
-    if ws > 1:
-        exchange_edges(plan.view("EDGE_D"), plan.view("EDGE_P"), plan.view("EDGE_CF"),
-                       plan.view("VALID"), ranges, group)
-    crossed = []
-    if rank == 0:
-        # the rest of stage 2 reads no cost: the tile range may stay
-        plan.prop()
-        plan.scan(beta)
-        crossed = [int(i) * plan.n2 + int(j) for i, j in plan.chain()]
-    if ws > 1:
-        bw = plan.view("BACKPTR").view(torch.int32).reshape(plan.n1 * plan.n2, -1)
-        exchange_backptr(bw, crossed, ranges, group)
-    if rank != 0:
-        torch.cuda.synchronize()
-        plan.close()
-        return None
-    plan.stitch()
-    best, end, found, n = plan.result()
-    wp = plan.path(n)
-    plan.close()
-    if wp.shape[0] == 0:
-        return best, np.array([[], []], dtype=np.int64)
-    return best, np.ascontiguousarray(wp.T)
+        return sp.run(beta, F1d, F2d)
+    finally:
+        sp.close()

@@ -286,9 +286,20 @@ PRUNE_NCU = PruneSpec("chroma12_pairs4_N8000-10000_L2000_pruned", 4, 8000, 10000
 PRUNE_NCU_W4 = PruneSpec("chroma12_pairs20_N5000-6000_L1000_pruned", 20, 5000, 6000,
                          L_choices=(1000,), pad_frac=0.10)
 
+
+class ShardSpec(PairSpec):
+    """Named one-pair workload whose tiles are sharded across ranks."""
+
+
+# One square pair of 100000 x 100000 frames at L = 4000: 26 x 26 = 676 tiles,
+# 1.0e10 DP cells, far more tiles than one GPU has SMs; its tiles split
+# across ranks (one edge exchange), or all on one GPU (89 GB of FP64 cost).
+SHARD1 = ShardSpec("chroma12_pair_100000x100000_L4000_tile_sharded", 100000, 100000, 4000)
+
 WORKLOADS = {"config0": CONFIG0, "config1": CONFIG1, "ncu_small": NCU_SMALL,
              "batch256": BATCH256, "precision2048": PRECISION2048, "prune64": PRUNE64,
-             "prune_ncu": PRUNE_NCU, "prune_ncu_w4": PRUNE_NCU_W4}
+             "prune_ncu": PRUNE_NCU, "prune_ncu_w4": PRUNE_NCU_W4,
+             "shard1": SHARD1}
 
 
 def make_pair(spec: PairSpec):
