@@ -160,6 +160,63 @@ class TileProposer:
                                     _p(arg), current_stream_ptr()))
         return score, arg, (n1, n2)
 
+    # -- inference into preallocated buffers (graph-capturable) ---------------
+    @staticmethod
+    def buffers(d, N, M, L, device):
+        """Device buffers of one proposer pass for pairs of up to N x M frames
+        at tile length L (every kernel takes its sizes explicitly, so a set
+        sized for the largest pair serves any smaller one)."""
+        P1, P2 = -(-N // POOL), -(-M // POOL)
+        H, W = P1, P2
+        dims = []
+        for st in STRIDES:
+            H, W = (H - 1) // st + 1, (W - 1) // st + 1
+            dims.append((H, W))
+        hop = L - 1
+        nt = -(-(N - 1) // hop) * -(-(M - 1) // hop)
+        f32, bf = dict(dtype=torch.float32, device=device), dict(dtype=torch.bfloat16,
+                                                                 device=device)
+        return {"A": torch.empty(d * P1, **f32), "B": torch.empty(d * P2, **f32),
+                "pooled": torch.empty(P1 * P2, **f32), "sc": torch.empty(P1 + P2 + 2, **f32),
+                "y1": torch.empty(CH * dims[0][0] * dims[0][1], **bf),
+                "y2": torch.empty(CH * dims[1][0] * dims[1][1], **bf),
+                "y3": torch.empty(dims[2][0] * dims[2][1], **f32),
+                "score": torch.empty(max(nt, 1), **f32),
+                "arg": torch.empty(max(nt, 1), dtype=torch.int32, device=device)}
+
+    def propose_into(self, f1, f2, L, bufs, mask, threshold=None, dilation=1, manhattan=None):
+        """The inference of ``propose`` from device features (d x N, d x M,
+        FP64) into preallocated ``bufs`` (``buffers``), writing the tile mask
+        into the uint8 device tensor ``mask`` (n1 * n2 entries).  Launches
+        only library kernels on the current stream, allocates nothing."""
+        lib = _lib.load()
+        s = current_stream_ptr()
+        d, N = int(f1.shape[0]), int(f1.shape[1])
+        M = int(f2.shape[1])
+        P1, P2 = -(-N // POOL), -(-M // POOL)
+        _lib.check(lib.pfx_pool_features(_p(f1), d, N, POOL, _p(bufs["A"]), s))
+        _lib.check(lib.pfx_pool_features(_p(f2), d, M, POOL, _p(bufs["B"]), s))
+        _lib.check(lib.pfx_pooled_cost(_p(bufs["A"]), _p(bufs["B"]), d, P1, P2,
+                                       _p(bufs["pooled"]), s))
+        _lib.check(lib.pfx_pooled_center(_p(bufs["pooled"]), P1, P2, _p(bufs["sc"]), s))
+        x, x_bf, cin, H, W = bufs["pooled"], 0, 1, P1, P2
+        layers = ((self.params["w1"], self.params["b1"], CH, STRIDES[0], 1, bufs["y1"], 1),
+                  (self.params["w2"], self.params["b2"], CH, STRIDES[1], 1, bufs["y2"], 1),
+                  (self.params["w3"], self.params["b3"], 1, STRIDES[2], 0, bufs["y3"], 0))
+        for w, b, cout, st, relu, y, y_bf in layers:
+            Ho, Wo = (H - 1) // st + 1, (W - 1) // st + 1
+            _lib.check(lib.pfx_conv3x3_forward(_p(x), x_bf, cin, H, W, _p(w), _p(b), cout, st,
+                                               relu, _p(y), y_bf, s))
+            x, x_bf, cin, H, W = y, y_bf, cout, Ho, Wo
+        hop = L - 1
+        n1, n2 = -(-(N - 1) // hop), -(-(M - 1) // hop)
+        _lib.check(lib.pfx_tile_max(_p(x), H, W, n1, n2, hop, L, N, M, FPP, _p(bufs["score"]),
+                                    _p(bufs["arg"]), s))
+        thr = self.threshold if threshold is None else float(threshold)
+        manhattan = self.manhattan if manhattan is None else manhattan
+        _lib.check(lib.pfx_tile_mask_from_scores(_p(bufs["score"]), n1, n2, thr, int(dilation),
+                                                 int(bool(manhattan)), _p(mask), s))
+
     def propose(self, pooled, N, M, L, threshold=None, dilation=1, manhattan=None):
         """Device uint8 mask (n1 x n2) of the tiles to run, and the scores:
         tiles above the threshold, dilated by `dilation` tiles (Chebyshev
@@ -341,6 +398,7 @@ class PrunedBatch:
         self.manhattan = manhattan
         self.expand = int(expand)
         self._streams = None
+        self._graph = None
         self.L = int(L)
         self.steps, self.weights, self.precision = steps, weights, precision
         self.shapes = [(int(n), int(m)) for n, m in shapes]
@@ -364,23 +422,7 @@ class PrunedBatch:
                 marks.append((name, _time.perf_counter()))
 
         mark("start")
-        masks = torch.empty(int(self.offs[-1]), dtype=torch.uint8, device=self.proposer.device)
-        # the proposer's kernels are small: pairs run on several streams at once
-        main = torch.cuda.current_stream()
-        if self._streams is None:
-            self._streams = [torch.cuda.Stream(device=self.proposer.device)
-                             for _ in range(min(8, len(self.shapes)))]
-        for st in self._streams:
-            st.wait_stream(main)  # features loaded, masks allocated
-        for i, (N, M) in enumerate(self.shapes):
-            with torch.cuda.stream(self._streams[i % len(self._streams)]):
-                f1, f2 = b.feature_views(i)
-                pooled = self.proposer.pooled_cost(f1, f2)
-                m, _ = self.proposer.propose(pooled, N, M, self.L, self.threshold,
-                                             self.dilation, self.manhattan)
-                masks[self.offs[i]:self.offs[i + 1]] = m.reshape(-1)
-        for st in self._streams:
-            main.wait_stream(st)
+        masks = self._propose_all()
         mark("proposer")
         self.last_masks = masks  # the proposed tiles, pairs' (n1, n2) masks concatenated
         b.set_masks(masks)
@@ -432,6 +474,49 @@ class PrunedBatch:
             info["align_ms"] = dict(zip(("cost", "stage1", "stage2"), align_ms))
         return out, info
 
+    def _launch_proposer(self):
+        """Every pair's proposer pass, pairs spread over the side streams
+        (the kernels are small), each stream with its own buffer set."""
+        main = torch.cuda.current_stream()
+        for st in self._streams:
+            st.wait_stream(main)  # features loaded
+        for i, (N, M) in enumerate(self.shapes):
+            k = i % len(self._streams)
+            with torch.cuda.stream(self._streams[k]):
+                f1, f2 = self._views[i]
+                self.proposer.propose_into(f1, f2, self.L, self._bufs[k],
+                                           self._masks[self.offs[i]:self.offs[i + 1]],
+                                           self.threshold, self.dilation, self.manhattan)
+        for st in self._streams:
+            main.wait_stream(st)
+
+    def _propose_all(self):
+        """The tile masks of all pairs (uint8 device tensor, pairs' (n1, n2)
+        masks concatenated): one eager pass on the first call, which also
+        records the whole phase into a CUDA graph; the graph is replayed on
+        every later call (the features are read from the batch's fixed
+        buffers)."""
+        if self._graph is None:
+            dev = self.proposer.device
+            self._masks = torch.empty(int(self.offs[-1]), dtype=torch.uint8, device=dev)
+            self._views = [self.batch.feature_views(i) for i in range(len(self.shapes))]
+            ns = min(8, len(self.shapes))
+            self._streams = [torch.cuda.Stream(device=dev) for _ in range(ns)]
+            self._bufs = []
+            for k in range(ns):
+                mine = self.shapes[k::ns]
+                self._bufs.append(TileProposer.buffers(self.batch.d, max(n for n, _ in mine),
+                                                       max(m for _, m in mine), self.L, dev))
+            self._launch_proposer()
+            torch.cuda.current_stream().synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._launch_proposer()
+            self._graph = g
+            return self._masks
+        self._graph.replay()
+        return self._masks
+
     def _expand(self, i, N, M, beta, add, mk):
         """Adds `add` (the pruned tiles the path came near) to pair i's run
         and aligns it again (stage 1 only on the added tiles), up to
@@ -472,4 +557,5 @@ class PrunedBatch:
             return bc, wp
 
     def close(self):
+        self._graph = None
         self.batch.close()

@@ -338,3 +338,34 @@ def test_trained_proposer_gain_on_held_out_pairs():
     assert t["skipped_fraction"] > 0.5, t
     assert t["tiles_run"] < 0.5 * t["tiles_total"], t
     assert u["tiles_run"] > t["tiles_run"], (t, u)
+
+
+def test_propose_into_and_graph_replay_match_propose():
+    """The preallocated, graph-captured proposer pass of PrunedBatch gives the
+    masks of the allocating per-pair path (propose), on the eager first run
+    and on later graph replays with other features in the same buffers."""
+    rng = np.random.default_rng(21)
+    sizes = [(5200, 6100), (4100, 3900), (6000, 5300)]
+    sets = [[W.warped_pair(rng, n, m) for n, m in sizes] for _ in range(2)]
+    L = 500
+    net = TileProposer.load()
+
+    def per_pair(pairs):
+        out = []
+        for F1, F2 in pairs:
+            f1, f2 = torch.from_numpy(F1).cuda(), torch.from_numpy(F2).cuda()
+            m, _ = net.propose(net.pooled_cost(f1, f2), f1.shape[1], f2.shape[1], L)
+            out.append(m.reshape(-1).cpu().numpy())
+        return np.concatenate(out)
+
+    want = [per_pair(p) for p in sets]
+    pb = pf.PrunedBatch(sizes, L, STD, WTS, 12, proposer=net)
+    results = []
+    for k in (0, 1, 0):
+        pb.load(sets[k])
+        out, _ = pb.run(0.1)
+        assert np.array_equal(pb.last_masks.cpu().numpy(), want[k]), k
+        results.append(out)
+    for (b1, w1), (b3, w3) in zip(results[0], results[2]):
+        assert b1 == b3 and np.array_equal(w1, w3)
+    pb.close()
