@@ -459,7 +459,7 @@ def batch_arm(args, spec):
     tuner = Autotuner(candidates_L=spec.L_choices)
     Ls, warps = tuner.choose(shapes, spec.steps, spec.weights, spec.d)
     tune_s = time.perf_counter() - t0
-    b = Batch(shapes, Ls, spec.steps, spec.weights, spec.d, warps=warps)
+    b = Batch(shapes, Ls, spec.steps, spec.weights, spec.d, warps=warps, cost=args.cost)
     cells = b.cells
     b.load(pairs)
     # one direct run with phase events (cost building, stage 1, stage 2)
@@ -562,6 +562,9 @@ def batch_arm(args, spec):
                     "autotune_table": {k: list(v) for k, v in tuner.table.items()},
                     "autotune_seconds": tune_s, "parallelism": "replicas",
                     "graph": "whole batch recorded once, replayed per step",
+                    "cost_build": ("inside the stage-1 kernel, tile by tile, one launch"
+                                   if b.cost_in_kernel else
+                                   "separate cost kernels into slabs, in waves"),
                     "l2": "cost slabs and features larger than L2 (no flush needed)",
                     "input": "features resident in HBM; the timed step builds the cost"})
         line = {
@@ -973,13 +976,14 @@ def prune_arm(args, spec):
         return float(t.item())
 
     # --- plain form: every tile, FP64, one batch (waves), graph replay --------
-    bp = Batch(shapes, Lb, spec.steps, spec.weights, 12)
+    bp = Batch(shapes, Lb, spec.steps, spec.weights, 12, cost=args.cost)
     bp.load(pairs)
     bp.run(spec.beta, use_graph=False)
     ph_plain = bp.timing()
     best0, end0, lens0 = bp.results()
     paths0 = bp.paths(lens0)
-    plain_info = {"waves": bp.waves, "warps_per_tile": bp.warps, "tiles": bp.tiles}
+    plain_info = {"waves": bp.waves, "warps_per_tile": bp.warps, "tiles": bp.tiles,
+                  "cost_in_stage1": bp.cost_in_kernel}
     for _ in range(max(1, args.warmup - 1)):
         bp.run(spec.beta)
     if ws > 1:
@@ -991,7 +995,8 @@ def prune_arm(args, spec):
     torch.cuda.empty_cache()
 
     # --- chosen form: proposer + kept tiles only, FP64 ----------------------
-    pb = pf.PrunedBatch(shapes, Lb, spec.steps, spec.weights, 12, proposer=net)
+    pb = pf.PrunedBatch(shapes, Lb, spec.steps, spec.weights, 12, proposer=net,
+                        cost=args.cost)
     pb.load(pairs)
     for _ in range(args.warmup):
         out, info = pb.run(spec.beta)
@@ -1110,6 +1115,9 @@ def prune_arm(args, spec):
             "config": dict(spec.describe(), pairs_run=n_pairs, cells_per_step=cells,
                            generation_seconds=gen_s, parallelism="replicas",
                            input="features resident in HBM; every step builds the cost",
+                           cost_build=("inside the stage-1 kernel, tile by tile"
+                                       if args.cost == "tile" else
+                                       "separate cost kernels into slabs, in waves"),
                            timing="CUDA events around whole steps (host-side proposer mask "
                                   "read-back and fallback checks included)",
                            l2="cost slabs larger than L2 (no flush needed)"),
@@ -1300,6 +1308,9 @@ def shard_arm(args, spec):
             "config": dict(spec.describe(), N=N, M=M, tiles=n1 * n2, cells_per_step=cells,
                            parallelism=f"tiles over {ws} rank(s)",
                            input="features resident in HBM; every step builds the cost",
+                           cost_build=("inside the stage-1 kernel, tile by tile"
+                                       if args.cost == "tile" else
+                                       "separate cost kernels into slabs, in waves"),
                            l2="cost slabs larger than L2 (no flush needed)"),
             "pairs_per_s": args.steps / (ms_total / 1e3),
             "per_rank": {"cost_ms_max": cost_ms, "stage1_ms_max": s1_ms,
@@ -1350,6 +1361,10 @@ def main():
     ap.add_argument("--cpu-repeats", type=int, default=3,
                     help="learned-pruning workload: timed runs of the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cost", default="slabs", choices=["slabs", "tile"],
+                    help="FP64 batches: build the cost with separate cost kernels into "
+                         "slabs, in waves (slabs), or inside the stage-1 kernel, tile by tile, "
+                         "in one launch (tile)")
     args = ap.parse_args()
     spec = W.WORKLOADS[args.workload]
     if isinstance(spec, W.ShardSpec):

@@ -279,14 +279,25 @@ int pfx_flexdtw_tile_noalloc(const double *C, int64_t ldc, int32_t R, int32_t W,
  * tensor cores as pfx_plan_load_features_bf16 does); pair i has its
  * own shape (N[i], M[i]) and tile length L[i].  It owns, in one device
  * arena, a plan per pair (pfx_batch_plan), the raw feature inputs, one
- * pool of tile-skewed cost slabs and the stage-1 tile queues.  Pairs are
- * packed into "waves" whose cost slabs fit the pool (wave_bytes; 0 = 70 %
- * of the device memory the batch's other buffers leave free); per wave, the cost of every pair is built
- * from its features, ONE persistent stage-1 launch runs all tiles of all
- * pairs of the wave (largest first) from a device work queue, and stage 2
- * of the pairs runs on forked streams, overlapping the next waves.
- * pfx_batch_run records this whole
- * sequence once into a CUDA graph and replays it.
+ * pool of tile-skewed cost slabs and the stage-1 tile queues.
+ *
+ * By default the cost of every tile is built into the pool by separate
+ * cost kernels first: pairs are packed into "waves" whose cost slabs fit the
+ * pool (wave_bytes; 0 = 70 % of the device memory the batch's other buffers
+ * leave free); per wave, the cost of every pair is built from its features,
+ * ONE persistent stage-1 launch runs all tiles of all pairs of the wave
+ * (largest first) from a device work queue, and stage 2 of the pairs runs
+ * on forked streams, overlapping the next waves.
+ *
+ * With PFX_BATCH_TILE_COST in `precision` (FP64, d <= 16) the stage-1
+ * kernel builds each tile's cost itself: the CTA that claims a tile writes
+ * its cost into the CTA's own slab of the pool (one slab per resident CTA),
+ * then runs the DP on it.  ONE persistent stage-1 launch then runs all
+ * tiles of all pairs, whatever the batch's size, with a pool of about
+ * 592 slabs instead of one per tile.
+ *
+ * pfx_batch_run records this whole sequence once into a CUDA graph and
+ * replays it.
  *
  * The reference has no batch entry point: its notebooks loop over pairs
  * calling parflex / tiled_stage1_from_features + run_stage2_from_tiled
@@ -295,15 +306,23 @@ int pfx_flexdtw_tile_noalloc(const double *C, int64_t ldc, int32_t R, int32_t W,
  * ------------------------------------------------------------------------- */
 typedef struct pfx_batch pfx_batch;
 
+/* Flag for pfx_batch_create's `precision` (or-ed with PFX_FP64, d <= 16):
+ * the stage-1 kernel builds each tile's cost itself, one launch for every
+ * tile of every pair, instead of separate cost kernels filling slabs in
+ * waves.  Same results; for batches whose slabs would need many waves. */
+#define PFX_BATCH_TILE_COST 0x100
+
 /* nw: stage-1 warps per tile CTA (4, 8 or 16; 0 = chosen from the tile
- * count).  The batch is created on the current CUDA device. */
+ * count).  precision: a pfx_precision, optionally or-ed with
+ * PFX_BATCH_TILE_COST.  The batch is created on the current CUDA device. */
 int pfx_batch_create(int32_t n, const int64_t *N, const int64_t *M, const int32_t *L,
                      const int64_t *steps, const double *weights, int32_t n_steps,
                      int32_t d, int64_t wave_bytes, int32_t nw, int32_t precision,
                      pfx_batch **out);
 void pfx_batch_destroy(pfx_batch *batch);
-/* info[0..7] = n, waves, total tiles, DP cells (sum of tile R*W), device
- * bytes, stage-1 warps per CTA, largest wave's tiles, cost-slab pool bytes. */
+/* info[0..8] = n, waves, total tiles, DP cells (sum of tile R*W), device
+ * bytes, stage-1 warps per CTA, largest wave's tiles, cost-slab pool bytes,
+ * 1 when stage 1 builds each tile's cost itself (else 0). */
 int pfx_batch_info(const pfx_batch *batch, int64_t *info);
 /* Device input buffers of pair i: F1 (d x N[i]) and F2 (d x M[i]),
  * row-major by feature.  Fill them before pfx_batch_run (any stream, but
@@ -315,8 +334,9 @@ int pfx_batch_features(pfx_batch *batch, int32_t i, double **F1, double **F2);
 int pfx_batch_plan(pfx_batch *batch, int32_t i, pfx_plan **plan);
 /* Restricts every pair to the tiles set in its mask (masks: the pairs' n1*n2
  * masks concatenated in pair order; device memory when on_device): cost
- * slabs are built and stage 1 runs only there (the pool now holds only
- * those slabs, so waves are repacked), other tiles keep +inf edges.  For the
+ * slabs are built and stage 1 runs only there (with separate cost kernels
+ * the pool now holds only those slabs, so waves are repacked), other tiles
+ * keep +inf edges.  For the
  * learned tile proposer; synchronises `stream`; invalidates the recorded
  * graph.  Either form (FP64 or FP32).  No reference counterpart. */
 int pfx_batch_set_masks(pfx_batch *batch, const uint8_t *masks, int32_t on_device,

@@ -8,11 +8,14 @@ calling ``tiled_stage1_from_features`` + ``run_stage2_from_tiled`` or
 of each pair is, by construction, that of those calls.
 
 Device side (``pfx_batch_*`` in include/parflexdtw_b200.h): one arena holds
-every pair's plan; pairs are packed into waves whose FP64 cost slabs fit a
-memory pool; per wave the cost of each pair is built from its features, ONE
-persistent stage-1 launch runs all tiles of all pairs of the wave from a
-device work queue, and stage 2 runs on forked streams.  The whole launch
-sequence is recorded once into a CUDA graph and replayed.
+every pair's plan.  Pairs are packed into waves whose cost slabs fit a
+memory pool; per wave the cost of each pair is built from its features by
+the cost kernels, then ONE persistent stage-1 launch runs all tiles of all
+pairs of the wave from a device work queue.  With ``cost="tile"`` (FP64,
+d <= 16) the stage-1 kernel builds each tile's cost itself, into one cost
+slab per resident CTA, and ONE launch runs every tile of every pair
+whatever the batch's size.  Stage 2 runs on forked streams.  The whole
+launch sequence is recorded once into a CUDA graph and replayed.
 """
 from __future__ import annotations
 
@@ -39,10 +42,13 @@ class Batch:
     of times (the CUDA graph is recorded on the first run)."""
 
     def __init__(self, shapes, L_per_pair, steps, weights, d, wave_bytes=0, warps=0,
-                 precision="fp64"):
+                 precision="fp64", cost="slabs"):
         lib = _lib.load()
         if precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32'")
+        if cost not in ("slabs", "tile"):
+            raise ValueError("cost must be 'slabs' (separate cost kernels, in waves) or 'tile' "
+                             "(FP64, d <= 16: built inside the stage-1 kernel, tile by tile)")
         self.precision = precision
         if not torch.cuda.is_available():
             raise RuntimeError("parflexdtw_b200 needs a CUDA device")
@@ -63,13 +69,16 @@ class Batch:
             n, _lib.i64_array([s[0] for s in self.shapes]), _lib.i64_array([s[1] for s in self.shapes]),
             _lib.i32_array(self.L), _lib.i64_array(st.reshape(-1)), _lib.f64_array(w), st.shape[0],
             self.d, int(wave_bytes), int(warps),
-            _lib.PFX_FP32 if precision == "fp32" else _lib.PFX_FP64, ct.byref(h)))
+            (_lib.PFX_FP32 if precision == "fp32" else _lib.PFX_FP64) |
+            (_lib.PFX_BATCH_TILE_COST if cost == "tile" else 0), ct.byref(h)))
         self._h = h
         self._fin = weakref.finalize(self, _free_batch, h)
-        info = (ct.c_int64 * 8)()
+        info = (ct.c_int64 * 9)()
         _lib.check(lib.pfx_batch_info(h, info))
         (self.n, self.waves, self.tiles, self.cells, self.device_bytes, self.warps,
-         self.max_wave_tiles, self.slab_bytes) = (int(x) for x in info)
+         self.max_wave_tiles, self.slab_bytes, gen) = (int(x) for x in info)
+        # True: stage 1 builds each tile's cost itself (one wave, one slab per CTA)
+        self.cost_in_kernel = bool(gen)
         self.device = torch.cuda.current_device()
         self._plans = {}
 
@@ -114,7 +123,7 @@ class Batch:
         m = masks.to(torch.uint8).contiguous()
         _lib.check(_lib.load().pfx_batch_set_masks(self._h, ct.c_void_p(m.data_ptr()), 1,
                                                    stream or current_stream_ptr()))
-        info = (ct.c_int64 * 8)()
+        info = (ct.c_int64 * 9)()
         _lib.check(_lib.load().pfx_batch_info(self._h, info))
         self.waves = int(info[1])
         self.masked = True
@@ -217,14 +226,17 @@ def _split_pair(pair):
 
 
 def parflex_batch(pairs, steps, weights, beta, L=None, wave_bytes=0, warps=0,
-                  use_graph=True, errors="raise", tuner=None, precision="fp64"):
+                  use_graph=True, errors="raise", tuner=None, precision="fp64", cost="slabs"):
     """ParFlex on every (F1, F2) feature pair of ``pairs`` in one device batch.
 
     Same argument conventions as ``parflex`` (features are d x frames, the
     cost is 1 - L2norm(F1)^T L2norm(F2) as in tiled_stage1_from_features).
     ``L``: one tile length for all pairs, one per pair, or None to let the
     autotuner pick per length bucket.  ``precision="fp32"`` runs the FP32
-    form (bf16 tensor-core cost, FP32 DP; d <= 256).  Returns a list with, per pair,
+    form (bf16 tensor-core cost, FP32 DP; d <= 256).  ``cost="tile"`` builds
+    the FP64 cost inside the stage-1 kernel, tile by tile, in one launch
+    instead of with separate cost kernels in waves (same results).  Returns
+    a list with, per pair,
     ``(best_cost, wp[2, K])``.  A pair whose scan finds no endpoint raises the
     reference's ValueError (``errors="raise"``) or yields None
     (``errors="none"``).
@@ -248,7 +260,7 @@ def parflex_batch(pairs, steps, weights, beta, L=None, wave_bytes=0, warps=0,
     else:
         Ls = L
     b = Batch(shapes, Ls, steps, weights, d, wave_bytes=wave_bytes, warps=warps,
-              precision=precision)
+              precision=precision, cost=cost)
     b.load(feats)
     b.run(beta, use_graph=use_graph)
     best, end, lens = b.results()

@@ -138,6 +138,10 @@ size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 struct pfx_batch {
     int n = 0, d = 0, nw = 0, device = 0, fp32 = 0, kp = 0;
+    // 1: stage 1 builds each tile's FP64 cost itself into the pool, one slab
+    // per resident CTA (gen), and every pair runs in one wave
+    int gen_cost = 0;
+    CostGen gen{nullptr, 0, 0, 0};
     Geo gq;  // step set and weights; L = largest tile length (ring sizing)
     std::vector<pfx_plan> plans;
     char* arena = nullptr;
@@ -233,9 +237,16 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
     if (!out || !N || !M || !L || !steps || !weights) return errf(PFX_ERR_ARG, "null argument");
     *out = nullptr;
     if (n < 1) return errf(PFX_ERR_ARG, "batch of %d pairs", n);
-    if (precision != PFX_FP64 && precision != PFX_FP32)
-        return errf(PFX_ERR_ARG, "precision %d: PFX_FP64 (0) or PFX_FP32 (1)", precision);
-    const int fp32 = precision == PFX_FP32;
+    const int form = precision & 0xff, flags = precision & ~0xff;
+    if ((form != PFX_FP64 && form != PFX_FP32) || (flags & ~PFX_BATCH_TILE_COST))
+        return errf(PFX_ERR_ARG,
+                    "precision %d: PFX_FP64 (0) or PFX_FP32 (1), optionally | "
+                    "PFX_BATCH_TILE_COST", precision);
+    const int fp32 = form == PFX_FP32;
+    const int gen_cost = (flags & PFX_BATCH_TILE_COST) != 0;
+    if (gen_cost && (fp32 || d < 1 || d > kGenMaxD))
+        return errf(PFX_ERR_ARG, "PFX_BATCH_TILE_COST needs PFX_FP64 and 1 <= d <= %d (d = %d)",
+                    kGenMaxD, d);
     if (d < 1 || (fp32 && d > 256))
         return errf(PFX_ERR_ARG, "feature dimension %d (the FP32 form takes 1..256)", d);
     const int kp = (d + 63) / 64 * 64;
@@ -253,6 +264,7 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
     b->n = n;
     b->d = d;
     b->fp32 = fp32;
+    b->gen_cost = gen_cost;
     b->kp = kp;
     b->plans.resize(n);
     int st = PFX_OK;
@@ -301,6 +313,8 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
     int64_t budget = wave_bytes;
     // default: 70 % of the memory the batch's other buffers leave free
     if (budget <= 0) budget = (int64_t)((freeb > fixed ? freeb - fixed : 0) / 10 * 7);
+    // stage 1 building the cost itself: no slab per tile, one wave
+    if (gen_cost) budget = INT64_MAX;
     std::vector<int> order(n);
     for (int i = 0; i < n; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return slab[a] > slab[c]; });
@@ -314,12 +328,12 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
     b->wave_first.push_back(0);
     for (int q = 0; q < n; ++q) {
         const int i = order[q];
-        if (cur + slab[i] > budget) {
+        if (!gen_cost && cur + slab[i] > budget) {
             b->wave_first.push_back(q);
             cur = 0;
         }
         pool_off[i] = cur;
-        cur += (slab[i] + 255) & ~(int64_t)255;
+        if (!gen_cost) cur += (slab[i] + 255) & ~(int64_t)255;
         pool = std::max(pool, cur);
         b->wave_pairs.push_back(i);
     }
@@ -342,6 +356,19 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
         batch_free(b);
         return errf(PFX_ERR_TOO_LARGE, "L=%d: the stage-1 rings do not fit in shared memory", maxL);
     }
+    if (gen_cost) {
+        // one slab (of the largest tile length) per CTA the stage-1 kernel keeps resident
+        const int slots = stage1_gen_slots(b->gq, b->nw, d);
+        if (slots <= 0) {
+            batch_free(b);
+            return errf(PFX_ERR_TOO_LARGE, "L=%d, %d warps: the in-kernel cost does not fit", maxL,
+                        b->nw);
+        }
+        b->gen.stride = skew_slab_elems(maxL);
+        b->gen.nslots = slots;
+        b->gen.d = d;
+        pool = (int64_t)slots * b->gen.stride * 8;
+    }
     // the remaining arena: raw features, descriptors, heads, status, results
     const size_t off_fin = arena;
     arena += fin_total;
@@ -358,6 +385,7 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
     cudaError_t e = cudaMalloc(&b->arena, arena);
     if (e == cudaSuccess) e = cudaMemset(b->arena, 0, arena);
     if (e == cudaSuccess) e = cudaMalloc(&b->slabs, (size_t)pool);
+    b->gen.slots = gen_cost ? b->slabs : nullptr;
     if (e != cudaSuccess) {
         batch_free(b);
         return errf(PFX_ERR_CUDA, "batch allocation (%zu + %lld B): %s", arena, (long long)pool,
@@ -391,7 +419,8 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
             p.feat = reinterpret_cast<double*>(b->arena + feat_off[i]);
             p.feat_d = d;
         }
-        p.Csk = reinterpret_cast<char*>(b->slabs) + pool_off[i];
+        p.Csk = gen_cost ? nullptr : reinterpret_cast<char*>(b->slabs) + pool_off[i];
+        p.gen_cost = gen_cost;
         p.cost_loaded = 1;
         p.s1.status = b->status;
         b->fin_off[i] = (int64_t)(fo / 8);
@@ -512,7 +541,7 @@ extern "C" int pfx_batch_set_masks(pfx_batch* b, const uint8_t* masks, int32_t o
     std::vector<int> order(n);
     for (int i = 0; i < n; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return bytes[a] > bytes[c]; });
-    if (bytes[order[0]] > (int64_t)b->slab_bytes)
+    if (!b->gen_cost && bytes[order[0]] > (int64_t)b->slab_bytes)
         return errf(PFX_ERR_TOO_LARGE, "pair %d needs %lld B of cost slabs; pool %zu B", order[0],
                     (long long)bytes[order[0]], b->slab_bytes);
     std::vector<int> wave_pairs, wave_first{0};
@@ -520,12 +549,12 @@ extern "C" int pfx_batch_set_masks(pfx_batch* b, const uint8_t* masks, int32_t o
     int64_t cur = 0;
     for (int q = 0; q < n; ++q) {
         const int i = order[q];
-        if (cur + bytes[i] > (int64_t)b->slab_bytes) {
+        if (!b->gen_cost && cur + bytes[i] > (int64_t)b->slab_bytes) {
             wave_first.push_back(q);
             cur = 0;
         }
         off[i] = cur;
-        cur += bytes[i];
+        if (!b->gen_cost) cur += bytes[i];
         wave_pairs.push_back(i);
     }
     wave_first.push_back(n);
@@ -565,7 +594,7 @@ extern "C" int pfx_batch_set_masks(pfx_batch* b, const uint8_t* masks, int32_t o
         for (int q = wave_first[w]; q < wave_first[w + 1]; ++q) {
             const int i = wave_pairs[q];
             pfx_plan& p = b->plans[i];
-            p.Csk = reinterpret_cast<char*>(b->slabs) + off[i];
+            p.Csk = b->gen_cost ? nullptr : reinterpret_cast<char*>(b->slabs) + off[i];
             const int nt = p.g.n1 * p.g.n2;
             BCK(cudaMemcpyAsync(p.tile_slot, stage(slots[i].data(), (size_t)nt * 4),
                                 (size_t)nt * 4, cudaMemcpyHostToDevice, s));
@@ -627,7 +656,7 @@ extern "C" int pfx_batch_complete(pfx_batch* b, int32_t i, double beta, const ui
     if (!b->ran) return errf(PFX_ERR_ARG, "pfx_batch_complete needs a run since pfx_batch_set_masks");
     pfx_plan& p = b->plans[i];
     const int nt = p.g.n1 * p.g.n2;
-    if (plan_slab_bytes(&p) > (int64_t)b->slab_bytes)
+    if (!b->gen_cost && plan_slab_bytes(&p) > (int64_t)b->slab_bytes)
         return errf(PFX_ERR_TOO_LARGE, "pair %d: its cost slabs exceed the pool", i);
     cudaStream_t s = (cudaStream_t)stream;
     BCK(cudaStreamSynchronize(s));  // the pool and the queue buffers are free again
@@ -647,7 +676,10 @@ extern "C" int pfx_batch_complete(pfx_batch* b, int32_t i, double beta, const ui
     BCK(cudaMemcpyAsync(p.tile_list, list.data(), list.size() * 4, cudaMemcpyHostToDevice, s));
     const double* F1 = b->fin + b->fin_off[i];
     const double* F2 = F1 + (int64_t)b->d * p.g.N;
-    if (b->fp32) {
+    if (b->gen_cost) {
+        // stage 1 builds the cost of the tiles it runs from the features the
+        // masked run normalised
+    } else if (b->fp32) {
         // the bf16 features of the run
         const char* A = static_cast<const char*>(p.fbf);
         const char* B = A + (size_t)p.g.N * b->kp * 2;
@@ -665,7 +697,7 @@ extern "C" int pfx_batch_complete(pfx_batch* b, int32_t i, double beta, const ui
     // stage 1 on the tiles added now (the others' outputs stand; tiles never
     // run keep the +inf edges of the masked run)
     std::vector<TileDesc> pd((size_t)nt), todo;
-    plan_tile_descs(&p, b->slabs, pd.data());
+    plan_tile_descs(&p, b->gen_cost ? nullptr : b->slabs, pd.data());
     for (const TileDesc& d : pd)
         if (run[d.tile]) todo.push_back(d);
     // queue space past the masked waves' queues: the masked-out tiles of
@@ -677,12 +709,15 @@ extern "C" int pfx_batch_complete(pfx_batch* b, int32_t i, double beta, const ui
         BCK(cudaMemcpyAsync(qd, todo.data(), todo.size() * sizeof(TileDesc),
                             cudaMemcpyHostToDevice, s));
         BCK(cudaMemsetAsync(head, 0, sizeof(int), s));
-        const int nw = stage1_queue_warps((int)todo.size(), b->gq.L, num_sms_cur());
+        // (the in-kernel cost's pool holds slabs for the batch's own warps choice)
+        const int nw = b->gen_cost ? 0 : stage1_queue_warps((int)todo.size(), b->gq.L,
+                                                            num_sms_cur());
         BCK(launch_stage1_queue(qd, (int)todo.size(), nullptr, head, b->gq, b->status,
-                                nw ? nw : b->nw, b->fp32 != 0, s));
+                                nw ? nw : b->nw, b->fp32 != 0, s,
+                                b->gen_cost ? &b->gen : nullptr));
     }
     void* masked_Csk = p.Csk;
-    p.Csk = b->slabs;
+    p.Csk = b->gen_cost ? nullptr : b->slabs;
     int st = pfx_stage2_propagate(&p, nullptr, 0, stream);
     if (!st) st = pfx_stage2_scan(&p, beta, stream);
     if (!st) st = pfx_stage2_stitch(&p, 1, 0, 0, 0, 0, stream);
@@ -707,6 +742,7 @@ extern "C" int pfx_batch_info(const pfx_batch* b, int64_t* info) {
     info[5] = b->nw;
     info[6] = b->max_wave_tiles;
     info[7] = (int64_t)b->slab_bytes;
+    info[8] = b->gen_cost;
     return PFX_OK;
 }
 
@@ -768,8 +804,9 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
                 double* Bn = p.feat + (int64_t)b->d * p.g.N;
                 BCK(launch_l2norm(F1, b->d, p.g.N, An, s));
                 BCK(launch_l2norm(F2, b->d, p.g.M, Bn, s));
-                BCK(launch_cost_skew(An, Bn, b->d, p.g, static_cast<double*>(p.Csk),
-                                     p.skew_stride, s, slot, list, p.n_kept));
+                if (!b->gen_cost)  // (else stage 1 builds each tile's cost)
+                    BCK(launch_cost_skew(An, Bn, b->d, p.g, static_cast<double*>(p.Csk),
+                                         p.skew_stride, s, slot, list, p.n_kept));
             }
             if (b->masked) {
                 // skipped tiles keep +inf edges and start 0 for stage 2
@@ -779,15 +816,20 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
         }
         BCK(mark(w, 1));
         BCK(launch_stage1_queue(b->descs + b->wave_desc_off[w], (int)b->wave_tiles[w], nullptr,
-                                b->heads + w,
-                                b->gq, b->status, b->nw, b->fp32 != 0, s));
+                                b->heads + w, b->gq, b->status, b->nw, b->fp32 != 0, s,
+                                b->gen_cost ? &b->gen : nullptr));
         BCK(mark(w, 2));
         // stage 2 reads the cost slabs only in its edge gather: that part
         // stays on the main stream, so the next wave may overwrite the pool
         // while the rest of this wave's stage 2 runs on the side streams
         for (int q = q0; q < q1; ++q) {
             const pfx_plan& p = b->plans[b->wave_pairs[q]];
-            BCK(launch_stage2_edges(nullptr, p.Csk, p.skew_stride, p.fp32 != 0, p.g, p.s2, s));
+            if (b->gen_cost)  // no slabs kept: overlap costs from the features
+                BCK(launch_stage2_edges(nullptr, nullptr, 0, false, p.g, p.s2, s, p.feat,
+                                        p.feat + (int64_t)b->d * p.g.N, b->d));
+            else
+                BCK(launch_stage2_edges(nullptr, p.Csk, p.skew_stride, p.fp32 != 0, p.g, p.s2,
+                                        s));
         }
         BCK(mark(w, 3));
         BCK(cudaEventRecord(b->fork_ev, s));

@@ -252,8 +252,15 @@ void pfx::plan_tile_descs(const pfx_plan* p, const void* Csk, TileDesc* out,
         memset(&d, 0, sizeof(d));
         tile_rect(g, t / g.n2, t % g.n2, &r0, &c0, &d.R, &d.W);
         const int64_t slab = slot ? slot[t] : t;
-        d.Csk = slab < 0 ? nullptr
-                         : static_cast<const char*>(Csk) + slab * p->skew_stride * (p->fp32 ? 4 : 8);
+        d.Csk = (slab < 0 || !Csk)
+                    ? nullptr
+                    : static_cast<const char*>(Csk) + slab * p->skew_stride * (p->fp32 ? 4 : 8);
+        if (p->feat && p->feat_d > 0) {  // for a stage 1 that builds the cost itself
+            d.fa = p->feat + r0;
+            d.fb = p->feat + (int64_t)p->feat_d * g.N + c0;
+            d.lda = (int32_t)g.N;
+            d.ldb = (int32_t)g.M;
+        }
         d.Bw = p->s1.Bw + (int64_t)t * g.b_words;
         d.eD = p->s1.edge_D + (int64_t)t * 2 * g.L;
         d.eP = p->s1.edge_P + (int64_t)t * 2 * g.L;
@@ -509,6 +516,9 @@ extern "C" int pfx_plan_load_features_bf16(pfx_plan* p, const double* F1, const 
 extern "C" int pfx_stage1(pfx_plan* p, const double* C, int64_t ldc, void* stream) {
     if (!p) return fail(PFX_ERR_ARG, "null plan");
     int st;
+    if (p->gen_cost)
+        return fail(PFX_ERR_ARG, "a batch plan whose stage 1 builds the cost itself keeps no "
+                                 "cost slabs: run it through pfx_batch_run");
     if (C && (st = pfx_plan_load_cost(p, C, ldc, stream))) return st;
     if (!p->cost_loaded) return fail(PFX_ERR_ARG, "no cost matrix loaded into the plan");
     cudaStream_t s = (cudaStream_t)stream;
@@ -566,6 +576,13 @@ extern "C" int pfx_stage2_edges(pfx_plan* p, const double* C, int64_t ldc, void*
         g.ldc = ldc;
     } else if (!p->cost_loaded) {
         return fail(PFX_ERR_ARG, "no cost matrix loaded into the plan");
+    }
+    if (p->gen_cost) {
+        // a batch whose stage 1 built each tile's cost itself keeps no slabs:
+        // the overlap costs come from the normalised features
+        CK(launch_stage2_edges(nullptr, nullptr, 0, false, g, p->s2, (cudaStream_t)stream,
+                               p->feat, p->feat + (int64_t)p->feat_d * g.N, p->feat_d));
+        return PFX_OK;
     }
     // the FP32 form reads overlap costs from its own FP32 slabs (the values
     // its DP used), never from an FP64 C

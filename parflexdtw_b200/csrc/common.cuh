@@ -132,7 +132,25 @@ struct TileDesc {
     int32_t R, W;       // tile rows / columns
     int32_t L;          // edge-array stride (the alignment's tile length)
     int32_t tile;       // tile index within its alignment (row-major)
+    // normalised features of the tile's first row / first column, feature f
+    // of frame r at fa[f * lda + r] (fb: ldb); read when the stage-1 kernel
+    // builds the tile's cost itself (null otherwise)
+    const double* fa;
+    const double* fb;
+    int32_t lda, ldb;
 };
+
+// Stage 1 building each tile's FP64 cost itself (d > 0): a CTA writes the
+// tile-skewed cost of the tile it claimed into its own slot of `slots`
+// (`stride` doubles per slot, one slot per resident CTA: nslots), then runs
+// the DP on it.  d = 0: the cost slabs come with the descriptors.
+struct CostGen {
+    double* slots;
+    int64_t stride;
+    int32_t nslots;
+    int32_t d;
+};
+constexpr int kGenMaxD = 16;  // feature dimensions the in-kernel cost takes
 
 // Status word values written by kernels.
 constexpr int32_t kStatusWaitTimeout = 1;
@@ -179,9 +197,15 @@ void count_launches(int n);
 // weights of g; tiles at most g.L x g.L); `*head` must be 0 at launch; nw in
 // {4, 8, 16} warps per tile.
 // `ntiles_dev` (nullable): the queue length read on the device (at most ntiles).
+// `gen` (FP64 only, nullable or d = 0: off): every CTA builds the cost of
+// the tile it claims from the descriptors' features into its slot of
+// gen->slots, which must hold stage1_gen_slots(g, nw, gen->d) slots.
 cudaError_t launch_stage1_queue(const TileDesc* descs, int ntiles, const int* ntiles_dev,
                                 int* head, const Geo& g, int32_t* status, int nw, bool fp32,
-                                cudaStream_t st);
+                                cudaStream_t st, const CostGen* gen = nullptr);
+// Cost slots the in-kernel-cost form of the queue kernel needs: the CTAs
+// that can be resident at once (0: it does not fit).
+int stage1_gen_slots(const Geo& g, int nw, int d);
 // slot[t] = mask[t] ? t : -1.
 cudaError_t launch_mask_slots(const uint8_t* mask, int n, int32_t* slot, cudaStream_t st);
 // Keeps the descriptors whose tile is set in `mask`, in order; *count = kept.
@@ -258,8 +282,13 @@ cudaError_t launch_stage2(const double* C, const void* Csk, int64_t skew_stride,
                           const Geo& g, const S2Buf& b, cudaStream_t st);
 // launch_stage2 in two parts: the edge tensors (the only part that reads the
 // cost slabs) and the cross-tile propagation.
+// With An (normalised features, [d][N] and [d][M]) the overlap costs are
+// computed from the features in the cost kernels' order, not read from C or
+// the slabs (a batch whose stage 1 built its cost itself keeps no slabs).
 cudaError_t launch_stage2_edges(const double* C, const void* Csk, int64_t skew_stride, bool f32,
-                                const Geo& g, const S2Buf& b, cudaStream_t st);
+                                const Geo& g, const S2Buf& b, cudaStream_t st,
+                                const double* An = nullptr, const double* Bn = nullptr,
+                                int d = 0);
 cudaError_t launch_stage2_prop(const Geo& g, const S2Buf& b, cudaStream_t st);
 cudaError_t launch_sync_scan(const Geo& g, const S2Buf& b, int64_t buf, cudaStream_t st);
 cudaError_t launch_stitch(const Geo& g, const S2Buf& b, cudaStream_t st, int from_best,

@@ -26,6 +26,8 @@ struct pfx_plan {
     void* fbf;            // FP32 form: bf16 features, [N + M][fbf_kp]
     int fbf_kp;
     int cost_loaded;
+    int gen_cost;         // batch plan whose stage 1 builds each tile's cost from feat
+                          // (no slabs kept: Csk is null)
     // stage-1 tile queue of this plan (descriptors in queue order) and its head
     pfx::TileDesc* descs;
     int* head;

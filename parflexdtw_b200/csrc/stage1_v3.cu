@@ -623,11 +623,127 @@ __host__ __device__ inline int ring_len(int lag, int nw, int smem_limit, int vby
     return rb >= lag - 29 ? rb : 0;
 }
 
-template <int NW, bool STD, typename T>
+// ---------------------------------------------------------------------------
+// In-kernel cost (CostGen).  The CTA that claimed a tile first writes the
+// tile's tile-skewed FP64 cost into its own slot, then runs the DP on it, so
+// a batch needs one slot per resident CTA instead of a slab per tile, and
+// CTAs in their cost phase (FP64-pipe bound) share the SMs with CTAs in their
+// DP phase (issue and latency bound).  Mapping and summation order are those
+// of k_cost_skew (layout.cu): units of two strips x (NW * 32) steps; the
+// unit's column features are staged in shared memory split by column parity
+// and the two strips' row features as one (A, B) pair per lane; each warp
+// computes 32 steps of both strips in passes of 8 steps, in which 9 column
+// vectors serve 32 cells of a lane.  Cells outside the tile are 0, as in the
+// slabs.  The staging reuses the rings' shared memory, which holds nothing
+// between tiles.
+constexpr int kGenCV = 4;
+
+__host__ __device__ constexpr int gen_window(int nw) { return nw * 32 + 66; }
+__host__ __device__ inline size_t gen_smem_bytes(int nw, int d) {
+    return (size_t)d * (gen_window(nw) + 128) * sizeof(double);
+}
+
+// 8-byte asynchronous global -> shared copy; `full` false: 8 zero bytes.
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool full) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src),
+                 "r"(full ? 8 : 0)
+                 : "memory");
+}
+
+template <int NW, int DMAX>
+__device__ __forceinline__ void gen_tile_cost(const double* __restrict__ fa, int lda,
+                                           const double* __restrict__ fb, int ldb, int R, int W,
+                                           int d, double* __restrict__ slab) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int U = NW * 32;
+    constexpr int CX = gen_window(NW), CH = CX / 2;
+    double* sB = reinterpret_cast<double*>(smem_raw);  // [d][2][CH]
+    double* sA = sB + d * CX;                          // [d][2 strips][64 rows]
+    const double2* sA2 = reinterpret_cast<const double2*>(sA);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int span = ceil_div32(W + kStripRows - 1, kBlk) * kBlk;
+    const int nS = ceil_div32(R, kStripRows);
+    const int nchunk = ceil_div32(span, U);
+    for (int kk = 0; 2 * kk < nS; ++kk) {
+        const bool two = 2 * kk + 1 < nS;
+        const int rA0 = 128 * kk + 2 * lane, rB0 = rA0 + 1, rA1 = rA0 + 64, rB1 = rA1 + 1;
+        double2* out0 = reinterpret_cast<double2*>(slab) + (int64_t)(2 * kk) * span * 32 + lane;
+        double2* out1 = out0 + (int64_t)span * 32;
+        for (int ch = 0; ch < nchunk; ++ch) {
+            const int ts = ch * U;
+            __syncthreads();  // every warp is done with the previous unit's features
+            // the unit's features, as asynchronous copies all in flight at once
+            // (zero-filled outside the tile)
+            for (int q = threadIdx.x; q < d * CX; q += NW * 32) {
+                const int f = q / CX, x = q - f * CX;
+                const int c = ts - 64 + x;
+                const bool in = c >= 0 && c < W;
+                cp_async8(sB + (f * 2 + (x & 1)) * CH + (x >> 1),
+                          in ? fb + (int64_t)f * ldb + c : fb, in);
+            }
+            if (ch == 0)
+                for (int q = threadIdx.x; q < d * 128; q += NW * 32) {
+                    const int f = q >> 7, r = 128 * kk + (q & 127);
+                    cp_async8(sA + q, r < R ? fa + (int64_t)f * lda + r : fa, r < R);
+                }
+            asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+            __syncthreads();
+#pragma unroll 1
+            for (int blk = 0; blk < 32 / kGenCV; ++blk) {
+                const int t0 = ts + 32 * warp + kGenCV * blk;  // warp-uniform
+                if (t0 >= span) break;
+                // b[j] holds window column x = xA0 - 1 + j, xA0 = t0 - ts + 64 - 2 lane
+                const int h0 = ((t0 - ts + 64) >> 1) - lane;
+                double accA0[kGenCV], accB0[kGenCV], accA1[kGenCV], accB1[kGenCV];
+#pragma unroll
+                for (int f = 0; f < DMAX; ++f) {
+                    if (f >= d) break;
+                    const double* se = sB + (f * 2) * CH;  // even x
+                    const double* so = se + CH;             // odd x
+                    double b[kGenCV + 1];
+#pragma unroll
+                    for (int j = 0; j <= kGenCV; ++j)
+                        b[j] = (j & 1) ? se[h0 + (j >> 1)] : so[h0 - 1 + (j >> 1)];
+                    const double2 a0 = sA2[(f * 2) * 32 + lane], a1 = sA2[(f * 2 + 1) * 32 + lane];
+#pragma unroll
+                    for (int v = 0; v < kGenCV; ++v) {
+                        const double pA0 = __dmul_rn(a0.x, b[v + 1]);
+                        const double pB0 = __dmul_rn(a0.y, b[v]);
+                        const double pA1 = __dmul_rn(a1.x, b[v + 1]);
+                        const double pB1 = __dmul_rn(a1.y, b[v]);
+                        accA0[v] = f == 0 ? pA0 : __dadd_rn(accA0[v], pA0);
+                        accB0[v] = f == 0 ? pB0 : __dadd_rn(accB0[v], pB0);
+                        accA1[v] = f == 0 ? pA1 : __dadd_rn(accA1[v], pA1);
+                        accB1[v] = f == 0 ? pB1 : __dadd_rn(accB1[v], pB1);
+                    }
+                }
+#pragma unroll
+                for (int v = 0; v < kGenCV; ++v) {
+                    const int tau = t0 + v;
+                    if (tau < span) {
+                        const int cA = tau - 2 * lane, cB = cA - 1;
+                        const bool inA = cA >= 0 && cA < W, inB = cB >= 0 && cB < W;
+                        out0[(int64_t)tau * 32] =
+                            make_double2((rA0 < R && inA) ? __dsub_rn(1.0, accA0[v]) : 0.0,
+                                         (rB0 < R && inB) ? __dsub_rn(1.0, accB0[v]) : 0.0);
+                        if (two)
+                            out1[(int64_t)tau * 32] =
+                                make_double2((rA1 < R && inA) ? __dsub_rn(1.0, accA1[v]) : 0.0,
+                                             (rB1 < R && inB) ? __dsub_rn(1.0, accB1[v]) : 0.0);
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();  // the slot holds the whole tile before any warp's DP reads it
+}
+
+template <int NW, bool STD, typename T, bool GEN = false>
 __global__ void __launch_bounds__(NW * 32, 16 / NW)
     k_stage1_v3(const TileDesc* __restrict__ descs, const int ntiles_max,
                 const int* __restrict__ ntiles_dev, int* __restrict__ head, const Geo g,
-                int32_t* __restrict__ status, const int RB) {
+                int32_t* __restrict__ status, const int RB, const CostGen gen) {
     using V2 = typename Vec2<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Rings<T> rg;
@@ -640,6 +756,7 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int prevw = (warp + NW - 1) % NW, nextw = (warp + 1) % NW;
     const int ntiles = ntiles_dev ? min(*ntiles_dev, ntiles_max) : ntiles_max;
+    if (GEN && (int)blockIdx.x >= gen.nslots) return;  // no cost slot (the launch prevents it)
     if (threadIdx.x == 0) s_abort = 0;
     cuda::atomic_ref<int, cuda::thread_scope_block> my_prog(prog[warp]);
     for (;;) {
@@ -652,9 +769,20 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW)
                 s_ttot = (s_sc.nS - 1) * s_sc.lag + s_sc.span;
             }
         }
-        if (threadIdx.x < NW) prog[threadIdx.x] = 0;
+        if (!GEN && threadIdx.x < NW) prog[threadIdx.x] = 0;
         __syncthreads();
         if (s_item >= ntiles || s_abort) return;
+        if constexpr (GEN) {
+            // the tile's cost into this CTA's slot (through the rings' shared
+            // memory, so the progress words are reset afterwards)
+            double* slot = gen.slots + (int64_t)blockIdx.x * gen.stride;
+            if (gen.d <= 12)
+                gen_tile_cost<NW, 12>(td.fa, td.lda, td.fb, td.ldb, td.R, td.W, gen.d, slot);
+            else
+                gen_tile_cost<NW, kGenMaxD>(td.fa, td.lda, td.fb, td.ldb, td.R, td.W, gen.d,
+                                            slot);
+            if (threadIdx.x < NW) prog[threadIdx.x] = 0;
+        }
         {
             // edge rows past the tile's extent stay +inf / 0 (the DP writes the rest)
             double* eD = td.eD;
@@ -669,7 +797,9 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW)
         const Sched2& sc = s_sc;
         const int lag = sc.lag;
         const int Ttot = s_ttot;
-        const V2* Ct = reinterpret_cast<const V2*>(td.Csk);
+        const V2* Ct =
+            GEN ? reinterpret_cast<const V2*>(gen.slots + (int64_t)blockIdx.x * gen.stride)
+                : reinterpret_cast<const V2*>(td.Csk);
 
         Wave<T> st;
         st.aD1 = st.aD2 = st.aD3 = st.bD1 = st.bD2 = st.xpD = 0;
@@ -955,27 +1085,51 @@ int stage1_queue_warps(int ntiles, int32_t L, int num_sms) {
     return smem_bytes(L, 16, cta_budget(16), 8) < (1u << 30) ? 16 : 0;
 }
 
-template <int NW, bool STD, typename T>
+// Dynamic shared memory of the queue kernel: the rings, or the in-kernel
+// cost's staging (gen_d > 0) where that is larger.
+static size_t queue_smem(int32_t L, int nw, int vbytes, int gen_d) {
+    const size_t ring = smem_bytes(L, nw, cta_budget(nw), vbytes);
+    const size_t gen = gen_d > 0 ? gen_smem_bytes(nw, gen_d) : 0;
+    return ring > gen ? ring : gen;
+}
+
+// CTAs of the queue kernel resident at once on this device (its grid size
+// for a long queue), or 0 when it does not fit.
+template <int NW, bool STD, typename T, bool GEN>
+static int queue_resident(const Geo& g, int gen_d, size_t* smem_out) {
+    const size_t smem = queue_smem(g.L, NW, (int)sizeof(T), gen_d);
+    if (smem >= ((size_t)1 << 30) || smem > (size_t)cta_budget(NW)) return 0;
+    auto kern = k_stage1_v3<NW, STD, T, GEN>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return 0;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NW * 32, smem) !=
+        cudaSuccess)
+        return 0;
+    if (smem_out) *smem_out = smem;
+    return sms * (per_sm < 1 ? 1 : per_sm);
+}
+
+template <int NW, bool STD, typename T, bool GEN>
 static cudaError_t launch_q_t(const TileDesc* descs, int ntiles, const int* ntiles_dev, int* head,
-                              const Geo& g, int32_t* status, cudaStream_t st) {
+                              const Geo& g, int32_t* status, cudaStream_t st,
+                              const CostGen& gen) {
     const int limit = cta_budget(NW);
     const Sched2 s = make_sched2(g.L, g.L, NW);
     const int rb = ring_len(s.lag, NW, limit, (int)sizeof(T));
     if (rb == 0) return cudaErrorInvalidValue;
-    const size_t smem = smem_bytes(g.L, NW, limit, (int)sizeof(T));
-    auto kern = k_stage1_v3<NW, STD, T>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NW * 32, smem);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) per_sm = 1;
-    const int grid = (int)std::min<int64_t>((int64_t)sms * per_sm, ntiles);
+    size_t smem = 0;
+    const int resident = queue_resident<NW, STD, T, GEN>(g, GEN ? gen.d : 0, &smem);
+    if (resident <= 0) return cudaErrorInvalidValue;
+    // with the in-kernel cost every CTA needs a cost slot of its own
+    if (GEN && gen.nslots < std::min(resident, ntiles)) return cudaErrorInvalidValue;
+    const int grid = std::min(resident, ntiles);
     if (grid <= 0) return cudaSuccess;
-    kern<<<grid, NW * 32, smem, st>>>(descs, ntiles, ntiles_dev, head, g, status, rb);
+    k_stage1_v3<NW, STD, T, GEN>
+        <<<grid, NW * 32, smem, st>>>(descs, ntiles, ntiles_dev, head, g, status, rb, gen);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -1061,28 +1215,59 @@ cudaError_t launch_stage1_cluster(const TileDesc* descs, int ntiles, int* head, 
                      : launch_cl_t<false, double>(descs, ntiles, head, g, status, st);
 }
 
-template <typename T>
+template <typename T, bool GEN>
 static cudaError_t launch_q_type(const TileDesc* descs, int ntiles, const int* nd, int* head,
-                                 const Geo& g, int32_t* status, int nw, cudaStream_t st) {
+                                 const Geo& g, int32_t* status, int nw, cudaStream_t st,
+                                 const CostGen& gen) {
     const bool std_steps = g.S == 3 && g.kind[0] == 0 && g.kind[1] == 1 && g.kind[2] == 2;
     switch (nw) {
         case 4:
-            return std_steps ? launch_q_t<4, true, T>(descs, ntiles, nd, head, g, status, st)
-                             : launch_q_t<4, false, T>(descs, ntiles, nd, head, g, status, st);
+            return std_steps
+                       ? launch_q_t<4, true, T, GEN>(descs, ntiles, nd, head, g, status, st, gen)
+                       : launch_q_t<4, false, T, GEN>(descs, ntiles, nd, head, g, status, st, gen);
         case 8:
-            return std_steps ? launch_q_t<8, true, T>(descs, ntiles, nd, head, g, status, st)
-                             : launch_q_t<8, false, T>(descs, ntiles, nd, head, g, status, st);
+            return std_steps
+                       ? launch_q_t<8, true, T, GEN>(descs, ntiles, nd, head, g, status, st, gen)
+                       : launch_q_t<8, false, T, GEN>(descs, ntiles, nd, head, g, status, st, gen);
         default:
-            return std_steps ? launch_q_t<16, true, T>(descs, ntiles, nd, head, g, status, st)
-                             : launch_q_t<16, false, T>(descs, ntiles, nd, head, g, status, st);
+            return std_steps
+                       ? launch_q_t<16, true, T, GEN>(descs, ntiles, nd, head, g, status, st, gen)
+                       : launch_q_t<16, false, T, GEN>(descs, ntiles, nd, head, g, status, st,
+                                                       gen);
     }
 }
 
 cudaError_t launch_stage1_queue(const TileDesc* descs, int ntiles, const int* ntiles_dev,
                                 int* head, const Geo& g, int32_t* status, int nw, bool fp32,
-                                cudaStream_t st) {
-    return fp32 ? launch_q_type<float>(descs, ntiles, ntiles_dev, head, g, status, nw, st)
-                : launch_q_type<double>(descs, ntiles, ntiles_dev, head, g, status, nw, st);
+                                cudaStream_t st, const CostGen* gen) {
+    const CostGen off{nullptr, 0, 0, 0};
+    if (gen && gen->d > 0) {
+        if (fp32 || gen->d > kGenMaxD || !gen->slots) return cudaErrorInvalidValue;
+        return launch_q_type<double, true>(descs, ntiles, ntiles_dev, head, g, status, nw, st,
+                                           *gen);
+    }
+    return fp32 ? launch_q_type<float, false>(descs, ntiles, ntiles_dev, head, g, status, nw, st,
+                                              off)
+                : launch_q_type<double, false>(descs, ntiles, ntiles_dev, head, g, status, nw,
+                                               st, off);
+}
+
+int stage1_gen_slots(const Geo& g, int nw, int d) {
+    if (d < 1 || d > kGenMaxD) return 0;
+    const bool std_steps = g.S == 3 && g.kind[0] == 0 && g.kind[1] == 1 && g.kind[2] == 2;
+    switch (nw) {
+        case 4:
+            return std_steps ? queue_resident<4, true, double, true>(g, d, nullptr)
+                             : queue_resident<4, false, double, true>(g, d, nullptr);
+        case 8:
+            return std_steps ? queue_resident<8, true, double, true>(g, d, nullptr)
+                             : queue_resident<8, false, double, true>(g, d, nullptr);
+        case 16:
+            return std_steps ? queue_resident<16, true, double, true>(g, d, nullptr)
+                             : queue_resident<16, false, double, true>(g, d, nullptr);
+        default:
+            return 0;
+    }
 }
 
 // Order-preserving compaction of a tile queue by a tile mask (one CTA: a

@@ -33,12 +33,23 @@ __global__ void k_fill_f64(double* p, int64_t n, double v) {
         p[i] = v;
 }
 
+// 1 - sum_f a[f * lda] * b[f * ldb], every product and sum rounded in the
+// order f = 0, 1, ..., d-1: the value the cost kernels store for that cell.
+__device__ __forceinline__ double cost_from_features(const double* a, int64_t lda,
+                                                     const double* b, int64_t ldb, int d) {
+    double acc = __dmul_rn(a[0], b[0]);
+    for (int f = 1; f < d; ++f) acc = __dadd_rn(acc, __dmul_rn(a[f * lda], b[f * ldb]));
+    return __dsub_rn(1.0, acc);
+}
+
 // Edge tensors + valid mask (Parflex.py:509-564, 347-373, 582-624) -------
 // C: row-major cost (leading dimension g.ldc), or null to read the tile-skewed
 // copy Csk (per-tile stride `skew_stride` elements; FP32 elements when `f32`,
-// widened exactly to FP64).
+// widened exactly to FP64), or, with An non-null, computed from the
+// normalised features (An: [d][N], Bn: [d][M]).
 __global__ void k_edges(const double* __restrict__ C, const void* __restrict__ Csk,
-                        int64_t skew_stride, bool f32, const Geo g, S2Buf b) {
+                        int64_t skew_stride, bool f32, const Geo g, S2Buf b,
+                        const double* __restrict__ An, const double* __restrict__ Bn, int d) {
     const int64_t total = (int64_t)g.n1 * g.n2 * 2 * g.L;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
          q += (int64_t)gridDim.x * blockDim.x) {
@@ -59,9 +70,10 @@ __global__ void k_edges(const double* __restrict__ C, const void* __restrict__ C
         const int64_t si = slab * skew_stride + skew_index(W, sr, sc);
         // a tile stage 1 skipped has no cost slab: its edges are +inf anyway
         b.edge_Cf[q] = slab < 0 ? 0.0
-                                : (C ? C[(r0 + sr) * g.ldc + c0 + sc]
-                                     : (f32 ? (double)static_cast<const float*>(Csk)[si]
-                                            : static_cast<const double*>(Csk)[si]));
+                       : An ? cost_from_features(An + r0 + sr, g.N, Bn + c0 + sc, g.M, d)
+                       : (C ? C[(r0 + sr) * g.ldc + c0 + sc]
+                            : (f32 ? (double)static_cast<const float*>(Csk)[si]
+                                   : static_cast<const double*>(Csk)[si]));
         // mandatory slots: whole top edge of the last tile row, whole right
         // edge of the last tile column, and both ends of every edge
         const bool last = e == 0 ? (i == g.n1 - 1) : (j == g.n2 - 1);
@@ -534,7 +546,8 @@ cudaError_t launch_stage2(const double* C, const void* Csk, int64_t skew_stride,
 }
 
 cudaError_t launch_stage2_edges(const double* C, const void* Csk, int64_t skew_stride, bool f32,
-                                const Geo& g, const S2Buf& b, cudaStream_t st) {
+                                const Geo& g, const S2Buf& b, cudaStream_t st, const double* An,
+                                const double* Bn, int d) {
     const int64_t nslots = (int64_t)g.n1 * g.n2 * 2 * g.L;
     cudaError_t e;
     if ((e = cudaMemsetAsync(b.valid, 0, (size_t)nslots, st)) != cudaSuccess) return e;
@@ -543,7 +556,7 @@ cudaError_t launch_stage2_edges(const double* C, const void* Csk, int64_t skew_s
     {
         int64_t blocks = (nslots + 255) / 256;
         if (blocks > 8192) blocks = 8192;
-        k_edges<<<(int)blocks, 256, 0, st>>>(C, Csk, skew_stride, f32, g, b);
+        k_edges<<<(int)blocks, 256, 0, st>>>(C, Csk, skew_stride, f32, g, b, An, Bn, d);
         count_launches(1);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }

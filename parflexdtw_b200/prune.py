@@ -388,10 +388,10 @@ class PrunedBatch:
 
     def __init__(self, shapes, L, steps, weights, d, proposer=None, threshold=None,
                  dilation=1, manhattan=None, precision="fp64", wave_bytes=0, warps=0,
-                 expand=2):
+                 expand=2, cost="slabs"):
         from .batch import Batch
         self.batch = Batch(shapes, L, steps, weights, d, wave_bytes=wave_bytes, warps=warps,
-                           precision=precision)
+                           precision=precision, cost=cost)
         self.proposer = proposer or TileProposer.load()
         self.threshold = threshold
         self.dilation = dilation

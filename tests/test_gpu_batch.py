@@ -53,11 +53,16 @@ def _check(b, refs):
         assert same(paths[i].T, ref["wp"]), i
 
 
+@pytest.mark.parametrize("cost", ["tile", "slabs"])
 @pytest.mark.parametrize("warps", [4, 8, 16])
-def test_batch_one_wave_vs_oracle(reference, warps):
+def test_batch_one_wave_vs_oracle(reference, warps, cost):
+    """Either way of building the cost: inside the stage-1 kernel, tile by
+    tile ("tile"), or with separate cost kernels ("slabs")."""
     pairs, refs = reference
-    b = Batch([(p[0].shape[1], p[1].shape[1]) for p in pairs], LS, STD, WTS, 12, warps=warps)
+    b = Batch([(p[0].shape[1], p[1].shape[1]) for p in pairs], LS, STD, WTS, 12, warps=warps,
+              cost=cost)
     assert b.waves == 1 and b.warps == warps
+    assert b.cost_in_kernel == (cost == "tile")
     b.load(pairs)
     b.run(0.1)
     _check(b, refs)
@@ -67,17 +72,57 @@ def test_batch_one_wave_vs_oracle(reference, warps):
     b.close()
 
 
-def test_batch_waves_and_direct_launch(reference):
+@pytest.mark.parametrize("cost", ["tile", "slabs"])
+def test_batch_waves_and_direct_launch(reference, cost):
+    """A small slab pool splits a batch with separate cost kernels into
+    waves; with the cost built inside stage 1 every pair runs in one wave
+    whatever the pool would have held."""
     pairs, refs = reference
     shapes = [(p[0].shape[1], p[1].shape[1]) for p in pairs]
-    b = Batch(shapes, LS, STD, WTS, 12, wave_bytes=56 << 20, warps=4)
-    assert b.waves >= 2
+    b = Batch(shapes, LS, STD, WTS, 12, wave_bytes=56 << 20, warps=4, cost=cost)
+    if cost == "slabs":
+        assert b.waves >= 2
+    else:
+        assert b.waves == 1 and b.cost_in_kernel
     b.load(pairs)
     b.run(0.1, use_graph=False)
     _check(b, refs)
     b.run(0.1, use_graph=True)
     _check(b, refs)
     b.close()
+
+
+@pytest.mark.parametrize("d,steps,weights", [
+    (1, STD, WTS),
+    (5, [(1, 1), (2, 1)], [1.0, 2.5]),
+    (16, [(1, 2), (1, 1), (2, 1)], [3.0, 1.25, 3.0]),
+    (13, [(1, 1)], [2.0]),
+])
+def test_batch_cost_in_kernel_dims_and_steps_vs_oracle(oracle_mod, d, steps, weights):
+    """The in-kernel cost for every feature dimension it takes (both of its
+    unrolled forms, d <= 12 and 13..16) and other step sets, uneven tile
+    lengths and tiles of one row or column: bit-exact with the oracle on the
+    fixed-order host cost, and with the batch that builds slabs first."""
+    sizes = [(700, 900), (301, 64), (65, 640), (1200, 1100)]
+    Ls = [256, 64, 128, 500]
+    rng = np.random.default_rng(31 + d)
+    pairs = [W.warped_pair(rng, n, m, d=d, noise=0.1, latent="gaussian") if d > 1 else
+             (np.abs(rng.standard_normal((1, n))) + 0.1, np.abs(rng.standard_normal((1, m))) + 0.1)
+             for n, m in sizes]
+    shapes = [(p[0].shape[1], p[1].shape[1]) for p in pairs]
+    refs = [oracle_mod.parflex_full(W.cost_matrix_det(F1, F2), steps, weights, 0.1, Lb)
+            for (F1, F2), Lb in zip(pairs, Ls)]
+    got = {}
+    for cost in ("tile", "slabs"):
+        b = Batch(shapes, Ls, steps, weights, d, cost=cost)
+        assert b.cost_in_kernel == (cost == "tile")
+        b.load(pairs)
+        b.run(0.1)
+        _check(b, refs)
+        got[cost] = [b.plan(i).host("D_ARR") for i in range(b.n)]
+        b.close()
+    for x, y in zip(got["tile"], got["slabs"]):
+        assert same(x, y)
 
 
 def test_batch_beta_change_rerecords(oracle_mod):

@@ -201,10 +201,12 @@ def test_parflex_pruned_equals_full_and_falls_back():
     assert b2 == best and np.array_equal(wp2, wp)
 
 
-def test_batch_masks_and_pruned_batch_exact(oracle_mod):
+@pytest.mark.parametrize("cost", ["tile", "slabs"])
+def test_batch_masks_and_pruned_batch_exact(oracle_mod, cost):
     """Masked batches: all-ones masks and path-dilated masks reproduce the
     unmasked results bit for bit; PrunedBatch (any proposer) returns the
-    full-tile results, through its fallback when needed."""
+    full-tile results, through its fallback when needed.  With the cost
+    built inside stage 1 ("tile") or by separate cost kernels ("slabs")."""
     from parflexdtw_b200.batch import Batch
     rng = np.random.default_rng(12)
     sizes = [(2600, 2900), (1800, 1500), (3100, 3300)]
@@ -213,7 +215,8 @@ def test_batch_masks_and_pruned_batch_exact(oracle_mod):
     L = 300
     refs = [oracle_mod.parflex_full(W.cost_matrix_det(F1, F2), STD, WTS, 0.1, L)
             for F1, F2 in pairs]
-    b = Batch(shapes, L, STD, WTS, 12, warps=4)
+    b = Batch(shapes, L, STD, WTS, 12, warps=4, cost=cost)
+    assert b.cost_in_kernel == (cost == "tile")
     b.load(pairs)
     grids = [(-(-(n - 1) // (L - 1)), -(-(m - 1) // (L - 1))) for n, m in shapes]
     ones = torch.ones(sum(a * c for a, c in grids), dtype=torch.uint8, device="cuda")
@@ -289,7 +292,7 @@ def test_batch_masks_and_pruned_batch_exact(oracle_mod):
     b.close()
     net = TileProposer(seed=6)
     for thr in (-1e30, 1e30):  # everything kept / nothing kept (all fall back)
-        pb = pf.PrunedBatch(shapes, L, STD, WTS, 12, proposer=net, threshold=thr)
+        pb = pf.PrunedBatch(shapes, L, STD, WTS, 12, proposer=net, threshold=thr, cost=cost)
         pb.load(pairs)
         out, info = pb.run(0.1)
         for (bc, wp), r in zip(out, refs):
