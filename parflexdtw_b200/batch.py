@@ -191,7 +191,9 @@ class Batch:
         if self.n > 1:
             offs[1:] = np.cumsum(lens)[:-1]
         total = int(lens.sum())
-        flat = np.empty(max(2 * total, 2), dtype=np.int64)
+        # page-locked (torch's caching host allocator reuses the block once
+        # the arrays are dropped), so the copy runs at full link speed
+        flat = torch.empty(max(2 * total, 2), dtype=torch.int64, pin_memory=True).numpy()
         _lib.check(_lib.load().pfx_batch_copy_paths_rows(
             self._h, stream or current_stream_ptr(), flat.ctypes.data_as(_I64P),
             offs.ctypes.data_as(_I64P), lens.ctypes.data_as(_I64P), max(total, 1)))

@@ -24,6 +24,22 @@ struct Geo {
 };
 
 __host__ __device__ inline int64_t ceil_div64(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+#ifdef __CUDACC__
+// 8-byte asynchronous global -> shared copy (cp.async); `full` false writes 8
+// zero bytes and reads nothing (src must still be a valid address).  Copies
+// of a thread complete at cp_async_wait_all(); a barrier after it publishes
+// them to the CTA.
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool full) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src),
+                 "r"(full ? 8 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+}
+#endif
 __host__ __device__ inline int32_t ceil_div32(int32_t a, int32_t b) { return (a + b - 1) / b; }
 
 __host__ __device__ inline void tile_rect(const Geo& g, int ti, int tj, int64_t* r0, int64_t* c0,

@@ -111,16 +111,20 @@ __global__ void __launch_bounds__(kCostThreads, 2)
     const int nS = ceil_div32(R, kStripRows);
     if (2 * kk >= nS || ts >= span) return;
     const bool two = 2 * kk + 1 < nS;
+    // the features, as asynchronous copies all in flight at once (one
+    // memory latency per CTA, not one per element of a thread)
     for (int q = threadIdx.x; q < d * kCX; q += kCostThreads) {
         const int f = q / kCX, x = q - f * kCX;
         const int c = ts - 64 + x;
-        sB[(f * 2 + (x & 1)) * kCH + (x >> 1)] =
-            (c >= 0 && c < W) ? __ldg(Bn + (int64_t)f * g.M + c0 + c) : 0.0;
+        const bool in = c >= 0 && c < W;
+        cp_async8(sB + (f * 2 + (x & 1)) * kCH + (x >> 1), in ? Bn + (int64_t)f * g.M + c0 + c : Bn,
+                  in);
     }
     for (int q = threadIdx.x; q < d * 128; q += kCostThreads) {
         const int f = q >> 7, r = 128 * kk + (q & 127);
-        sA[q] = r < R ? __ldg(An + (int64_t)f * g.N + r0 + r) : 0.0;
+        cp_async8(sA + q, r < R ? An + (int64_t)f * g.N + r0 + r : An, r < R);
     }
+    cp_async_wait_all();
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int rA0 = 128 * kk + 2 * lane, rB0 = rA0 + 1, rA1 = rA0 + 64, rB1 = rA1 + 1;
@@ -214,9 +218,11 @@ __global__ void __launch_bounds__(kCostThreads, 2)
         for (int q = threadIdx.x; q < nf * kCX2; q += kCostThreads) {
             const int f = q / kCX2, x = q - f * kCX2;
             const int c = ts - 64 + x;
-            sB[(f * 2 + (x & 1)) * kCH2 + (x >> 1)] =
-                (c >= 0 && c < W) ? __ldg(Bn + (int64_t)(f0 + f) * g.M + c0 + c) : 0.0;
+            const bool in = c >= 0 && c < W;
+            cp_async8(sB + (f * 2 + (x & 1)) * kCH2 + (x >> 1),
+                      in ? Bn + (int64_t)(f0 + f) * g.M + c0 + c : Bn, in);
         }
+        cp_async_wait_all();
         __syncthreads();
         if (t0 < span) {
 #pragma unroll 4

@@ -494,13 +494,24 @@ __device__ __forceinline__ SelOut<T> select_exact_std_call(T w0, T w1, T w2, int
 // (each reads outputs of two steps back), and a small loop body stays in the
 // instruction cache (a 16-step unroll, or a second copy of the body, each
 // measured slower).
+//
+// MASK (a run-time flag, so that one copy of the loop body serves both: a
+// second inlined copy measured slower): the same path for a block of strip
+// k >= 1 at tau0 >= 80 (every cell at r >= 64, c >= 18, so every
+// predecessor of a cell inside the tile is inside too) that reaches the
+// tile's last column or its last row, or lies partly outside the tile (the
+// right end of a strip, the last strip): cells outside the tile (r >= R or
+// c >= W) are set to 0 and never call for the exact routine, cells on the
+// last row / column store their edge values, and the cost loads stop at the
+// strip's span.  Same results as run_block<true, true, PUSH, T>.
 template <bool PUSH, typename T>
 __device__ __forceinline__ void run_block_std(const Geo& g, Wave<T>& st, const Rings<T>& rg,
                                               char* wbase,
                                               const typename Vec2<T>::type* __restrict__ Cs,
                                               int tau0, int k, int lane, int prev_base,
                                               int mine_base, int rmask, int Tb, int lag,
-                                              const TileDesc& td, int nP, uint2* bw) {
+                                              const TileDesc& td, int nP, uint2* bw,
+                                              const bool MASK, int R, int W, int span) {
     using V2 = typename Vec2<T>::type;
     const unsigned F = 0xffffffffu;
     const T w0 = (T)g.w[0], w1 = (T)g.w[1], w2 = (T)g.w[2];
@@ -522,7 +533,7 @@ __device__ __forceinline__ void run_block_std(const Geo& g, Wave<T>& st, const R
             const int t = tq + u;
             const T rc = addr(rcq, (T)u);
             const V2 cc = st.q[u & 1];
-            st.q[u & 1] = __ldcs(cp + (int64_t)t * 32);
+            if (!MASK || tau0 + t + 2 < span) st.q[u & 1] = __ldcs(cp + (int64_t)t * 32);
             const int rs = (rs0 + t) & rmask;
             const V2 ringD = rD[rs];  // every lane reads the same slot; lane 0 keeps it
             const int2 ringP = rP[rs];
@@ -545,10 +556,18 @@ __device__ __forceinline__ void run_block_std(const Geo& g, Wave<T>& st, const R
             m1B_next = addr(m0B, (T)1);
             T oAD, oBD;
             int oAP, oBP, codeA, codeB;
-            const bool okA = select_std_m<T>(cc.x, w0, w1, w2, x1D, x1P, m0A, x2D, x2P, m1A,
-                                             x3D, x3P, m2A, oAD, oAP, codeA);
-            const bool okB = select_std_m<T>(cc.y, w0, w1, w2, st.aD2, st.aP2, m0B, st.aD3,
-                                             st.aP3, m1B, x2D, x2P, m1A, oBD, oBP, codeB);
+            bool okA = select_std_m<T>(cc.x, w0, w1, w2, x1D, x1P, m0A, x2D, x2P, m1A, x3D,
+                                       x3P, m2A, oAD, oAP, codeA);
+            bool okB = select_std_m<T>(cc.y, w0, w1, w2, st.aD2, st.aP2, m0B, st.aD3, st.aP3,
+                                       m1B, x2D, x2P, m1A, oBD, oBP, codeB);
+            bool actA = true, actB = true;
+            if (MASK) {
+                const int cA = tau0 + t - 2 * lane;
+                actA = rA < R && cA < W;
+                actB = rB < R && cA - 1 < W;
+                okA = okA || !actA;
+                okB = okB || !actB;
+            }
             if (__any_sync(F, !(okA && okB))) {
                 const int cA = tau0 + t - 2 * lane;
                 if (!okA) {
@@ -567,7 +586,19 @@ __device__ __forceinline__ void run_block_std(const Geo& g, Wave<T>& st, const R
                     codeB = o.code;
                 }
             }
-            if (lane == 31) {
+            if (MASK) {
+                const int cA = tau0 + t - 2 * lane, cB = cA - 1;
+                if (!actA) { oAD = 0; oAP = 0; codeA = 0; }
+                if (!actB) { oBD = 0; oBP = 0; codeB = 0; }
+                // edges are FP64 for stage 2 (exact widening in the FP32 form)
+                double* eD = td.eD;
+                int32_t* eP = td.eP;
+                if (actA && rA == R - 1) { eD[cA] = (double)oAD; eP[cA] = oAP; }
+                if (actB && rB == R - 1) { eD[cB] = (double)oBD; eP[cB] = oBP; }
+                if (actA && cA == W - 1) { eD[td.L + rA] = (double)oAD; eP[td.L + rA] = oAP; }
+                if (actB && cB == W - 1) { eD[td.L + rB] = (double)oBD; eP[td.L + rB] = oBP; }
+            }
+            if (lane == 31 && actB) {
                 // B of this step and A of the previous one: slot (step - 63)
                 const int ws = mine_base + ((Tb + t - 63) & rmask);
                 if (PUSH) {
@@ -590,7 +621,7 @@ __device__ __forceinline__ void run_block_std(const Geo& g, Wave<T>& st, const R
     }
     if (bw) {
         *bw = make_uint2(bitsA, bitsB);
-    } else {
+    } else if (!MASK || rA < R) {
         uint2* Bt = reinterpret_cast<uint2*>(td.Bw);
         Bt[((int64_t)k * nP + (tau0 >> 4)) * 32 + lane] = make_uint2(bitsA, bitsB);
     }
@@ -643,14 +674,6 @@ __host__ __device__ inline size_t gen_smem_bytes(int nw, int d) {
     return (size_t)d * (gen_window(nw) + 128) * sizeof(double);
 }
 
-// 8-byte asynchronous global -> shared copy; `full` false: 8 zero bytes.
-__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool full) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src),
-                 "r"(full ? 8 : 0)
-                 : "memory");
-}
-
 template <int NW, int DMAX>
 __device__ __forceinline__ void gen_tile_cost(const double* __restrict__ fa, int lda,
                                            const double* __restrict__ fb, int ldb, int R, int W,
@@ -687,7 +710,7 @@ __device__ __forceinline__ void gen_tile_cost(const double* __restrict__ fa, int
                     const int f = q >> 7, r = 128 * kk + (q & 127);
                     cp_async8(sA + q, r < R ? fa + (int64_t)f * lda + r : fa, r < R);
                 }
-            asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+            cp_async_wait_all();
             __syncthreads();
 #pragma unroll 1
             for (int blk = 0; blk < 32 / kGenCV; ++blk) {
@@ -837,18 +860,17 @@ __global__ void __launch_bounds__(NW * 32, 16 / NW)
 #pragma unroll
                     for (int q = 0; q < 2; ++q) st.q[q] = __ldcs(Cs + q * 32);
                 }
-                const bool interior = k >= 1 && k <= sc.nS - 2 && tau0 >= 80 && tau0 + 17 <= W;
-                if (interior) {
-                    if constexpr (STD)
-                        run_block_std<false, T>(g, st, rg, reinterpret_cast<char*>(rg.D), Cs,
-                                                tau0, k, lane, prevw * RB, warp * RB, RB - 1, Tb,
-                                                lag, td, sc.nP, nullptr);
-                    else
-                        run_block<false, STD, false>(g, st, rg,
-                                                     reinterpret_cast<const char*>(rg.D),
-                                                     reinterpret_cast<char*>(rg.D), Cs, sc.span,
-                                                     tau0, k, R, W, lane, prevw * RB, warp * RB,
-                                                     RB - 1, Tb, lag, td, sc.nP);
+                const bool lean = k >= 1 && tau0 >= 80;
+                const bool interior = lean && k <= sc.nS - 2 && tau0 + 17 <= W;
+                if (STD && lean) {
+                    run_block_std<false, T>(g, st, rg, reinterpret_cast<char*>(rg.D), Cs, tau0,
+                                            k, lane, prevw * RB, warp * RB, RB - 1, Tb, lag, td,
+                                            sc.nP, nullptr, !interior, R, W, sc.span);
+                } else if (!STD && interior) {
+                    run_block<false, STD, false>(g, st, rg, reinterpret_cast<const char*>(rg.D),
+                                                 reinterpret_cast<char*>(rg.D), Cs, sc.span, tau0,
+                                                 k, R, W, lane, prevw * RB, warp * RB, RB - 1, Tb,
+                                                 lag, td, sc.nP);
                 } else
                     run_block<true, STD, false>(g, st, rg, reinterpret_cast<const char*>(rg.D),
                                          reinterpret_cast<char*>(rg.D), Cs,
@@ -1009,17 +1031,17 @@ __global__ void __launch_bounds__(kClW * 32, 1)
 #pragma unroll
                     for (int q = 0; q < 2; ++q) st.q[q] = __ldcs(Cs + q * 32);
                 }
-                const bool interior = k >= 1 && k <= sc.nS - 2 && tau0 >= 80 && tau0 + 17 <= W;
-                if (interior) {
-                    if constexpr (STD)
-                        run_block_std<true, T>(g, st, rg, wbase, Cs, tau0, k, lane,
-                                               (pv % kClW) * RB, warp * RB, RB - 1, Tb, lag, td,
-                                               sc.nP, &bw);
-                    else
-                        run_block<false, STD, true>(g, st, rg, rbase, wbase, Cs, sc.span, tau0, k,
-                                                    R, W, lane, (pv % kClW) * RB, warp * RB,
-                                                    RB - 1, Tb, lag, td, sc.nP, &bw);
-                } else
+                const bool lean = k >= 1 && tau0 >= 80;
+                const bool interior = lean && k <= sc.nS - 2 && tau0 + 17 <= W;
+                if (STD && lean)
+                    run_block_std<true, T>(g, st, rg, wbase, Cs, tau0, k, lane,
+                                           (pv % kClW) * RB, warp * RB, RB - 1, Tb, lag, td,
+                                           sc.nP, &bw, !interior, R, W, sc.span);
+                else if (!STD && interior)
+                    run_block<false, STD, true>(g, st, rg, rbase, wbase, Cs, sc.span, tau0, k, R,
+                                                W, lane, (pv % kClW) * RB, warp * RB, RB - 1, Tb,
+                                                lag, td, sc.nP, &bw);
+                else
                     run_block<true, STD, true>(g, st, rg, rbase, wbase, Cs, sc.span, tau0, k, R, W,
                                          lane,
                                          (pv % kClW) * RB, warp * RB, RB - 1, Tb, lag, td,

@@ -388,7 +388,7 @@ class PrunedBatch:
 
     def __init__(self, shapes, L, steps, weights, d, proposer=None, threshold=None,
                  dilation=1, manhattan=None, precision="fp64", wave_bytes=0, warps=0,
-                 expand=2, cost="slabs"):
+                 expand=2, cost="slabs", proposer_streams=8):
         from .batch import Batch
         self.batch = Batch(shapes, L, steps, weights, d, wave_bytes=wave_bytes, warps=warps,
                            precision=precision, cost=cost)
@@ -397,6 +397,7 @@ class PrunedBatch:
         self.dilation = dilation
         self.manhattan = manhattan
         self.expand = int(expand)
+        self.proposer_streams = int(proposer_streams)
         self._streams = None
         self._graph = None
         self.L = int(L)
@@ -500,7 +501,7 @@ class PrunedBatch:
             dev = self.proposer.device
             self._masks = torch.empty(int(self.offs[-1]), dtype=torch.uint8, device=dev)
             self._views = [self.batch.feature_views(i) for i in range(len(self.shapes))]
-            ns = min(8, len(self.shapes))
+            ns = max(1, min(self.proposer_streams, len(self.shapes)))
             self._streams = [torch.cuda.Stream(device=dev) for _ in range(ns)]
             self._bufs = []
             for k in range(ns):
