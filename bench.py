@@ -306,12 +306,12 @@ def b200_arm(args, spec):
                 "alg_bytes_per_cell": 8.25,
                 "fp64_dp_cells_per_s": cells / (ms_s1 / 1e3),
                 "traffic_source": "profiles/stage1_traffic.txt: dram read+write per cell of "
-                                  "k_stage1_cl (8.49 B, profiles/k_stage1_cl_ncu_small.md), "
+                                  "k_stage1_cl (8.50 B, profiles/k_stage1_cl_ncu_small.md), "
                                   "scaled by cells",
                 "limiter": "the strip pipeline, not HBM: each strip follows the one above "
-                           "it (producer waits dominate), about 300 warp instructions per "
-                           "64-cell warp-step at 43 % issue, FP64 pipe 16 % "
-                           "(profiles/k_stage1_cl_ncu_small.md)"}
+                           "it; about 226 warp instructions per 64-cell warp-step at 39 % "
+                           "issue, FP64 pipe 16 %, the pipeline fill and drain of 32 warps "
+                           "per tile the largest stall (profiles/k_stage1_cl_ncu_small.md)"}
 
     # --- row-major C input: the relayout into the tile-skewed layout --------
     C_dev = pf.cost_matrix_from_features_gpu(F1, F2)
@@ -976,7 +976,7 @@ def prune_arm(args, spec):
         return float(t.item())
 
     # --- plain form: every tile, FP64, one batch (waves), graph replay --------
-    bp = Batch(shapes, Lb, spec.steps, spec.weights, 12, cost=args.cost)
+    bp = Batch(shapes, Lb, spec.steps, spec.weights, 12, cost=args.cost, warps=args.warps)
     bp.load(pairs)
     bp.run(spec.beta, use_graph=False)
     ph_plain = bp.timing()
@@ -996,7 +996,7 @@ def prune_arm(args, spec):
 
     # --- chosen form: proposer + kept tiles only, FP64 ----------------------
     pb = pf.PrunedBatch(shapes, Lb, spec.steps, spec.weights, 12, proposer=net,
-                        cost=args.cost)
+                        cost=args.cost, warps=args.warps)
     pb.load(pairs)
     for _ in range(args.warmup):
         out, info = pb.run(spec.beta)
@@ -1361,6 +1361,9 @@ def main():
     ap.add_argument("--cpu-repeats", type=int, default=3,
                     help="learned-pruning workload: timed runs of the CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--warps", type=int, default=0, choices=[0, 4, 8, 16],
+                    help="learned-pruning workloads: stage-1 warps per tile CTA (0: chosen "
+                         "from the tile count)")
     ap.add_argument("--cost", default="slabs", choices=["slabs", "tile"],
                     help="FP64 batches: build the cost with separate cost kernels into "
                          "slabs, in waves (slabs), or inside the stage-1 kernel, tile by tile, "

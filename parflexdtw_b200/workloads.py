@@ -286,6 +286,12 @@ PRUNE_NCU = PruneSpec("chroma12_pairs4_N8000-10000_L2000_pruned", 4, 8000, 10000
 PRUNE_NCU_W4 = PruneSpec("chroma12_pairs20_N5000-6000_L1000_pruned", 20, 5000, 6000,
                          L_choices=(1000,), pad_frac=0.10)
 
+# Per-cell counters of the stage-1 kernel at the learned-pruning workload's
+# tile length (L = 2000, run with --warps 4 for its kernel variant): 4 pairs,
+# N ~ U(10000, 12000), about 5 GB of cost slabs.
+PRUNE_NCU_L2000 = PruneSpec("chroma12_pairs4_N10000-12000_L2000_pruned", 4, 10000, 12000,
+                            L_choices=(2000,), pad_frac=0.10)
+
 
 class ShardSpec(PairSpec):
     """Named one-pair workload whose tiles are sharded across ranks."""
@@ -299,6 +305,7 @@ SHARD1 = ShardSpec("chroma12_pair_100000x100000_L4000_tile_sharded", 100000, 100
 WORKLOADS = {"config0": CONFIG0, "config1": CONFIG1, "ncu_small": NCU_SMALL,
              "batch256": BATCH256, "precision2048": PRECISION2048, "prune64": PRUNE64,
              "prune_ncu": PRUNE_NCU, "prune_ncu_w4": PRUNE_NCU_W4,
+             "prune_ncu_l2000": PRUNE_NCU_L2000,
              "shard1": SHARD1}
 
 
