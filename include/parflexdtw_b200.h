@@ -409,6 +409,24 @@ int pfx_pooled_cost(const float *A, const float *B, int32_t d, int64_t P1, int64
 /* In place: x <- (x - row mean - column mean + mean) / std over the
  * P1 x P2 map (the proposer's input).  scratch: P1 + P2 + 2 floats. */
 int pfx_pooled_center(float *x, int64_t P1, int64_t P2, float *scratch, void *stream);
+/* The proposer's input without the P1 x P2 map: in place, A (d x P1) <-
+ * -(A - its row means) / s and B (d x P2) <- B - its row means, where s is
+ * the standard deviation of the double-centred map.  Then A^T B is the map
+ * pfx_pooled_center makes from pfx_pooled_cost's 1 - A^T B (equal in real
+ * arithmetic: the pooled cost is bilinear in the features; FP32 rounding
+ * differs).  d <= 16.  scratch: pfx_pooled_center_scratch(P1, P2) bytes of
+ * device memory (the chunks' moments; FP64 sums in a fixed order). */
+int pfx_pooled_center_features(float *A, float *B, int32_t d, int64_t P1, int64_t P2,
+                               void *scratch, void *stream);
+/* Bytes of scratch pfx_pooled_center_features needs for a P1 x P2 map. */
+int64_t pfx_pooled_center_scratch(int64_t P1, int64_t P2);
+/* pfx_conv3x3_forward's first layer (Cin = 1, Cout = 32) on the map
+ * x = A^T B (H = P1 rows, W = P2 columns), computed per input patch from the
+ * features instead of read from memory.  d <= 16. */
+int pfx_conv3x3_forward_features(const float *A, const float *B, int32_t d, int32_t H,
+                                 int32_t W, const float *w, const float *b, int32_t Cout,
+                                 int32_t stride, int32_t relu, void *y, int32_t y_bf16,
+                                 void *stream);
 /* y (Cout x Ho x Wo) = act(conv3x3(x) + b), zero padding 1, stride 1, 2 or 4,
  * Ho = (H - 1) / stride + 1; w is [Cout][Cin][3][3]; act = ReLU if relu. */
 int pfx_conv3x3_forward(const void *x, int32_t x_bf16, int32_t Cin, int32_t H, int32_t W,

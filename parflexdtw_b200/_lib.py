@@ -93,6 +93,10 @@ SIGNATURES = [
     ("pfx_pool_features", ct.c_int, [_vp, _i32, _i64, _i32, _vp, _vp]),
     ("pfx_pooled_cost", ct.c_int, [_vp, _vp, _i32, _i64, _i64, _vp, _vp]),
     ("pfx_pooled_center", ct.c_int, [_vp, _i64, _i64, _vp, _vp]),
+    ("pfx_pooled_center_features", ct.c_int, [_vp, _vp, _i32, _i64, _i64, _vp, _vp]),
+    ("pfx_pooled_center_scratch", ct.c_int64, [_i64, _i64]),
+    ("pfx_conv3x3_forward_features", ct.c_int, [_vp, _vp, _i32, _i32, _i32, _vp, _vp, _i32,
+                                                _i32, _i32, _vp, _i32, _vp]),
     ("pfx_conv3x3_forward", ct.c_int, [_vp, _i32, _i32, _i32, _i32, _vp, _vp, _i32, _i32, _i32,
                                        _vp, _i32, _vp]),
     ("pfx_conv3x3_backward", ct.c_int, [_vp, _i32, _i32, _i32, _vp, _i32, _i32, _vp, _i32, _vp,

@@ -27,6 +27,37 @@ __device__ __forceinline__ void st_act(__nv_bfloat16* p, float v) { *p = __float
 // it has).
 constexpr int kPoolMaxD = 32;
 
+// pool <= 16 and d <= 16: 16 lanes per pooled block (two blocks per
+// warp), lane l holds frame i0 + l; the normalised frames are summed by a
+// fixed butterfly over the 16 lanes.
+__global__ void __launch_bounds__(256)
+    k_pool_features_warp(const double* __restrict__ F, int d, int64_t n, int pool,
+                         float* __restrict__ out, int64_t P) {
+    const int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 4;  // pooled block
+    const int l = threadIdx.x & 15;
+    const int64_t i0 = g * pool, i1 = min(n, i0 + pool);
+    const int64_t i = i0 + l;
+    const bool on = g < P && l < pool && i < i1;
+    double x[16];
+    double ss = 0.0;
+#pragma unroll
+    for (int f = 0; f < 16; ++f) {
+        x[f] = (on && f < d) ? F[(int64_t)f * n + i] : 0.0;
+        ss += x[f] * x[f];
+    }
+    const double nr = sqrt(ss);
+    const double inv = nr > 0.0 ? 1.0 / nr : 0.0;
+    double v = 0.0;
+    for (int f = 0; f < d; ++f) {
+        double a = x[f] * inv;
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (f == l) v = a;  // lane f keeps feature f's sum
+    }
+    // lanes f < d of each half write their feature (d <= 16 here)
+    if (g < P && l < d) out[(int64_t)l * P + g] = (float)(v / (double)(i1 - i0));
+}
+
 __global__ void k_pool_features(const double* __restrict__ F, int d, int64_t n, int pool,
                                 float* __restrict__ out, int64_t P) {
     const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -187,37 +218,60 @@ __global__ void k_scale(float* __restrict__ x, int64_t n, const float* __restric
 // memory.  y = act(conv(x) + b), act = ReLU or identity.
 constexpr int kCvT = 16;  // output tile edge
 
-// One thread per output pixel of a 16 x 16 tile, CO output channels per CTA;
-// CIB input channels are staged in shared memory per barrier.  The sum over
-// (ci, tap) runs in the same order for every CO / CIB.
-template <int S, int CO, int CIB, typename Tin, typename Tout>
-__global__ void __launch_bounds__(kCvT * kCvT)
+// PX output pixels per thread (columns tx, tx + 16/PX, ... of a 16 x 16
+// tile) and CO/CS of the CTA's CO output channels (channel group tc of CS);
+// CIB input channels are staged in shared memory per barrier.  Every weight
+// vector read from shared memory serves the PX pixels, every input value the
+// thread's CO/CS channels.  Each output sums over (ci, tap) in the same
+// order whatever CO, CIB, PX and CS, so every variant gives the same bits.
+template <int S, int CO, int CIB, int PX, int CS, typename Tin, typename Tout>
+__global__ void __launch_bounds__(kCvT * kCvT / PX * CS)
     k_conv3x3_fwd(const Tin* __restrict__ x, int Cin, int H, int W, const float* __restrict__ w,
                   const float* __restrict__ b, int Cout, int Ho, int Wo, int relu,
                   Tout* __restrict__ y) {
+    constexpr int NT = kCvT * kCvT / PX * CS;  // threads
+    constexpr int TXN = kCvT / PX;             // threads along x
+    constexpr int CT = CO / CS;                // channels per thread
     constexpr int PT = (kCvT - 1) * S + 3;  // input patch edge
     __shared__ float patch[CIB][PT * PT];
     __shared__ __align__(16) float ws[CIB][9 * CO];
     const int ox0 = blockIdx.x * kCvT, oy0 = blockIdx.y * kCvT, co0 = blockIdx.z * CO;
-    const int tx = threadIdx.x % kCvT, ty = threadIdx.x / kCvT;
-    const int ox = ox0 + tx, oy = oy0 + ty;
+    const int tc = threadIdx.x % CS, tp = threadIdx.x / CS;
+    const int tx = tp % TXN, ty = tp / TXN;
+    const int oy = oy0 + ty;
     const int nco = min(CO, Cout - co0);
-    float acc[CO];
+    float acc[PX][CT];
 #pragma unroll
-    for (int c = 0; c < CO; ++c) acc[c] = 0.f;
+    for (int p = 0; p < PX; ++p)
+#pragma unroll
+        for (int c = 0; c < CT; ++c) acc[p][c] = 0.f;
     const int ix0 = ox0 * S - 1, iy0 = oy0 * S - 1;
     for (int ci0 = 0; ci0 < Cin; ci0 += CIB) {
         const int ncb = min(CIB, Cin - ci0);
         __syncthreads();
-        for (int q = threadIdx.x; q < CIB * PT * PT; q += kCvT * kCvT) {
-            const int cb = q / (PT * PT), r = q % (PT * PT);
-            const int py = r / PT, px = r % PT;
-            const int iy = iy0 + py, ix = ix0 + px;
-            patch[cb][r] = (cb < ncb && iy >= 0 && iy < H && ix >= 0 && ix < W)
-                               ? ld_act(x + ((int64_t)(ci0 + cb) * H + iy) * W + ix)
-                               : 0.f;
+        // the patch in batches of 8 loads per thread, each batch issued
+        // before its stores (one memory latency per batch, not per element)
+        constexpr int NQB = 8;
+        for (int q0 = 0; q0 < CIB * PT * PT; q0 += NQB * NT) {
+            float v[NQB];
+#pragma unroll
+            for (int u = 0; u < NQB; ++u) {
+                const int q = q0 + threadIdx.x + u * NT;
+                const int cb = q / (PT * PT), r = q % (PT * PT);
+                const int py = r / PT, px = r % PT;
+                const int iy = iy0 + py, ix = ix0 + px;
+                v[u] = (q < CIB * PT * PT && cb < ncb && iy >= 0 && iy < H && ix >= 0 &&
+                        ix < W)
+                           ? ld_act(x + ((int64_t)(ci0 + cb) * H + iy) * W + ix)
+                           : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < NQB; ++u) {
+                const int q = q0 + threadIdx.x + u * NT;
+                if (q < CIB * PT * PT) (&patch[0][0])[q] = v[u];
+            }
         }
-        for (int q = threadIdx.x; q < CIB * 9 * CO; q += kCvT * kCvT) {
+        for (int q = threadIdx.x; q < CIB * 9 * CO; q += NT) {
             const int cb = q / (9 * CO), r = q % (9 * CO);
             const int tap = r / CO, c = r % CO;
             ws[cb][r] = (c < nco && cb < ncb)
@@ -228,22 +282,227 @@ __global__ void __launch_bounds__(kCvT * kCvT)
         for (int cb = 0; cb < ncb; ++cb) {
 #pragma unroll
             for (int tap = 0; tap < 9; ++tap) {
-                const float xv = patch[cb][(ty * S + tap / 3) * PT + tx * S + tap % 3];
-                if constexpr (CO % 4 == 0) {
-                    const float4* w4 = reinterpret_cast<const float4*>(&ws[cb][tap * CO]);
+                float xv[PX];
 #pragma unroll
-                    for (int c4 = 0; c4 < CO / 4; ++c4) {
+                for (int p = 0; p < PX; ++p)
+                    xv[p] = patch[cb][(ty * S + tap / 3) * PT + (tx + p * TXN) * S + tap % 3];
+                if constexpr (CT % 4 == 0) {
+                    const float4* w4 =
+                        reinterpret_cast<const float4*>(&ws[cb][tap * CO + tc * CT]);
+#pragma unroll
+                    for (int c4 = 0; c4 < CT / 4; ++c4) {
                         const float4 wv = w4[c4];
-                        acc[4 * c4 + 0] = fmaf(wv.x, xv, acc[4 * c4 + 0]);
-                        acc[4 * c4 + 1] = fmaf(wv.y, xv, acc[4 * c4 + 1]);
-                        acc[4 * c4 + 2] = fmaf(wv.z, xv, acc[4 * c4 + 2]);
-                        acc[4 * c4 + 3] = fmaf(wv.w, xv, acc[4 * c4 + 3]);
+#pragma unroll
+                        for (int p = 0; p < PX; ++p) {
+                            acc[p][4 * c4 + 0] = fmaf(wv.x, xv[p], acc[p][4 * c4 + 0]);
+                            acc[p][4 * c4 + 1] = fmaf(wv.y, xv[p], acc[p][4 * c4 + 1]);
+                            acc[p][4 * c4 + 2] = fmaf(wv.z, xv[p], acc[p][4 * c4 + 2]);
+                            acc[p][4 * c4 + 3] = fmaf(wv.w, xv[p], acc[p][4 * c4 + 3]);
+                        }
                     }
                 } else {
 #pragma unroll
-                    for (int c = 0; c < CO; ++c) acc[c] = fmaf(ws[cb][tap * CO + c], xv, acc[c]);
+                    for (int c = 0; c < CT; ++c) {
+                        const float wv = ws[cb][tap * CO + tc * CT + c];
+#pragma unroll
+                        for (int p = 0; p < PX; ++p) acc[p][c] = fmaf(wv, xv[p], acc[p][c]);
+                    }
                 }
             }
+        }
+    }
+    if (oy >= Ho) return;
+#pragma unroll
+    for (int p = 0; p < PX; ++p) {
+        const int ox = ox0 + tx + p * TXN;
+        if (ox >= Wo) continue;
+#pragma unroll
+        for (int c = 0; c < CT; ++c) {
+            const int cc = tc * CT + c;
+            if (cc < nco) {
+                float v = acc[p][c] + b[co0 + cc];
+                if (relu) v = fmaxf(v, 0.f);
+                st_act(y + ((int64_t)(co0 + cc) * Ho + oy) * Wo + ox, v);
+            }
+        }
+    }
+}
+
+// The network's input from the pooled features, without the map.  The pooled
+// cost 1 - a_i . b_j is bilinear, so its double centring is
+// -(a_i - abar) . (b_j - bbar), and the mean square of that map is
+// sum_{f,g} GA[f][g] GB[f][g] / (P1 P2) with GA, GB the Gram matrices of the
+// centred features.  Two kernels (d <= 16, FP64 sums in a fixed order):
+// k_feat_moments gives each chunk of kCfChunk frames of A (d x P1) or B
+// (d x P2) its feature sums and its raw Gram matrix (upper triangle);
+// k_center_features adds the chunks in order, centres the Gram matrices
+// (G - P m m^T), and centres A and B in place, scaling A by -1/std so that
+// A^T B is the centred, standardised map.
+constexpr int kCfChunk = 64;
+constexpr int kCfMom = 16 + 136;  // sums, then the upper-triangle Gram entries
+
+__host__ __device__ inline int feat_chunks(int64_t P) { return (int)((P + kCfChunk - 1) / kCfChunk); }
+
+__device__ __forceinline__ void tri_index(int p, int d, int* f, int* g) {
+    int r = p, ff = 0;
+    while (r >= d - ff) { r -= d - ff; ++ff; }
+    *f = ff;
+    *g = ff + r;
+}
+
+constexpr int kCfMomThreads = 160;  // >= 16 + 136: one thread per moment
+
+__global__ void __launch_bounds__(kCfMomThreads)
+    k_feat_moments(const float* __restrict__ A, const float* __restrict__ B, int d, int64_t P1,
+                   int64_t P2, double* __restrict__ mom) {
+    __shared__ float X[16][kCfChunk];
+    const int ncA = feat_chunks(P1);
+    const bool isB = (int)blockIdx.x >= ncA;
+    const int c = isB ? (int)blockIdx.x - ncA : (int)blockIdx.x;
+    const float* src = isB ? B : A;
+    const int64_t P = isB ? P2 : P1;
+    const int64_t i0 = (int64_t)c * kCfChunk;
+    const int n = P - i0 < kCfChunk ? (int)(P - i0) : kCfChunk;
+    for (int q = threadIdx.x; q < d * kCfChunk; q += kCfMomThreads) {
+        const int f = q / kCfChunk, i = q % kCfChunk;
+        X[f][i] = i < n ? src[(int64_t)f * P + i0 + i] : 0.f;
+    }
+    __syncthreads();
+    const int npair = d * (d + 1) / 2;
+    double* out = mom + (int64_t)blockIdx.x * kCfMom;
+    const int t = threadIdx.x;
+    if (t < d) {
+        double acc = 0.0;
+        for (int i = 0; i < n; ++i) acc += (double)X[t][i];
+        out[t] = acc;
+    } else if (t >= 16 && t < 16 + npair) {
+        int f, g;
+        tri_index(t - 16, d, &f, &g);
+        double acc = 0.0;
+        for (int i = 0; i < n; ++i) acc += (double)X[f][i] * (double)X[g][i];
+        out[t] = acc;
+    }
+}
+
+constexpr int kCfThreads = 256;
+constexpr int kCfPer = 2048;  // frames x features centred per CTA
+
+// Every CTA derives the means and the scale from the chunks' moments (the
+// same sums in the same order, so every CTA gets the same values), then
+// centres its slice of A and B: slice j covers kCfPer consecutive entries of
+// the d x P1 array A followed by the d x P2 array B.
+__global__ void __launch_bounds__(kCfThreads)
+    k_center_features(float* __restrict__ A, float* __restrict__ B, int d, int64_t P1,
+                      int64_t P2, const double* __restrict__ mom) {
+    __shared__ double mean[2][16];
+    __shared__ double gram[2][136];
+    __shared__ float scale;
+    const int t = threadIdx.x;
+    const int npair = d * (d + 1) / 2;
+    const int ncA = feat_chunks(P1), ncB = feat_chunks(P2);
+    for (int q = t; q < 2 * kCfMom; q += kCfThreads) {
+        const int s = q / kCfMom, k = q % kCfMom;
+        const int c0 = s ? ncA : 0, nc = s ? ncB : ncA;
+        const bool used = k < d || (k >= 16 && k < 16 + npair);
+        double acc = 0.0;
+        if (used)
+            for (int c = 0; c < nc; ++c) acc += mom[(int64_t)(c0 + c) * kCfMom + k];
+        if (k < d) mean[s][k] = acc / (double)(s ? P2 : P1);
+        if (k >= 16 && k < 16 + npair) gram[s][k - 16] = acc;
+    }
+    __syncthreads();
+    if (t < 2 * npair) {  // centred Gram: G - P m_f m_g
+        const int s = t / npair, p = t % npair;
+        int f, g;
+        tri_index(p, d, &f, &g);
+        gram[s][p] -= (double)(s ? P2 : P1) * mean[s][f] * mean[s][g];
+    }
+    __syncthreads();
+    if (t == 0) {
+        double v = 0.0;
+        for (int p = 0; p < npair; ++p) {
+            int f, g;
+            tri_index(p, d, &f, &g);
+            v += (f == g ? 1.0 : 2.0) * gram[0][p] * gram[1][p];
+        }
+        v /= (double)P1 * (double)P2;
+        scale = v > 0.0 ? (float)(-1.0 / sqrt(v)) : 0.f;
+    }
+    __syncthreads();
+    const int64_t nA = (int64_t)d * P1, n = nA + (int64_t)d * P2;
+    const int64_t q0 = (int64_t)blockIdx.x * kCfPer;
+    const int64_t q1 = q0 + kCfPer < n ? q0 + kCfPer : n;
+    for (int64_t q = q0 + t; q < q1; q += kCfThreads) {
+        if (q < nA) {
+            const int f = (int)(q / P1);
+            A[q] = (float)((double)A[q] - mean[0][f]) * scale;
+        } else {
+            const int f = (int)((q - nA) / P2);
+            B[q - nA] = (float)((double)B[q - nA] - mean[1][f]);
+        }
+    }
+}
+
+// The first layer (Cin = 1, CO output channels) on the map x = A^T B: each
+// thread computes the 9 inputs of its own output pixel from the CTA's rows of
+// A and columns of B staged in shared memory (zero outside the map, as the
+// convolution's padding), then the 3 x 3 x CO products in the order of
+// k_conv3x3_fwd.
+template <int S, int CO, typename Tout>
+__global__ void __launch_bounds__(kCvT * kCvT)
+    k_conv3x3_fwd_feat(const float* __restrict__ A, const float* __restrict__ B, int d, int H,
+                       int W, const float* __restrict__ w, const float* __restrict__ b, int Cout,
+                       int Ho, int Wo, int relu, Tout* __restrict__ y) {
+    constexpr int NT = kCvT * kCvT;
+    constexpr int PT = (kCvT - 1) * S + 3;  // input patch edge
+    __shared__ float sA[16][PT], sB[16][PT];
+    __shared__ __align__(16) float ws[9 * CO];
+    const int ox0 = blockIdx.x * kCvT, oy0 = blockIdx.y * kCvT, co0 = blockIdx.z * CO;
+    const int tx = threadIdx.x % kCvT, ty = threadIdx.x / kCvT;
+    const int ox = ox0 + tx, oy = oy0 + ty;
+    const int nco = min(CO, Cout - co0);
+    const int ix0 = ox0 * S - 1, iy0 = oy0 * S - 1;
+    for (int q = threadIdx.x; q < d * PT; q += NT) {
+        const int f = q / PT, r = q % PT;
+        const int iy = iy0 + r, ix = ix0 + r;
+        sA[f][r] = (iy >= 0 && iy < H) ? A[(int64_t)f * H + iy] : 0.f;
+        sB[f][r] = (ix >= 0 && ix < W) ? B[(int64_t)f * W + ix] : 0.f;
+    }
+    for (int q = threadIdx.x; q < 9 * CO; q += NT) {
+        const int tap = q / CO, c = q % CO;
+        ws[q] = c < nco ? w[(int64_t)(co0 + c) * 9 + tap] : 0.f;
+    }
+    __syncthreads();
+    // inputs of taps (ky, kx): rows ty*S + ky, columns tx*S + kx of the patch
+    float xin[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) xin[k] = 0.f;
+    for (int f = 0; f < d; ++f) {
+        float ra[3], cb[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            ra[k] = sA[f][ty * S + k];
+            cb[k] = sB[f][tx * S + k];
+        }
+#pragma unroll
+        for (int ky = 0; ky < 3; ++ky)
+#pragma unroll
+            for (int kx = 0; kx < 3; ++kx) xin[ky * 3 + kx] = fmaf(ra[ky], cb[kx], xin[ky * 3 + kx]);
+    }
+    float acc[CO];
+#pragma unroll
+    for (int c = 0; c < CO; ++c) acc[c] = 0.f;
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+        const float xv = xin[tap];
+        const float4* w4 = reinterpret_cast<const float4*>(&ws[tap * CO]);
+#pragma unroll
+        for (int c4 = 0; c4 < CO / 4; ++c4) {
+            const float4 wv = w4[c4];
+            acc[4 * c4 + 0] = fmaf(wv.x, xv, acc[4 * c4 + 0]);
+            acc[4 * c4 + 1] = fmaf(wv.y, xv, acc[4 * c4 + 1]);
+            acc[4 * c4 + 2] = fmaf(wv.z, xv, acc[4 * c4 + 2]);
+            acc[4 * c4 + 3] = fmaf(wv.w, xv, acc[4 * c4 + 3]);
         }
     }
     if (ox >= Wo || oy >= Ho) return;
@@ -454,7 +713,10 @@ cudaError_t cnn_pool_features(const double* F, int d, int64_t n, int pool, float
                               cudaStream_t st) {
     const int64_t P = (n + pool - 1) / pool;
     if (P <= 0) return cudaSuccess;
-    k_pool_features<<<blocks_for(P, 128), 128, 0, st>>>(F, d, n, pool, out, P);
+    if (pool <= 16 && d <= 16)
+        k_pool_features_warp<<<blocks_for(P * 16, 256), 256, 0, st>>>(F, d, n, pool, out, P);
+    else
+        k_pool_features<<<blocks_for(P, 128), 128, 0, st>>>(F, d, n, pool, out, P);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -468,12 +730,12 @@ cudaError_t cnn_pooled_cost(const float* A, const float* B, int d, int64_t P1, i
     return cudaGetLastError();
 }
 
-template <int S, int CO, int CIB, typename Tin, typename Tout>
+template <int S, int CO, int CIB, int PX, int CS, typename Tin, typename Tout>
 static cudaError_t conv_fwd_launch(const void* x, int Cin, int H, int W, const float* w,
                                    const float* b, int Cout, int relu, void* y, cudaStream_t st) {
     const int Ho = (H - 1) / S + 1, Wo = (W - 1) / S + 1;
     const dim3 grid(blocks_for(Wo, kCvT), blocks_for(Ho, kCvT), blocks_for(Cout, CO));
-    k_conv3x3_fwd<S, CO, CIB, Tin, Tout><<<grid, kCvT * kCvT, 0, st>>>(
+    k_conv3x3_fwd<S, CO, CIB, PX, CS, Tin, Tout><<<grid, kCvT * kCvT / PX * CS, 0, st>>>(
         static_cast<const Tin*>(x), Cin, H, W, w, b, Cout, Ho, Wo, relu, static_cast<Tout*>(y));
     count_launches(1);
     return cudaGetLastError();
@@ -486,8 +748,12 @@ static cudaError_t conv_fwd_t(const void* x, int Cin, int H, int W, const float*
                               int Cout, int relu, void* y, cudaStream_t st) {
     constexpr int CIB = S == 4 ? 1 : 4;
     if (Cout < 8)
-        return conv_fwd_launch<S, 1, 2 * CIB, Tin, Tout>(x, Cin, H, W, w, b, Cout, relu, y, st);
-    return conv_fwd_launch<S, 32, CIB, Tin, Tout>(x, Cin, H, W, w, b, Cout, relu, y, st);
+        return conv_fwd_launch<S, 1, 2 * CIB, 1, 1, Tin, Tout>(x, Cin, H, W, w, b, Cout, relu, y,
+                                                               st);
+    if (Cin >= 8)  // two pixels x 16 channels per thread: 6 shared loads per 32 FMAs
+        return conv_fwd_launch<S, 32, CIB, 2, 2, Tin, Tout>(x, Cin, H, W, w, b, Cout, relu, y,
+                                                            st);
+    return conv_fwd_launch<S, 32, CIB, 1, 1, Tin, Tout>(x, Cin, H, W, w, b, Cout, relu, y, st);
 }
 
 // in_bf16 / out_bf16: activation storage types (FP32 otherwise).
@@ -587,6 +853,56 @@ extern "C" int pfx_pooled_center(float* x, int64_t P1, int64_t P2, float* scratc
     k_scale<<<blocks_for(n, 256), 256, 0, st>>>(x, n, scratch + P1 + P2 + 1);
     count_launches(5);
     PFX_CNN_RET(cudaGetLastError());
+}
+
+extern "C" int64_t pfx_pooled_center_scratch(int64_t P1, int64_t P2) {
+    if (P1 < 1 || P2 < 1) return 0;
+    return (int64_t)(feat_chunks(P1) + feat_chunks(P2)) * kCfMom * (int64_t)sizeof(double);
+}
+
+extern "C" int pfx_pooled_center_features(float* A, float* B, int32_t d, int64_t P1,
+                                          int64_t P2, void* scratch, void* stream) {
+    if (!A || !B || !scratch || d < 1 || d > 16 || P1 < 1 || P2 < 1)
+        return report_status(PFX_ERR_ARG, "pfx_pooled_center_features: bad argument (d <= 16)");
+    cudaStream_t st = (cudaStream_t)stream;
+    double* mom = static_cast<double*>(scratch);
+    k_feat_moments<<<(unsigned)(feat_chunks(P1) + feat_chunks(P2)), kCfMomThreads, 0, st>>>(
+        A, B, d, P1, P2, mom);
+    const int64_t n = (int64_t)d * (P1 + P2);
+    k_center_features<<<(unsigned)((n + kCfPer - 1) / kCfPer), kCfThreads, 0, st>>>(A, B, d, P1,
+                                                                                   P2, mom);
+    count_launches(2);
+    PFX_CNN_RET(cudaGetLastError());
+}
+
+extern "C" int pfx_conv3x3_forward_features(const float* A, const float* B, int32_t d, int32_t H,
+                                            int32_t W, const float* w, const float* b,
+                                            int32_t Cout, int32_t stride, int32_t relu, void* y,
+                                            int32_t y_bf16, void* stream) {
+    if (!A || !B || !w || !b || !y || d < 1 || d > 16 || Cout != 32 || H < 1 || W < 1 ||
+        (stride != 1 && stride != 2 && stride != 4) || (int64_t)H * W > (1LL << 31) / 64)
+        return report_status(PFX_ERR_ARG,
+                             "pfx_conv3x3_forward_features: bad argument (d <= 16, Cout = 32)");
+    cudaStream_t st = (cudaStream_t)stream;
+#define PFX_CONV_FEAT(S_)                                                                     \
+    do {                                                                                     \
+        const int Ho = (H - 1) / S_ + 1, Wo = (W - 1) / S_ + 1;                               \
+        const dim3 grid(blocks_for(Wo, kCvT), blocks_for(Ho, kCvT), 1);                       \
+        if (y_bf16)                                                                          \
+            k_conv3x3_fwd_feat<S_, 32, __nv_bfloat16><<<grid, kCvT * kCvT, 0, st>>>(          \
+                A, B, d, H, W, w, b, Cout, Ho, Wo, relu, static_cast<__nv_bfloat16*>(y));    \
+        else                                                                                 \
+            k_conv3x3_fwd_feat<S_, 32, float><<<grid, kCvT * kCvT, 0, st>>>(                  \
+                A, B, d, H, W, w, b, Cout, Ho, Wo, relu, static_cast<float*>(y));            \
+    } while (0)
+    if (stride == 4)
+        PFX_CONV_FEAT(4);
+    else if (stride == 2)
+        PFX_CONV_FEAT(2);
+    else
+        PFX_CONV_FEAT(1);
+#undef PFX_CONV_FEAT
+    PFX_CNN_LAUNCHED();
 }
 
 extern "C" int pfx_conv3x3_forward(const void* x, int32_t x_bf16, int32_t Cin, int32_t H,

@@ -176,8 +176,9 @@ class TileProposer:
         nt = -(-(N - 1) // hop) * -(-(M - 1) // hop)
         f32, bf = dict(dtype=torch.float32, device=device), dict(dtype=torch.bfloat16,
                                                                  device=device)
+        mom = int(_lib.load().pfx_pooled_center_scratch(P1, P2))
         return {"A": torch.empty(d * P1, **f32), "B": torch.empty(d * P2, **f32),
-                "pooled": torch.empty(P1 * P2, **f32), "sc": torch.empty(P1 + P2 + 2, **f32),
+                "mom": torch.empty(max(mom, 8), dtype=torch.uint8, device=device),
                 "y1": torch.empty(CH * dims[0][0] * dims[0][1], **bf),
                 "y2": torch.empty(CH * dims[1][0] * dims[1][1], **bf),
                 "y3": torch.empty(dims[2][0] * dims[2][1], **f32),
@@ -188,20 +189,31 @@ class TileProposer:
         """The inference of ``propose`` from device features (d x N, d x M,
         FP64) into preallocated ``bufs`` (``buffers``), writing the tile mask
         into the uint8 device tensor ``mask`` (n1 * n2 entries).  Launches
-        only library kernels on the current stream, allocates nothing."""
+        only library kernels on the current stream, allocates nothing.
+
+        The network's centred, standardised input is never stored: the pooled
+        features are centred and scaled (``pfx_pooled_center_features``) so
+        that their product is that map, and the first layer computes it per
+        input patch (``pfx_conv3x3_forward_features``).  In real arithmetic
+        this is the input ``propose`` builds; FP32 rounding differs."""
         lib = _lib.load()
         s = current_stream_ptr()
         d, N = int(f1.shape[0]), int(f1.shape[1])
         M = int(f2.shape[1])
+        if d > 16:
+            raise ValueError("propose_into takes d <= 16 features (use propose)")
         P1, P2 = -(-N // POOL), -(-M // POOL)
         _lib.check(lib.pfx_pool_features(_p(f1), d, N, POOL, _p(bufs["A"]), s))
         _lib.check(lib.pfx_pool_features(_p(f2), d, M, POOL, _p(bufs["B"]), s))
-        _lib.check(lib.pfx_pooled_cost(_p(bufs["A"]), _p(bufs["B"]), d, P1, P2,
-                                       _p(bufs["pooled"]), s))
-        _lib.check(lib.pfx_pooled_center(_p(bufs["pooled"]), P1, P2, _p(bufs["sc"]), s))
-        x, x_bf, cin, H, W = bufs["pooled"], 0, 1, P1, P2
-        layers = ((self.params["w1"], self.params["b1"], CH, STRIDES[0], 1, bufs["y1"], 1),
-                  (self.params["w2"], self.params["b2"], CH, STRIDES[1], 1, bufs["y2"], 1),
+        _lib.check(lib.pfx_pooled_center_features(_p(bufs["A"]), _p(bufs["B"]), d, P1, P2,
+                                                  _p(bufs["mom"]), s))
+        w, b = self.params["w1"], self.params["b1"]
+        _lib.check(lib.pfx_conv3x3_forward_features(_p(bufs["A"]), _p(bufs["B"]), d, P1, P2,
+                                                    _p(w), _p(b), CH, STRIDES[0], 1,
+                                                    _p(bufs["y1"]), 1, s))
+        H, W = (P1 - 1) // STRIDES[0] + 1, (P2 - 1) // STRIDES[0] + 1
+        x, x_bf, cin = bufs["y1"], 1, CH
+        layers = ((self.params["w2"], self.params["b2"], CH, STRIDES[1], 1, bufs["y2"], 1),
                   (self.params["w3"], self.params["b3"], 1, STRIDES[2], 0, bufs["y3"], 0))
         for w, b, cout, st, relu, y, y_bf in layers:
             Ho, Wo = (H - 1) // st + 1, (W - 1) // st + 1
