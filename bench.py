@@ -976,7 +976,9 @@ def prune_arm(args, spec):
         return float(t.item())
 
     # --- plain form: every tile, FP64, one batch (waves), graph replay --------
-    bp = Batch(shapes, Lb, spec.steps, spec.weights, 12, cost=args.cost, warps=args.warps)
+    cost_fma = args.cost_def == "fma" and args.cost == "slabs"
+    bp = Batch(shapes, Lb, spec.steps, spec.weights, 12, cost=args.cost, warps=args.warps,
+               cost_fma=cost_fma)
     bp.load(pairs)
     bp.run(spec.beta, use_graph=False)
     ph_plain = bp.timing()
@@ -996,7 +998,7 @@ def prune_arm(args, spec):
 
     # --- chosen form: proposer + kept tiles only, FP64 ----------------------
     pb = pf.PrunedBatch(shapes, Lb, spec.steps, spec.weights, 12, proposer=net,
-                        cost=args.cost, warps=args.warps)
+                        cost=args.cost, warps=args.warps, cost_fma=cost_fma)
     pb.load(pairs)
     for _ in range(args.warmup):
         out, info = pb.run(spec.beta)
@@ -1118,6 +1120,11 @@ def prune_arm(args, spec):
                            cost_build=("inside the stage-1 kernel, tile by tile"
                                        if args.cost == "tile" else
                                        "separate cost kernels into slabs, in waves"),
+                           cost_definition=(
+                               "1 - sum_f a_f b_f as a fixed-order FP64 FMA chain "
+                               "(PFX_BATCH_COST_FMA), both forms" if cost_fma else
+                               "1 - sum_f a_f b_f with separately rounded FP64 products and "
+                               "sums, both forms"),
                            timing="CUDA events around whole steps (host-side proposer mask "
                                   "read-back and fallback checks included)",
                            l2="cost slabs larger than L2 (no flush needed)"),
@@ -1311,6 +1318,11 @@ def shard_arm(args, spec):
                            cost_build=("inside the stage-1 kernel, tile by tile"
                                        if args.cost == "tile" else
                                        "separate cost kernels into slabs, in waves"),
+                           cost_definition=(
+                               "1 - sum_f a_f b_f as a fixed-order FP64 FMA chain "
+                               "(PFX_BATCH_COST_FMA), both forms" if cost_fma else
+                               "1 - sum_f a_f b_f with separately rounded FP64 products and "
+                               "sums, both forms"),
                            l2="cost slabs larger than L2 (no flush needed)"),
             "pairs_per_s": args.steps / (ms_total / 1e3),
             "per_rank": {"cost_ms_max": cost_ms, "stage1_ms_max": s1_ms,
@@ -1364,6 +1376,10 @@ def main():
     ap.add_argument("--warps", type=int, default=0, choices=[0, 4, 8, 16],
                     help="learned-pruning workloads: stage-1 warps per tile CTA (0: chosen "
                          "from the tile count)")
+    ap.add_argument("--cost-def", default="fma", choices=["fma", "det"],
+                    help="learned-pruning workloads: the FP64 cost of both forms as a "
+                         "fixed-order FMA chain (fma) or as separately rounded products and "
+                         "sums (det, the drop-in path's definition)")
     ap.add_argument("--cost", default="slabs", choices=["slabs", "tile"],
                     help="FP64 batches: build the cost with separate cost kernels into "
                          "slabs, in waves (slabs), or inside the stage-1 kernel, tile by tile, "

@@ -311,10 +311,18 @@ typedef struct pfx_batch pfx_batch;
  * tile of every pair, instead of separate cost kernels filling slabs in
  * waves.  Same results; for batches whose slabs would need many waves. */
 #define PFX_BATCH_TILE_COST 0x100
+/* Flag for pfx_batch_create's `precision` (or-ed with PFX_FP64, not with
+ * PFX_BATCH_TILE_COST): the cost is 1 - sum_f a_f b_f formed in the order
+ * f = 0, 1, ..., d-1 as a chain of fused multiply-adds (the first product
+ * rounded on its own), 13 FP64 operations per cell, instead of separately
+ * rounded products and sums (24).  Another fixed, deterministic rounding of
+ * the same cosine cost, as a BLAS product would form it; stage 1 and stage 2
+ * are the same on either cost. */
+#define PFX_BATCH_COST_FMA 0x200
 
 /* nw: stage-1 warps per tile CTA (4, 8 or 16; 0 = chosen from the tile
  * count).  precision: a pfx_precision, optionally or-ed with
- * PFX_BATCH_TILE_COST.  The batch is created on the current CUDA device. */
+ * PFX_BATCH_TILE_COST or PFX_BATCH_COST_FMA.  The batch is created on the current CUDA device. */
 int pfx_batch_create(int32_t n, const int64_t *N, const int64_t *M, const int32_t *L,
                      const int64_t *steps, const double *weights, int32_t n_steps,
                      int32_t d, int64_t wave_bytes, int32_t nw, int32_t precision,

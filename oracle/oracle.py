@@ -81,6 +81,7 @@ def lib():
         L.oracle_backtrace_tile.argtypes = [_i8p, ct.c_int64, ct.c_int64, _i64p,
                                             ct.c_int, ct.c_int64, ct.c_int64,
                                             _i64p]
+        L.oracle_cost_fma.argtypes = [_f64p, _f64p, ct.c_int, ct.c_int64, ct.c_int64, _f64p]
         if L.oracle_result_size() != ct.sizeof(_Result):
             raise RuntimeError("oracle_result layout mismatch")
         _lib = L
@@ -89,6 +90,20 @@ def lib():
 
 def _ptr(a, t):
     return a.ctypes.data_as(t)
+
+
+def cost_matrix_fma(F1, F2):
+    """The device's FMA cost mode on the host: L2-normalised features
+    (``workloads.l2norm``), then C = 1 - sum_f a_f b_f as a fixed-order chain
+    of fused multiply-adds (``oracle_cost_fma``)."""
+    from parflexdtw_b200.workloads import l2norm
+    A = np.ascontiguousarray(l2norm(np.asarray(F1, dtype=np.float64)))
+    B = np.ascontiguousarray(l2norm(np.asarray(F2, dtype=np.float64)))
+    d, N = A.shape
+    M = B.shape[1]
+    C = np.empty((N, M), dtype=np.float64)
+    lib().oracle_cost_fma(_ptr(A, _f64p), _ptr(B, _f64p), d, N, M, _ptr(C, _f64p))
+    return C
 
 
 def _steps_weights(steps, weights):

@@ -843,3 +843,24 @@ int oracle_parflex(const double *C, int64_t N, int64_t M, int64_t ldc,
 
 /* Size of oracle_result, so the Python side can check its struct layout. */
 int64_t oracle_result_size(void) { return (int64_t)sizeof(oracle_result); }
+
+/* The cosine cost as a fixed-order chain of fused multiply-adds, the
+ * definition of the device's FMA cost mode (PFX_BATCH_COST_FMA; the reference
+ * forms C = 1 - F1^T F2 with a BLAS product, FlexDTW.py:213-216,
+ * Parflex.py:1470, whose rounding order is the library's): for L2-normalised
+ * A (d x N) and B (d x M), row-major by feature,
+ *   acc = A[0][i] * B[0][j];  acc = fma(A[f][i], B[f][j], acc), f = 1..d-1;
+ *   C[i][j] = 1 - acc.
+ * fma() is correctly rounded (C99); nothing else is contracted
+ * (-ffp-contract=off). */
+void oracle_cost_fma(const double *A, const double *B, int d, int64_t N, int64_t M, double *C)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < N; ++i) {
+        for (int64_t j = 0; j < M; ++j) {
+            double acc = A[i] * B[j];
+            for (int f = 1; f < d; ++f) acc = fma(A[(int64_t)f * N + i], B[(int64_t)f * M + j], acc);
+            C[i * M + j] = 1.0 - acc;
+        }
+    }
+}

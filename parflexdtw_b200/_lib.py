@@ -31,6 +31,7 @@ PFX_ERR_NO_DEVICE = 6
 PFX_FP64 = 0
 PFX_FP32 = 1
 PFX_BATCH_TILE_COST = 0x100
+PFX_BATCH_COST_FMA = 0x200
 
 NO_ENDPOINT_MSG = "Stage 2: No valid endpoint found on global top/right edges."
 

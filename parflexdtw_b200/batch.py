@@ -42,13 +42,17 @@ class Batch:
     of times (the CUDA graph is recorded on the first run)."""
 
     def __init__(self, shapes, L_per_pair, steps, weights, d, wave_bytes=0, warps=0,
-                 precision="fp64", cost="slabs"):
+                 precision="fp64", cost="slabs", cost_fma=False):
         lib = _lib.load()
         if precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32'")
         if cost not in ("slabs", "tile"):
             raise ValueError("cost must be 'slabs' (separate cost kernels, in waves) or 'tile' "
                              "(FP64, d <= 16: built inside the stage-1 kernel, tile by tile)")
+        if cost_fma and (precision != "fp64" or cost != "slabs"):
+            raise ValueError("cost_fma needs precision='fp64' and cost='slabs'")
+        # True: the FP64 cost as a fixed-order FMA chain (PFX_BATCH_COST_FMA)
+        self.cost_fma = bool(cost_fma)
         self.precision = precision
         if not torch.cuda.is_available():
             raise RuntimeError("parflexdtw_b200 needs a CUDA device")
@@ -70,7 +74,8 @@ class Batch:
             _lib.i32_array(self.L), _lib.i64_array(st.reshape(-1)), _lib.f64_array(w), st.shape[0],
             self.d, int(wave_bytes), int(warps),
             (_lib.PFX_FP32 if precision == "fp32" else _lib.PFX_FP64) |
-            (_lib.PFX_BATCH_TILE_COST if cost == "tile" else 0), ct.byref(h)))
+            (_lib.PFX_BATCH_TILE_COST if cost == "tile" else 0) |
+            (_lib.PFX_BATCH_COST_FMA if cost_fma else 0), ct.byref(h)))
         self._h = h
         self._fin = weakref.finalize(self, _free_batch, h)
         info = (ct.c_int64 * 9)()
@@ -228,7 +233,8 @@ def _split_pair(pair):
 
 
 def parflex_batch(pairs, steps, weights, beta, L=None, wave_bytes=0, warps=0,
-                  use_graph=True, errors="raise", tuner=None, precision="fp64", cost="slabs"):
+                  use_graph=True, errors="raise", tuner=None, precision="fp64", cost="slabs",
+                  cost_fma=False):
     """ParFlex on every (F1, F2) feature pair of ``pairs`` in one device batch.
 
     Same argument conventions as ``parflex`` (features are d x frames, the
@@ -237,8 +243,10 @@ def parflex_batch(pairs, steps, weights, beta, L=None, wave_bytes=0, warps=0,
     autotuner pick per length bucket.  ``precision="fp32"`` runs the FP32
     form (bf16 tensor-core cost, FP32 DP; d <= 256).  ``cost="tile"`` builds
     the FP64 cost inside the stage-1 kernel, tile by tile, in one launch
-    instead of with separate cost kernels in waves (same results).  Returns
-    a list with, per pair,
+    instead of with separate cost kernels in waves (same results).
+    ``cost_fma=True`` forms the FP64 cost as a fixed-order FMA chain (13 FP64
+    operations per cell instead of 24; another deterministic rounding of the
+    same cost).  Returns a list with, per pair,
     ``(best_cost, wp[2, K])``.  A pair whose scan finds no endpoint raises the
     reference's ValueError (``errors="raise"``) or yields None
     (``errors="none"``).
@@ -262,7 +270,7 @@ def parflex_batch(pairs, steps, weights, beta, L=None, wave_bytes=0, warps=0,
     else:
         Ls = L
     b = Batch(shapes, Ls, steps, weights, d, wave_bytes=wave_bytes, warps=warps,
-              precision=precision, cost=cost)
+              precision=precision, cost=cost, cost_fma=cost_fma)
     b.load(feats)
     b.run(beta, use_graph=use_graph)
     best, end, lens = b.results()

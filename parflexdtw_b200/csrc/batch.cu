@@ -142,6 +142,8 @@ struct pfx_batch {
     // per resident CTA (gen), and every pair runs in one wave
     int gen_cost = 0;
     CostGen gen{nullptr, 0, 0, 0};
+    // 1: the FP64 cost as a fixed-order FMA chain (PFX_BATCH_COST_FMA)
+    int cost_fma = 0;
     Geo gq;  // step set and weights; L = largest tile length (ring sizing)
     std::vector<pfx_plan> plans;
     char* arena = nullptr;
@@ -238,15 +240,19 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
     *out = nullptr;
     if (n < 1) return errf(PFX_ERR_ARG, "batch of %d pairs", n);
     const int form = precision & 0xff, flags = precision & ~0xff;
-    if ((form != PFX_FP64 && form != PFX_FP32) || (flags & ~PFX_BATCH_TILE_COST))
+    if ((form != PFX_FP64 && form != PFX_FP32) ||
+        (flags & ~(PFX_BATCH_TILE_COST | PFX_BATCH_COST_FMA)))
         return errf(PFX_ERR_ARG,
                     "precision %d: PFX_FP64 (0) or PFX_FP32 (1), optionally | "
-                    "PFX_BATCH_TILE_COST", precision);
+                    "PFX_BATCH_TILE_COST or PFX_BATCH_COST_FMA", precision);
     const int fp32 = form == PFX_FP32;
     const int gen_cost = (flags & PFX_BATCH_TILE_COST) != 0;
+    const int cost_fma = (flags & PFX_BATCH_COST_FMA) != 0;
     if (gen_cost && (fp32 || d < 1 || d > kGenMaxD))
         return errf(PFX_ERR_ARG, "PFX_BATCH_TILE_COST needs PFX_FP64 and 1 <= d <= %d (d = %d)",
                     kGenMaxD, d);
+    if (cost_fma && (fp32 || gen_cost))
+        return errf(PFX_ERR_ARG, "PFX_BATCH_COST_FMA needs PFX_FP64 without PFX_BATCH_TILE_COST");
     if (d < 1 || (fp32 && d > 256))
         return errf(PFX_ERR_ARG, "feature dimension %d (the FP32 form takes 1..256)", d);
     const int kp = (d + 63) / 64 * 64;
@@ -265,6 +271,7 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
     b->d = d;
     b->fp32 = fp32;
     b->gen_cost = gen_cost;
+    b->cost_fma = cost_fma;
     b->kp = kp;
     b->plans.resize(n);
     int st = PFX_OK;
@@ -692,7 +699,7 @@ extern "C" int pfx_batch_complete(pfx_batch* b, int32_t i, double beta, const ui
         BCK(launch_l2norm(F1, b->d, p.g.N, An, s));
         BCK(launch_l2norm(F2, b->d, p.g.M, Bn, s));
         BCK(launch_cost_skew(An, Bn, b->d, p.g, b->slabs, p.skew_stride, s, p.tile_slot,
-                             p.tile_list, (int)list.size()));
+                             p.tile_list, (int)list.size(), b->cost_fma != 0));
     }
     // stage 1 on the tiles added now (the others' outputs stand; tiles never
     // run keep the +inf edges of the masked run)
@@ -806,7 +813,8 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
                 BCK(launch_l2norm(F2, b->d, p.g.M, Bn, s));
                 if (!b->gen_cost)  // (else stage 1 builds each tile's cost)
                     BCK(launch_cost_skew(An, Bn, b->d, p.g, static_cast<double*>(p.Csk),
-                                         p.skew_stride, s, slot, list, p.n_kept));
+                                         p.skew_stride, s, slot, list, p.n_kept,
+                                         b->cost_fma != 0));
             }
             if (b->masked) {
                 // skipped tiles keep +inf edges and start 0 for stage 2

@@ -285,9 +285,11 @@ cudaError_t launch_gemm_cost_skew(const void* Abf, const void* Bbf, int Kp, cons
 cudaError_t launch_relayout_skew_f32(const double* C64, const float* C32, int64_t ldc,
                                      const Geo& g, float* Csk, int64_t stride, cudaStream_t st,
                                      const int32_t* slot = nullptr);
+// fma: the cost as a fixed-order chain of fused multiply-adds (13 FP64
+// operations per cell) instead of separately rounded products and sums.
 cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Geo& g, double* Csk,
                              int64_t skew_stride, cudaStream_t st, const int32_t* slot = nullptr,
-                             const int32_t* list = nullptr, int nlist = 0);
+                             const int32_t* list = nullptr, int nlist = 0, bool fma = false);
 cudaError_t launch_l2norm(const double* F, int d, int64_t n, double* out, cudaStream_t st);
 cudaError_t launch_stage1(const double* C, const Geo& g, const S1Out& o, int tile0, int ntiles,
                           int nw, bool full, cudaStream_t st);

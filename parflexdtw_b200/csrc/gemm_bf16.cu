@@ -561,7 +561,8 @@ static bool make_map(CUtensorMap* m, const void* base, int64_t rows, int Kp, int
 
 // Operand stages and skew staging buffers within the 227 KB of shared memory:
 // KB 1: 2 + 2, KB 2: 1 + 2 (the second accumulator already overlaps the next
-// block's loads with this block's epilogue), KB 3-4: 1 + 1.
+// block's loads with this block's epilogue; 2 + 1 measured the same), KB 3-4:
+// 1 + 1.
 constexpr int gemm_stages(int KB) { return KB == 1 ? 2 : 1; }
 constexpr int gemm_skew_bufs(int KB) { return KB <= 2 ? 2 : 1; }
 

@@ -9,7 +9,10 @@
 // From features the value is 1 - sum_f A[f][row] * B[f][col] with the sum
 // taken in the fixed order f = 0, 1, ..., d-1 and every product and sum
 // rounded separately: bit-identical to k_cost_f64 and to the fixed-order host
-// restatement used by the tests.
+// restatement used by the tests.  The FMA variant (FMA = true) forms the
+// same sum as a chain of fused multiply-adds in the same order (the first
+// product rounded on its own): 13 FP64 operations per cell instead of 24,
+// bit-identical to the oracle's fma chain (oracle_cost_fma).
 #include "common.cuh"
 
 namespace pfx {
@@ -91,7 +94,7 @@ constexpr int kCH = kCX / 2;            // per parity
 // read from shared memory serves four cells of a lane.  The rows' features
 // are staged in shared memory too ([f][strip][64 rows], one 16-byte (A, B)
 // pair per lane: conflict-free), which keeps the registers to 32 sums.
-template <int DMAX>
+template <int DMAX, bool FMA>
 __global__ void __launch_bounds__(kCostThreads, 2)
     k_cost_skew(const double* __restrict__ An, const double* __restrict__ Bn, const int d,
                 const Geo g, double* __restrict__ Csk, const int64_t stride,
@@ -154,14 +157,21 @@ __global__ void __launch_bounds__(kCostThreads, 2)
             const double2 a0 = sA2[(f * 2) * 32 + lane], a1 = sA2[(f * 2 + 1) * 32 + lane];
 #pragma unroll
             for (int v = 0; v < kCV; ++v) {
-                const double pA0 = __dmul_rn(a0.x, b[v + 1]);
-                const double pB0 = __dmul_rn(a0.y, b[v]);
-                const double pA1 = __dmul_rn(a1.x, b[v + 1]);
-                const double pB1 = __dmul_rn(a1.y, b[v]);
-                accA0[v] = f == 0 ? pA0 : __dadd_rn(accA0[v], pA0);
-                accB0[v] = f == 0 ? pB0 : __dadd_rn(accB0[v], pB0);
-                accA1[v] = f == 0 ? pA1 : __dadd_rn(accA1[v], pA1);
-                accB1[v] = f == 0 ? pB1 : __dadd_rn(accB1[v], pB1);
+                if (FMA && f > 0) {
+                    accA0[v] = __fma_rn(a0.x, b[v + 1], accA0[v]);
+                    accB0[v] = __fma_rn(a0.y, b[v], accB0[v]);
+                    accA1[v] = __fma_rn(a1.x, b[v + 1], accA1[v]);
+                    accB1[v] = __fma_rn(a1.y, b[v], accB1[v]);
+                } else {
+                    const double pA0 = __dmul_rn(a0.x, b[v + 1]);
+                    const double pB0 = __dmul_rn(a0.y, b[v]);
+                    const double pA1 = __dmul_rn(a1.x, b[v + 1]);
+                    const double pB1 = __dmul_rn(a1.y, b[v]);
+                    accA0[v] = f == 0 ? pA0 : __dadd_rn(accA0[v], pA0);
+                    accB0[v] = f == 0 ? pB0 : __dadd_rn(accB0[v], pB0);
+                    accA1[v] = f == 0 ? pA1 : __dadd_rn(accA1[v], pA1);
+                    accB1[v] = f == 0 ? pB1 : __dadd_rn(accB1[v], pB1);
+                }
             }
         }
 #pragma unroll
@@ -190,6 +200,7 @@ constexpr int kCT2 = 64;
 constexpr int kCX2 = kCT2 + 66;
 constexpr int kCH2 = kCX2 / 2;
 
+template <bool FMA>
 __global__ void __launch_bounds__(kCostThreads, 2)
     k_cost_skew_chunked(const double* __restrict__ An, const double* __restrict__ Bn, const int d,
                         const Geo g, double* __restrict__ Csk, const int64_t stride,
@@ -238,10 +249,15 @@ __global__ void __launch_bounds__(kCostThreads, 2)
                 const bool first = f0 + f == 0;
 #pragma unroll
                 for (int v = 0; v < kCV; ++v) {
-                    const double pA = __dmul_rn(aA, b[v + 1]);
-                    const double pB = __dmul_rn(aB, b[v]);
-                    accA[v] = first ? pA : __dadd_rn(accA[v], pA);
-                    accB[v] = first ? pB : __dadd_rn(accB[v], pB);
+                    if (FMA && !first) {
+                        accA[v] = __fma_rn(aA, b[v + 1], accA[v]);
+                        accB[v] = __fma_rn(aB, b[v], accB[v]);
+                    } else {
+                        const double pA = __dmul_rn(aA, b[v + 1]);
+                        const double pB = __dmul_rn(aB, b[v]);
+                        accA[v] = first ? pA : __dadd_rn(accA[v], pA);
+                        accB[v] = first ? pB : __dadd_rn(accB[v], pB);
+                    }
                 }
             }
         }
@@ -292,15 +308,13 @@ cudaError_t launch_relayout_skew_f32(const double* C64, const float* C32, int64_
                : relayout_t(C64, ldc, g, Csk, stride, st, slot);
 }
 
-cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Geo& g, double* Csk,
-                             int64_t stride, cudaStream_t st, const int32_t* slot,
-                             const int32_t* list, int nlist) {
-    if (d < 1) return cudaErrorInvalidValue;
-    const int64_t nt = list ? nlist : -1;
-    if (list && nlist == 0) return cudaSuccess;
+template <bool FMA>
+static cudaError_t cost_skew_t(const double* An, const double* Bn, int d, const Geo& g,
+                               double* Csk, int64_t stride, cudaStream_t st, const int32_t* slot,
+                               const int32_t* list, int64_t nt) {
     if (d > kMaxFeat) {
-        k_cost_skew_chunked<<<region_grid(g, kCT2, nt), kCostThreads, 0, st>>>(An, Bn, d, g, Csk,
-                                                                              stride, slot, list);
+        k_cost_skew_chunked<FMA><<<region_grid(g, kCT2, nt), kCostThreads, 0, st>>>(
+            An, Bn, d, g, Csk, stride, slot, list);
         count_launches(1);
         return cudaGetLastError();
     }
@@ -309,19 +323,30 @@ cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Ge
     grid.y = (grid.y + 1) / 2;  // strip pairs
     cudaError_t e;
     if (d == 12) {
-        e = cudaFuncSetAttribute(k_cost_skew<12>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e != cudaSuccess) return e;
-        k_cost_skew<12><<<grid, kCostThreads, smem, st>>>(An, Bn, d, g, Csk, stride, slot, list);
-    } else {
-        e = cudaFuncSetAttribute(k_cost_skew<kMaxFeat>,
+        e = cudaFuncSetAttribute(k_cost_skew<12, FMA>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        k_cost_skew<kMaxFeat><<<grid, kCostThreads, smem, st>>>(An, Bn, d, g, Csk, stride, slot,
-                                                                 list);
+        k_cost_skew<12, FMA><<<grid, kCostThreads, smem, st>>>(An, Bn, d, g, Csk, stride, slot,
+                                                               list);
+    } else {
+        e = cudaFuncSetAttribute(k_cost_skew<kMaxFeat, FMA>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        k_cost_skew<kMaxFeat, FMA><<<grid, kCostThreads, smem, st>>>(An, Bn, d, g, Csk, stride,
+                                                                     slot, list);
     }
     count_launches(1);
     return cudaGetLastError();
+}
+
+cudaError_t launch_cost_skew(const double* An, const double* Bn, int d, const Geo& g, double* Csk,
+                             int64_t stride, cudaStream_t st, const int32_t* slot,
+                             const int32_t* list, int nlist, bool fma) {
+    if (d < 1) return cudaErrorInvalidValue;
+    const int64_t nt = list ? nlist : -1;
+    if (list && nlist == 0) return cudaSuccess;
+    return fma ? cost_skew_t<true>(An, Bn, d, g, Csk, stride, st, slot, list, nt)
+               : cost_skew_t<false>(An, Bn, d, g, Csk, stride, st, slot, list, nt);
 }
 
 }  // namespace pfx

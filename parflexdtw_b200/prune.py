@@ -400,10 +400,10 @@ class PrunedBatch:
 
     def __init__(self, shapes, L, steps, weights, d, proposer=None, threshold=None,
                  dilation=1, manhattan=None, precision="fp64", wave_bytes=0, warps=0,
-                 expand=2, cost="slabs", proposer_streams=8):
+                 expand=2, cost="slabs", proposer_streams=8, cost_fma=False):
         from .batch import Batch
         self.batch = Batch(shapes, L, steps, weights, d, wave_bytes=wave_bytes, warps=warps,
-                           precision=precision, cost=cost)
+                           precision=precision, cost=cost, cost_fma=cost_fma)
         self.proposer = proposer or TileProposer.load()
         self.threshold = threshold
         self.dilation = dilation
@@ -558,8 +558,8 @@ class PrunedBatch:
         try:
             return self.batch.complete(i, beta)
         except ValueError as e:
-            if str(e) == _lib.NO_ENDPOINT_MSG:
-                raise
+            if str(e) == _lib.NO_ENDPOINT_MSG or self.batch.cost_fma:
+                raise  # (a plan of its own has no FMA-chain cost)
             f1, f2 = self.batch.feature_views(i)
             plan = Plan(N, M, self.L, self.steps, self.weights, precision=self.precision)
             plan.load_features(f1, f2)

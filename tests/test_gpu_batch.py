@@ -125,6 +125,48 @@ def test_batch_cost_in_kernel_dims_and_steps_vs_oracle(oracle_mod, d, steps, wei
         assert same(x, y)
 
 
+@pytest.mark.parametrize("d,steps,weights", [
+    (12, STD, WTS),
+    (5, [(1, 1), (2, 1)], [1.0, 2.5]),
+    (40, STD, WTS),
+])
+def test_batch_cost_fma_vs_oracle(oracle_mod, d, steps, weights):
+    """PFX_BATCH_COST_FMA: the cost as a fixed-order FMA chain, bit-exact with
+    the oracle's fma chain (oracle_cost_fma), and the whole alignment
+    bit-exact with the oracle on that cost; both cost kernels (d <= 16 and the
+    chunked d > 16 one), masked runs and completions included."""
+    sizes = [(700, 900), (1500, 1200), (333, 410), (1200, 1700)]
+    Ls = [256, 300, 128, 500]
+    rng = np.random.default_rng(41 + d)
+    pairs = [W.warped_pair(rng, n, m, d=d, noise=0.1, latent="gaussian") for n, m in sizes]
+    shapes = [(p[0].shape[1], p[1].shape[1]) for p in pairs]
+    Cs = [oracle_mod.cost_matrix_fma(F1, F2) for F1, F2 in pairs]
+    refs = [oracle_mod.parflex_full(C, steps, weights, 0.1, Lb) for C, Lb in zip(Cs, Ls)]
+    b = Batch(shapes, Ls, steps, weights, d, cost_fma=True)
+    assert b.cost_fma
+    b.load(pairs)
+    b.run(0.1)
+    _check(b, refs)
+    torch.cuda.synchronize()
+    assert same(b.plan(3).cost_matrix(), Cs[3])
+    # masked run on every tile, then completion of one pair from a sparse mask
+    grids = [(-(-(n - 1) // (Lb - 1)), -(-(m - 1) // (Lb - 1))) for (n, m), Lb in zip(shapes, Ls)]
+    b.set_masks(torch.ones(sum(a * c for a, c in grids), dtype=torch.uint8, device="cuda"))
+    b.run(0.1, use_graph=False)
+    _check(b, refs)
+    rng2 = np.random.default_rng(3)
+    sparse = torch.from_numpy((rng2.random(sum(a * c for a, c in grids)) < 0.5)
+                              .astype(np.uint8)).cuda()
+    b.set_masks(sparse)
+    b.run(0.1, use_graph=False)
+    for i, r in enumerate(refs):
+        bc, wp = b.complete(i, 0.1)
+        assert bc == r["best_cost"] and same(wp.T, r["wp"]), i
+    b.close()
+    with pytest.raises(ValueError):
+        Batch(shapes, Ls, steps, weights, d, cost_fma=True, cost="tile")
+
+
 def test_batch_beta_change_rerecords(oracle_mod):
     pairs = _pairs(2, [(800, 950), (640, 600)])
     C = [W.cost_matrix_det(F1, F2) for F1, F2 in pairs]

@@ -301,6 +301,34 @@ def test_batch_masks_and_pruned_batch_exact(oracle_mod, cost):
         pb.close()
 
 
+def test_pruned_batch_cost_fma_equals_full_tiles(oracle_mod):
+    """Learned pruning over an FMA-cost batch: every path equals the full-tile
+    FMA-cost result, which equals the oracle's on the oracle's fma-chain cost."""
+    from parflexdtw_b200.batch import Batch
+    rng = np.random.default_rng(44)
+    sizes = [(2600, 2900), (1800, 1500), (3100, 3300)]
+    pairs = [W.warped_pair(rng, n, m, pad_frac=0.1) for n, m in sizes]
+    shapes = [(p[0].shape[1], p[1].shape[1]) for p in pairs]
+    L = 300
+    refs = [oracle_mod.parflex_full(oracle_mod.cost_matrix_fma(F1, F2), STD, WTS, 0.1, L)
+            for F1, F2 in pairs]
+    full = Batch(shapes, L, STD, WTS, 12, cost_fma=True)
+    full.load(pairs)
+    full.run(0.1)
+    best, end, lens = full.results()
+    paths = full.paths(lens)
+    for i, r in enumerate(refs):
+        assert best[i] == r["best_cost"] and np.array_equal(paths[i].T, r["wp"])
+    full.close()
+    pb = pf.PrunedBatch(shapes, L, STD, WTS, 12, proposer=TileProposer.load(), cost_fma=True)
+    pb.load(pairs)
+    for _ in range(2):
+        out, info = pb.run(0.1)
+        for (bc, wp), r in zip(out, refs):
+            assert bc == r["best_cost"] and np.array_equal(wp, r["wp"])
+    pb.close()
+
+
 def test_trained_proposer_gain_on_held_out_pairs():
     """What the shipped, trained network gains over the method without it.
 

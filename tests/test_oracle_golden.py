@@ -70,3 +70,31 @@ def test_stage2_matches_reference(oracle_mod, name):
         et, si, ci, cj, e, ix, gr, gc = (int(x) for x in row)
         assert r["seg_best_norm"][et, si] == norm
         assert tuple(r["seg_best_meta"][et, si]) == (ci, cj, e, ix, gr, gc)
+
+
+def test_oracle_cost_fma_is_the_fma_chain():
+    """oracle_cost_fma: C = 1 - (fma chain over the features in order); it
+    differs from the separately rounded cost by a few ulps at most, and
+    equals an independent evaluation of the chain (math.fma where Python has
+    it, else the exact rational product-sum rounded once per step)."""
+    import math
+    from fractions import Fraction
+    from parflexdtw_b200 import workloads as W
+    from oracle import oracle as O
+    rng = np.random.default_rng(8)
+    F1, F2 = W.warped_pair(rng, 40, 35, d=7, noise=0.1, latent="gaussian")
+    C = O.cost_matrix_fma(F1, F2)
+    C0 = W.cost_matrix_det(F1, F2)
+    assert np.abs(C - C0).max() < 1e-14
+    A, B = W.l2norm(F1), W.l2norm(F2)
+
+    def fma(a, b, c):
+        if hasattr(math, "fma"):
+            return math.fma(a, b, c)
+        return float(Fraction(a) * Fraction(b) + Fraction(c))  # one rounding
+
+    for i, j in [(0, 0), (3, 17), (39, 34), (20, 5)]:
+        acc = A[0, i] * B[0, j]
+        for f in range(1, A.shape[0]):
+            acc = fma(A[f, i], B[f, j], acc)
+        assert C[i, j] == 1.0 - acc
