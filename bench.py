@@ -926,6 +926,23 @@ def _masked_cells(masks, shapes, Lb):
     return tot
 
 
+def _masked_slab_bytes(masks, shapes, Lb, elem=8):
+    """Bytes the cost kernels write for the kept tiles: per tile its strips x
+    skewed steps x 64 rows (span = W + 63 rounded up to 16 steps)."""
+    hop = Lb - 1
+    tot, off = 0, 0
+    for N, M in shapes:
+        n1, n2 = -(-(N - 1) // hop), -(-(M - 1) // hop)
+        rows = np.minimum(Lb, N - np.arange(n1) * hop).astype(np.int64)
+        cols = np.minimum(Lb, M - np.arange(n2) * hop).astype(np.int64)
+        strips = -(-rows // 64)
+        spans = -(-(cols + 63) // 16) * 16
+        m = np.asarray(masks[off:off + n1 * n2], bool).reshape(n1, n2)
+        tot += int(strips @ m.astype(np.int64) @ spans) * 64 * elem
+        off += n1 * n2
+    return tot
+
+
 def prune_arm(args, spec):
     import torch
     import torch.distributed as dist
@@ -1010,7 +1027,8 @@ def prune_arm(args, spec):
     launches = lib.pfx_kernel_launches() - launches0
     ms_pruned = max_ranks(ms_pruned)
     _, prof = pb.run(spec.beta, profile=True)
-    kept_cells = _masked_cells(pb.last_masks.cpu().numpy(), shapes, Lb)
+    pb_masks = pb.last_masks.cpu().numpy()
+    kept_cells = _masked_cells(pb_masks, shapes, Lb)
     agree = sum(int(bc == best0[i] and np.array_equal(wp, paths0[i].T))
                 for i, (bc, wp) in enumerate(out))
     # e2e: pinned host features in, results out
@@ -1080,6 +1098,17 @@ def prune_arm(args, spec):
         if peak_kind == "measured" else "fallback",
         "alg_bytes_per_cell": 8.25, "kept_cells": kept_cells, "stage1_ms": s1_ms,
         "fp64_dp_cells_per_s": kept_cells / (s1_ms / 1e3)}
+    # the FP64 cost kernel of the masked run: its slab writes against HBM
+    slab_bytes = _masked_slab_bytes(pb_masks, shapes, Lb)
+    cost_ms = prof["align_ms"]["cost"]
+    roofline["cost_kernel"] = {
+        "kernel": "k_cost_skew<12, %s> (FP64 cost into the kept tiles' slabs)"
+                  % ("true: FMA chain" if cost_fma else "false: separately rounded"),
+        "bound": "hbm", "slab_bytes": slab_bytes, "ms": cost_ms,
+        "achieved_GBps": slab_bytes / (cost_ms / 1e3) / 1e9,
+        "frac": slab_bytes / (cost_ms / 1e3) / 1e9 / peak,
+        "note": "algorithmic bytes = the slab elements written (8 B each, the skewed layout's "
+                "zero padding included); the features it reads are L2-resident"}
     if "inst_per_cell" in ctr and clocks.get("sm_mhz"):
         smsp = 4 * torch.cuda.get_device_properties(dev).multi_processor_count
         inst = ctr["inst_per_cell"] * kept_cells / (s1_ms / 1e3)
