@@ -336,6 +336,13 @@ int pfx_batch_info(const pfx_batch *batch, int64_t *info);
  * row-major by feature.  Fill them before pfx_batch_run (any stream, but
  * ordered before the run). */
 int pfx_batch_features(pfx_batch *batch, int32_t i, double **F1, double **F2);
+/* Copies pair i's features from host memory (F1: d x N[i], F2: d x M[i],
+ * row-major by feature) into the batch's input buffers, asynchronously on
+ * `stream` (page-locked host memory makes it truly asynchronous; a copy
+ * into the same pair's buffers may be recorded into a CUDA graph, so that a
+ * pair's upload overlaps the work on other pairs). */
+int pfx_batch_load_async(pfx_batch *batch, int32_t i, const double *F1, const double *F2,
+                         void *stream);
 /* The plan of pair i (owned by the batch: do not destroy; do not load a
  * cost into it).  pfx_result / pfx_copy_path / pfx_plan_buffer read pair
  * i's results after pfx_batch_run. */

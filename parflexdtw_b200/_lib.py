@@ -82,6 +82,7 @@ SIGNATURES = [
     ("pfx_batch_destroy", None, [_vp]),
     ("pfx_batch_info", ct.c_int, [_vp, _i64p]),
     ("pfx_batch_features", ct.c_int, [_vp, _i32, ct.POINTER(_vp), ct.POINTER(_vp)]),
+    ("pfx_batch_load_async", ct.c_int, [_vp, _i32, _vp, _vp, _vp]),
     ("pfx_batch_plan", ct.c_int, [_vp, _i32, ct.POINTER(_vp)]),
     ("pfx_batch_set_masks", ct.c_int, [_vp, _vp, _i32, _vp]),
     ("pfx_batch_complete", ct.c_int, [_vp, _i32, _f64, _vp, _vp]),

@@ -761,6 +761,20 @@ extern "C" int pfx_batch_features(pfx_batch* b, int32_t i, double** F1, double**
     return PFX_OK;
 }
 
+extern "C" int pfx_batch_load_async(pfx_batch* b, int32_t i, const double* F1,
+                                    const double* F2, void* stream) {
+    if (!b || !F1 || !F2) return errf(PFX_ERR_ARG, "null argument");
+    if (i < 0 || i >= b->n) return errf(PFX_ERR_ARG, "pair %d of %d", i, b->n);
+    cudaStream_t s = (cudaStream_t)stream;
+    double* d1 = b->fin + b->fin_off[i];
+    double* d2 = d1 + (int64_t)b->d * b->plans[i].g.N;
+    BCK(cudaMemcpyAsync(d1, F1, sizeof(double) * (size_t)b->d * b->plans[i].g.N,
+                        cudaMemcpyHostToDevice, s));
+    BCK(cudaMemcpyAsync(d2, F2, sizeof(double) * (size_t)b->d * b->plans[i].g.M,
+                        cudaMemcpyHostToDevice, s));
+    return PFX_OK;
+}
+
 extern "C" int pfx_batch_plan(pfx_batch* b, int32_t i, pfx_plan** plan) {
     if (!b || !plan) return errf(PFX_ERR_ARG, "null argument");
     if (i < 0 || i >= b->n) return errf(PFX_ERR_ARG, "pair %d of %d", i, b->n);

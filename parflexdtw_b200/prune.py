@@ -422,9 +422,16 @@ class PrunedBatch:
     def load(self, pairs, non_blocking=True):
         self.batch.load(pairs, non_blocking=non_blocking)
 
-    def run(self, beta, profile=False):
+    def run(self, beta, profile=False, host_pairs=None):
         """[(best_cost, wp[2, K]) per pair], info.  profile: synchronise
-        between phases and report their wall times (ms) in info."""
+        between phases and report their wall times (ms) in info.
+
+        host_pairs: the pairs' features as page-locked host tensors (d x N,
+        d x M, float64), uploaded as part of the run: each pair's upload runs
+        on the proposer stream of that pair, just before its proposer pass, so
+        that it overlaps the other pairs' passes (the phase, uploads included,
+        is recorded once per set of host buffers into a CUDA graph).  Without
+        it the features are the ones ``load`` put on the device."""
         import time as _time
         b = self.batch
         marks = []
@@ -435,7 +442,7 @@ class PrunedBatch:
                 marks.append((name, _time.perf_counter()))
 
         mark("start")
-        masks = self._propose_all()
+        masks = self._propose_all(host_pairs)
         mark("proposer")
         self.last_masks = masks  # the proposed tiles, pairs' (n1, n2) masks concatenated
         b.set_masks(masks)
@@ -487,15 +494,23 @@ class PrunedBatch:
             info["align_ms"] = dict(zip(("cost", "stage1", "stage2"), align_ms))
         return out, info
 
-    def _launch_proposer(self):
+    def _launch_proposer(self, host=None):
         """Every pair's proposer pass, pairs spread over the side streams
-        (the kernels are small), each stream with its own buffer set."""
+        (the kernels are small), each stream with its own buffer set; with
+        `host` ((F1, F2) page-locked host tensors per pair), each pair's
+        upload first, on the same stream."""
         main = torch.cuda.current_stream()
+        lib = _lib.load()
         for st in self._streams:
-            st.wait_stream(main)  # features loaded
+            st.wait_stream(main)  # features loaded (or their buffers free)
         for i, (N, M) in enumerate(self.shapes):
             k = i % len(self._streams)
             with torch.cuda.stream(self._streams[k]):
+                if host is not None:
+                    h1, h2 = host[i]
+                    _lib.check(lib.pfx_batch_load_async(
+                        self.batch.handle, i, ct.c_void_p(h1.data_ptr()),
+                        ct.c_void_p(h2.data_ptr()), current_stream_ptr()))
                 f1, f2 = self._views[i]
                 self.proposer.propose_into(f1, f2, self.L, self._bufs[k],
                                            self._masks[self.offs[i]:self.offs[i + 1]],
@@ -503,23 +518,59 @@ class PrunedBatch:
         for st in self._streams:
             main.wait_stream(st)
 
-    def _propose_all(self):
+    def _setup_proposer(self):
+        dev = self.proposer.device
+        self._masks = torch.empty(int(self.offs[-1]), dtype=torch.uint8, device=dev)
+        self._views = [self.batch.feature_views(i) for i in range(len(self.shapes))]
+        ns = max(1, min(self.proposer_streams, len(self.shapes)))
+        self._streams = [torch.cuda.Stream(device=dev) for _ in range(ns)]
+        self._bufs = []
+        for k in range(ns):
+            mine = self.shapes[k::ns]
+            self._bufs.append(TileProposer.buffers(self.batch.d, max(n for n, _ in mine),
+                                                   max(m for _, m in mine), self.L, dev))
+        self._host_graphs = {}
+
+    def _check_host(self, host_pairs):
+        if len(host_pairs) != len(self.shapes):
+            raise ValueError(f"{len(host_pairs)} pairs for a batch of {len(self.shapes)}")
+        out = []
+        for i, (F1, F2) in enumerate(host_pairs):
+            for t, n in ((F1, self.shapes[i][0]), (F2, self.shapes[i][1])):
+                if not (isinstance(t, torch.Tensor) and t.device.type == "cpu" and t.is_pinned()
+                        and t.dtype == torch.float64 and t.is_contiguous()):
+                    raise ValueError("host_pairs: contiguous page-locked float64 CPU tensors "
+                                     "(torch.Tensor.pin_memory())")
+                if tuple(t.shape) != (self.batch.d, n):
+                    raise ValueError(f"pair {i}: features {tuple(t.shape)}, expected "
+                                     f"({self.batch.d}, {n})")
+            out.append((F1, F2))
+        return out
+
+    def _propose_all(self, host_pairs=None):
         """The tile masks of all pairs (uint8 device tensor, pairs' (n1, n2)
         masks concatenated): one eager pass on the first call, which also
         records the whole phase into a CUDA graph; the graph is replayed on
         every later call (the features are read from the batch's fixed
-        buffers)."""
+        buffers; with host_pairs, a graph per set of host buffers uploads
+        them first)."""
+        if self._streams is None:
+            self._setup_proposer()
+        if host_pairs is not None:
+            host = self._check_host(host_pairs)
+            key = tuple((a.data_ptr(), c.data_ptr()) for a, c in host)
+            g = self._host_graphs.get(key)
+            if g is None:
+                self._launch_proposer(host)
+                torch.cuda.current_stream().synchronize()
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g):
+                    self._launch_proposer(host)
+                self._host_graphs[key] = (g, host)  # the graph reads these buffers
+                return self._masks
+            g[0].replay()
+            return self._masks
         if self._graph is None:
-            dev = self.proposer.device
-            self._masks = torch.empty(int(self.offs[-1]), dtype=torch.uint8, device=dev)
-            self._views = [self.batch.feature_views(i) for i in range(len(self.shapes))]
-            ns = max(1, min(self.proposer_streams, len(self.shapes)))
-            self._streams = [torch.cuda.Stream(device=dev) for _ in range(ns)]
-            self._bufs = []
-            for k in range(ns):
-                mine = self.shapes[k::ns]
-                self._bufs.append(TileProposer.buffers(self.batch.d, max(n for n, _ in mine),
-                                                       max(m for _, m in mine), self.L, dev))
             self._launch_proposer()
             torch.cuda.current_stream().synchronize()
             g = torch.cuda.CUDAGraph()
@@ -571,4 +622,5 @@ class PrunedBatch:
 
     def close(self):
         self._graph = None
+        self._host_graphs = {}
         self.batch.close()

@@ -329,6 +329,38 @@ def test_pruned_batch_cost_fma_equals_full_tiles(oracle_mod):
     pb.close()
 
 
+def test_pruned_batch_host_pairs_upload_in_the_graph():
+    """run(host_pairs=...) uploads each pair's page-locked features on its
+    proposer stream inside the recorded graph: the results equal those of
+    load() + run(), on the first (eager) run and on replays, and new contents
+    of the same host buffers are picked up by the replay."""
+    rng = np.random.default_rng(52)
+    sizes = [(2600, 2900), (1800, 1500), (3100, 3300)]
+    sets = [[W.warped_pair(rng, n, m) for n, m in sizes] for _ in range(2)]  # same shapes
+    shapes = [(p[0].shape[1], p[1].shape[1]) for p in sets[0]]
+    L = 300
+    net = TileProposer.load()
+    want = []
+    pb = pf.PrunedBatch(shapes, L, STD, WTS, 12, proposer=net)
+    for pairs in sets:
+        pb.load(pairs)
+        out, _ = pb.run(0.1)
+        want.append(out)
+    pinned = [(torch.from_numpy(F1).pin_memory(), torch.from_numpy(F2).pin_memory())
+              for F1, F2 in sets[0]]
+    for k in (0, 0, 1, 0):
+        for (h1, h2), (F1, F2) in zip(pinned, sets[k]):
+            h1.copy_(torch.from_numpy(F1))
+            h2.copy_(torch.from_numpy(F2))
+        out, _ = pb.run(0.1, host_pairs=pinned)
+        for (b1, w1), (b2, w2) in zip(out, want[k]):
+            assert b1 == b2 and np.array_equal(w1, w2), k
+    with pytest.raises(ValueError):
+        pb.run(0.1, host_pairs=[(torch.from_numpy(F1), torch.from_numpy(F2))
+                                for F1, F2 in sets[0]])  # not page-locked
+    pb.close()
+
+
 def test_trained_proposer_gain_on_held_out_pairs():
     """What the shipped, trained network gains over the method without it.
 
