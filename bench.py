@@ -37,6 +37,7 @@ host cores for the same workload (rank 0 only).
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -976,6 +977,7 @@ def prune_arm(args, spec):
         return torch.cuda.Event(enable_timing=True)
 
     def timed(fn, steps):
+        gc.collect()  # (automatic collection is off: no pause inside a timed step)
         torch.cuda.synchronize()
         a, b = ev(), ev()
         a.record()
@@ -1378,6 +1380,11 @@ def shard_arm(args, spec):
 
 
 def main():
+    # Python's cyclic garbage collector stays off while the arms run, so that
+    # no collection pause lands inside a timed step; reference counting still
+    # frees everything that is not in a cycle, and each timed region of the
+    # learned-pruning arm starts after an explicit collection.
+    gc.disable()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)

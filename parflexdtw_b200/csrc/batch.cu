@@ -28,6 +28,34 @@ struct PairOut {
     const int64_t* wp_len;
 };
 
+// One host-to-device upload scattered to many buffers: segment s copies
+// segs[s].bytes bytes from base + segs[s].src to segs[s].dst (16-byte words
+// where both ends are aligned).
+struct CopySeg {
+    int64_t src;
+    void* dst;
+    int64_t bytes;
+};
+constexpr int64_t kSegChunk = 1 << 16;  // bytes per segment (one CTA each)
+
+__global__ void __launch_bounds__(256) k_scatter_segments(const char* __restrict__ base,
+                                                          const CopySeg* __restrict__ segs,
+                                                          int nseg) {
+    if ((int)blockIdx.x >= nseg) return;
+    const CopySeg g = segs[blockIdx.x];
+    const char* src = base + g.src;
+    char* dst = static_cast<char*>(g.dst);
+    int64_t done = 0;
+    if (((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0) {
+        const int64_t n16 = g.bytes >> 4;
+        const int4* s4 = reinterpret_cast<const int4*>(src);
+        int4* d4 = reinterpret_cast<int4*>(dst);
+        for (int64_t i = threadIdx.x; i < n16; i += blockDim.x) d4[i] = s4[i];
+        done = n16 << 4;
+    }
+    for (int64_t i = done + threadIdx.x; i < g.bytes; i += blockDim.x) dst[i] = src[i];
+}
+
 __global__ void k_gather_results(const PairOut* __restrict__ po, int n, int64_t* __restrict__ out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -180,7 +208,8 @@ struct pfx_batch {
     FbSeg* fbsegs = nullptr;  // FP32 form: every feature matrix's bf16 conversion
     int fb_nseg = 0;
     int64_t fb_blocks = 0;
-    char* stage = nullptr;  // pinned staging of pfx_batch_set_masks' uploads
+    char* stage = nullptr;   // pinned staging of pfx_batch_set_masks' uploads
+    char* dstage = nullptr;  // and its device copy (scattered from there)
     size_t stage_bytes = 0;
     // masked batches, per pair: the slot map and kept-tile list of the mask
     // (host copies), and the tiles whose stage 1 ran since the last run
@@ -211,6 +240,7 @@ static void batch_free(pfx_batch* b) {
     if (b->arena) cudaFree(b->arena);
     if (b->slabs) cudaFree(b->slabs);
     if (b->stage) cudaFreeHost(b->stage);
+    if (b->dstage) cudaFree(b->dstage);
     if (b->fbsegs) cudaFree(b->fbsegs);
     if (b->gpairs) cudaFree(b->gpairs);
     if (b->pref) cudaFree(b->pref);
@@ -565,78 +595,126 @@ extern "C" int pfx_batch_set_masks(pfx_batch* b, const uint8_t* masks, int32_t o
         wave_pairs.push_back(i);
     }
     wave_first.push_back(n);
-    // pinned staging for the uploads (per pair: slot map, mask, its queue of
-    // every tile; then the waves' queues of kept tiles), copied asynchronously
-    size_t need = (size_t)b->total_tiles * sizeof(TileDesc) + 16;
+    // Everything the device needs is laid out once in pinned staging memory
+    // (per pair: slot map, mask, kept-tile list, its queue of every tile and
+    // of its kept tiles, their count; then the waves' queues of kept tiles;
+    // then the copy table), uploaded with one copy and scattered by one
+    // kernel.  Descriptors are built in place.
+    auto al16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    std::vector<int32_t> kept_n(n);
+    size_t need = 0;
     for (int i = 0; i < n; ++i) {
         const int64_t nt = moff[i + 1] - moff[i];
-        need += (size_t)nt * (4 + 4 + 1 + sizeof(TileDesc)) + 4 * 16;
+        int kept = 0;
+        for (int64_t t = 0; t < nt; ++t) kept += slots[i][t] >= 0;
+        kept_n[i] = kept;
+        need += al16(nt * 4) + al16(nt) + al16((size_t)kept * 4) +
+                al16(nt * sizeof(TileDesc)) + al16((size_t)kept * sizeof(TileDesc)) + 16;
     }
-    BCK(cudaStreamSynchronize(s));  // the staging buffer may still feed earlier copies
+    int64_t kept_total = 0;
+    for (int i = 0; i < n; ++i) kept_total += kept_n[i];
+    need += al16((size_t)kept_total * sizeof(TileDesc));
+    const size_t table_cap = (size_t)6 * n + (need >> 16) + 16;  // chunks of <= 64 KB
+    need += table_cap * sizeof(CopySeg);
+    BCK(cudaStreamSynchronize(s));  // the staging buffers may still feed earlier copies
     if (need > b->stage_bytes) {
         if (b->stage) cudaFreeHost(b->stage);
+        if (b->dstage) cudaFree(b->dstage);
         b->stage = nullptr;
+        b->dstage = nullptr;
         b->stage_bytes = 0;
         BCK(cudaMallocHost(&b->stage, need));
+        BCK(cudaMalloc(&b->dstage, need));
         b->stage_bytes = need;
     }
     size_t so = 0;
-    auto stage = [&](const void* src, size_t bytes) {
-        char* dst = b->stage + so;
-        memcpy(dst, src, bytes);
-        so += (bytes + 15) & ~(size_t)15;
-        return dst;
+    std::vector<CopySeg> segs;
+    // reserve `bytes` of staging for device address dst (copied later)
+    auto reserve = [&](void* dst, size_t bytes) {
+        char* h = b->stage + so;
+        for (size_t c = 0; c < bytes; c += (size_t)kSegChunk) {
+            CopySeg g;
+            g.src = (int64_t)(so + c);
+            g.dst = static_cast<char*>(dst) + c;
+            g.bytes = (int64_t)std::min((size_t)kSegChunk, bytes - c);
+            segs.push_back(g);
+        }
+        so += al16(bytes);
+        return h;
     };
     b->mask_slots.assign(n, {});
     b->mask_lists.assign(n, {});
     b->mask_host.assign(n, {});
     b->ran = false;
-    // plans: slab base, slot map, mask; queues of the kept tiles
-    std::vector<TileDesc> all;
+    // plans: slab base, slot map, mask, kept-tile lists, queues
     std::vector<int64_t> wdo, wt;
     const int waves = (int)wave_first.size() - 1;
+    std::vector<std::vector<const TileDesc*>> wave_kept(waves);  // staged descriptors
     for (int w = 0; w < waves; ++w) {
-        wdo.push_back((int64_t)all.size());
-        std::vector<TileDesc> wv;
         for (int q = wave_first[w]; q < wave_first[w + 1]; ++q) {
             const int i = wave_pairs[q];
             pfx_plan& p = b->plans[i];
             p.Csk = b->gen_cost ? nullptr : reinterpret_cast<char*>(b->slabs) + off[i];
             const int nt = p.g.n1 * p.g.n2;
-            BCK(cudaMemcpyAsync(p.tile_slot, stage(slots[i].data(), (size_t)nt * 4),
-                                (size_t)nt * 4, cudaMemcpyHostToDevice, s));
-            BCK(cudaMemcpyAsync(p.tile_mask, stage(m.data() + moff[i], (size_t)nt), (size_t)nt,
-                                cudaMemcpyHostToDevice, s));
+            const int kept = kept_n[i];
+            memcpy(reserve(p.tile_slot, (size_t)nt * 4), slots[i].data(), (size_t)nt * 4);
+            memcpy(reserve(p.tile_mask, (size_t)nt), m.data() + moff[i], (size_t)nt);
             std::vector<int32_t> kl;
+            kl.reserve(kept);
             for (int t = 0; t < nt; ++t)
                 if (slots[i][t] >= 0) kl.push_back(t);
-            p.n_kept = (int32_t)kl.size();
-            b->mask_lists[i] = kl;
+            if (kept) memcpy(reserve(p.tile_list, (size_t)kept * 4), kl.data(), (size_t)kept * 4);
+            p.n_kept = kept;
+            b->mask_lists[i] = std::move(kl);
             b->mask_slots[i] = slots[i];
             b->mask_host[i].assign(m.begin() + moff[i], m.begin() + moff[i + 1]);
-            if (!kl.empty())
-                BCK(cudaMemcpyAsync(p.tile_list, stage(kl.data(), kl.size() * 4), kl.size() * 4,
-                                    cudaMemcpyHostToDevice, s));
-            std::vector<TileDesc> pd((size_t)nt);
-            plan_tile_descs(&p, p.Csk, pd.data(), slots[i].data());
-            // the pair's own queue keeps every tile (pfx_stage1 compacts it by the mask)
-            BCK(cudaMemcpyAsync(p.descs, stage(pd.data(), pd.size() * sizeof(TileDesc)),
-                                pd.size() * sizeof(TileDesc), cudaMemcpyHostToDevice, s));
-            BCK(launch_compact_descs(p.descs, nt, p.tile_mask, p.descs_sub, p.nsub, s));
-            for (const TileDesc& d : pd)
-                if (slots[i][d.tile] >= 0) wv.push_back(d);
+            // the pair's own queue keeps every tile; its kept tiles, in tile
+            // order, are the queue pfx_stage1 runs for the mask
+            TileDesc* pd = reinterpret_cast<TileDesc*>(
+                reserve(p.descs, (size_t)nt * sizeof(TileDesc)));
+            plan_tile_descs(&p, p.Csk, pd, slots[i].data());
+            if (kept) {
+                TileDesc* sub = reinterpret_cast<TileDesc*>(
+                    reserve(p.descs_sub, (size_t)kept * sizeof(TileDesc)));
+                int o = 0;
+                for (int t = 0; t < nt; ++t)
+                    if (slots[i][pd[t].tile] >= 0) {
+                        sub[o++] = pd[t];
+                        wave_kept[w].push_back(&pd[t]);
+                    }
+            }
+            int32_t* cnt = reinterpret_cast<int32_t*>(reserve(p.nsub, sizeof(int32_t)));
+            *cnt = kept;
             p.mask_active = 1;
             p.s2.tile_slot = p.tile_slot;
         }
-        std::stable_sort(wv.begin(), wv.end(), [](const TileDesc& a, const TileDesc& c) {
-            return (int64_t)a.R * a.W > (int64_t)c.R * c.W;
-        });
-        wt.push_back((int64_t)wv.size());
-        all.insert(all.end(), wv.begin(), wv.end());
     }
-    if (!all.empty())
-        BCK(cudaMemcpyAsync(b->descs, stage(all.data(), all.size() * sizeof(TileDesc)),
-                            all.size() * sizeof(TileDesc), cudaMemcpyHostToDevice, s));
+    // the waves' queues, largest tile first (stable: tile order among equals)
+    TileDesc* qall = kept_total ? reinterpret_cast<TileDesc*>(
+                                      reserve(b->descs, (size_t)kept_total * sizeof(TileDesc)))
+                                : nullptr;
+    int64_t qo = 0;
+    for (int w = 0; w < waves; ++w) {
+        std::vector<const TileDesc*>& kv = wave_kept[w];
+        std::stable_sort(kv.begin(), kv.end(), [](const TileDesc* a, const TileDesc* c) {
+            return (int64_t)a->R * a->W > (int64_t)c->R * c->W;
+        });
+        wdo.push_back(qo);
+        for (const TileDesc* d : kv) qall[qo++] = *d;
+        wt.push_back((int64_t)kv.size());
+    }
+    if (segs.size() > table_cap)
+        return errf(PFX_ERR_TOO_LARGE, "copy table: %zu segments > %zu", segs.size(), table_cap);
+    const size_t toff = so;
+    memcpy(b->stage + toff, segs.data(), segs.size() * sizeof(CopySeg));
+    so += segs.size() * sizeof(CopySeg);
+    BCK(cudaMemcpyAsync(b->dstage, b->stage, so, cudaMemcpyHostToDevice, s));
+    if (!segs.empty()) {
+        k_scatter_segments<<<(unsigned)segs.size(), 256, 0, s>>>(
+            b->dstage, reinterpret_cast<const CopySeg*>(b->dstage + toff), (int)segs.size());
+        count_launches(1);
+        BCK(cudaGetLastError());
+    }
     BCK(cudaStreamSynchronize(s));
     b->wave_pairs = wave_pairs;
     b->wave_first = wave_first;
