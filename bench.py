@@ -1347,14 +1347,9 @@ def shard_arm(args, spec):
             "config": dict(spec.describe(), N=N, M=M, tiles=n1 * n2, cells_per_step=cells,
                            parallelism=f"tiles over {ws} rank(s)",
                            input="features resident in HBM; every step builds the cost",
-                           cost_build=("inside the stage-1 kernel, tile by tile"
-                                       if args.cost == "tile" else
-                                       "separate cost kernels into slabs, in waves"),
-                           cost_definition=(
-                               "1 - sum_f a_f b_f as a fixed-order FP64 FMA chain "
-                               "(PFX_BATCH_COST_FMA), both forms" if cost_fma else
-                               "1 - sum_f a_f b_f with separately rounded FP64 products and "
-                               "sums, both forms"),
+                           cost_build="each rank's cost kernel into its tile range's slabs",
+                           cost_definition=("1 - sum_f a_f b_f with separately rounded FP64 "
+                                            "products and sums"),
                            l2="cost slabs larger than L2 (no flush needed)"),
             "pairs_per_s": args.steps / (ms_total / 1e3),
             "per_rank": {"cost_ms_max": cost_ms, "stage1_ms_max": s1_ms,

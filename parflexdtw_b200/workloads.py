@@ -302,11 +302,19 @@ class ShardSpec(PairSpec):
 # across ranks (one edge exchange), or all on one GPU (89 GB of FP64 cost).
 SHARD1 = ShardSpec("chroma12_pair_100000x100000_L4000_tile_sharded", 100000, 100000, 4000)
 
+# Small cases of the batch, precision and sharded-pair workloads (seconds per
+# run): every arm of the benchmark is exercised end to end by the tests.
+BATCH_SMALL = BatchSpec("chroma12_batch12_N2000-6000_fp64", 12, 2000, 6000)
+PRECISION_SMALL = PrecisionSpec("gauss128_batch24_N1000-3000_L1000_fp32_vs_fp64", 24,
+                                1000, 3000)
+SHARD_SMALL = ShardSpec("chroma12_pair_12000x12000_L2000_tile_sharded", 12000, 12000, 2000)
+
 WORKLOADS = {"config0": CONFIG0, "config1": CONFIG1, "ncu_small": NCU_SMALL,
              "batch256": BATCH256, "precision2048": PRECISION2048, "prune64": PRUNE64,
              "prune_ncu": PRUNE_NCU, "prune_ncu_w4": PRUNE_NCU_W4,
              "prune_ncu_l2000": PRUNE_NCU_L2000,
-             "shard1": SHARD1}
+             "shard1": SHARD1, "batch_small": BATCH_SMALL,
+             "precision_small": PRECISION_SMALL, "shard_small": SHARD_SMALL}
 
 
 def make_pair(spec: PairSpec):
