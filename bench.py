@@ -1386,7 +1386,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="prune64", choices=sorted(W.WORKLOADS))
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--ref-tile-rows", type=int, default=0,
                     help="single-pair workloads: tile rows the reference arm times "
                          "(0 = the whole pair)")

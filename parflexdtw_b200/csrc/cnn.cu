@@ -756,11 +756,164 @@ static cudaError_t conv_fwd_t(const void* x, int Cin, int H, int W, const float*
     return conv_fwd_launch<S, 32, CIB, 1, 1, Tin, Tout>(x, Cin, H, W, w, b, Cout, relu, y, st);
 }
 
+// --------------------------------------------------------------------------
+// The inference network's 32 -> 32-channel 3x3 convolution with bf16
+// activations (in and out) on the tensor cores: an implicit GEMM, output
+// pixels x (tap, input channel) x output channels, with
+// mma.sync.m16n8k16 (bf16 operands, FP32 accumulation).  The layer is bound
+// by moving its activations, not by its 9216 MACs per pixel, so warp-level
+// MMAs out of registers suffice.  Each weight is split into bf16 high and
+// low parts (two MMAs), so the products keep the FP32 weight to about 2^-17;
+// the sum order differs from k_conv3x3_fwd (results agree to FP32 rounding
+// of the sums, not bit for bit).
+//
+// A CTA computes 8 output rows x 16 columns for all 32 output channels; warp
+// w takes rows 2w, 2w + 1 (one m16 tile of 16 pixels each).  Shared memory:
+// the input patch as [row][column][channel] with a 36-channel pixel stride
+// and the weights as [tap][co][ci] (hi and lo) with a 40-channel row stride,
+// so that every fragment load of a warp touches 32 distinct banks.
+constexpr int kMmaRows = 8, kMmaCols = 16, kMmaPix = 36, kMmaWRow = 40;
+
+template <int S>
+struct MmaConvGeo {
+    static constexpr int PR = (kMmaRows - 1) * S + 3;  // patch rows
+    static constexpr int PC = (kMmaCols - 1) * S + 3;  // patch columns
+    static constexpr int patch_elems = PR * PC * kMmaPix;
+    static constexpr int w_elems = 9 * 32 * kMmaWRow;
+    static constexpr size_t smem = (size_t)(patch_elems + 2 * w_elems) * 2;
+};
+
+__device__ __forceinline__ void mma_bf16_16816(float (&c)[4], uint32_t a0, uint32_t a1,
+                                               uint32_t a2, uint32_t a3, uint32_t b0,
+                                               uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, "
+        "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+template <int S>
+__global__ void __launch_bounds__(128)
+    k_conv3x3_mma32(const __nv_bfloat16* __restrict__ x, int H, int W,
+                    const float* __restrict__ w, const float* __restrict__ b, int Ho, int Wo,
+                    int relu, __nv_bfloat16* __restrict__ y) {
+    using G = MmaConvGeo<S>;
+    extern __shared__ __align__(16) unsigned char cv_smem[];
+    __nv_bfloat16* patch = reinterpret_cast<__nv_bfloat16*>(cv_smem);
+    __nv_bfloat16* whi = patch + G::patch_elems;
+    __nv_bfloat16* wlo = whi + G::w_elems;
+    const int ox0 = blockIdx.x * kMmaCols, oy0 = blockIdx.y * kMmaRows;
+    const int iy0 = oy0 * S - 1, ix0 = ox0 * S - 1;
+    // the patch: a thread takes pixels, each as 16 channel pairs (loads of
+    // one channel plane coalesce across the warp's consecutive columns)
+    for (int q = threadIdx.x; q < G::PR * G::PC; q += 128) {
+        const int r = q / G::PC, c = q - r * G::PC;
+        const int iy = iy0 + r, ix = ix0 + c;
+        const bool in = iy >= 0 && iy < H && ix >= 0 && ix < W;
+        const __nv_bfloat16* src = x + (int64_t)(in ? iy : 0) * W + (in ? ix : 0);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(patch + q * kMmaPix);
+        unsigned short v[32];
+#pragma unroll
+        for (int ci = 0; ci < 32; ++ci)
+            v[ci] = in ? __bfloat16_as_ushort(src[(int64_t)ci * H * W]) : (unsigned short)0;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) dst[k] = (uint32_t)v[2 * k] | ((uint32_t)v[2 * k + 1] << 16);
+    }
+    // the weights, [tap][co][ci], each FP32 weight as bf16 hi + lo
+    for (int q = threadIdx.x; q < 9 * 32 * 32; q += 128) {
+        const int tap = q / 1024, co = (q >> 5) & 31, ci = q & 31;
+        const float v = w[(co * 32 + ci) * 9 + tap];
+        const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+        whi[(tap * 32 + co) * kMmaWRow + ci] = hi;
+        wlo[(tap * 32 + co) * kMmaWRow + ci] = lo;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    float acc[2][4][4];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[mt][j][e] = 0.f;
+    const uint32_t* P32 = reinterpret_cast<const uint32_t*>(patch);
+    const uint32_t* H32 = reinterpret_cast<const uint32_t*>(whi);
+    const uint32_t* L32 = reinterpret_cast<const uint32_t*>(wlo);
+#pragma unroll 1
+    for (int tap = 0; tap < 9; ++tap) {
+        const int ky = tap / 3, kx = tap - 3 * ky;
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const int ci0 = 16 * half;
+            uint32_t bh[4][2], bl[4][2];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int wi = ((tap * 32 + 8 * j + g) * kMmaWRow + ci0 + 2 * t) >> 1;
+                bh[j][0] = H32[wi];
+                bh[j][1] = H32[wi + 4];
+                bl[j][0] = L32[wi];
+                bl[j][1] = L32[wi + 4];
+            }
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+                const int pr = (2 * warp + mt) * S + ky;
+                const int p0 = ((pr * G::PC + g * S + kx) * kMmaPix + ci0 + 2 * t) >> 1;
+                const int p1 = p0 + ((8 * S * kMmaPix) >> 1);  // pixel g + 8
+                const uint32_t a0 = P32[p0], a1 = P32[p1], a2 = P32[p0 + 4], a3 = P32[p1 + 4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    mma_bf16_16816(acc[mt][j], a0, a1, a2, a3, bh[j][0], bh[j][1]);
+                    mma_bf16_16816(acc[mt][j], a0, a1, a2, a3, bl[j][0], bl[j][1]);
+                }
+            }
+        }
+    }
+    // y = act(acc + b): c0, c1 at pixel g, channels 8j + 2t (+1); c2, c3 at pixel g + 8
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+        const int oy = oy0 + 2 * warp + mt;
+        if (oy >= Ho) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int co = 8 * j + 2 * t + (e & 1);
+                const int ox = ox0 + g + (e >> 1) * 8;
+                if (ox >= Wo) continue;
+                float v = acc[mt][j][e] + b[co];
+                if (relu) v = fmaxf(v, 0.f);
+                y[((int64_t)co * Ho + oy) * Wo + ox] = __float2bfloat16_rn(v);
+            }
+    }
+}
+
+template <int S>
+static cudaError_t conv_mma32_launch(const __nv_bfloat16* x, int H, int W, const float* w,
+                                     const float* b, int relu, __nv_bfloat16* y,
+                                     cudaStream_t st) {
+    const int Ho = (H - 1) / S + 1, Wo = (W - 1) / S + 1;
+    const size_t smem = MmaConvGeo<S>::smem;
+    cudaError_t e = cudaFuncSetAttribute(k_conv3x3_mma32<S>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const dim3 grid(blocks_for(Wo, kMmaCols), blocks_for(Ho, kMmaRows));
+    k_conv3x3_mma32<S><<<grid, 128, smem, st>>>(x, H, W, w, b, Ho, Wo, relu, y);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 // in_bf16 / out_bf16: activation storage types (FP32 otherwise).
 cudaError_t cnn_conv_forward(const void* x, int in_bf16, int Cin, int H, int W, const float* w,
                              const float* b, int Cout, int stride, int relu, void* y,
                              int out_bf16, cudaStream_t st) {
     using bf = __nv_bfloat16;
+    // the inference network's 32 -> 32 layer (bf16 activations): tensor cores
+    if (in_bf16 && out_bf16 && Cin == 32 && Cout == 32 && stride == 2)
+        return conv_mma32_launch<2>(static_cast<const bf*>(x), H, W, w, b, relu,
+                                    static_cast<bf*>(y), st);
 #define PFX_CONV(S)                                                                             \
     if (in_bf16 && out_bf16) return conv_fwd_t<S, bf, bf>(x, Cin, H, W, w, b, Cout, relu, y, st); \
     if (in_bf16) return conv_fwd_t<S, bf, float>(x, Cin, H, W, w, b, Cout, relu, y, st);          \

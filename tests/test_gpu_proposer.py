@@ -403,6 +403,38 @@ def test_trained_proposer_gain_on_held_out_pairs():
     assert u["tiles_run"] > t["tiles_run"], (t, u)
 
 
+@pytest.mark.parametrize("H,W,relu", [(19, 23, 1), (70, 61, 0), (33, 130, 1), (1, 5, 1)])
+def test_conv_tensor_core_layer_vs_oracle(H, W, relu):
+    """The 32 -> 32-channel stride-2 layer with bf16 activations in and out
+    runs on the tensor cores (k_conv3x3_mma32, weights split into bf16 high and
+    low parts): within bf16 output rounding of the oracle's convolution of the
+    same bf16 inputs, and of the CUDA-core kernel's FP32-output result, on maps
+    whose output tiles are partial."""
+    rng = np.random.default_rng(H * 1000 + W)
+    x = rng.standard_normal((32, H, W)).astype(np.float32)
+    w = (rng.standard_normal((32, 32, 3, 3)) * 0.1).astype(np.float32)
+    b = (rng.standard_normal(32) * 0.1).astype(np.float32)
+    xb = torch.from_numpy(x).cuda().to(torch.bfloat16)
+    xr = xb.float().cpu().numpy()  # the bf16 inputs, exactly
+    wd, bd = torch.from_numpy(w).cuda(), torch.from_numpy(b).cuda()
+    Ho, Wo = (H - 1) // 2 + 1, (W - 1) // 2 + 1
+    y = torch.full((32, Ho, Wo), float("nan"), dtype=torch.bfloat16, device="cuda")
+    lib = _lib.load()
+    s = pf.plan.current_stream_ptr()
+    _lib.check(lib.pfx_conv3x3_forward(_p(xb), 1, 32, H, W, _p(wd), _p(bd), 32, 2, relu,
+                                       _p(y), 1, s))
+    got = y.float().cpu().numpy()
+    assert np.isfinite(got).all()
+    yref = CO.conv3x3(xr, w, b, 2, relu)
+    assert close(got, yref, 1e-2)
+    # the CUDA-core kernel on the same inputs, FP32 output
+    yf = torch.empty((32, Ho, Wo), dtype=torch.float32, device="cuda")
+    _lib.check(lib.pfx_conv3x3_forward(_p(xb), 1, 32, H, W, _p(wd), _p(bd), 32, 2, relu,
+                                       _p(yf), 0, s))
+    assert close(yf.cpu().numpy(), yref)
+    assert close(got, yf.cpu().numpy(), 1e-2)
+
+
 def test_center_features_and_first_layer_vs_materialised_map():
     """pfx_pooled_center_features makes A^T B the centred, standardised map that
     pfx_pooled_center makes from 1 - A^T B (the pooled cost is bilinear), and
