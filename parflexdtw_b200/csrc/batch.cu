@@ -20,7 +20,8 @@ using namespace pfx;
 
 namespace {
 
-constexpr int kSide = 32;  // streams stage 2 of a wave is spread over
+constexpr int kSide = 32;     // streams stage 2 of a wave is spread over
+constexpr int kCostSide = 3;  // extra streams a wave's per-pair cost work is spread over
 
 struct PairOut {
     const double* best;
@@ -194,6 +195,9 @@ struct pfx_batch {
     cudaStream_t side[kSide] = {};
     cudaEvent_t fork_ev = nullptr;
     cudaEvent_t join_ev[kSide] = {};
+    cudaStream_t cside[kCostSide] = {};  // the per-pair cost and edge-gather launches
+    cudaEvent_t cfork_ev = nullptr;
+    cudaEvent_t cjoin_ev[kCostSide] = {};
     cudaGraphExec_t exec = nullptr;
     double graph_beta = 0.0;
     int64_t graph_kernels = 0;  // kernel launches recorded in the graph
@@ -235,6 +239,11 @@ static void batch_free(pfx_batch* b) {
         if (b->join_ev[k]) cudaEventDestroy(b->join_ev[k]);
     }
     if (b->fork_ev) cudaEventDestroy(b->fork_ev);
+    for (int k = 0; k < kCostSide; ++k) {
+        if (b->cside[k]) cudaStreamDestroy(b->cside[k]);
+        if (b->cjoin_ev[k]) cudaEventDestroy(b->cjoin_ev[k]);
+    }
+    if (b->cfork_ev) cudaEventDestroy(b->cfork_ev);
     for (cudaEvent_t e : b->phase_ev) cudaEventDestroy(e);
     if (b->cap) cudaStreamDestroy(b->cap);
     if (b->arena) cudaFree(b->arena);
@@ -539,6 +548,11 @@ extern "C" int pfx_batch_create(int32_t n, const int64_t* N, const int64_t* M, c
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join_ev[k], cudaEventDisableTiming);
     }
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming);
+    for (int k = 0; k < kCostSide && e == cudaSuccess; ++k) {
+        e = cudaStreamCreateWithFlags(&b->cside[k], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->cjoin_ev[k], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->cfork_ev, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         batch_free(b);
         return errf(PFX_ERR_CUDA, "batch setup: %s", cudaGetErrorString(e));
@@ -875,6 +889,26 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
     };
     int st;
     int used_side = 0;  // side streams forked so far (joined at the end)
+    // a wave's per-pair launches (cost, edge gathers) spread over s and up to
+    // kCostSide more streams, forked from s and joined back into it, so that
+    // one pair's kernel tail overlaps the next pair's kernels
+    auto cost_fork = [&](int npairs, int* nc) -> cudaError_t {
+        *nc = std::min(kCostSide, npairs - 1);
+        if (*nc <= 0) return cudaSuccess;
+        cudaError_t e = cudaEventRecord(b->cfork_ev, s);
+        for (int k = 0; k < *nc && e == cudaSuccess; ++k)
+            e = cudaStreamWaitEvent(b->cside[k], b->cfork_ev, 0);
+        return e;
+    };
+    auto cost_join = [&](int nc) -> cudaError_t {
+        cudaError_t e = cudaSuccess;
+        for (int k = 0; k < nc && e == cudaSuccess; ++k) {
+            e = cudaEventRecord(b->cjoin_ev[k], b->cside[k]);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(s, b->cjoin_ev[k], 0);
+        }
+        return e;
+    };
+    auto cost_stream = [&](int q, int nc) { return q % (nc + 1) == 0 ? s : b->cside[q % (nc + 1) - 1]; };
     for (int w = 0; w < waves; ++w) {
         const int q0 = b->wave_first[w], q1 = b->wave_first[w + 1];
         BCK(mark(w, 0));
@@ -883,7 +917,10 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
         if (b->fp32 && !b->masked)  // the wave's cost GEMM, one launch
             BCK(launch_gemm_cost_multi(b->gpairs + b->wave_gp_off[w], q1 - q0,
                                        b->wave_gp_blocks[w], b->kp, b->status, s));
+        int nc = 0;
+        BCK(cost_fork(q1 - q0, &nc));
         for (int q = q0; q < q1; ++q) {
+            const cudaStream_t cs = cost_stream(q - q0, nc);
             const int i = b->wave_pairs[q];
             pfx_plan& p = b->plans[i];
             const double* F1 = b->fin + b->fin_off[i];
@@ -896,41 +933,45 @@ static int batch_enqueue(pfx_batch* b, double beta, cudaStream_t s, bool timed) 
                 const char* A = static_cast<const char*>(p.fbf);
                 const char* B = A + (size_t)p.g.N * b->kp * 2;
                 BCK(launch_gemm_cost_skew(A, B, b->kp, p.g, static_cast<float*>(p.Csk),
-                                          p.skew_stride, b->status, s, slot, list, p.n_kept,
+                                          p.skew_stride, b->status, cs, slot, list, p.n_kept,
                                           b->masked ? (int64_t)p.n_kept * p.skew_stride : -1));
             } else {
                 double* An = p.feat;
                 double* Bn = p.feat + (int64_t)b->d * p.g.N;
-                BCK(launch_l2norm(F1, b->d, p.g.N, An, s));
-                BCK(launch_l2norm(F2, b->d, p.g.M, Bn, s));
+                BCK(launch_l2norm(F1, b->d, p.g.N, An, cs));
+                BCK(launch_l2norm(F2, b->d, p.g.M, Bn, cs));
                 if (!b->gen_cost)  // (else stage 1 builds each tile's cost)
                     BCK(launch_cost_skew(An, Bn, b->d, p.g, static_cast<double*>(p.Csk),
-                                         p.skew_stride, s, slot, list, p.n_kept,
+                                         p.skew_stride, cs, slot, list, p.n_kept,
                                          b->cost_fma != 0));
             }
             if (b->masked) {
                 // skipped tiles keep +inf edges and start 0 for stage 2
-                BCK(launch_fill(p.s1.edge_D, p.n4, HUGE_VAL, s));
-                BCK(cudaMemsetAsync(p.s1.edge_P, 0, (size_t)p.n4 * 4, s));
+                BCK(launch_fill(p.s1.edge_D, p.n4, HUGE_VAL, cs));
+                BCK(cudaMemsetAsync(p.s1.edge_P, 0, (size_t)p.n4 * 4, cs));
             }
         }
+        BCK(cost_join(nc));
         BCK(mark(w, 1));
         BCK(launch_stage1_queue(b->descs + b->wave_desc_off[w], (int)b->wave_tiles[w], nullptr,
                                 b->heads + w, b->gq, b->status, b->nw, b->fp32 != 0, s,
                                 b->gen_cost ? &b->gen : nullptr));
         BCK(mark(w, 2));
-        // stage 2 reads the cost slabs only in its edge gather: that part
-        // stays on the main stream, so the next wave may overwrite the pool
-        // while the rest of this wave's stage 2 runs on the side streams
+        // stage 2 reads the cost slabs only in its edge gather: that part is
+        // joined back into the main stream, so the next wave may overwrite the
+        // pool while the rest of this wave's stage 2 runs on the side streams
+        BCK(cost_fork(q1 - q0, &nc));
         for (int q = q0; q < q1; ++q) {
+            const cudaStream_t cs = cost_stream(q - q0, nc);
             const pfx_plan& p = b->plans[b->wave_pairs[q]];
             if (b->gen_cost)  // no slabs kept: overlap costs from the features
-                BCK(launch_stage2_edges(nullptr, nullptr, 0, false, p.g, p.s2, s, p.feat,
+                BCK(launch_stage2_edges(nullptr, nullptr, 0, false, p.g, p.s2, cs, p.feat,
                                         p.feat + (int64_t)b->d * p.g.N, b->d));
             else
                 BCK(launch_stage2_edges(nullptr, p.Csk, p.skew_stride, p.fp32 != 0, p.g, p.s2,
-                                        s));
+                                        cs));
         }
+        BCK(cost_join(nc));
         BCK(mark(w, 3));
         BCK(cudaEventRecord(b->fork_ev, s));
         const int nside = std::min(kSide, q1 - q0);
