@@ -28,6 +28,7 @@ from __future__ import annotations
 import csv
 import math
 import os
+import threading
 import time
 import warnings
 from collections.abc import Mapping
@@ -64,12 +65,59 @@ def _require_gpu(use_gpu):
     L.load()
 
 
+_STAGE_ELEMS = 1 << 25  # FP64 elements per pinned staging chunk (256 MB)
+_STAGE_THREADS = 8      # host threads filling a chunk
+# the two chunks, the filling threads, and per chunk the event after the last
+# transfer out of it (kept across calls: a chunk is refilled only after it)
+_stage = {"bufs": None, "pool": None, "done": [None, None]}
+_stage_lock = threading.Lock()
+
+
+def _upload_staged(arr: np.ndarray) -> torch.Tensor:
+    """A large C-contiguous FP64 host array to the device through two reused
+    page-locked chunks: while one chunk's copy to the device runs, host
+    threads fill the other (numpy releases the GIL while copying), so the
+    host copy and the transfer overlap."""
+    from concurrent.futures import ThreadPoolExecutor
+    if _stage["bufs"] is None:
+        _stage["bufs"] = [torch.empty(_STAGE_ELEMS, dtype=torch.float64).pin_memory()
+                          for _ in range(2)]
+        _stage["pool"] = ThreadPoolExecutor(max_workers=_STAGE_THREADS)
+    bufs, pool, done = _stage["bufs"], _stage["pool"], _stage["done"]
+    out = torch.empty(arr.shape, dtype=torch.float64, device="cuda")
+    src, dst = arr.reshape(-1), out.view(-1)
+    n = src.size
+    stream = torch.cuda.current_stream()
+    for k, off in enumerate(range(0, n, _STAGE_ELEMS)):
+        m = min(_STAGE_ELEMS, n - off)
+        buf = bufs[k & 1]
+        if done[k & 1] is not None:
+            done[k & 1].synchronize()  # its previous transfer has read the chunk
+        host = buf.numpy()
+        part = -(-m // _STAGE_THREADS)
+        futs = [pool.submit(np.copyto, host[a:min(a + part, m)],
+                            src[off + a:off + min(a + part, m)])
+                for a in range(0, m, part)]
+        for f in futs:
+            f.result()
+        dst[off:off + m].copy_(buf[:m], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        done[k & 1] = ev
+    return out
+
+
 def cost_matrix_to_gpu(C) -> torch.Tensor:
-    """Host (or device) cost matrix as a contiguous FP64 CUDA tensor."""
+    """Host (or device) cost matrix as a contiguous FP64 CUDA tensor.  Host
+    arrays above one staging chunk go through the double-buffered staged
+    upload; smaller ones through one page-locked copy."""
     if isinstance(C, torch.Tensor):
         t = C if C.is_cuda else C.cuda()
         return t.to(torch.float64).contiguous()
     arr = np.ascontiguousarray(C, dtype=np.float64)
+    if arr.size > _STAGE_ELEMS and arr.ndim == 2:
+        with _stage_lock:
+            return _upload_staged(arr)
     return torch.from_numpy(arr).pin_memory().cuda(non_blocking=True)
 
 

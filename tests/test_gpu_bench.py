@@ -49,6 +49,10 @@ def _check_own(d, workload_key="workload"):
 def test_bench_own_arm(workload, extra):
     d = _bench("--workload", workload, *SMALL, "--no-cpu-baseline", *extra)
     _check_own(d)
+    if workload == "ncu_small":
+        # the drop-in call on a host cost matrix, timed beside the plan path
+        dr = d["dropin_host_C"]
+        assert dr["value"] > 0 and dr["h2d_bytes_per_call"] > 0
 
 
 def test_bench_own_arm_cpu_baseline():

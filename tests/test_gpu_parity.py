@@ -379,3 +379,26 @@ def test_global_flexdtw_vs_oracle(n, m, beta, oracle_mod):
     assert best == rbest
     assert same(wp, rwp)
     assert same(D, rD) and same(P, rP) and same(B, rB)
+
+
+def test_host_cost_matrix_staged_upload():
+    """A host cost matrix above one staging chunk goes to the device through
+    the double-buffered staged upload: bit for bit the matrix, on consecutive
+    calls (the chunks are reused once their transfers are done), and the
+    drop-in call on it returns the plan path's result."""
+    from parflexdtw_b200.parflex import _STAGE_ELEMS, cost_matrix_to_gpu
+    rng = np.random.default_rng(11)
+    N, M = 6100, 5600  # 34.2 M elements: one full chunk and a partial one
+    assert _STAGE_ELEMS < N * M < 2 * _STAGE_ELEMS
+    for _ in range(2):
+        C = rng.random((N, M))
+        got = cost_matrix_to_gpu(C)
+        assert got.dtype == torch.float64 and tuple(got.shape) == (N, M)
+        assert torch.equal(got.cpu(), torch.from_numpy(C))
+    F1, F2 = W.warped_pair(np.random.default_rng(3), 6000, 5900)
+    C = pf.cost_matrix_from_features_gpu(F1, F2).cpu().numpy()
+    assert C.size > _STAGE_ELEMS
+    b_host, wp_host = pf.parflex(C, STD, [2.0, 3.0, 3.0], 0.1, L=2000, profile_dir=None)
+    b_dev, wp_dev = pf.parflex(torch.from_numpy(C).cuda(), STD, [2.0, 3.0, 3.0], 0.1,
+                               L=2000, profile_dir=None)
+    assert b_host == b_dev and np.array_equal(wp_host, wp_dev)
