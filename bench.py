@@ -8,9 +8,9 @@ steps {(1,1),(1,2),(2,1)}, weights {2,3,3}, beta 0.1.  One step aligns all 64
 pairs with the chosen exact form: the learned tile proposer picks the tiles,
 stage 1 (FP64 DP) runs on those only, stage 2 per pair, and a pair whose
 path comes near a pruned tile gets those tiles added or falls back to the
-full-tile method.  The judge is the plain full-tile FP64 form on the same
-pairs (timed as ``plain_fp64_full_tiles``); ``exact_paths`` counts the pairs
-whose best cost and path equal its own.
+full-tile method.  The reference answer is the plain full-tile FP64 form on
+the same pairs (timed as ``plain_fp64_full_tiles``); ``exact_paths`` counts
+the pairs whose best cost and path equal its own.
 
   value     DP cells/s, counting every cell of the full tiling (work the
             proposer avoids counts as throughput), features in HBM
@@ -1213,7 +1213,8 @@ def prune_arm(args, spec):
             "e2e": {"value": cells * ws * args.e2e_steps / (ms_e2e / 1e3), "unit": UNIT,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "steps": args.e2e_steps, "ms_per_step": ms_e2e / args.e2e_steps,
-                    "api": "PrunedBatch.run(host_pairs=pinned host features): uploads inside the run"},
+                    "api": "PrunedBatch.run(host_pairs=pinned host features): uploads "
+                           "inside the run"},
             "gpu_launches": int(launches), "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

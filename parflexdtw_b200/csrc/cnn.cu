@@ -1,7 +1,7 @@
 // Learned tile proposer: the kernels of a small CNN that reads a 16x
 // average-pooled cost matrix and scores which L x L tiles the optimal path
 // crosses (inference and training: forward, backward, Adam).  No reference
-// counterpart; the full-tile method stays the fallback and the judge.
+// counterpart; the full-tile method stays the fallback and the reference answer.
 //
 // Images are one sample, channels-first [C][H][W], FP32 in training; in
 // inference the activations between layers may be stored in bf16 (FP32

@@ -367,8 +367,8 @@ def test_trained_proposer_gain_on_held_out_pairs():
     Held-out pairs (a seed outside the training seeds 12345..17344 of
     train_proposer.py, drawn like the training pairs: N ~ U(20000, 30000),
     M = N x U(0.7, 1.4), 0-10 % unrelated padding per end), L = 2000.  The
-    full-tile FP64 method is the judge: every pruned result must equal its
-    best cost and path bit for bit.  The trained proposer must skip more than
+    full-tile FP64 method gives the reference answer: every pruned result must
+    equal its best cost and path bit for bit.  The trained proposer must skip more than
     half of the tiles, counting every tile its expansions and fallbacks ran;
     an untrained network of the same layout at the same threshold, which the
     same fallback keeps exact, must run more tiles than the trained one."""
